@@ -1,0 +1,218 @@
+/* tomgpu — B200-native (sm_100a) template matching for TOM.
+ *
+ * C ABI of libtomgpu.so.  Every entry point returns a tomgpu_status; nothing
+ * longjmps or throws across this boundary.  Pointers ending in _dev are
+ * device pointers owned by the caller; all other array pointers are host
+ * pointers owned by the caller.  Volumes are single precision, x fastest
+ * (MATLAB column-major order): element (x, y, z) sits at x + nx*(y + ny*z).
+ *
+ * Each entry point names the reference interface it replaces.  Reference
+ * paths are relative to the TOM toolbox source tree.
+ */
+#ifndef TOMGPU_H
+#define TOMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    TOMGPU_OK = 0,
+    TOMGPU_ERR_ARG = 1,         /* invalid argument: null pointer, size, mode */
+    TOMGPU_ERR_UNSUPPORTED = 2, /* size the kernels are not built for (FFT length) */
+    TOMGPU_ERR_OOM = 3,         /* device allocation failed */
+    TOMGPU_ERR_CUDA = 4,        /* CUDA runtime error (details: tomgpu_last_error) */
+    TOMGPU_ERR_STATE = 5,       /* call order: e.g. run before a volume is set */
+    TOMGPU_ERR_DEVICE = 6,      /* a kernel reported an internal error flag */
+    TOMGPU_ERR_TIMEOUT = 7      /* a bounded device wait ran out */
+} tomgpu_status;
+
+typedef struct tomgpu_ctx tomgpu_ctx;
+typedef struct tomgpu_match_plan tomgpu_match_plan;
+
+/* ------------------------------------------------------------ context --- */
+/* Library version string, e.g. "tomgpu 0.1 sm_100a". */
+const char* tomgpu_version(void);
+/* Human-readable name of a status code. */
+const char* tomgpu_status_string(int status);
+/* Message of the last failing call on this context (or of the last
+ * tomgpu_ctx_create failure when ctx is NULL). */
+const char* tomgpu_last_error(const tomgpu_ctx* ctx);
+
+/* Create a context on a CUDA device.  The context owns a stream (replaceable
+ * with tomgpu_ctx_set_stream) and its workspaces.  One context per host
+ * thread; calls on one context are not thread-safe. */
+int tomgpu_ctx_create(int device, tomgpu_ctx** out);
+int tomgpu_ctx_destroy(tomgpu_ctx* ctx);
+/* Issue all further work of this context on an existing cudaStream_t (passed
+ * as void*); NULL selects the CUDA legacy default stream. */
+int tomgpu_ctx_set_stream(tomgpu_ctx* ctx, void* cuda_stream);
+int tomgpu_ctx_synchronize(tomgpu_ctx* ctx);
+/* Device kernel launches issued by this context since creation. */
+int64_t tomgpu_ctx_launch_count(const tomgpu_ctx* ctx);
+
+/* Device time per kernel class of the matching loop, measured with CUDA
+ * events recorded on the context stream around each launch while profiling
+ * is enabled (no host synchronisation until the read). */
+enum {
+    TOMGPU_K_ROTATE = 0,   /* rotation * mask of the template batch */
+    TOMGPU_K_FILTER = 1,   /* weight (psf) filter of the rotated templates */
+    TOMGPU_K_SPEC_X = 2,   /* x-stage of the template spectrum */
+    TOMGPU_K_SPEC_Z = 3,   /* z-stage of the template spectrum */
+    TOMGPU_K_CORR_Y = 4,   /* y-DFT, product with the tomogram spectrum, inverse y-DFT */
+    TOMGPU_K_INV_Z = 5,    /* inverse z-DFT */
+    TOMGPU_K_C2R_FLCF = 6, /* inverse x (complex-to-real), FLCF, running max/arg-max */
+    TOMGPU_K_COUNT = 7
+};
+/* enable != 0 starts (and resets) the timers, 0 stops recording. */
+int tomgpu_ctx_profile(tomgpu_ctx* ctx, int enable);
+/* Total milliseconds and launch count of one kernel class; synchronises the stream. */
+int tomgpu_ctx_profile_read(tomgpu_ctx* ctx, int kernel, double* total_ms, int64_t* launches);
+
+/* ----------------------------------------------------------- rotation --- */
+enum { TOMGPU_EULER_DEG = 1, TOMGPU_MATRIX = 3 };
+
+/* Replaces the tom_rotatec MEX: tom_rotatec(in, out, euler, 'linear', center)
+ * (Sptrans/tom_rotatec.c:407-480, compute in rot3d :146-401; called from
+ * Sptrans/tom_rotate.m:126).  mode TOMGPU_EULER_DEG: euler = [phi psi theta]
+ * in degrees, ZXZ; TOMGPU_MATRIX: 9 floats in MATLAB column-major order of the
+ * 3x3 matrix.  center is 0-based (tom_rotate passes ceil(size/2)).  Output
+ * voxel x samples in at center + R^T (x - center), trilinear, 0 outside.
+ * Bit-exact with rot3d.  Host buffers. */
+int tomgpu_rotate3d(tomgpu_ctx* ctx, const float* in, float* out, const int dims[3],
+                    const float* euler_or_matrix, int mode, const float center[3]);
+
+/* Batched rot3d on device buffers: R rotations (eulers R x 3 degrees, host
+ * array) of one volume into out_dev (R volumes back to back); optional
+ * mask_dev multiplies every output voxel (tom_os3_findTemplate.m:264). */
+int tomgpu_rotate3d_batch_dev(tomgpu_ctx* ctx, const float* in_dev, float* out_dev,
+                              const int dims[3], const float* eulers, int R,
+                              const float center[3], const float* mask_dev);
+
+/* ZXZ rotation matrix of tom_rotatec for one Euler triplet (degrees), 9 floats
+ * rm00, rm10, rm20, rm01, rm11, rm21, rm02, rm12, rm22 (Sptrans/tom_rotatec.c:164-288). */
+int tomgpu_euler_matrix(const float euler[3], float m9[9]);
+
+/* -------------------------------------------------------------- peaks --- */
+/* Replaces the tom_peakinc MEX (Analysis/tom_peakinc.c:23-77, via
+ * Analysis/tom_peakc.m:70): first strict maximum in x-fastest order starting
+ * from -99999; pos1 is 1-based.  Host buffer. */
+int tomgpu_peak(tomgpu_ctx* ctx, const float* v, const int dims[3], float* val, int pos1[3]);
+int tomgpu_peak_dev(tomgpu_ctx* ctx, const float* v_dev, const int dims[3], float* val, int pos1[3]);
+
+/* K peaks by repeated [c val M] = tom_peak(A, R) (Analysis/tom_peak.m:203-279):
+ * each round takes the first maximum and zeroes the ball of radius R around
+ * it.  work_dev: a scratch copy of A is made internally (A is not modified).
+ * vals: K floats, pos1: K x 3 ints (1-based). */
+int tomgpu_topk_dev(tomgpu_ctx* ctx, const float* v_dev, const int dims[3], int K, double radius,
+                    float* vals, int* pos1);
+
+/* One round of [c val M] = tom_peak(A, R) in place: the first maximum of
+ * v_dev, then the ball of radius R around it set to 0 (v_dev becomes M). */
+int tomgpu_peak_radius_dev(tomgpu_ctx* ctx, float* v_dev, const int dims[3], double radius, float* val,
+                           int pos1[3]);
+
+/* tom_peak(A, 'spline') sub-voxel refinement at a given 1-based integer peak
+ * (tom_intpeak, Analysis/tom_peak.m:437-525): per axis the parabola through
+ * the 3 neighbours maximised on a 0.001 grid.  coord: 3 doubles, val: max. */
+int tomgpu_peak_spline_dev(tomgpu_ctx* ctx, const float* v_dev, const int dims[3],
+                           const int pos1[3], double coord[3], double* val);
+
+/* ------------------------------------------------------ weights, masks --- */
+/* Replaces tom_calc_weight_functioninc (Filtrans/tom_calc_weight_functioninc.c:152-289):
+ * Radermacher exact weighting, angles 2 x n_tilt (phi, theta pairs, degrees),
+ * output dims[0]*dims[1]*dims[2] floats (host). */
+int tomgpu_weight3d(tomgpu_ctx* ctx, const int dims[3], const double* angles, int n_tilt,
+                    double thickness, float* out);
+
+/* Binary missing wedge on a centred grid (Filtrans/tom_wedge.m:62-77): 0 where
+ * tan(angle) > |x|/|z|.  av3 form (av3/utils/av3_wedge.m:23-26) when
+ * av3 != 0: 0 where tan(pi/2-max) > x/z and tan(-pi/2-min) < x/z.
+ * Output on the device (dims product floats). */
+int tomgpu_wedge_dev(tomgpu_ctx* ctx, const int dims[3], double angle_or_min, double max_angle,
+                     int av3, float* out_dev);
+
+/* ------------------------------------------------------------- FFTs --- */
+/* Replaces fftn / tom_fourier and ifftn / tom_ifourier (Filtrans/tom_fourier.m:44-50,
+ * Filtrans/tom_ifourier.m:36-44) on device buffers.  Complex data are
+ * interleaved (re, im) pairs, x fastest.  dir -1: forward, +1: inverse scaled
+ * by 1/numel.  precision 32 or 64 (the buffer holds float or double pairs). */
+int tomgpu_fft3d_c2c_dev(tomgpu_ctx* ctx, void* data_dev, const int dims[3], int dir, int precision);
+/* Real-to-half-complex forward (nx/2+1 complex along x) and its inverse
+ * (scaled by 1/numel); out-of-place for r2c, in-place spectrum for c2r. */
+int tomgpu_fft3d_r2c_dev(tomgpu_ctx* ctx, const void* real_dev, void* half_dev, const int dims[3],
+                         int precision);
+int tomgpu_fft3d_c2r_dev(tomgpu_ctx* ctx, void* half_dev, void* real_dev, const int dims[3],
+                         int precision);
+
+/* ---------------------------------------------------- FLCF matching --- */
+typedef struct {
+    int batch;          /* rotations per batch; 0 = default (8) */
+    int wedge_fp64;     /* reserved, 0 */
+    int reserved[6];
+} tomgpu_match_params;
+
+/* A matching plan for one volume size and one template size.  It holds the
+ * tomogram spectrum, the FP64 local statistics and per-batch workspaces.
+ * Volume and template sizes must be FFT lengths the library is built for
+ * (8,16,24,32,40,48,64,80,96,128,160,192,232,256,464,512,928 per axis; the
+ * template edge along x must keep nx/2 in that list).  params may be NULL. */
+int tomgpu_match_plan_create(tomgpu_ctx* ctx, const int vol_dims[3], const int tmpl_dims[3],
+                             const tomgpu_match_params* params, tomgpu_match_plan** out);
+int tomgpu_match_plan_destroy(tomgpu_match_plan* plan);
+/* Bytes of device memory the plan holds. */
+int64_t tomgpu_match_plan_bytes(const tomgpu_match_plan* plan);
+
+/* Once per tomogram (tom_os3_findTemplate.m:243-245; statistics/tom_os3_mean.m:49-62,
+ * statistics/tom_os3_std.m:48-67): the tomogram spectrum and the local mean and
+ * standard deviation under the mask, accumulated in FP64.  The mask must be
+ * given first (tomgpu_match_set_template) or here: mask_dev (template-sized)
+ * may be NULL when a template is already set. */
+int tomgpu_match_set_volume_dev(tomgpu_match_plan* plan, const float* vol_dev);
+
+/* Template, mask and optional weight (psf) volume, template-sized, device
+ * buffers.  Applies findTemplate's preprocessing: tom_norm(1e5*(t+1),
+ * 'mean0+1std') (tom_os3_findTemplate.m:157) and the unrotated, filtered
+ * template statistics (tom_os3_normUnderMask on tom_os3_modifyImage,
+ * :233-234).  psf_dev is the centred weight of tom_apply_weight_function
+ * (NULL: no filter).  Must precede tomgpu_match_set_volume_dev. */
+int tomgpu_match_set_template_dev(tomgpu_match_plan* plan, const float* tmpl_dev,
+                                  const float* mask_dev, const float* psf_dev);
+
+/* Fill maxcc_dev with -1000 and angidx_dev with -1 (findTemplate's initial
+ * ccc/angles, :215-218, with 0-based indices). */
+int tomgpu_match_init_results_dev(tomgpu_match_plan* plan, float* maxcc_dev, int32_t* angidx_dev);
+
+/* The hot loop (tom_os3_findTemplate.m:255-307): for each of R Euler triplets
+ * (host array R x 3, degrees), rotate the template (rot3d), multiply the mask,
+ * apply the weight (tom_os3_modifyImage), correlate with the tomogram
+ * (tom_os3_corr FLCF, search/tom_os3_corr.m:151-176) and update the running
+ * maximum where it strictly increases (tom_os3_bestPeak ccc mode,
+ * search/tom_os3_bestPeak.m:42-47,94-96).  angidx receives index_offset + r
+ * (0-based).  Results are device buffers of volume size. */
+int tomgpu_match_run_dev(tomgpu_match_plan* plan, const float* eulers, int R, int index_offset,
+                         float* maxcc_dev, int32_t* angidx_dev);
+
+/* Single-rotation FLCF map (tom_os3_corr on an already rotated, masked and
+ * filtered template, search/tom_os3_corr.m:151-176): the template statistics
+ * are the plan's (set by tomgpu_match_set_template_dev).  t_dev: template-sized,
+ * cc_dev: volume-sized. */
+int tomgpu_match_corr_dev(tomgpu_match_plan* plan, const float* t_dev, float* cc_dev);
+
+/* Local statistics computed by set_volume (volume-sized outputs, may be NULL). */
+int tomgpu_match_stats_dev(tomgpu_match_plan* plan, float* mean_dev, float* std_dev);
+
+/* One-shot, host buffers (what a MEX gateway calls): plan, upload, set
+ * template and volume, run all R angles, download.  maxcc/angidx: volume-sized
+ * host arrays; angidx is 0-based (-1 where never updated). */
+int tomgpu_match(tomgpu_ctx* ctx, const float* tomo, const int vol_dims[3], const float* tmpl,
+                 const int tmpl_dims[3], const float* mask, const float* psf, const float* eulers,
+                 int R, const tomgpu_match_params* params, float* maxcc, int32_t* angidx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TOMGPU_H */

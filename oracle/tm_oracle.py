@@ -1,0 +1,491 @@
+"""CPU oracle for TOM's template-matching hot path.
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` import this module, and only as the checker
+(or, for the baseline, as the timed CPU restatement).  The CUDA library in
+``tom_b200`` never imports, links or calls anything here.
+
+Two layers:
+
+* ``liboracle.so`` (``oracle/flcf_oracle.c``): C restatements of the
+  reference's C routines with the same float arithmetic, bit-exact with the
+  compiled reference (``oracle/_ref/libref_*.so``, built from the reference's
+  own sources by ``oracle/Makefile``).
+* this file: numpy restatement of the MATLAB-level FLCF search (Oscar3
+  MATLAB picker) in FP64, following
+
+  - ``Oscar3/matlabPicker/search/tom_os3_findTemplate.m:157-307``
+  - ``Oscar3/matlabPicker/search/tom_os3_corr.m:77-192``
+  - ``Oscar3/matlabPicker/statistics/tom_os3_mean.m:44-62``
+  - ``Oscar3/matlabPicker/statistics/tom_os3_std.m:43-67``
+  - ``Oscar3/matlabPicker/statistics/tom_os3_normUnderMask.m:3-8``
+  - ``Oscar3/matlabPicker/search/tom_os3_sphereMask.m:4-37``
+  - ``Oscar3/matlabPicker/tools/tom_os3_pasteCenter.m:17-39``
+  - ``Oscar3/matlabPicker/search/tom_os3_bestPeak.m:42-47,94-96``
+  - ``Filtrans/tom_apply_weight_function.m:56-62``, ``Filtrans/tom_wedge.m:62-77``
+  - ``Analysis/tom_peak.m:80-108,203-279,437-525``
+  - ``Analysis/tom_corr.m:51-121``, ``av3_new/tom_av3_align.m:97-189``
+
+The FFT itself is third-party arithmetic in the reference (MATLAB ``fftn``,
+FFTW inside); the DFT is mathematically defined, so numpy's pocketfft in FP64
+is the reference value here.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+_LIBS: dict = {}
+
+
+def _load(name):
+    if name not in _LIBS:
+        path = os.path.join(REF_DIR, name)
+        if not os.path.exists(path):
+            raise FileNotFoundError(
+                f"{path} missing: run `make -C oracle` (reference libraries need the reference sources)")
+        _LIBS[name] = ctypes.CDLL(path)
+    return _LIBS[name]
+
+
+def oracle_lib():
+    lib = _load("liboracle.so")
+    lib.oracle_euler_matrix.argtypes = [_f32p, _f32p]
+    lib.oracle_rot3d.argtypes = [_f32p, _f32p, ctypes.c_long, ctypes.c_long, ctypes.c_long,
+                                 _f32p, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+    lib.oracle_rot3d_batch.argtypes = [_f32p, _f32p, ctypes.c_long, ctypes.c_long, ctypes.c_long,
+                                       _f32p, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_float]
+    lib.oracle_find_max.argtypes = [_f32p, _i32p, _f32p, _i32p]
+    lib.oracle_weight3d.argtypes = [_f32p, _i32p, _f64p, ctypes.c_int, ctypes.c_double]
+    return lib
+
+
+def ref_available() -> bool:
+    return all(os.path.exists(os.path.join(REF_DIR, n))
+               for n in ("libref_rotate.so", "libref_peak.so", "libref_weight.so"))
+
+
+def ref_rotate_lib():
+    lib = _load("libref_rotate.so")
+    # rot3d(float*, float*, long, long, long, float*, char, float, float, float, int)
+    lib.rot3d.argtypes = [_f32p, _f32p, ctypes.c_long, ctypes.c_long, ctypes.c_long, _f32p,
+                          ctypes.c_char, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                          ctypes.c_int]
+    return lib
+
+
+def ref_peak_lib():
+    lib = _load("libref_peak.so")
+    lib.find_max.argtypes = [_f32p, _i32p, _f32p, _i32p]
+    return lib
+
+
+def ref_weight_lib():
+    lib = _load("libref_weight.so")
+    lib.weight3d.argtypes = [_f32p, _i32p, _f64p, ctypes.c_int, _f64p]
+    return lib
+
+
+# ---------------------------------------------------------------------------
+# Arrays: volumes are numpy arrays indexed [x, y, z] (MATLAB order) stored in
+# Fortran order, so the flat memory is x-fastest like MATLAB and the C code.
+# ---------------------------------------------------------------------------
+
+def _f32_fortran(a):
+    return np.asfortranarray(a, dtype=np.float32)
+
+
+def default_center(shape):
+    """tom_rotate default centre ceil(size/2) passed 0-based (Sptrans/tom_rotate.m:105)."""
+    return tuple(float(np.ceil(s / 2)) for s in shape)
+
+
+def euler_matrix(euler_deg):
+    """9 floats rm00, rm10, rm20, rm01, rm11, rm21, rm02, rm12, rm22."""
+    e = np.asarray(euler_deg, dtype=np.float32).reshape(3).copy()
+    m = np.zeros(9, np.float32)
+    oracle_lib().oracle_euler_matrix(_p(e, _f32p), _p(m, _f32p))
+    return m
+
+
+def rotate(vol, euler_deg, center=None):
+    """tom_rotate(vol, [phi psi theta], 'linear', center) in FP32 (C restatement of rot3d)."""
+    v = _f32_fortran(vol)
+    c = default_center(v.shape) if center is None else tuple(float(x) for x in center)
+    out = np.zeros(v.shape, np.float32, order="F")
+    m = euler_matrix(euler_deg)
+    sx, sy, sz = v.shape
+    oracle_lib().oracle_rot3d(_p(v, _f32p), _p(out, _f32p), sx, sy, sz, _p(m, _f32p), *c)
+    return out
+
+
+def rotate_matrix(vol, m9, center=None):
+    """tom_rotate with a 3x3 matrix argument (matrix mode of rot3d): m9 in rm00, rm10, ... order."""
+    v = _f32_fortran(vol)
+    c = default_center(v.shape) if center is None else tuple(float(x) for x in center)
+    out = np.zeros(v.shape, np.float32, order="F")
+    m = np.asarray(m9, np.float32).reshape(9).copy()
+    sx, sy, sz = v.shape
+    oracle_lib().oracle_rot3d(_p(v, _f32p), _p(out, _f32p), sx, sy, sz, _p(m, _f32p), *c)
+    return out
+
+
+def rotate_batch(vol, eulers, center=None):
+    v = _f32_fortran(vol)
+    c = default_center(v.shape) if center is None else tuple(float(x) for x in center)
+    e = np.ascontiguousarray(eulers, dtype=np.float32).reshape(-1, 3)
+    R = e.shape[0]
+    out = np.zeros((R,) + v.shape[::-1], np.float32)  # C order [r][z][y][x]
+    sx, sy, sz = v.shape
+    oracle_lib().oracle_rot3d_batch(_p(v, _f32p), _p(out, _f32p), sx, sy, sz, _p(e, _f32p), R, *c)
+    return [np.asfortranarray(out[r].transpose(2, 1, 0)) for r in range(R)]
+
+
+def ref_rotate(vol, euler_or_matrix, center=None):
+    """The reference's own compiled rot3d (oracle/_ref)."""
+    v = _f32_fortran(vol)
+    c = default_center(v.shape) if center is None else tuple(float(x) for x in center)
+    out = np.zeros(v.shape, np.float32, order="F")
+    e = np.asarray(euler_or_matrix, np.float32).reshape(-1).copy()
+    euler_dim = 1 if e.size == 3 else 3
+    sx, sy, sz = v.shape
+    ref_rotate_lib().rot3d(_p(v, _f32p), _p(out, _f32p), sx, sy, sz, _p(e, _f32p), b"l",
+                           c[0], c[1], c[2], euler_dim)
+    return out
+
+
+def find_max(v):
+    a = _f32_fortran(v)
+    dims = np.array(a.shape + (1,) * (3 - a.ndim), np.int32)
+    val = np.zeros(1, np.float32)
+    pos = np.zeros(3, np.int32)
+    oracle_lib().oracle_find_max(_p(a, _f32p), _p(dims, _i32p), _p(val, _f32p), _p(pos, _i32p))
+    return float(val[0]), tuple(int(x) for x in pos)
+
+
+def ref_find_max(v):
+    a = _f32_fortran(v)
+    dims = np.array(a.shape + (1,) * (3 - a.ndim), np.int32)
+    val = np.zeros(1, np.float32)
+    pos = np.zeros(3, np.int32)
+    ref_peak_lib().find_max(_p(a, _f32p), _p(dims, _i32p), _p(val, _f32p), _p(pos, _i32p))
+    return float(val[0]), tuple(int(x) for x in pos)
+
+
+def weight3d(dims, angles_2xn, thickness):
+    d = np.array(dims, np.int32)
+    ang = np.ascontiguousarray(np.asarray(angles_2xn, np.float64).T)  # n x 2 -> (phi, theta) pairs
+    out = np.zeros(tuple(dims), np.float32, order="F")
+    oracle_lib().oracle_weight3d(_p(out, _f32p), _p(d, _i32p), _p(ang, _f64p), ang.shape[0],
+                                 float(thickness))
+    return out
+
+
+def ref_weight3d(dims, angles_2xn, thickness):
+    d = np.array(dims, np.int32)
+    ang = np.ascontiguousarray(np.asarray(angles_2xn, np.float64).T)
+    out = np.zeros(tuple(dims), np.float32, order="F")
+    th = np.array([float(thickness)], np.float64)
+    ref_weight_lib().weight3d(_p(out, _f32p), _p(d, _i32p), _p(ang, _f64p), ang.shape[0],
+                              _p(th, _f64p))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# MATLAB-level restatement (FP64)
+# ---------------------------------------------------------------------------
+
+def tom_norm_mean0_1std(a):
+    """tom_norm(a,'mean0+1std') (Sptrans/tom_norm.m:83-119 with tom_dev's population std)."""
+    a = np.asarray(a, np.float64) * 2 + 100
+    m = a.mean()
+    s = a.std()
+    return (a - m) / s if s != 0 else a - m
+
+
+def os3_sphere_mask(shape):
+    """tom_os3_sphereMask(template): radius floor(min/2)-1, centre floor(n/2)+1 (1-based),
+    zero where distance >= radius; non-cubic input -> all ones."""
+    shape = tuple(shape)
+    if len(set(shape)) != 1:
+        return np.ones(shape), int(np.prod(shape))
+    radius = np.floor(min(shape) / 2) - 1
+    return sphere_mask(shape, radius, strict=False), None
+
+
+def sphere_mask(shape, radius, center=None, strict=False):
+    """Binary sphere: 1 where distance < radius (os3 sphMask, strict=False) or
+    distance <= radius (tom_sphere, strict=True).  centre is 1-based like MATLAB."""
+    if center is None:
+        center = [np.floor(s / 2) + 1 for s in shape]
+    g = np.meshgrid(*[np.arange(s, dtype=np.float64) for s in shape], indexing="ij")
+    d = np.sqrt(sum((gi + 1 - c) ** 2 for gi, c in zip(g, center)))
+    m = np.ones(shape)
+    if strict:
+        m[d > radius] = 0
+    else:
+        m[d >= radius] = 0
+    return m
+
+
+def centered_grid(shape):
+    return np.meshgrid(*[np.arange(-(s // 2), -(s // 2) + s, dtype=np.float64) for s in shape],
+                       indexing="ij")
+
+
+def tom_wedge(shape, angle_deg):
+    """Filtrans/tom_wedge.m:62-77: zero where tan(angle) > |x|/|z| on a centred grid."""
+    x, _, z = centered_grid(shape)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.abs(x) / np.abs(z)
+    w = np.ones(shape)
+    w[np.tan(np.deg2rad(angle_deg)) > r] = 0
+    return w
+
+
+def av3_wedge(shape, minangle, maxangle):
+    """av3_new/tom_av3_wedge.m / av3/utils/av3_wedge.m:23-26."""
+    x, _, z = centered_grid(shape)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = x / z
+    a = np.tan(np.pi / 2 - np.deg2rad(maxangle)) > r
+    b = np.tan(-np.pi / 2 - np.deg2rad(minangle)) < r
+    w = np.ones(shape)
+    w[a & b] = 0
+    return w
+
+
+def apply_weight_function(vol, w):
+    """Filtrans/tom_apply_weight_function.m:56-62: real(ifftn(ifftshift(fftshift(fftn(in)).*w)))."""
+    f = np.fft.fftshift(np.fft.fftn(np.asarray(vol, np.float64)))
+    return np.real(np.fft.ifftn(np.fft.ifftshift(f * w)))
+
+
+def norm_under_mask(vol, mask):
+    """statistics/tom_os3_normUnderMask.m:3-8: mean and population std under the mask."""
+    m = mask != 0
+    n = m.sum()
+    v = np.asarray(vol, np.float64)
+    mea = ((v * m) * (v != 0)).sum() / n
+    st = np.sqrt(((((~m) * mea) + (v * m) - mea) ** 2).sum() / n)
+    return ((v - mea) / st) * m, mea, st
+
+
+def paste_center(shape, small):
+    """tools/tom_os3_pasteCenter.m:36-39 (3-D case)."""
+    out = np.zeros(shape)
+    o = [s // 2 - t // 2 for s, t in zip(shape, small.shape)]
+    out[o[0]:o[0] + small.shape[0], o[1]:o[1] + small.shape[1], o[2]:o[2] + small.shape[2]] = small
+    return out
+
+
+def local_stats(volume, mask):
+    """tom_os3_mean / tom_os3_std: local mean and std under the mask, FP64.
+
+    mean = real(ifftshift(ifftn(F_I . F_M)))/M ;
+    std  = sqrt(max(real(ifftshift(ifftn(F_{I^2} . F_M)))/M - mean^2, 0)).
+    """
+    vol = np.asarray(volume, np.float64)
+    N = vol.shape
+    mp = paste_center(N, np.asarray(mask, np.float64))
+    M = float((mask != 0).sum())
+    fm = np.fft.rfftn(mp)
+    mean = np.fft.ifftshift(np.fft.irfftn(np.fft.rfftn(vol) * fm, s=N)) / M
+    e2 = np.fft.ifftshift(np.fft.irfftn(np.fft.rfftn(vol * vol) * fm, s=N)) / M
+    var = np.maximum(e2 - mean * mean, 0)
+    return mean, np.sqrt(var), M
+
+
+class FLCF:
+    """Per-volume state of tom_os3_corr's FLCF branch (statistics cached once)."""
+
+    def __init__(self, volume, mask):
+        self.N = tuple(volume.shape)
+        self.mask = np.asarray(mask, np.float64)
+        self.mean, self.std, self.M = local_stats(volume, self.mask)
+        self.fimage = np.fft.rfftn(np.asarray(volume, np.float64))
+
+    def corr(self, t, tmean, tstd):
+        """search/tom_os3_corr.m:151-176 for one (already rotated/modified) template."""
+        p = paste_center(self.N, np.asarray(t, np.float64) * self.mask)
+        ft = np.fft.rfftn(p)
+        num = np.fft.ifftshift(np.fft.irfftn(self.fimage * np.conj(ft), s=self.N)) / self.M
+        num = num - self.mean * tmean
+        den = tstd * self.std
+        res = np.zeros(self.N)
+        eps = np.finfo(np.float64).eps
+        nz = np.abs(den - eps) > eps
+        res[nz] = num[nz] / den[nz]
+        return res
+
+
+def prepare_template(template, mask, psf=None):
+    """findTemplate preprocessing (tom_os3_findTemplate.m:157,233-234):
+    tom_norm(1e5*(t+1),'mean0+1std'); statistics of the unrotated, modified template."""
+    t = tom_norm_mean0_1std(1e5 * (np.asarray(template, np.float64) + 1))
+    tmp = t if psf is None else apply_weight_function(t, psf)
+    _, tmean, tstd = norm_under_mask(tmp, mask)
+    return t, tmean, tstd
+
+
+def find_template(volume, template, mask, angles, psf=None, keep_second=False):
+    """Exhaustive FLCF search, tom_os3_findTemplate.m:255-307 + tom_os3_bestPeak (ccc mode).
+
+    Returns (ccc, idx) with idx the 0-based angle index (reference: 1-based
+    iterator) and -1 where never updated (reference init -1000).  With
+    keep_second, also returns the second-best CC per voxel (for tie analysis).
+    """
+    t, tmean, tstd = prepare_template(template, mask, psf)
+    st = FLCF(volume, mask)
+    ccc = np.full(st.N, -1000.0)
+    idx = np.full(st.N, -1, np.int64)
+    second = np.full(st.N, -1000.0)
+    for it, ang in enumerate(np.asarray(angles, np.float64).reshape(-1, 3)):
+        tr = rotate(t.astype(np.float32), ang).astype(np.float64) * mask
+        if psf is not None:
+            tr = apply_weight_function(tr, psf)
+        cc = st.corr(tr.astype(np.float32).astype(np.float64), tmean, tstd)
+        upd = ccc < cc
+        if keep_second:
+            second = np.where(upd, ccc, np.maximum(second, cc))
+        ccc[upd] = cc[upd]
+        idx[upd] = it
+    return (ccc, idx, second) if keep_second else (ccc, idx)
+
+
+# ---------------------------------------------------------------------------
+# Angles
+# ---------------------------------------------------------------------------
+
+def av3_angle_grid(start, incr, end):
+    """Euler triplets in tom_av3_angle2index order (phi fastest, theta slowest),
+    inclusive ranges (av3_new/tom_av3_angle2index.m:45-51)."""
+    rng = [np.arange(s, e + incr_i * 0.5, incr_i) for s, incr_i, e in zip(start, incr, end)]
+    out = [(ph, ps, th) for th in rng[2] for ps in rng[1] for ph in rng[0]]
+    return np.array(out, np.float64)
+
+
+def av3_angle2index(angle, start, incr, end):
+    n = [int(round((e - s) / i)) + 1 for s, i, e in zip(start, incr, end)]
+    k = [int(round((a - s) / i)) for a, s, i in zip(angle, start, incr)]
+    return k[2] * n[0] * n[1] + k[1] * n[0] + k[0]
+
+
+def av3_index2angle(index, start, incr, end):
+    """av3_new/tom_av3_index2angle.m:47-54."""
+    n = [(e - s) / i + 1 for s, i, e in zip(start, incr, end)]
+    a3 = np.floor(index / (n[0] * n[1]))
+    rest = index - a3 * n[0] * n[1]
+    a2 = np.floor(rest / n[0])
+    a1 = rest - a2 * n[0]
+    return np.array([a1, a2, a3]) * np.array(incr) + np.array(start)
+
+
+# ---------------------------------------------------------------------------
+# Peaks
+# ---------------------------------------------------------------------------
+
+def tom_peak(a):
+    """[c val] = tom_peak(A): first maximum in column-major order, 1-based coordinates."""
+    a = np.asarray(a)
+    v = a.max()
+    flat = np.flatnonzero(np.ravel(a, order="F") == v)[0]
+    c = np.unravel_index(flat, a.shape, order="F")
+    return tuple(int(x) + 1 for x in c), float(v)
+
+
+def tom_peak_radius(a, radius):
+    """[c val M] = tom_peak(A,R) (Analysis/tom_peak.m:203-279): also zero a ball
+    (tom_sphere / tom_circle: distance <= R) around the first maximum."""
+    a = np.array(a, dtype=np.float64, copy=True)
+    c, v = tom_peak(a)
+    g = np.meshgrid(*[np.arange(s) for s in a.shape], indexing="ij")
+    d2 = sum((gi - (ci - 1)) ** 2 for gi, ci in zip(g, c))
+    a[d2 <= radius * radius] = 0
+    return c, v, a
+
+
+def tom_peak_spline(a):
+    """[c val] = tom_peak(A,'spline') via tom_intpeak (Analysis/tom_peak.m:437-525).
+
+    A 3-point not-a-knot spline is the parabola through the points; its
+    maximum is searched on the grid 1:0.001:3 like interp1 + max."""
+    a = np.asarray(a, np.float64)
+    c1, v = tom_peak(a)
+    x1 = np.arange(2001) * 0.001 + 1.0
+    cs, vals = [], []
+    for d in range(a.ndim):
+        s = c1[d]
+        if s == 1 or s == a.shape[d]:
+            cs.append(float(s))
+            vals.append(v)
+            continue
+        idx = [ci - 1 for ci in c1]
+        pk = []
+        for o in (-1, 0, 1):
+            ii = list(idx)
+            ii[d] += o
+            pk.append(a[tuple(ii)])
+        y0, y1, y2 = pk
+        # parabola through (1,y0),(2,y1),(3,y2)
+        A = (y0 - 2 * y1 + y2) / 2
+        B = (y1 - y0) - A * 3
+        C = y0 - A - B
+        yy = A * x1 * x1 + B * x1 + C
+        j = int(np.argmax(yy))
+        vals.append(float(yy[j]))
+        cs.append(s - 1 + j * 0.001)
+    return tuple(cs), max(vals)
+
+
+def topk_peaks(a, k, radius):
+    """Repeated tom_peak(A,R): K peaks, each followed by zeroing a ball of radius R."""
+    a = np.array(a, np.float64, copy=True)
+    out = []
+    for _ in range(k):
+        c, v, a = tom_peak_radius(a, radius)
+        out.append((c, v))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# tom_corr 'norm' and tom_av3_align
+# ---------------------------------------------------------------------------
+
+def norm_inside_mask(vol, mask):
+    """Analysis/tom_corr.m:98-121 (sample std, n-1)."""
+    m = mask != 0
+    n = m.sum()
+    v = np.asarray(vol, np.float64)
+    mea = ((v * m) * (v != 0)).sum() / n
+    st = np.sqrt(((((~m) * mea) + (v * m) - mea) ** 2).sum() / (n - 1))
+    return ((v - mea) / st) * m, mea, st, n
+
+
+def tom_corr_norm(a, b, mask, psf1=None, psf2=None):
+    """ccf = tom_corr(a,b,'norm',mask[,psf1,psf2]) (Analysis/tom_corr.m:75-95)."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if psf1 is not None:
+        a = np.fft.ifftn(np.fft.fftn(a) * np.fft.fftn(psf2))
+        b = np.fft.ifftn(np.fft.fftn(b) * np.fft.fftn(psf1))
+        a = np.real(a)
+        b = np.real(b)
+    a, _, _, n = norm_inside_mask(a, mask)
+    b, _, _, _ = norm_inside_mask(b, mask)
+    return np.real(np.fft.fftshift(np.fft.ifftn(np.fft.fftn(b) * np.conj(np.fft.fftn(a))))) / n

@@ -1,0 +1,85 @@
+"""FLCF matching parity on the GPU against the FP64 oracle.
+
+Tolerance: |cc_gpu - cc_oracle| <= 1e-4 * max|cc_oracle|
+over every voxel, and identical angle indices wherever the oracle's best CC
+beats its runner-up by more than that tolerance."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+REL = 1e-4
+
+
+def _compare(cc, idx, ref_cc, ref_idx, ref_second):
+    scale = np.abs(ref_cc).max()
+    err = np.abs(cc.astype(np.float64) - ref_cc).max()
+    assert err <= REL * scale, f"max |dcc| {err:.3e} > {REL * scale:.3e}"
+    sep = (ref_cc - ref_second) > 2 * REL * scale
+    assert np.array_equal(idx[sep], ref_idx[sep]), f"{(idx[sep] != ref_idx[sep]).sum()} index mismatches"
+    return err / scale
+
+
+def test_local_stats(gpu, oracle):
+    rng = np.random.default_rng(21)
+    vol = (rng.standard_normal((64, 48, 40)) * 2 + 5).astype(np.float32)
+    T = 16
+    t = rng.standard_normal((T, T, T)).astype(np.float32)
+    mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
+    plan = gpu.MatchPlan(vol.shape, t.shape)
+    plan.set_template(gpu.to_device(t), gpu.to_device(mask))
+    plan.set_volume(gpu.to_device(vol))
+    m, s = plan.stats()
+    mean, std, _ = oracle.local_stats(vol.astype(np.float64), mask)
+    assert np.abs(gpu.from_device(m) - mean).max() < 1e-5 * np.abs(mean).max()
+    assert np.abs(gpu.from_device(s) - std).max() < 1e-5 * std.max()
+
+
+@pytest.mark.parametrize("with_psf", [False, True])
+def test_os3_corr_single_map(gpu, oracle, with_psf):
+    rng = np.random.default_rng(22)
+    vol = rng.standard_normal((64, 64, 32)).astype(np.float32)
+    T = 16
+    tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
+    mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
+    psf = oracle.tom_wedge((T, T, T), 30).astype(np.float32) if with_psf else None
+    # template statistics of the preprocessed template (findTemplate:157,233-234)
+    tn, tmean, tstd = oracle.prepare_template(tmpl, mask, psf)
+    rot = oracle.rotate(tn.astype(np.float32), (30, 45, 60)) * mask
+    if psf is not None:
+        rot = oracle.apply_weight_function(rot, psf)
+    rot = rot.astype(np.float32)
+    st = oracle.FLCF(vol.astype(np.float64), mask)
+    ref = st.corr(rot.astype(np.float64), tmean, tstd)
+    opts = {"mask": mask, "template": tmpl, "psf": psf}
+    got, _ = gpu.tom_os3_corr(vol, rot, opts)
+    assert np.abs(got - ref).max() <= REL * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("with_psf", [False, True])
+def test_find_template_small(gpu, oracle, with_psf):
+    rng = np.random.default_rng(23)
+    N, T = (64, 48, 40), 16
+    vol = rng.standard_normal(N).astype(np.float32)
+    tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
+    mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
+    psf = oracle.tom_wedge((T, T, T), 30).astype(np.float32) if with_psf else None
+    angles = oracle.av3_angle_grid((0, 0, 0), (45, 45, 60), (315, 90, 120))[:37]
+    ref_cc, ref_idx, ref_2 = oracle.find_template(vol, tmpl, mask, angles, psf=psf, keep_second=True)
+    ccc, ang = gpu.tom_os3_findTemplate(vol, tmpl, angles, mask=mask, psf=psf, batch=5)
+    idx = np.where(ang > 0, ang - 1, -1).astype(np.int64)
+    _compare(ccc, idx, ref_cc, ref_idx, ref_2)
+
+
+def test_exhaustive_128_angle_subset(gpu, oracle):
+    """The 128^3 / 32^3 exhaustive workload (6 blobs, 10 copies, SNR 0.1, +-60 wedge,
+    mask radius 14) on the first 24 angles of its 30-degree grid."""
+    from tom_b200 import synth
+    cfg = synth.CONFIGS["exhaustive_128"]
+    grid = oracle.av3_angle_grid(*cfg["angles"])
+    d = synth.make_tomogram(cfg["N"], cfg["T"], cfg["n_copies"], cfg["n_blobs"], cfg["rho"], cfg["snr"],
+                            cfg["max_tilt"], seed=100, euler_pool=grid[:24])
+    mask = synth.sphere_mask(cfg["T"], cfg["mask_radius"])
+    ref_cc, ref_idx, ref_2 = oracle.find_template(d["tomo"], d["template"], mask, grid[:24], keep_second=True)
+    ccc, ang = gpu.tom_os3_findTemplate(d["tomo"], d["template"], grid[:24], mask=mask, batch=8)
+    idx = np.where(ang > 0, ang - 1, -1).astype(np.int64)
+    _compare(ccc, idx, ref_cc, ref_idx, ref_2)

@@ -1,0 +1,131 @@
+"""The oracle pinned against the reference: its C restatements equal the
+compiled reference routines bit for bit, and its MATLAB-level restatements
+reproduce every known-answer example of the reference's docstrings."""
+import numpy as np
+import pytest
+
+TABLE = [0, 30, 45, 60, 90, 120, 135, 150, 180, 210, 225, 240, 270, 300, 315, 330]
+
+
+def test_rot3d_bit_exact_vs_reference(ref_libs):
+    O = ref_libs
+    rng = np.random.default_rng(1)
+    for trial in range(40):
+        s = tuple(int(x) for x in rng.integers(4, 18, 3))
+        v = rng.standard_normal(s).astype(np.float32)
+        if trial % 2:
+            e = rng.choice(TABLE + [10, 17.5, -20, 33.3], 3)
+        else:
+            e = rng.random(3) * 360
+        c = None if trial % 3 else tuple(float(x) for x in rng.integers(0, 6, 3))
+        a = O.rotate(v, e, c)
+        b = O.ref_rotate(v, e, c)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (s, e, c)
+        m = O.euler_matrix(e)
+        assert np.array_equal(O.rotate_matrix(v, m, c), O.ref_rotate(v, m, c))
+
+
+def test_find_max_vs_reference(ref_libs):
+    O = ref_libs
+    rng = np.random.default_rng(2)
+    for _ in range(20):
+        v = rng.integers(-3, 4, (6, 5, 4)).astype(np.float32)  # many ties
+        assert O.find_max(v) == O.ref_find_max(v)
+    v = np.full((3, 3, 3), -1e6, np.float32)
+    v[1, 2, 0] = -99998.0
+    assert O.ref_find_max(v)[1] == (1, 2, 0)
+
+
+def test_weight3d_vs_reference(ref_libs):
+    O = ref_libs
+    for dims, ang, th in [((16, 12, 10), [[0, 0, 0, 0], [-60, -20, 20, 60]], 16),
+                          ((9, 8, 7), [[10, 30], [-45, 50]], 5),
+                          ((20, 20, 20), np.vstack([np.zeros(41), np.arange(-60, 61, 3)]), 64)]:
+        a = O.weight3d(dims, np.asarray(ang, float), th)
+        b = O.ref_weight3d(dims, np.asarray(ang, float), th)
+        assert np.array_equal(a, b)
+
+
+def test_tom_peak_kats(oracle):
+    """Analysis/tom_peak.m:27-50."""
+    A = np.array([[1, 2, 3, 4, 17], [5, 6, 7, 8, 18], [10, 9, 40, 6, 20], [12, 16, 17, 20, 30],
+                  [5, 23, 35, 12, 6]], float)
+    assert oracle.tom_peak(A) == ((3, 3), 40.0)
+    c, v = oracle.tom_peak_spline(A)
+    assert np.allclose(c, [3.0890, 2.9770], atol=5e-5) and abs(v - 40.2232) < 5e-5
+    _, _, M = oracle.tom_peak_radius(A, 2)
+    expect = np.array([[1, 2, 0, 4, 17], [5, 0, 0, 0, 18], [0, 0, 0, 0, 0], [12, 0, 0, 0, 30],
+                       [5, 23, 0, 12, 6]], float)
+    assert np.array_equal(M, expect)
+
+
+def test_tom_fourier_kat():
+    """Filtrans/tom_fourier.m:18-22.  Two printed entries contradict the table's own
+    Hermitian symmetry for a real input (c(1,2) must be conj(c(1,4)) and c(2,2)
+    conj(c(4,4))); the other 14 entries are pinned exactly."""
+    a = np.array([[11, 3, -6, -14], [1, -13, 9, 6], [0, 8, 13, -3], [-8, 17, -15, 7]], float)
+    c = np.fft.fft2(a)
+    expect = np.array([[16, 3 + 19j, -6, 3 + 19j], [-24 - 2j, 50 + 9j, 8 - 64j, 1 + 21j],
+                       [8, 5 - 37j, 54, 5 + 37j], [-24 + 2j, 1 - 21j, 8 + 64j, 59 - 9j]])
+    ok = np.ones((4, 4), bool)
+    ok[0, 1] = ok[1, 1] = False
+    assert np.allclose(c[ok], expect[ok])
+    assert np.isclose(c[0, 1], np.conj(expect[0, 3])) and np.isclose(c[1, 1], np.conj(expect[3, 3]))
+
+
+def test_rotation_axis_conventions(oracle):
+    """Sptrans/tom_rotate.m:59-61: X axis ~ phi=0 psi=0 the=a; Y ~ phi=270 psi=90 the=a; Z ~ phi=a."""
+    for a in (20.0, 37.0, 90.0):
+        for e, axis in (((0, 0, a), 0), ((270, 90, a), 1), ((a, 0, 0), 2)):
+            m = oracle.euler_matrix(e).reshape(3, 3).T  # rows: r = M p
+            u = np.zeros(3)
+            u[axis] = 1
+            assert np.allclose(m @ u, u, atol=1e-6), (e, axis)
+
+
+def test_local_stats_direct(oracle):
+    """tom_os3_mean/std via FFT equal the direct masked sums (Roseman FLCF denominators)."""
+    rng = np.random.default_rng(3)
+    vol = rng.standard_normal((12, 10, 8))
+    mask = oracle.sphere_mask((6, 6, 6), 2.5)
+    mean, std, M = oracle.local_stats(vol, mask)
+    c = 3
+    for p in [(0, 0, 0), (5, 4, 3), (11, 9, 7)]:
+        vals = []
+        for j in np.argwhere(mask != 0):
+            q = [(p[d] + j[d] - c) % vol.shape[d] for d in range(3)]
+            vals.append(vol[tuple(q)])
+        vals = np.array(vals)
+        assert abs(mean[p] - vals.mean()) < 1e-12
+        assert abs(std[p] - vals.std()) < 1e-10
+
+
+def test_flcf_direct(oracle):
+    """tom_os3_corr's FLCF equals the direct correlation sum at every voxel."""
+    rng = np.random.default_rng(4)
+    vol = rng.standard_normal((10, 12, 8))
+    t = rng.standard_normal((6, 6, 6))
+    mask = oracle.sphere_mask((6, 6, 6), 2.9)
+    st = oracle.FLCF(vol, mask)
+    tm, ts = 0.1, 1.3
+    cc = st.corr(t, tm, ts)
+    c = 3
+    for p in [(0, 0, 0), (4, 7, 2), (9, 11, 7)]:
+        s = 0.0
+        for j in np.argwhere(mask != 0):
+            q = [(p[d] + j[d] - c) % vol.shape[d] for d in range(3)]
+            s += t[tuple(j)] * vol[tuple(q)]
+        num = s / st.M - st.mean[p] * tm
+        assert abs(cc[p] - num / (ts * st.std[p])) < 1e-10
+
+
+def test_angle_grids(oracle):
+    g0 = oracle.av3_angle_grid((0, 0, 0), (30, 30, 30), (330, 330, 180))
+    assert len(g0) == 1008
+    g1 = oracle.av3_angle_grid((0, 0, 0), (10, 10, 10), (350, 350, 180))
+    assert len(g1) == 24624
+    st, inc, en = (0, 0, 0), (30, 30, 30), (330, 330, 180)
+    for i in (0, 1, 11, 12, 143, 144, 1007):
+        a = g0[i]
+        assert oracle.av3_angle2index(a, st, inc, en) == i
+        assert np.allclose(oracle.av3_index2angle(i, st, inc, en), a)

@@ -1,0 +1,193 @@
+// Generic batched FFTs along one axis of a 3-D array, and 3-D r2c / c2r / c2c
+// transforms built from them (FP32 and FP64).
+//
+// These are the library's own replacement for MATLAB fftn/ifftn and the FFTW
+// plans of the C++ picker (Filtrans/tom_fourier.m:44-50,
+// Oscar3/c++Picker/src/tom/core/fftw_plan.cpp).  The matching hot loop does
+// not use them: it runs its own fused kernels (match.cu).  They serve the
+// once-per-volume set-up (tomogram spectrum, FP64 local statistics), the small
+// template-sized wedge filter, and the tom_fourier entry points.
+#include "fft3d.h"
+#include "fft_engine.cuh"
+#include "twiddles.h"
+
+#include <cstdio>
+
+namespace tg {
+
+template <int L> struct LineCfg {
+    static constexpr int NL = (2048 / L) < 1 ? 1 : ((2048 / L) > 64 ? 64 : (2048 / L));
+    static constexpr int NT = 256;
+    static constexpr int LS = L + 1;
+};
+
+template <int L, int DIR, int MODE, typename C>
+__global__ void __launch_bounds__(256) k_fft_lines(const void* in, void* out,
+                                                   LineGeom gi, LineGeom go, const C* __restrict__ tw,
+                                                   double scale, long nlines) {
+    typedef typename CTraits<C>::R Rt;
+    constexpr int NL = LineCfg<L>::NL, NT = LineCfg<L>::NT, LS = LineCfg<L>::LS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    const int tid = threadIdx.x;
+    const long line0 = (long)blockIdx.x * NL;
+    const Rt* rin = reinterpret_cast<const Rt*>(in);
+    const C* cin = reinterpret_cast<const C*>(in);
+
+    for (int i = tid; i < NL * L; i += NT) {
+        int l, e;
+        if (gi.es == 1) { l = i / L; e = i - l * L; }
+        else { e = i / NL; l = i - e * NL; }
+        const long gl = line0 + l;
+        C v = CTraits<C>::make(0, 0);
+        if (gl < nlines) {
+            const long off = (gl % gi.cnt0) * gi.s0 + (gl / gi.cnt0) * gi.s1;
+            if (MODE == FFT_R2C) {
+                v = CTraits<C>::make(rin[off + e * gi.es], 0);
+            } else if (MODE == FFT_C2R) {
+                if (e <= L / 2) v = cin[off + e * gi.es];
+                else v = cconj(cin[off + (L - e) * gi.es]);
+            } else {
+                v = cin[off + e * gi.es];
+            }
+        }
+        s[l * LS + e] = v;
+    }
+    __syncthreads();
+    tgfft::smem_fft<L, DIR, NL, NT, LS, C>(s, tw, tid);
+
+    Rt* rout = reinterpret_cast<Rt*>(out);
+    C* cout = reinterpret_cast<C*>(out);
+    const Rt sc = (Rt)scale;
+    for (int i = tid; i < NL * L; i += NT) {
+        int l, e;
+        if (go.es == 1) { l = i / L; e = i - l * L; }
+        else { e = i / NL; l = i - e * NL; }
+        const long gl = line0 + l;
+        if (gl >= nlines) continue;
+        const long off = (gl % go.cnt0) * go.s0 + (gl / go.cnt0) * go.s1;
+        const C v = s[l * LS + e];
+        if (MODE == FFT_R2C) {
+            if (e <= L / 2) cout[off + e * go.es] = cscale(v, sc);
+        } else if (MODE == FFT_C2R) {
+            rout[off + e * go.es] = v.x * sc;
+        } else {
+            cout[off + e * go.es] = cscale(v, sc);
+        }
+    }
+}
+
+template <int L, int DIR, int MODE, typename C>
+static cudaError_t launch_lines_t(const void* in, void* out, const LineGeom& gi, const LineGeom& go,
+                                  long nlines, double scale, cudaStream_t st) {
+    constexpr int NL = LineCfg<L>::NL, NT = LineCfg<L>::NT, LS = LineCfg<L>::LS;
+    const size_t smem = (size_t)NL * LS * sizeof(C);
+    auto kern = k_fft_lines<L, DIR, MODE, C>;
+    static unsigned attr_mask = 0;  // one bit per device: attribute already raised
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (smem > 48 * 1024 && dev < 32 && !(attr_mask & (1u << dev))) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_mask |= 1u << dev;
+    }
+    const C* tw = twiddle_table<C>(L);
+    if (!tw) return cudaErrorInvalidValue;
+    const long blocks = (nlines + NL - 1) / NL;
+    if (blocks <= 0) return cudaSuccess;
+    kern<<<(unsigned)blocks, NT, smem, st>>>(in, out, gi, go, tw, scale, nlines);
+    return cudaGetLastError();
+}
+
+template <int DIR, int MODE, typename C>
+static cudaError_t dispatch_len(int L, const void* in, void* out, const LineGeom& gi, const LineGeom& go,
+                                long nlines, double scale, cudaStream_t st) {
+#define TG_CASE(N) \
+    case N: return launch_lines_t<N, DIR, MODE, C>(in, out, gi, go, nlines, scale, st);
+    switch (L) {
+        TG_CASE(8) TG_CASE(16) TG_CASE(24) TG_CASE(32) TG_CASE(40) TG_CASE(48) TG_CASE(64)
+        TG_CASE(80) TG_CASE(96) TG_CASE(128) TG_CASE(160) TG_CASE(192) TG_CASE(232)
+        TG_CASE(256) TG_CASE(464) TG_CASE(512) TG_CASE(928)
+        default: return cudaErrorInvalidValue;
+    }
+#undef TG_CASE
+}
+
+bool fft_length_supported(int L) {
+    switch (L) {
+        case 8: case 16: case 24: case 32: case 40: case 48: case 64: case 80: case 96:
+        case 128: case 160: case 192: case 232: case 256: case 464: case 512: case 928:
+            return true;
+        default: return false;
+    }
+}
+
+template <typename C>
+cudaError_t fft_lines(int L, int dir, int mode, const void* in, void* out, const LineGeom& gi,
+                      const LineGeom& go, long nlines, double scale, cudaStream_t st) {
+    if (mode == FFT_R2C) return dispatch_len<-1, FFT_R2C, C>(L, in, out, gi, go, nlines, scale, st);
+    if (mode == FFT_C2R) return dispatch_len<+1, FFT_C2R, C>(L, in, out, gi, go, nlines, scale, st);
+    if (dir < 0) return dispatch_len<-1, FFT_C2C, C>(L, in, out, gi, go, nlines, scale, st);
+    return dispatch_len<+1, FFT_C2C, C>(L, in, out, gi, go, nlines, scale, st);
+}
+
+template cudaError_t fft_lines<float2>(int, int, int, const void*, void*, const LineGeom&,
+                                       const LineGeom&, long, double, cudaStream_t);
+template cudaError_t fft_lines<double2>(int, int, int, const void*, void*, const LineGeom&,
+                                        const LineGeom&, long, double, cudaStream_t);
+
+// ------------------------------------------------------------ 3-D drivers
+// Real arrays are [nz][ny][nx] (x fastest); half spectra [nz][ny][nx/2+1].
+template <typename C>
+cudaError_t r2c3d(const void* real_in, C* half_out, const int n[3], cudaStream_t st) {
+    const long nx = n[0], ny = n[1], nz = n[2], nh = nx / 2 + 1;
+    cudaError_t e;
+    LineGeom gi{1, (int)ny, nx, (int)nz, nx * ny};
+    LineGeom go{1, (int)ny, nh, (int)nz, nh * ny};
+    if ((e = fft_lines<C>((int)nx, -1, FFT_R2C, real_in, half_out, gi, go, ny * nz, 1.0, st))) return e;
+    LineGeom gy{nh, (int)nh, 1, (int)nz, nh * ny};
+    if (ny > 1 && (e = fft_lines<C>((int)ny, -1, FFT_C2C, half_out, half_out, gy, gy, nh * nz, 1.0, st)))
+        return e;
+    LineGeom gz{nh * ny, (int)(nh * ny), 1, 1, 0};
+    if (nz > 1 && (e = fft_lines<C>((int)nz, -1, FFT_C2C, half_out, half_out, gz, gz, nh * ny, 1.0, st)))
+        return e;
+    return cudaSuccess;
+}
+
+template <typename C>
+cudaError_t c2r3d(C* half_inout, void* real_out, const int n[3], double scale, cudaStream_t st) {
+    const long nx = n[0], ny = n[1], nz = n[2], nh = nx / 2 + 1;
+    cudaError_t e;
+    LineGeom gz{nh * ny, (int)(nh * ny), 1, 1, 0};
+    if (nz > 1 && (e = fft_lines<C>((int)nz, +1, FFT_C2C, half_inout, half_inout, gz, gz, nh * ny, 1.0, st)))
+        return e;
+    LineGeom gy{nh, (int)nh, 1, (int)nz, nh * ny};
+    if (ny > 1 && (e = fft_lines<C>((int)ny, +1, FFT_C2C, half_inout, half_inout, gy, gy, nh * nz, 1.0, st)))
+        return e;
+    LineGeom gi{1, (int)ny, nh, (int)nz, nh * ny};
+    LineGeom go{1, (int)ny, nx, (int)nz, nx * ny};
+    return fft_lines<C>((int)nx, +1, FFT_C2R, half_inout, real_out, gi, go, ny * nz, scale, st);
+}
+
+// Full complex 3-D transform in place, [nz][ny][nx] complex.
+template <typename C>
+cudaError_t c2c3d(C* data, const int n[3], int dir, double scale, cudaStream_t st) {
+    const long nx = n[0], ny = n[1], nz = n[2];
+    cudaError_t e;
+    const double sx = (ny > 1 || nz > 1) ? 1.0 : scale, sy = nz > 1 ? 1.0 : scale;
+    LineGeom gx{1, (int)ny, nx, (int)nz, nx * ny};
+    if ((e = fft_lines<C>((int)nx, dir, FFT_C2C, data, data, gx, gx, ny * nz, sx, st))) return e;
+    LineGeom gy{nx, (int)nx, 1, (int)nz, nx * ny};
+    if (ny > 1 && (e = fft_lines<C>((int)ny, dir, FFT_C2C, data, data, gy, gy, nx * nz, sy, st))) return e;
+    LineGeom gz{nx * ny, (int)(nx * ny), 1, 1, 0};
+    if (nz > 1 && (e = fft_lines<C>((int)nz, dir, FFT_C2C, data, data, gz, gz, nx * ny, scale, st))) return e;
+    return cudaSuccess;
+}
+
+template cudaError_t r2c3d<float2>(const void*, float2*, const int[3], cudaStream_t);
+template cudaError_t r2c3d<double2>(const void*, double2*, const int[3], cudaStream_t);
+template cudaError_t c2r3d<float2>(float2*, void*, const int[3], double, cudaStream_t);
+template cudaError_t c2r3d<double2>(double2*, void*, const int[3], double, cudaStream_t);
+template cudaError_t c2c3d<float2>(float2*, const int[3], int, double, cudaStream_t);
+template cudaError_t c2c3d<double2>(double2*, const int[3], int, double, cudaStream_t);
+
+}  // namespace tg

@@ -1,0 +1,62 @@
+// FLCF matching plan (see match.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ctx.h"
+
+namespace tg {
+
+bool match_sizes_supported(const int N[3], const int T[3]);
+cudaError_t c2c3d_batch(float2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
+
+struct MatchPlan {
+    tomgpu_ctx* ctx = nullptr;
+    int N[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+    int B = 8;
+    long long nvox = 0, nh1 = 0, tn = 0;
+    int64_t bytes_held = 0;
+    bool has_template = false, has_volume = false, has_psf = false;
+    double msize = 0, tmean = 0, tstd = 0, vmean = 0;
+    // template state
+    float* d_tmpl = nullptr;  // tom_norm'ed template
+    float* d_mask = nullptr;
+    float* d_wu = nullptr;    // ifftshift(psf): weight in unshifted frequency order
+    // volume state
+    float2* d_fimg = nullptr;  // spectrum of I - c, [kx][kz][ky]
+    float* d_mu0 = nullptr;    // local mean of I - c
+    float* d_sig = nullptr;    // local std
+    float* d_gam = nullptr;    // 1 / (sigma_T sigma_I) or 0
+    // per-batch work
+    float* d_mats = nullptr;
+    float* h_mats = nullptr;
+    int mats_cap = 0;
+    cudaEvent_t ev_mats = nullptr;
+    float* d_t1 = nullptr;
+    float2* d_tc = nullptr;
+    double* d_tsum = nullptr;
+    float2* d_A = nullptr;
+    float2* d_Z = nullptr;
+    float2* d_Q = nullptr;
+    float2* d_H = nullptr;
+    double* d_tmp64 = nullptr;
+
+    ~MatchPlan();
+    void release();
+    int alloc(void** p, size_t bytes);
+    int create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batch);
+    int ensure_mats(int R);
+    int upload_mats(const float* eulers, int R);
+    int set_template(const float* tmpl, const float* mask, const float* psf);
+    int set_volume(const float* vol);
+    int prepare_batch(int off, int nb);
+    int run(const float* eulers, int R, int index_offset, float* maxcc, int* angidx);
+    int corr(const float* t, float* cc);
+    int init_results(float* maxcc, int* angidx);
+};
+
+}  // namespace tg
+
+struct tomgpu_match_plan {
+    tg::MatchPlan p;
+};

@@ -1,0 +1,566 @@
+"""TOM-compatible host API over libtomgpu.
+
+Functions keep the names, argument meaning and return conventions of the
+TOM toolbox's MATLAB functions on the template-matching path, so calling code
+reads like the reference:
+
+  tom_rotate            Sptrans/tom_rotate.m:89-165 (-> tom_rotatec MEX)
+  tom_peak              Analysis/tom_peak.m:80-525 (-> tom_peakinc MEX)
+  tom_calc_weight_functioninc  Filtrans/tom_calc_weight_functioninc.c:259-289
+  tom_wedge / av3_wedge Filtrans/tom_wedge.m:62-77, av3/utils/av3_wedge.m:23-26
+  tom_fourier / tom_ifourier   Filtrans/tom_fourier.m, Filtrans/tom_ifourier.m
+  tom_os3_sphereMask    Oscar3/matlabPicker/search/tom_os3_sphereMask.m:4-37
+  tom_os3_corr          Oscar3/matlabPicker/search/tom_os3_corr.m:56-192 (FLCF)
+  tom_os3_findTemplate  Oscar3/matlabPicker/search/tom_os3_findTemplate.m:157-307
+  tom_os3_angleList     Oscar3/matlabPicker/tools/tom_os3_angleList.m:44-97
+  tom_av3_angle2index / tom_av3_index2angle  av3_new/tom_av3_angle2index.m, tom_av3_index2angle.m
+
+Volumes are numpy arrays indexed [x, y, z] (MATLAB order).  Every compute
+step runs on the GPU through the C ABI; nothing here falls back to the CPU.
+Device-resident work (the fast path) goes through :class:`MatchPlan` with
+torch CUDA tensors shaped (z, y, x).
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import numpy as np
+
+from . import _lib
+from ._lib import MatchParams, check, lib
+
+# ---------------------------------------------------------------- context
+
+
+class Context:
+    """A libtomgpu context on one CUDA device (own stream unless set)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        st = lib().tomgpu_ctx_create(int(device), ctypes.byref(h))
+        check(st, None)
+        self.handle = h
+        self.device = device
+        self.use_torch_stream()
+
+    def close(self):
+        if self.handle:
+            lib().tomgpu_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None):
+        check(lib().tomgpu_ctx_set_stream(self.handle, ctypes.c_void_p(stream_ptr or 0)), self.handle)
+
+    def use_torch_stream(self):
+        """Issue this context's work on torch's current stream of its device."""
+        import torch
+        self.set_stream(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def synchronize(self):
+        check(lib().tomgpu_ctx_synchronize(self.handle), self.handle)
+
+    @property
+    def launches(self) -> int:
+        return int(lib().tomgpu_ctx_launch_count(self.handle))
+
+    def check(self, status):
+        check(status, self.handle)
+
+    def profile(self, enable: bool):
+        """Start (and reset) or stop the per-kernel-class event timers."""
+        self.check(lib().tomgpu_ctx_profile(self.handle, 1 if enable else 0))
+
+    def kernel_times(self):
+        """{class name: (total ms, launches)} of the matching loop's kernels."""
+        out = {}
+        for k, name in enumerate(_lib.KERNEL_CLASSES):
+            ms = ctypes.c_double()
+            n = ctypes.c_int64()
+            self.check(lib().tomgpu_ctx_profile_read(self.handle, k, ctypes.byref(ms), ctypes.byref(n)))
+            out[name] = (ms.value, n.value)
+        return out
+
+
+_ctx_lock = threading.Lock()
+_default: dict = {}
+
+
+def default_context(device: int = 0) -> Context:
+    with _ctx_lock:
+        if device not in _default:
+            _default[device] = Context(device)
+        return _default[device]
+
+
+# ---------------------------------------------------------------- helpers
+
+def _dims(a):
+    a = np.asarray(a)
+    if a.ndim == 2:
+        return (a.shape[0], a.shape[1], 1)
+    if a.ndim != 3:
+        raise ValueError("volume must be 2-D or 3-D")
+    return tuple(int(s) for s in a.shape)
+
+
+def _cdims(d):
+    return (ctypes.c_int * 3)(*[int(x) for x in d])
+
+
+def _f32_xfast(a):
+    """Host buffer with x fastest (MATLAB column-major) as float32."""
+    return np.asfortranarray(np.asarray(a, dtype=np.float32))
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def to_device(a, device=0):
+    """numpy [x, y, z] -> torch CUDA tensor (z, y, x), float32 contiguous."""
+    import torch
+    a = np.asarray(a, np.float32)
+    if a.ndim == 2:
+        a = a[:, :, None]
+    return torch.from_numpy(np.ascontiguousarray(a.transpose(2, 1, 0))).to(f"cuda:{device}")
+
+
+def from_device(t):
+    """torch (z, y, x) -> numpy [x, y, z] (a Fortran-ordered view)."""
+    return t.detach().cpu().numpy().transpose(2, 1, 0)
+
+
+def _tptr(t):
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+# --------------------------------------------------------------- rotation
+
+def euler_matrix(euler):
+    """The 9 floats rm00, rm10, rm20, rm01, rm11, rm21, rm02, rm12, rm22 of tom_rotatec."""
+    e = (ctypes.c_float * 3)(*[float(x) for x in np.asarray(euler).reshape(3)])
+    m = (ctypes.c_float * 9)()
+    check(lib().tomgpu_euler_matrix(e, m))
+    return np.array(m[:], np.float32)
+
+
+def tom_rotatec(in_, out, euler, interp, center, ctx: Context | None = None):
+    """MEX form: writes the rotation of in_ into the pre-allocated float32 array out
+    (Sptrans/tom_rotatec.c:407-480; 5 inputs, 0 outputs)."""
+    if interp != "linear":
+        raise ValueError("Unknown interpolation type ... only linear interpolation implemented")
+    a = np.asarray(in_)
+    if a.dtype != np.float32 or out.dtype != np.float32:
+        raise TypeError("Input volumes must be single.")
+    if a.shape != out.shape:
+        raise ValueError("Volumes must have same size.")
+    res = _rotate(a, euler, center, ctx)
+    out[...] = res
+
+
+def _rotate(a, euler, center, ctx):
+    ctx = ctx or default_context()
+    d = _dims(a)
+    src = _f32_xfast(a.reshape(d, order="F") if a.ndim == 2 else a)
+    dst = np.zeros(d, np.float32, order="F")
+    e = np.asarray(euler, np.float32)
+    if e.size == 3:
+        mode, buf = _lib.TOMGPU_EULER_DEG, e.reshape(3)
+    elif e.size == 9:
+        mode, buf = _lib.TOMGPU_MATRIX, np.asarray(e.reshape(3, 3).flatten(order="F"), np.float32)
+    else:
+        raise ValueError("euler must be [phi psi theta] or a 3x3 matrix")
+    buf = np.ascontiguousarray(buf, np.float32)
+    c = np.asarray(center, np.float32).reshape(-1)
+    if c.size == 2:
+        c = np.array([c[0], c[1], 0], np.float32)
+    ctx.check(lib().tomgpu_rotate3d(ctx.handle, _ptr(src), _ptr(dst), _cdims(d),
+                                    buf.ctypes.data_as(_lib.c_float_p), mode,
+                                    np.ascontiguousarray(c, np.float32).ctypes.data_as(_lib.c_float_p)))
+    return dst.reshape(a.shape, order="F")
+
+
+def tom_rotate(in_, euler_angles, interp="linear", center=None, ctx: Context | None = None):
+    """out = tom_rotate(in, [phi psi theta] | 3x3, 'linear', [center]) (Sptrans/tom_rotate.m:89-165).
+    Default centre ceil(size/2), 0-based.  Returns double like the reference."""
+    if interp != "linear":
+        raise ValueError("only linear interpolation implemented")
+    a = np.asarray(in_)
+    if a.ndim != 3:
+        raise ValueError("tom_rotate: only 3-D volumes are supported on the GPU path")
+    if center is None:
+        center = [np.ceil(s / 2) for s in a.shape]
+    return _rotate(a, euler_angles, center, ctx).astype(np.float64)
+
+
+# ------------------------------------------------------------------ peaks
+
+def _peak_host(a, ctx):
+    d = _dims(a)
+    buf = _f32_xfast(np.asarray(a).reshape(d, order="F"))
+    val = ctypes.c_float()
+    pos = (ctypes.c_int * 3)(0, 0, 0)
+    ctx.check(lib().tomgpu_peak(ctx.handle, _ptr(buf), _cdims(d), ctypes.byref(val), pos))
+    return tuple(pos[:]), float(val.value)
+
+
+def tom_peakc(a, ctx: Context | None = None):
+    """[pos val] via the tom_peakinc MEX semantics (strict '>' from -99999, 1-based)."""
+    ctx = ctx or default_context()
+    pos, val = _peak_host(a, ctx)
+    nd = np.asarray(a).ndim
+    return pos[:nd], val
+
+
+def tom_peak(a, *args, ctx: Context | None = None):
+    """[c val] = tom_peak(A); [c val] = tom_peak(A,'spline'); [c val M] = tom_peak(A,R);
+    [c val M] = tom_peak(A,R,'spline')   (Analysis/tom_peak.m).  3-D volumes."""
+    ctx = ctx or default_context()
+    A = np.asarray(a, np.float64)
+    if A.ndim != 3:
+        raise ValueError("tom_peak: 3-D volumes on the GPU path")
+    spline = any(isinstance(x, str) and x == "spline" for x in args)
+    radius = None
+    for x in args:
+        if isinstance(x, str):
+            if x != "spline":
+                raise ValueError("unknown flag " + x)
+        else:
+            radius = float(x)
+    dev = to_device(A, ctx.device)
+    d = _cdims(A.shape)
+    val = ctypes.c_float()
+    pos = (ctypes.c_int * 3)(0, 0, 0)
+    ctx.check(lib().tomgpu_peak_dev(ctx.handle, _tptr(dev), d, ctypes.byref(val), pos))
+    c = tuple(pos[:])
+    v = float(val.value)
+    if spline:
+        coord = (ctypes.c_double * 3)()
+        sv = ctypes.c_double()
+        ctx.check(lib().tomgpu_peak_spline_dev(ctx.handle, _tptr(dev), d, pos, coord, ctypes.byref(sv)))
+        c, v = tuple(coord[:]), float(sv.value)
+    if radius is None:
+        return c, v
+    # zero the ball around the integer maximum on the device (the spline variant
+    # reports the sub-voxel position but zeroes around the integer peak, like
+    # the reference)
+    vr = ctypes.c_float()
+    p1 = (ctypes.c_int * 3)()
+    ctx.check(lib().tomgpu_peak_radius_dev(ctx.handle, _tptr(dev), d, float(radius), ctypes.byref(vr), p1))
+    ctx.synchronize()
+    M = from_device(dev).astype(np.float64)
+    return c, v, np.asfortranarray(M)
+
+
+def topk_peaks(vol_dev, K, radius, ctx: Context | None = None):
+    """K peaks of a device volume by repeated tom_peak(A, R) (first maximum, then
+    zero the ball of radius R).  Returns (vals[K], pos1[K,3])."""
+    ctx = ctx or default_context()
+    z, y, x = vol_dev.shape
+    vals = (ctypes.c_float * K)()
+    pos = (ctypes.c_int * (3 * K))()
+    ctx.check(lib().tomgpu_topk_dev(ctx.handle, _tptr(vol_dev), _cdims((x, y, z)), int(K), float(radius), vals, pos))
+    return np.array(vals[:], np.float32), np.array(pos[:], np.int32).reshape(K, 3)
+
+
+# ------------------------------------------------------ weights and masks
+
+def tom_calc_weight_functioninc(dims, angles, thickness, ctx: Context | None = None):
+    """Exact (Radermacher) weighting, angles 2 x n (phi; theta) in degrees."""
+    ctx = ctx or default_context()
+    d = [int(x) for x in dims]
+    ang = np.asarray(angles, np.float64)
+    if ang.ndim != 2 or ang.shape[0] != 2:
+        raise ValueError("angles must be 2 x n_tilt")
+    flat = np.ascontiguousarray(ang.T)  # (phi, theta) pairs
+    out = np.zeros(d, np.float32, order="F")
+    ctx.check(lib().tomgpu_weight3d(ctx.handle, _cdims(d), flat.ctypes.data_as(_lib.c_double_p), flat.shape[0],
+                                    float(thickness), _ptr(out)))
+    return out
+
+
+def _wedge(shape, a, b, av3, ctx):
+    ctx = ctx or default_context()
+    import torch
+    d = _dims(np.empty(shape, np.int8))
+    out = torch.empty((d[2], d[1], d[0]), dtype=torch.float32, device=f"cuda:{ctx.device}")
+    ctx.check(lib().tomgpu_wedge_dev(ctx.handle, _cdims(d), float(a), float(b), int(av3), _tptr(out)))
+    return from_device(out).astype(np.float64).reshape(shape, order="F")
+
+
+def tom_wedge(image, angle, ctx: Context | None = None):
+    """Binary missing wedge, 0 where tan(angle) > |x|/|z| (Filtrans/tom_wedge.m:62-77)."""
+    return _wedge(np.shape(image), angle, 0.0, 0, ctx)
+
+
+def av3_wedge(image, minangle, maxangle, ctx: Context | None = None):
+    """av3 wedge (av3/utils/av3_wedge.m:23-26)."""
+    return _wedge(np.shape(image), minangle, maxangle, 1, ctx)
+
+
+def tom_os3_sphereMask(template):
+    """[mask maskSize] = tom_os3_sphereMask(template): radius floor(min/2)-1 around
+    floor(n/2)+1 (1-based), zero where distance >= radius; non-cubic input -> ones."""
+    shape = np.shape(template)
+    if len(set(shape)) != 1:
+        m = np.ones(shape, np.float32)
+        return m, int(m.size)
+    radius = np.floor(min(shape) / 2) - 1
+    center = [np.floor(s / 2) + 1 for s in shape]
+    g = np.meshgrid(*[np.arange(s, dtype=np.float64) for s in shape], indexing="ij")
+    dist = np.sqrt(sum((gi + 1 - c) ** 2 for gi, c in zip(g, center)))
+    m = np.ones(shape, np.float32)
+    m[dist >= radius] = 0
+    return m, int((m > 0).sum())
+
+
+def tom_fourier(a, ctx: Context | None = None):
+    """fftn in FP64 on the GPU (Filtrans/tom_fourier.m)."""
+    return _fft(a, -1, ctx)
+
+
+def tom_ifourier(a, ctx: Context | None = None):
+    """ifftn in FP64 on the GPU (Filtrans/tom_ifourier.m)."""
+    return _fft(a, +1, ctx)
+
+
+def _fft(a, direction, ctx):
+    import torch
+    ctx = ctx or default_context()
+    A = np.asarray(a, np.complex128)
+    shape = A.shape
+    d = _dims(A)
+    t = torch.from_numpy(np.ascontiguousarray(A.reshape(d, order="F").transpose(2, 1, 0))).to(f"cuda:{ctx.device}")
+    t = torch.view_as_real(t).contiguous()
+    ctx.check(lib().tomgpu_fft3d_c2c_dev(ctx.handle, _tptr(t), _cdims(d), int(direction), 64))
+    ctx.synchronize()
+    out = torch.view_as_complex(t).cpu().numpy().transpose(2, 1, 0)
+    return out.reshape(shape, order="F")
+
+
+# ---------------------------------------------------------------- angles
+
+def _rotmatrix(phi, psi, theta):
+    """tom_angles2rotmatrix (Sptrans/tom_sum_rotation.m): Rz(psi) Rx(theta) Rz(phi), double."""
+    ph, ps, th = np.deg2rad([phi, psi, theta])
+    rz = lambda a: np.array([[np.cos(a), -np.sin(a), 0], [np.sin(a), np.cos(a), 0], [0, 0, 1]])
+    rx = np.array([[1, 0, 0], [0, np.cos(th), -np.sin(th)], [0, np.sin(th), np.cos(th)]])
+    return rz(ps) @ rx @ rz(ph)
+
+
+def _os3_axis(start, inc, end):
+    if start < end:
+        vals = []
+        i = start
+        while i <= end + 1e-9:
+            vals.append(np.mod(i, 360))
+            i += inc
+        return vals
+    vals = []
+    i = start + 1
+    while i <= end + 360 - 1 + 1e-9:
+        vals.append(np.mod(i, 360))
+        i += inc
+    return vals
+
+
+def tom_os3_angleList(start, increment, end, dedup=True):
+    """3-D angle list of tom_os3_angleList: phi outer, psi, theta inner; equivalent
+    rotations (equal floor(R*1e4)) dropped.  Returns N x 3 [phi psi theta]."""
+    phis = _os3_axis(start[0], increment[0], end[0])
+    psis = _os3_axis(start[1], increment[1], end[1])
+    ths = _os3_axis(start[2], increment[2], end[2])
+    out, seen = [], set()
+    for ph in phis:
+        for ps in psis:
+            for th in ths:
+                if dedup:
+                    key = tuple(np.floor(_rotmatrix(ph, ps, th) * 10000).astype(np.int64).ravel())
+                    if key in seen:
+                        continue
+                    seen.add(key)
+                out.append((ph, ps, th))
+    return np.array(out, np.float64)
+
+
+def tom_av3_angle_grid(start, incr, end):
+    """Triplets in tom_av3_angle2index order: phi fastest, theta slowest, inclusive."""
+    axes = [np.arange(s, e + i * 0.5, i) for s, i, e in zip(start, incr, end)]
+    return np.array([(ph, ps, th) for th in axes[2] for ps in axes[1] for ph in axes[0]], np.float64)
+
+
+def tom_av3_angle2index(angle, angle_start, angular_incr, angle_end):
+    n = [int(round((e - s) / i)) + 1 for s, i, e in zip(angle_start, angular_incr, angle_end)]
+    k = [int(round((a - s) / i)) for a, s, i in zip(angle, angle_start, angular_incr)]
+    for kk, nn in zip(k, n):
+        if kk < 0 or kk >= nn:
+            return int(np.prod(n))  # the reference's loop runs to the end without a match
+    return k[2] * n[0] * n[1] + k[1] * n[0] + k[0]
+
+
+def tom_av3_index2angle(index, angle_start, angular_incr, angle_end):
+    n = [(e - s) / i + 1 for s, i, e in zip(angle_start, angular_incr, angle_end)]
+    a3 = np.floor(index / (n[0] * n[1]))
+    rest = index - a3 * n[0] * n[1]
+    a2 = np.floor(rest / n[0])
+    a1 = rest - a2 * n[0]
+    return np.array([a1, a2, a3]) * np.asarray(angular_incr) + np.asarray(angle_start)
+
+
+# ------------------------------------------------------------- matching
+
+class MatchPlan:
+    """Device-resident FLCF search for one tomogram size and one template size.
+
+    Tensors are torch CUDA float32, shaped (z, y, x).  Usage mirrors
+    tom_os3_findTemplate: set_template (template, mask, optional psf) ->
+    set_volume -> init_results -> run(eulers) [repeat] -> results.
+    """
+
+    def __init__(self, vol_shape_xyz, tmpl_shape_xyz, batch: int = 0, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.vol_shape = tuple(int(s) for s in vol_shape_xyz)
+        self.tmpl_shape = tuple(int(s) for s in tmpl_shape_xyz)
+        p = MatchParams()
+        p.batch = int(batch)
+        h = ctypes.c_void_p()
+        self.ctx.check(lib().tomgpu_match_plan_create(self.ctx.handle, _cdims(self.vol_shape),
+                                                      _cdims(self.tmpl_shape), ctypes.byref(p), ctypes.byref(h)))
+        self.handle = h
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().tomgpu_match_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def bytes(self):
+        return int(lib().tomgpu_match_plan_bytes(self.handle))
+
+    def set_template(self, tmpl_dev, mask_dev, psf_dev=None):
+        self._keep = [tmpl_dev, mask_dev, psf_dev]
+        self.ctx.check(lib().tomgpu_match_set_template_dev(self.handle, _tptr(tmpl_dev), _tptr(mask_dev),
+                                                           _tptr(psf_dev) if psf_dev is not None else None))
+
+    def set_volume(self, vol_dev):
+        self.ctx.check(lib().tomgpu_match_set_volume_dev(self.handle, _tptr(vol_dev)))
+
+    def new_results(self):
+        import torch
+        x, y, z = self.vol_shape
+        cc = torch.empty((z, y, x), dtype=torch.float32, device=f"cuda:{self.ctx.device}")
+        idx = torch.empty((z, y, x), dtype=torch.int32, device=f"cuda:{self.ctx.device}")
+        self.ctx.check(lib().tomgpu_match_init_results_dev(self.handle, _tptr(cc), _tptr(idx)))
+        return cc, idx
+
+    def run(self, eulers, maxcc_dev, angidx_dev, index_offset: int = 0):
+        e = np.ascontiguousarray(np.asarray(eulers, np.float32).reshape(-1, 3))
+        self.ctx.check(lib().tomgpu_match_run_dev(self.handle, e.ctypes.data_as(_lib.c_float_p), e.shape[0],
+                                                  int(index_offset), _tptr(maxcc_dev), _tptr(angidx_dev)))
+
+    def corr(self, t_dev, out_dev):
+        self.ctx.check(lib().tomgpu_match_corr_dev(self.handle, _tptr(t_dev), _tptr(out_dev)))
+
+    def stats(self):
+        import torch
+        x, y, z = self.vol_shape
+        m = torch.empty((z, y, x), dtype=torch.float32, device=f"cuda:{self.ctx.device}")
+        s = torch.empty_like(m)
+        self.ctx.check(lib().tomgpu_match_stats_dev(self.handle, _tptr(m), _tptr(s)))
+        return m, s
+
+
+def match_host(tomo, template, mask, eulers, psf=None, batch: int = 0, ctx: Context | None = None):
+    """One-shot search through the C ABI with host buffers (tomgpu_match): returns
+    (maxcc float32 [x,y,z], angle index int32 [x,y,z], 0-based, -1 where unset)."""
+    ctx = ctx or default_context()
+    vol = _f32_xfast(tomo)
+    t = _f32_xfast(template)
+    m = _f32_xfast(mask)
+    p = _f32_xfast(psf) if psf is not None else None
+    e = np.ascontiguousarray(np.asarray(eulers, np.float32).reshape(-1, 3))
+    cc = np.zeros(vol.shape, np.float32, order="F")
+    idx = np.zeros(vol.shape, np.int32, order="F")
+    prm = MatchParams()
+    prm.batch = int(batch)
+    ctx.check(lib().tomgpu_match(ctx.handle, _ptr(vol), _cdims(vol.shape), _ptr(t), _cdims(t.shape), _ptr(m),
+                                 _ptr(p) if p is not None else None, e.ctypes.data_as(_lib.c_float_p), e.shape[0],
+                                 ctypes.byref(prm), _ptr(cc), _ptr(idx)))
+    return cc, idx
+
+
+def tom_os3_findTemplate(volume, template, angle_list, mask=None, psf=None, batch: int = 0,
+                         ctx: Context | None = None):
+    """[ccc angles] of tom_os3_findTemplate for in-memory inputs (the job/file
+    plumbing of the reference is out of scope): template normalised with
+    tom_norm(1e5*(t+1),'mean0+1std'), mask = tom_os3_sphereMask(template) when
+    not given, psf = optional centred weight.  Returns ccc (float32 [x,y,z],
+    -1000 where never updated) and angles (1-based angle-list index as float32,
+    -1000 where never updated), the reference's conventions."""
+    ctx = ctx or default_context()
+    import torch
+    vol = np.asarray(volume, np.float32)
+    t = np.asarray(template, np.float32)
+    if mask is None:
+        mask, _ = tom_os3_sphereMask(t)
+    plan = MatchPlan(vol.shape, t.shape, batch=batch, ctx=ctx)
+    try:
+        td, md = to_device(t, ctx.device), to_device(mask, ctx.device)
+        pd = to_device(psf, ctx.device) if psf is not None else None
+        plan.set_template(td, md, pd)
+        plan.set_volume(to_device(vol, ctx.device))
+        cc, idx = plan.new_results()
+        plan.run(angle_list, cc, idx)
+        torch.cuda.synchronize(ctx.device)
+        ccc = from_device(cc)
+        ang = from_device(idx).astype(np.float32)
+        ang = np.where(ang >= 0, ang + 1, -1000).astype(np.float32)
+        return np.asfortranarray(ccc), np.asfortranarray(ang)
+    finally:
+        plan.close()
+
+
+def tom_os3_corr(img, template, options=None, ctx: Context | None = None):
+    """FLCF map of one (already rotated, masked, filtered) template against img
+    (search/tom_os3_corr.m FLCF branch).  options is a dict that caches the
+    search statistics between calls like the reference's options.correlation:
+    keys 'mask' (template-sized), 'templateMean'/'templateSTD' are taken from
+    the plan's template preprocessing of options['template'] when given, else
+    from this template."""
+    import torch
+    ctx = ctx or default_context()
+    options = {} if options is None else options
+    t = np.asarray(template, np.float32)
+    vol = np.asarray(img, np.float32)
+    mask = options.get("mask")
+    if mask is None:
+        mask, _ = tom_os3_sphereMask(t)
+        options["mask"] = mask
+    plan = options.get("_plan")
+    if plan is None or plan.vol_shape != vol.shape or plan.tmpl_shape != t.shape:
+        plan = MatchPlan(vol.shape, t.shape, ctx=ctx)
+        src = options.get("template", t)
+        plan.set_template(to_device(src, ctx.device), to_device(mask, ctx.device),
+                          to_device(options["psf"], ctx.device) if options.get("psf") is not None else None)
+        plan.set_volume(to_device(vol, ctx.device))
+        options["_plan"] = plan
+    out = torch.empty((vol.shape[2], vol.shape[1], vol.shape[0]), dtype=torch.float32, device=f"cuda:{ctx.device}")
+    plan.corr(to_device(t, ctx.device), out)
+    ctx.synchronize()
+    return np.asfortranarray(from_device(out)), options
