@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=20.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", default=WORKLOAD,
+                   help="exhaustive_512x512x256 (the benchmark) or profile_256x256x128 (profiler captures)")
     return p.parse_args()
 
 
@@ -123,9 +125,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_workload():
+def make_workload(name=WORKLOAD):
     from tom_b200 import synth
-    cfg = synth.CONFIGS[WORKLOAD]
+    cfg = synth.CONFIGS[name]
     grid = __import__("tom_b200").tom_av3_angle_grid(*cfg["angles"])
     d = synth.make_tomogram(cfg["N"], cfg["T"], cfg["n_copies"], cfg["n_blobs"], cfg["rho"], cfg["snr"],
                             cfg["max_tilt"], seed=2024, euler_pool=grid, mask_radius=cfg["mask_radius"])
@@ -214,7 +216,7 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    cfg, grid, d, mask = make_workload()
+    cfg, grid, d, mask = make_workload(args.workload)
     nvox = int(np.prod(cfg["N"]))
     ctx = tb.default_context(local)
     plan = tb.MatchPlan(cfg["N"], (cfg["T"],) * 3, batch=args.batch, ctx=ctx)
@@ -267,7 +269,7 @@ def main():
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
-            traffic = json.load(f).get(WORKLOAD, {}).get(dom)
+            traffic = json.load(f).get(args.workload, {}).get(dom)
     shares = {k: round(v[0] / max(sum(x[0] for x in kt.values()), 1e-9), 4) for k, v in kt.items()}
 
     # end to end through the one-shot C-ABI call with pinned host buffers
@@ -313,7 +315,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "tomogram": list(cfg["N"]), "template": cfg["T"],
+                "config": {"workload": args.workload, "tomogram": list(cfg["N"]), "template": cfg["T"],
                            "angles": len(grid), "rot_per_step": rps, "rotation_batch": args.batch,
                            "parallelism": f"angle-partitioned x{world}",
                            "l2": "inputs larger than L2 (tomogram spectrum 269 MB, per-batch spectra 2.2 GB)"},

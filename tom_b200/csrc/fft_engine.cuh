@@ -22,7 +22,9 @@ template <int... Rs> struct seq {};
 // of two.  Only lengths listed here are supported (the host checks).
 template <int L> struct Radices;
 template <> struct Radices<8> { typedef seq<8> type; };
+template <> struct Radices<12> { typedef seq<4, 3> type; };
 template <> struct Radices<16> { typedef seq<16> type; };
+template <> struct Radices<20> { typedef seq<4, 5> type; };
 template <> struct Radices<24> { typedef seq<8, 3> type; };
 template <> struct Radices<32> { typedef seq<8, 4> type; };
 template <> struct Radices<40> { typedef seq<8, 5> type; };

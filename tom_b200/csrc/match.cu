@@ -402,8 +402,8 @@ template <typename K> static void raise_smem(K kern, size_t smem) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-#define TG_HOT_LENGTHS(X) X(32) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256) X(464) X(512) X(928)
-#define TG_HALF_LENGTHS(X) X(16) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(232) X(256) X(464)
+#define TG_HOT_LENGTHS(X) X(16) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256) X(464) X(512) X(928)
+#define TG_HALF_LENGTHS(X) X(8) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(232) X(256) X(464)
 
 static bool hot_len(int L) {
     switch (L) {
@@ -415,9 +415,20 @@ static bool hot_len(int L) {
     }
 }
 
+static bool half_len(int L) {
+    switch (L) {
+#define C_(N) case N:
+        TG_HALF_LENGTHS(C_)
+#undef C_
+        return true;
+        default: return false;
+    }
+}
+
 bool match_sizes_supported(const int N[3], const int T[3]) {
     for (int d = 0; d < 3; ++d)
         if (!hot_len(N[d]) || T[d] > N[d] || T[d] < 1) return false;
+    if (N[0] % 2 || !half_len(N[0] / 2)) return false;
     if (!fft_length_supported(T[0]) || !fft_length_supported(T[1]) || !fft_length_supported(T[2])) return false;
     return true;
 }

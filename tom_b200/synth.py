@@ -152,6 +152,9 @@ def sphere_mask(T, radius):
 CONFIGS = {
     "exhaustive_128": dict(N=(128, 128, 128), T=32, n_copies=10, n_blobs=6, rho=12, snr=0.1, max_tilt=60,
                            mask_radius=14, angles=((0, 0, 0), (30, 30, 30), (330, 330, 180))),
+    # a reduced volume with the 512x512x256 workload's template, for profiler captures
+    "profile_256x256x128": dict(N=(256, 256, 128), T=40, n_copies=10, n_blobs=8, rho=16, snr=0.1,
+                                max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
     "exhaustive_512x512x256": dict(N=(512, 512, 256), T=40, n_copies=40, n_blobs=8, rho=16, snr=0.1,
                                    max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
 }
