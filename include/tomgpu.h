@@ -152,7 +152,8 @@ int tomgpu_fft3d_c2r_dev(tomgpu_ctx* ctx, void* half_dev, void* real_dev, const 
 typedef struct {
     int batch;          /* rotations per batch; 0 = default (8) */
     int wedge_fp64;     /* reserved, 0 */
-    int reserved[6];
+    int path;           /* 0: fastest kernels for the sizes; 1: generic kernels only */
+    int reserved[5];
 } tomgpu_match_params;
 
 /* A matching plan for one volume size and one template size.  It holds the

@@ -305,8 +305,8 @@ def local_stats(volume, mask):
     mp = paste_center(N, np.asarray(mask, np.float64))
     M = float((mask != 0).sum())
     fm = np.fft.rfftn(mp)
-    mean = np.fft.ifftshift(np.fft.irfftn(np.fft.rfftn(vol) * fm, s=N)) / M
-    e2 = np.fft.ifftshift(np.fft.irfftn(np.fft.rfftn(vol * vol) * fm, s=N)) / M
+    mean = np.fft.ifftshift(np.fft.irfftn(np.fft.rfftn(vol) * fm, s=N, axes=(0, 1, 2))) / M
+    e2 = np.fft.ifftshift(np.fft.irfftn(np.fft.rfftn(vol * vol) * fm, s=N, axes=(0, 1, 2))) / M
     var = np.maximum(e2 - mean * mean, 0)
     return mean, np.sqrt(var), M
 
@@ -324,7 +324,7 @@ class FLCF:
         """search/tom_os3_corr.m:151-176 for one (already rotated/modified) template."""
         p = paste_center(self.N, np.asarray(t, np.float64) * self.mask)
         ft = np.fft.rfftn(p)
-        num = np.fft.ifftshift(np.fft.irfftn(self.fimage * np.conj(ft), s=self.N)) / self.M
+        num = np.fft.ifftshift(np.fft.irfftn(self.fimage * np.conj(ft), s=self.N, axes=(0, 1, 2))) / self.M
         num = num - self.mean * tmean
         den = tstd * self.std
         res = np.zeros(self.N)
@@ -366,6 +366,50 @@ def find_template(volume, template, mask, angles, psf=None, keep_second=False):
         ccc[upd] = cc[upd]
         idx[upd] = it
     return (ccc, idx, second) if keep_second else (ccc, idx)
+
+
+def flcf_direct_at(volume, t, mask, tmean, tstd, voxels):
+    """FLCF of one rotated/masked/filtered template at given voxels (0-based, [x,y,z])
+    by direct FP64 sums: the correlation sum of tom_os3_corr.m:151-153 and the
+    convolution sums of tom_os3_mean/std, without any FFT."""
+    vol = np.asarray(volume, np.float64)
+    N = np.array(vol.shape)
+    T = np.array(mask.shape)
+    c = T // 2
+    jj = np.argwhere(np.ones(tuple(T), bool))
+    tw = (np.asarray(t, np.float64) * mask)[tuple(jj.T)]
+    mw = np.asarray(mask, np.float64)[tuple(jj.T)]
+    M = float((mask != 0).sum())
+    out = []
+    for x in np.asarray(voxels).reshape(-1, 3):
+        q = (x[None, :] + jj - c[None, :]) % N            # correlation: I(x + j - c)
+        s = float((tw * vol[tuple(q.T)]).sum())
+        qc = (x[None, :] + c[None, :] - jj) % N           # convolution: I(x + c - j)
+        iv = vol[tuple(qc.T)]
+        mu = float((mw * iv).sum()) / M
+        e2 = float((mw * iv * iv).sum()) / M
+        sig = np.sqrt(max(e2 - mu * mu, 0.0))
+        den = tstd * sig
+        out.append((s / M - mu * tmean) / den if den != 0 else 0.0)
+    return np.array(out)
+
+
+def find_template_direct_at(volume, template, mask, angles, voxels, psf=None):
+    """Per-voxel max over angles and its first index (bestPeak rule) at given voxels, direct sums."""
+    t, tmean, tstd = prepare_template(template, mask, psf)
+    best = np.full(len(voxels), -1000.0)
+    second = np.full(len(voxels), -1000.0)
+    idx = np.full(len(voxels), -1, np.int64)
+    for it, ang in enumerate(np.asarray(angles, np.float64).reshape(-1, 3)):
+        tr = rotate(t.astype(np.float32), ang).astype(np.float64) * mask
+        if psf is not None:
+            tr = apply_weight_function(tr, psf)
+        cc = flcf_direct_at(volume, tr.astype(np.float32), mask, tmean, tstd, voxels)
+        upd = best < cc
+        second = np.where(upd, best, np.maximum(second, cc))
+        best = np.where(upd, cc, best)
+        idx = np.where(upd, it, idx)
+    return best, idx, second
 
 
 # ---------------------------------------------------------------------------

@@ -1,0 +1,47 @@
+"""The register-resident hot kernels (power-of-two sizes) against the generic
+kernels and against FP64 direct sums at sampled voxels, at the benchmark size."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+REL = 1e-4
+
+
+def _run(gpu, vol, tmpl, mask, angles, generic, batch):
+    import torch
+    plan = gpu.MatchPlan(vol.shape, tmpl.shape, batch=batch, generic=generic)
+    plan.set_template(gpu.to_device(tmpl), gpu.to_device(mask))
+    plan.set_volume(gpu.to_device(vol))
+    cc, idx = plan.new_results()
+    plan.run(angles, cc, idx)
+    torch.cuda.synchronize()
+    out = gpu.from_device(cc).copy(), gpu.from_device(idx).copy()
+    plan.close()
+    return out
+
+
+@pytest.mark.parametrize("workload,n_ang", [("profile_256x256x128", 12), ("exhaustive_512x512x256", 10)])
+def test_fast_equals_generic_and_direct_sums(gpu, oracle, workload, n_ang):
+    from tom_b200 import synth
+    cfg = synth.CONFIGS[workload]
+    grid = oracle.av3_angle_grid(*cfg["angles"])
+    sel = np.linspace(0, len(grid) - 1, n_ang).astype(int)
+    d = synth.make_tomogram(cfg["N"], cfg["T"], cfg["n_copies"], cfg["n_blobs"], cfg["rho"], cfg["snr"],
+                            cfg["max_tilt"], seed=7, euler_pool=grid[sel], mask_radius=cfg["mask_radius"])
+    mask = synth.sphere_mask(cfg["T"], cfg["mask_radius"])
+    angles = grid[sel]
+    fcc, fidx = _run(gpu, d["tomo"], d["template"], mask, angles, False, 4)
+    gcc, gidx = _run(gpu, d["tomo"], d["template"], mask, angles, True, 3)
+    scale = np.abs(gcc).max()
+    assert np.abs(fcc - gcc).max() <= 1e-5 * scale
+    rng = np.random.default_rng(8)
+    vox = np.vstack([d["positions"].astype(int),
+                     np.column_stack([rng.integers(0, n, 40) for n in cfg["N"]])])
+    best, ridx, second = oracle.find_template_direct_at(d["tomo"], d["template"], mask, angles, vox)
+    got = fcc[tuple(vox.T)]
+    assert np.abs(got - best).max() <= REL * np.abs(best).max()
+    sep = best - second > 2 * REL * np.abs(best).max()
+    assert np.array_equal(fidx[tuple(vox.T)][sep], ridx[sep])
+    # planted copies are found at their own orientation
+    hits = fidx[tuple(d["positions"].astype(int).T)]
+    assert (hits == d["euler_index"]).mean() >= 0.8

@@ -38,7 +38,8 @@ class TomGpuError(RuntimeError):
 
 
 class MatchParams(ctypes.Structure):
-    _fields_ = [("batch", ctypes.c_int), ("wedge_fp64", ctypes.c_int), ("reserved", ctypes.c_int * 6)]
+    _fields_ = [("batch", ctypes.c_int), ("wedge_fp64", ctypes.c_int), ("path", ctypes.c_int),
+                ("reserved", ctypes.c_int * 5)]
 
 
 # name -> (restype, argtypes)

@@ -513,7 +513,7 @@ int tomgpu_match_plan_create(tomgpu_ctx* ctx, const int vol[3], const int tm[3],
     if (params && params->batch < 0) return fail(ctx, TOMGPU_ERR_ARG, "negative batch");
     TG_TRY(use_device(ctx));
     tomgpu_match_plan* p = new tomgpu_match_plan();
-    int rc = p->p.create(ctx, vol, tm, params ? params->batch : 0);
+    int rc = p->p.create(ctx, vol, tm, params ? params->batch : 0, params ? params->path == 1 : false);
     if (rc) {
         delete p;
         return rc;

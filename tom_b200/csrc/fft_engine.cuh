@@ -17,6 +17,7 @@
 namespace tgfft {
 
 template <int... Rs> struct seq {};
+template <int A, int... Rs> struct seq_first { static constexpr int value = A; };
 
 // Radix plans: odd radices last so that every stride NS before them is a power
 // of two.  Only lengths listed here are supported (the host checks).

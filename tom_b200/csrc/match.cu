@@ -576,8 +576,9 @@ int MatchPlan::alloc(void** p, size_t bytes) {
     return TOMGPU_OK;
 }
 
-int MatchPlan::create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batch) {
+int MatchPlan::create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batch, bool generic) {
     ctx = c;
+    generic_only = generic;
     for (int d = 0; d < 3; ++d) { N[d] = vol[d]; T[d] = tm[d]; }
     if (!match_sizes_supported(N, T))
         return fail(ctx, TOMGPU_ERR_UNSUPPORTED,
@@ -804,18 +805,29 @@ int MatchPlan::run(const float* eulers, int R, int index_offset, float* maxcc, i
     for (int off = 0; off < R; off += B) {
         const int nb = std::min(B, R - off);
         TG_TRY(prepare_batch(off, nb));
+        const int d0y = d0_corr(N[1], T[1]);
         {
             ProfScope ps(ctx, TOMGPU_K_CORR_Y);
-            TG_TRY_CUDA(ctx, launch_corr_y(N[1], d_fimg, d_Z, d_Q, T[1], d0_corr(N[1], T[1]), ncols, nb, st));
+            if (!generic_only && fast_corr_y(N[1]))
+                TG_TRY_CUDA(ctx, launch_corr_y_fast(N[1], d_fimg, d_Z, d_Q, T[1], d0y, ncols, nb, st));
+            else
+                TG_TRY_CUDA(ctx, launch_corr_y(N[1], d_fimg, d_Z, d_Q, T[1], d0y, ncols, nb, st));
         }
         {
             ProfScope ps(ctx, TOMGPU_K_INV_Z);
-            TG_TRY_CUDA(ctx, launch_inv_z(N[2], d_Q, d_H, N[1], (int)nh1, nb, st));
+            if (!generic_only && fast_inv_z(N[2]))
+                TG_TRY_CUDA(ctx, launch_inv_z_fast(N[2], d_Q, d_H, N[1], (int)nh1, nb, st));
+            else
+                TG_TRY_CUDA(ctx, launch_inv_z(N[2], d_Q, d_H, N[1], (int)nh1, nb, st));
         }
         {
             ProfScope ps(ctx, TOMGPU_K_C2R_FLCF);
-            TG_TRY_CUDA(ctx, launch_c2r_flcf(N[0] / 2, d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean,
-                                             1.0 / msize, tmean, index_offset + off, maxcc, angidx, st));
+            if (!generic_only && fast_c2r(N[0] / 2))
+                TG_TRY_CUDA(ctx, launch_c2r_fast(N[0] / 2, d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean,
+                                                 1.0 / msize, tmean, index_offset + off, maxcc, angidx, st));
+            else
+                TG_TRY_CUDA(ctx, launch_c2r_flcf(N[0] / 2, d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean,
+                                                 1.0 / msize, tmean, index_offset + off, maxcc, angidx, st));
         }
         ctx->launches += 3;
     }

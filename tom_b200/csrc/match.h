@@ -8,12 +8,24 @@
 namespace tg {
 
 bool match_sizes_supported(const int N[3], const int T[3]);
+
+// register-resident hot kernels (match_fast.cu) for the sizes they cover
+bool fast_corr_y(int NY);
+bool fast_inv_z(int NZ);
+bool fast_c2r(int NH);
+cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
+                               long long ncols, int nb, cudaStream_t st);
+cudaError_t launch_inv_z_fast(int NZ, const float2* Q, float2* H, int Ny, int nh1, int nb, cudaStream_t st);
+cudaError_t launch_c2r_fast(int NH, const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny,
+                            int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
+                            float* maxcc, int* angidx, cudaStream_t st);
 cudaError_t c2c3d_batch(float2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
 
 struct MatchPlan {
     tomgpu_ctx* ctx = nullptr;
     int N[3] = {0, 0, 0}, T[3] = {0, 0, 0};
     int B = 8;
+    bool generic_only = false;  // force the generic kernels (tests compare both paths)
     long long nvox = 0, nh1 = 0, tn = 0;
     int64_t bytes_held = 0;
     bool has_template = false, has_volume = false, has_psf = false;
@@ -44,7 +56,7 @@ struct MatchPlan {
     ~MatchPlan();
     void release();
     int alloc(void** p, size_t bytes);
-    int create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batch);
+    int create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batch, bool generic);
     int ensure_mats(int R);
     int upload_mats(const float* eulers, int R);
     int set_template(const float* tmpl, const float* mask, const float* psf);

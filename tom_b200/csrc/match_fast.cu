@@ -1,0 +1,225 @@
+// Register-resident variants of the three hot FLCF kernels for the common
+// power-of-two sizes (y edge 256/512, z edge 256, x edge 256/512).  Same
+// arithmetic contract as the generic kernels in match.cu; faster data flow:
+//
+//   corr_y_w  one warp per spectrum column; the y-DFT of the template, the
+//             product with F_I (kept in registers for the whole batch) and the
+//             inverse y-DFT all stay in registers with two warp-private
+//             exchanges per transform (warp_fft.cuh).
+//   inv_z_b   16 consecutive y lines per block, 16 threads per line holding
+//             16 values: radix 16 straight from global memory, one block-wide
+//             exchange, radix 16 straight back to global memory.
+//   c2r_w     one warp per x line, the next rotation's tile prefetched with
+//             cp.async while the current one is transformed; running max and
+//             the FLCF coefficients of the lane's voxels stay in registers.
+#include "ctx.h"
+#include "match.h"
+#include "twiddles.h"
+#include "warp_fft.cuh"
+
+namespace tg {
+
+template <int NY>
+__global__ void __launch_bounds__(256, 2) k_corr_y_w(const float2* __restrict__ fimg, const float2* __restrict__ Z,
+                                                  float2* __restrict__ Q, int Ty, int d0y, long long ncols, int nb,
+                                                  const float2* __restrict__ tw) {
+    constexpr int EPT = NY / 32;
+    __shared__ __align__(16) float2 sbuf[8][NY];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long col = (long long)blockIdx.x * 8 + warp;
+    if (col >= ncols) return;  // no block-wide barrier below
+    float2* buf = sbuf[warp];
+    const float2* fc = fimg + col * NY;  // re-read per rotation: an L1 hit after the first
+    for (int b = 0; b < nb; ++b) {
+        const float2* zc = Z + ((long long)b * ncols + col) * Ty;
+        float2 v[EPT];
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int jy = (tgwfft::in_pos<NY>(i, lane) - d0y) & (NY - 1);
+            v[i] = jy < Ty ? zc[jy] : make_float2(0.f, 0.f);
+        }
+        tgwfft::warp_fft<NY, -1>(v, buf, tw, lane);
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) v[i] = cmulc(__ldg(fc + tgwfft::out_pos<NY>(i, lane)), v[i]);
+        tgwfft::warp_fft<NY, +1>(v, buf, tw, lane);
+        float2* qc = Q + ((long long)b * ncols + col) * NY;
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) qc[tgwfft::out_pos<NY>(i, lane)] = v[i];
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_inv_z_b256(const float2* __restrict__ Q, float2* __restrict__ H, int Ny,
+                                                    int nh1, const float2* __restrict__ tw) {
+    constexpr int NZ = 256, LS = NZ + 1;
+    __shared__ __align__(16) float2 s[16 * LS];
+    const int tid = threadIdx.x, l = tid & 15, j = tid >> 4;
+    const int y = blockIdx.x * 16 + l, kx = blockIdx.y, b = blockIdx.z;
+    const bool ok = y < Ny;
+    const long long base = ((long long)b * nh1 + kx) * NZ * Ny;
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = ok ? Q[base + (long long)(j + 16 * r) * Ny + y] : make_float2(0.f, 0.f);
+    tgfft::dft16<+1>(v);
+#pragma unroll
+    for (int r = 0; r < 16; ++r) s[l * LS + 16 * j + r] = v[r];
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = s[l * LS + j + 16 * r];
+    float2 w[16];
+    tgwfft::twiddle_powers<16, +1>(tw, j, w);
+#pragma unroll
+    for (int r = 1; r < 16; ++r) v[r] = cmul(v[r], w[r]);
+    tgfft::dft16<+1>(v);
+    if (ok) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) H[base + (long long)(j + 16 * r) * Ny + y] = v[r];
+    }
+}
+
+TG_D void cp_async8(void* smem_dst, const void* gsrc, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
+}
+TG_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> TG_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <int NH>
+__global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, const float* __restrict__ mu0,
+                                               const float* __restrict__ gam, const double* __restrict__ tsum, int Ny,
+                                               int Nz, int nb, float inv_nm, double c_mean, double inv_m, double mu_t,
+                                               int index0, float* __restrict__ maxcc, int* __restrict__ angidx,
+                                               const float2* __restrict__ tw_h, const float2* __restrict__ tw_x) {
+    constexpr int YT = 8, NH1 = NH + 1, TS = NH + 2, EPT = NH / 32, NX = 2 * NH;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* tile = reinterpret_cast<float2*>(smem_raw);  // [2][YT][TS]
+    float2* xbuf = tile + 2 * YT * TS;                    // [8][NH]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int y0 = blockIdx.x * YT, z = blockIdx.y, y = y0 + warp;
+    const bool yok = y < Ny;
+    const long long nh1l = NH1;
+    const float mt = (float)mu_t;
+    float m0[EPT][2], g0[EPT][2], bm[EPT][2];
+    int bi[EPT][2];
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+        bm[i][0] = bm[i][1] = -INFINITY;
+        bi[i][0] = bi[i][1] = -1;
+        m0[i][0] = m0[i][1] = g0[i][0] = g0[i][1] = 0.f;
+        if (yok) {
+            const long long v = ((long long)z * Ny + y) * NX + 2 * tgwfft::out_pos<NH>(i, lane);
+            const float2 a = *reinterpret_cast<const float2*>(mu0 + v);
+            const float2 g = *reinterpret_cast<const float2*>(gam + v);
+            m0[i][0] = a.x; m0[i][1] = a.y;
+            g0[i][0] = g.x; g0[i][1] = g.y;
+        }
+    }
+    auto issue = [&](int b, int which) {
+        float2* t = tile + which * YT * TS;
+        const long long hb = (long long)b * nh1l * Nz * Ny;
+        for (int e = tid; e < YT * NH1; e += 256) {
+            const int kx = e / YT, yl = e - kx * YT;
+            const bool ok = y0 + yl < Ny;
+            const float2* src = H + hb + ((long long)kx * Nz + z) * Ny + (ok ? y0 + yl : 0);
+            cp_async8(t + yl * TS + kx, src, ok ? 8 : 0);
+        }
+        cp_async_commit();
+    };
+    issue(0, 0);
+    for (int b = 0; b < nb; ++b) {
+        if (b + 1 < nb) {
+            issue(b + 1, (b + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float2* X = tile + (b & 1) * YT * TS + warp * TS;
+        float2 v[EPT];
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            // unpack: Z[k] = (X[k] + X*[NH-k]) + i w^k (X[k] - X*[NH-k]), w = exp(+2 pi i / NX)
+            const int k = tgwfft::in_pos<NH>(i, lane);
+            const float2 xa = X[k], xb = cconj(X[NH - k]);
+            const float2 w = cconj(__ldg(tw_x + k));
+            const float2 d = cmul(w, csub(xa, xb));
+            v[i] = cadd(cadd(xa, xb), make_float2(-d.y, d.x));
+        }
+        tgwfft::warp_fft<NH, +1>(v, xbuf + warp * NH, tw_h, lane);
+        const float kap = (float)(c_mean * (tsum[b] * inv_m - mu_t));
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const float c0 = (fmaf(v[i].x, inv_nm, -m0[i][0] * mt) + kap) * g0[i][0];
+            const float c1 = (fmaf(v[i].y, inv_nm, -m0[i][1] * mt) + kap) * g0[i][1];
+            if (c0 > bm[i][0]) { bm[i][0] = c0; bi[i][0] = index0 + b; }
+            if (c1 > bm[i][1]) { bm[i][1] = c1; bi[i][1] = index0 + b; }
+        }
+        __syncthreads();
+    }
+    if (!yok) return;
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+        const long long v = ((long long)z * Ny + y) * NX + 2 * tgwfft::out_pos<NH>(i, lane);
+        float2 cur = *reinterpret_cast<float2*>(maxcc + v);
+        int2 ci = *reinterpret_cast<int2*>(angidx + v);
+        bool ch = false;
+        if (bm[i][0] > cur.x) { cur.x = bm[i][0]; ci.x = bi[i][0]; ch = true; }
+        if (bm[i][1] > cur.y) { cur.y = bm[i][1]; ci.y = bi[i][1]; ch = true; }
+        if (ch) {
+            *reinterpret_cast<float2*>(maxcc + v) = cur;
+            *reinterpret_cast<int2*>(angidx + v) = ci;
+        }
+    }
+}
+
+// ------------------------------------------------------------- dispatch
+bool fast_corr_y(int NY) { return NY == 256 || NY == 512; }
+bool fast_inv_z(int NZ) { return NZ == 256; }
+bool fast_c2r(int NH) { return NH == 128 || NH == 256; }
+
+cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
+                               long long ncols, int nb, cudaStream_t st) {
+    const unsigned g = (unsigned)((ncols + 7) / 8);
+    if (NY == 512) k_corr_y_w<512><<<g, 256, 0, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(512));
+    else if (NY == 256) k_corr_y_w<256><<<g, 256, 0, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(256));
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_inv_z_fast(int NZ, const float2* Q, float2* H, int Ny, int nh1, int nb, cudaStream_t st) {
+    if (NZ != 256) return cudaErrorInvalidValue;
+    dim3 g((Ny + 15) / 16, nh1, nb);
+    k_inv_z_b256<<<g, 256, 0, st>>>(Q, H, Ny, nh1, twiddle_table<float2>(256));
+    return cudaGetLastError();
+}
+
+template <int NH>
+static cudaError_t launch_c2r_t(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny,
+                                int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
+                                float* maxcc, int* angidx, cudaStream_t st) {
+    constexpr int YT = 8, TS = NH + 2;
+    const size_t smem = sizeof(float2) * (2 * YT * TS + 8 * NH);
+    static unsigned raised = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 32 && !(raised & (1u << dev))) {
+        cudaFuncSetAttribute(k_c2r_w<NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        raised |= 1u << dev;
+    }
+    dim3 g((Ny + YT - 1) / YT, Nz);
+    k_c2r_w<NH><<<g, 256, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx,
+                                      twiddle_table<float2>(NH), twiddle_table<float2>(2 * NH));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_c2r_fast(int NH, const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny,
+                            int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
+                            float* maxcc, int* angidx, cudaStream_t st) {
+    if (NH == 256)
+        return launch_c2r_t<256>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
+    if (NH == 128)
+        return launch_c2r_t<128>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace tg

@@ -1,0 +1,148 @@
+// Warp-owned line FFTs with the data in registers (sm_100a, FP32).
+//
+// One warp holds one line of length L: lane `l` keeps EPT = L/32 complex
+// values.  A stage of radix R runs EPT/R Stockham butterflies per lane
+// (butterfly j = l + 32 q); its inputs sit at positions j + r L/R and its
+// outputs go to (j - j mod NS) R + j mod NS + r NS.  Between stages the warp
+// exchanges its line through a private shared-memory buffer (write outputs,
+// __syncwarp, read next inputs), so a transform of S stages costs S-1
+// exchanges and no block-wide barrier, and the first stage reads, and the last
+// stage writes, registers directly.
+//
+// Register pattern: before the first stage v[q R1 + r] is x[l + 32 q + r L/R1];
+// after the last stage v[q RL + r] is X[l + 32 q + r L/RL].  Plans with
+// R1 == RL leave the spectrum in the same pattern the inverse transform
+// starts from, so a product between a forward and an inverse transform needs
+// no exchange.
+//
+// Bank conflicts: slot p of the exchange buffer lives at p ^ S(p >> 4) with S
+// linear over GF(2) on the row bits (coefficients 15, 14, 10, 15, 13); this
+// places every half-warp's 16 float2 accesses of every stage of the plans
+// below in 16 distinct bank pairs (checked exhaustively on the host).
+//
+// Twiddles w^(r m) for r < R come from three or four table loads (w^m, w^2m,
+// w^4m, w^8m) and at most three complex products, within a few ulp of the
+// double-precision table.
+#pragma once
+#include "fft_engine.cuh"
+
+namespace tgwfft {
+
+using tgfft::seq;
+
+template <int L> struct WPlan;
+template <> struct WPlan<512> { typedef seq<8, 8, 8> type; static constexpr int R1 = 8, RL = 8; };
+template <> struct WPlan<256> { typedef seq<8, 4, 8> type; static constexpr int R1 = 8, RL = 8; };
+template <> struct WPlan<128> { typedef seq<4, 2, 4, 4> type; static constexpr int R1 = 4, RL = 4; };
+
+TG_D int swz(int p) {
+    const int row = p >> 4;
+    int s = 0;
+    s ^= (row & 1) ? 15 : 0;
+    s ^= (row & 2) ? 14 : 0;
+    s ^= (row & 4) ? 10 : 0;
+    s ^= (row & 8) ? 15 : 0;
+    s ^= (row & 16) ? 13 : 0;
+    return p ^ s;
+}
+
+// w[r] = tw^(r m) (forward sign), conjugated for DIR > 0
+template <int R, int DIR>
+TG_D void twiddle_powers(const float2* __restrict__ tw, int m, float2* w) {
+    w[0] = make_float2(1.f, 0.f);
+    if constexpr (R >= 2) w[1] = __ldg(tw + m);
+    if constexpr (R >= 4) {
+        w[2] = __ldg(tw + 2 * m);
+        w[3] = cmul(w[1], w[2]);
+    }
+    if constexpr (R >= 8) {
+        w[4] = __ldg(tw + 4 * m);
+        w[5] = cmul(w[4], w[1]);
+        w[6] = cmul(w[4], w[2]);
+        w[7] = cmul(w[4], w[3]);
+    }
+    if constexpr (R >= 16) {
+        w[8] = __ldg(tw + 8 * m);
+#pragma unroll
+        for (int i = 9; i < 16; ++i) w[i] = cmul(w[8], w[i - 8]);
+    }
+    if constexpr (DIR > 0) {
+#pragma unroll
+        for (int i = 1; i < R; ++i) w[i] = cconj(w[i]);
+    }
+}
+
+template <int L, int R, int NS, int DIR>
+TG_D void wstage(float2* v, const float2* __restrict__ tw, int lane) {
+    constexpr int EPT = L / 32, NB = EPT / R;
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        if constexpr (NS > 1) {
+            const int j = lane + 32 * q;
+            float2 w[R];
+            twiddle_powers<R, DIR>(tw, (j % NS) * (L / (NS * R)), w);
+#pragma unroll
+            for (int r = 1; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], w[r]);
+        }
+        tgfft::dft<R, DIR>(v + q * R, tw, L / R);
+    }
+}
+
+template <int L, int R, int NS>
+TG_D void wstore(const float2* v, float2* buf, int lane) {
+    constexpr int EPT = L / 32, NB = EPT / R;
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        const int j = lane + 32 * q, k = j % NS;
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) buf[swz(base + r * NS)] = v[q * R + r];
+    }
+}
+
+template <int L, int R>
+TG_D void wload(float2* v, const float2* buf, int lane) {
+    constexpr int EPT = L / 32, NB = EPT / R;
+#pragma unroll
+    for (int q = 0; q < NB; ++q) {
+        const int j = lane + 32 * q;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[q * R + r] = buf[swz(j + r * (L / R))];
+    }
+}
+
+template <int L, int DIR, int NS, int R, int... Rest>
+TG_D void wrun(float2* v, float2* buf, const float2* __restrict__ tw, int lane) {
+    wstage<L, R, NS, DIR>(v, tw, lane);
+    if constexpr (sizeof...(Rest) > 0) {
+        constexpr int Rn = tgfft::seq_first<Rest...>::value;
+        wstore<L, R, NS>(v, buf, lane);
+        __syncwarp();
+        wload<L, Rn>(v, buf, lane);
+        __syncwarp();
+        wrun<L, DIR, NS * R, Rest...>(v, buf, tw, lane);
+    }
+}
+
+template <int L, int DIR, int... Rs>
+TG_D void warp_fft_impl(float2* v, float2* buf, const float2* __restrict__ tw, int lane, seq<Rs...>) {
+    wrun<L, DIR, 1, Rs...>(v, buf, tw, lane);
+}
+
+// In-register transform of one line per warp; buf: L float2 private to the warp.
+template <int L, int DIR>
+TG_D void warp_fft(float2* v, float2* buf, const float2* __restrict__ tw, int lane) {
+    warp_fft_impl<L, DIR>(v, buf, tw, lane, typename WPlan<L>::type{});
+}
+
+// Position of register i (0 <= i < L/32) before the first / after the last stage.
+template <int L> TG_D int in_pos(int i, int lane) {
+    constexpr int R = WPlan<L>::R1;
+    return lane + 32 * (i / R) + (i % R) * (L / R);
+}
+template <int L> TG_D int out_pos(int i, int lane) {
+    constexpr int R = WPlan<L>::RL;
+    return lane + 32 * (i / R) + (i % R) * (L / R);
+}
+
+}  // namespace tgwfft
