@@ -63,6 +63,8 @@ _SIGS = {
     "tomgpu_topk_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, ctypes.c_int, ctypes.c_double, c_float_p,
                                        c_int_p]),
     "tomgpu_peak_radius_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, ctypes.c_double, c_float_p, c_int_p]),
+    "tomgpu_topk_noalloc_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, ctypes.c_int, ctypes.c_double,
+                                               c_void_p, c_void_p]),
     "tomgpu_peak_spline_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_int_p, c_double_p, c_double_p]),
     "tomgpu_weight3d": (ctypes.c_int, [c_void_p, c_int_p, c_double_p, ctypes.c_int, ctypes.c_double, c_void_p]),
     "tomgpu_wedge_dev": (ctypes.c_int, [c_void_p, c_int_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
