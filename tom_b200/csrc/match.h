@@ -10,7 +10,7 @@ namespace tg {
 bool match_sizes_supported(const int N[3], const int T[3]);
 
 // register-resident hot kernels (match_fast.cu) for the sizes they cover
-bool fast_corr_y(int NY);
+bool fast_corr_y(int NY, int Ty);
 bool fast_inv_z(int NZ);
 bool fast_c2r(int NH);
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,

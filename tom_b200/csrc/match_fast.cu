@@ -3,9 +3,10 @@
 // arithmetic contract as the generic kernels in match.cu; faster data flow:
 //
 //   corr_y_w  one warp per spectrum column; the y-DFT of the template, the
-//             product with F_I (kept in registers for the whole batch) and the
-//             inverse y-DFT all stay in registers with two warp-private
-//             exchanges per transform (warp_fft.cuh).
+//             product with F_I (staged once in shared memory) and the inverse
+//             y-DFT all stay in registers with two warp-private exchanges per
+//             transform (warp_fft.cuh); the next rotation's template values
+//             are fetched while the current one is transformed.
 //   inv_z_b   16 consecutive y lines per block, 16 threads per line holding
 //             16 values: radix 16 straight from global memory, one block-wide
 //             exchange, radix 16 straight back to global memory.
@@ -21,38 +22,67 @@ namespace tg {
 
 template <int NY>
 __global__ void __launch_bounds__(256, 2) k_corr_y_w(const float2* __restrict__ fimg, const float2* __restrict__ Z,
-                                                  float2* __restrict__ Q, int Ty, int d0y, long long ncols, int nb,
-                                                  const float2* __restrict__ tw) {
+                                                     float2* __restrict__ Q, int Ty, int d0y, long long ncols, int nb,
+                                                     const float2* __restrict__ tw_g) {
     constexpr int EPT = NY / 32;
-    __shared__ __align__(16) float2 sbuf[8][NY];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* tw = reinterpret_cast<float2*>(smem_raw);  // [NY] twiddles
+    float2* xb = tw + NY;                               // [8][NY] exchange
+    float2* fs = xb + 8 * NY;                           // [8][NY] F_I columns
+    float2* zs = fs + 8 * NY;                           // [8][2][64] template column, double buffered
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long col = (long long)blockIdx.x * 8 + warp;
-    if (col >= ncols) return;  // no block-wide barrier below
-    float2* buf = sbuf[warp];
-    const float2* fc = fimg + col * NY;  // re-read per rotation: an L1 hit after the first
+    tgwfft::stage_table(tw, tw_g, NY);
+    float2* buf = xb + warp * NY;
+    float2* fw = fs + warp * NY;
+    float2* zw = zs + warp * 128;
+    if (col < ncols) {
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int p = tgwfft::out_pos<NY>(i, lane);
+            fw[p] = fimg[col * NY + p];  // each lane later reads only its own entries
+        }
+        const float2* zc = Z + col * Ty;  // rotation 0
+        if (lane < Ty) zw[lane] = zc[lane];
+        if (lane + 32 < Ty) zw[lane + 32] = zc[lane + 32];
+    }
+    __syncthreads();  // the table; the only block-wide barrier
+    if (col >= ncols) return;
     for (int b = 0; b < nb; ++b) {
-        const float2* zc = Z + ((long long)b * ncols + col) * Ty;
+        // next rotation's column: two loads per lane, parked in registers
+        float2 n0 = make_float2(0.f, 0.f), n1 = make_float2(0.f, 0.f);
+        if (b + 1 < nb) {
+            const float2* zc = Z + ((long long)(b + 1) * ncols + col) * Ty;
+            if (lane < Ty) n0 = zc[lane];
+            if (lane + 32 < Ty) n1 = zc[lane + 32];
+        }
+        const float2* cur = zw + (b & 1) * 64;
         float2 v[EPT];
 #pragma unroll
         for (int i = 0; i < EPT; ++i) {
             const int jy = (tgwfft::in_pos<NY>(i, lane) - d0y) & (NY - 1);
-            v[i] = jy < Ty ? zc[jy] : make_float2(0.f, 0.f);
+            v[i] = jy < Ty ? cur[jy] : make_float2(0.f, 0.f);
         }
         tgwfft::warp_fft<NY, -1>(v, buf, tw, lane);
 #pragma unroll
-        for (int i = 0; i < EPT; ++i) v[i] = cmulc(__ldg(fc + tgwfft::out_pos<NY>(i, lane)), v[i]);
+        for (int i = 0; i < EPT; ++i) v[i] = cmulc(fw[tgwfft::out_pos<NY>(i, lane)], v[i]);
         tgwfft::warp_fft<NY, +1>(v, buf, tw, lane);
         float2* qc = Q + ((long long)b * ncols + col) * NY;
 #pragma unroll
         for (int i = 0; i < EPT; ++i) qc[tgwfft::out_pos<NY>(i, lane)] = v[i];
+        float2* nx = zw + ((b + 1) & 1) * 64;
+        if (lane < Ty) nx[lane] = n0;
+        if (lane + 32 < Ty) nx[lane + 32] = n1;
         __syncwarp();
     }
 }
 
 __global__ void __launch_bounds__(256) k_inv_z_b256(const float2* __restrict__ Q, float2* __restrict__ H, int Ny,
-                                                    int nh1, const float2* __restrict__ tw) {
+                                                    int nh1, const float2* __restrict__ tw_g) {
     constexpr int NZ = 256, LS = NZ + 1;
     __shared__ __align__(16) float2 s[16 * LS];
+    __shared__ __align__(16) float2 tw[NZ];
+    tgwfft::stage_table(tw, tw_g, NZ);
     const int tid = threadIdx.x, l = tid & 15, j = tid >> 4;
     const int y = blockIdx.x * 16 + l, kx = blockIdx.y, b = blockIdx.z;
     const bool ok = y < Ny;
@@ -94,6 +124,9 @@ __global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* tile = reinterpret_cast<float2*>(smem_raw);  // [2][YT][TS]
     float2* xbuf = tile + 2 * YT * TS;                    // [8][NH]
+    float2* twh = xbuf + 8 * NH;                          // [NH]
+    float2* twx = twh + NH;                               // [NX]
+    float* kaps = reinterpret_cast<float*>(twx + NX);    // [nb]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int y0 = blockIdx.x * YT, z = blockIdx.y, y = y0 + warp;
     const bool yok = y < Ny;
@@ -114,6 +147,9 @@ __global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, 
             g0[i][0] = g.x; g0[i][1] = g.y;
         }
     }
+    tgwfft::stage_table(twh, tw_h, NH);
+    tgwfft::stage_table(twx, tw_x, NX);
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) kaps[b] = (float)(c_mean * (tsum[b] * inv_m - mu_t));
     auto issue = [&](int b, int which) {
         float2* t = tile + which * YT * TS;
         const long long hb = (long long)b * nh1l * Nz * Ny;
@@ -141,12 +177,12 @@ __global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, 
             // unpack: Z[k] = (X[k] + X*[NH-k]) + i w^k (X[k] - X*[NH-k]), w = exp(+2 pi i / NX)
             const int k = tgwfft::in_pos<NH>(i, lane);
             const float2 xa = X[k], xb = cconj(X[NH - k]);
-            const float2 w = cconj(__ldg(tw_x + k));
+            const float2 w = cconj(twx[k]);
             const float2 d = cmul(w, csub(xa, xb));
             v[i] = cadd(cadd(xa, xb), make_float2(-d.y, d.x));
         }
-        tgwfft::warp_fft<NH, +1>(v, xbuf + warp * NH, tw_h, lane);
-        const float kap = (float)(c_mean * (tsum[b] * inv_m - mu_t));
+        tgwfft::warp_fft<NH, +1>(v, xbuf + warp * NH, twh, lane);
+        const float kap = kaps[b];
 #pragma unroll
         for (int i = 0; i < EPT; ++i) {
             const float c0 = (fmaf(v[i].x, inv_nm, -m0[i][0] * mt) + kap) * g0[i][0];
@@ -173,16 +209,23 @@ __global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, 
 }
 
 // ------------------------------------------------------------- dispatch
-bool fast_corr_y(int NY) { return NY == 256 || NY == 512; }
+bool fast_corr_y(int NY, int Ty) { return (NY == 256 || NY == 512) && Ty <= 64; }
 bool fast_inv_z(int NZ) { return NZ == 256; }
 bool fast_c2r(int NH) { return NH == 128 || NH == 256; }
 
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
                                long long ncols, int nb, cudaStream_t st) {
     const unsigned g = (unsigned)((ncols + 7) / 8);
-    if (NY == 512) k_corr_y_w<512><<<g, 256, 0, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(512));
-    else if (NY == 256) k_corr_y_w<256><<<g, 256, 0, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(256));
-    else return cudaErrorInvalidValue;
+    const size_t smem = sizeof(float2) * (NY * 17 + 8 * 128);
+    if (NY == 512) {
+        cudaFuncSetAttribute(k_corr_y_w<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_corr_y_w<512><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(512));
+    } else if (NY == 256) {
+        cudaFuncSetAttribute(k_corr_y_w<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_corr_y_w<256><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(256));
+    } else {
+        return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
@@ -198,14 +241,8 @@ static cudaError_t launch_c2r_t(const float2* H, const float* mu0, const float* 
                                 int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
                                 float* maxcc, int* angidx, cudaStream_t st) {
     constexpr int YT = 8, TS = NH + 2;
-    const size_t smem = sizeof(float2) * (2 * YT * TS + 8 * NH);
-    static unsigned raised = 0;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 32 && !(raised & (1u << dev))) {
-        cudaFuncSetAttribute(k_c2r_w<NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        raised |= 1u << dev;
-    }
+    const size_t smem = sizeof(float2) * (2 * YT * TS + 8 * NH + 3 * NH) + sizeof(float) * nb;
+    cudaFuncSetAttribute(k_c2r_w<NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 g((Ny + YT - 1) / YT, Nz);
     k_c2r_w<NH><<<g, 256, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx,
                                       twiddle_table<float2>(NH), twiddle_table<float2>(2 * NH));

@@ -46,23 +46,24 @@ TG_D int swz(int p) {
     return p ^ s;
 }
 
-// w[r] = tw^(r m) (forward sign), conjugated for DIR > 0
+// w[r] = tw^(r m) (forward sign), conjugated for DIR > 0.  tw is a table of
+// L entries, in shared memory in the hot kernels.
 template <int R, int DIR>
-TG_D void twiddle_powers(const float2* __restrict__ tw, int m, float2* w) {
+TG_D void twiddle_powers(const float2* tw, int m, float2* w) {
     w[0] = make_float2(1.f, 0.f);
-    if constexpr (R >= 2) w[1] = __ldg(tw + m);
+    if constexpr (R >= 2) w[1] = tw[m];
     if constexpr (R >= 4) {
-        w[2] = __ldg(tw + 2 * m);
+        w[2] = tw[2 * m];
         w[3] = cmul(w[1], w[2]);
     }
     if constexpr (R >= 8) {
-        w[4] = __ldg(tw + 4 * m);
+        w[4] = tw[4 * m];
         w[5] = cmul(w[4], w[1]);
         w[6] = cmul(w[4], w[2]);
         w[7] = cmul(w[4], w[3]);
     }
     if constexpr (R >= 16) {
-        w[8] = __ldg(tw + 8 * m);
+        w[8] = tw[8 * m];
 #pragma unroll
         for (int i = 9; i < 16; ++i) w[i] = cmul(w[8], w[i - 8]);
     }
@@ -73,7 +74,7 @@ TG_D void twiddle_powers(const float2* __restrict__ tw, int m, float2* w) {
 }
 
 template <int L, int R, int NS, int DIR>
-TG_D void wstage(float2* v, const float2* __restrict__ tw, int lane) {
+TG_D void wstage(float2* v, const float2* tw, int lane) {
     constexpr int EPT = L / 32, NB = EPT / R;
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
@@ -84,8 +85,13 @@ TG_D void wstage(float2* v, const float2* __restrict__ tw, int lane) {
 #pragma unroll
             for (int r = 1; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], w[r]);
         }
-        tgfft::dft<R, DIR>(v + q * R, tw, L / R);
+        tgfft::dft<R, DIR>(v + q * R, static_cast<const float2*>(nullptr), L / R);  // radices <= 16: no table
     }
+}
+
+// Copy a twiddle table into shared memory (all threads of the block).
+TG_D void stage_table(float2* dst, const float2* __restrict__ src, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
 }
 
 template <int L, int R, int NS>
@@ -112,7 +118,7 @@ TG_D void wload(float2* v, const float2* buf, int lane) {
 }
 
 template <int L, int DIR, int NS, int R, int... Rest>
-TG_D void wrun(float2* v, float2* buf, const float2* __restrict__ tw, int lane) {
+TG_D void wrun(float2* v, float2* buf, const float2* tw, int lane) {
     wstage<L, R, NS, DIR>(v, tw, lane);
     if constexpr (sizeof...(Rest) > 0) {
         constexpr int Rn = tgfft::seq_first<Rest...>::value;
@@ -125,13 +131,13 @@ TG_D void wrun(float2* v, float2* buf, const float2* __restrict__ tw, int lane) 
 }
 
 template <int L, int DIR, int... Rs>
-TG_D void warp_fft_impl(float2* v, float2* buf, const float2* __restrict__ tw, int lane, seq<Rs...>) {
+TG_D void warp_fft_impl(float2* v, float2* buf, const float2* tw, int lane, seq<Rs...>) {
     wrun<L, DIR, 1, Rs...>(v, buf, tw, lane);
 }
 
 // In-register transform of one line per warp; buf: L float2 private to the warp.
 template <int L, int DIR>
-TG_D void warp_fft(float2* v, float2* buf, const float2* __restrict__ tw, int lane) {
+TG_D void warp_fft(float2* v, float2* buf, const float2* tw, int lane) {
     warp_fft_impl<L, DIR>(v, buf, tw, lane, typename WPlan<L>::type{});
 }
 
