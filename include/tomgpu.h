@@ -221,6 +221,16 @@ int tomgpu_match_corr_dev(tomgpu_match_plan* plan, const float* t_dev, float* cc
 /* Local statistics computed by set_volume (volume-sized outputs, may be NULL). */
 int tomgpu_match_stats_dev(tomgpu_match_plan* plan, float* mean_dev, float* std_dev);
 
+/* FP64 rescoring of K candidate peaks (e.g. the top-K of a search): the FLCF
+ * of the template at Euler eulers[k] (host, K x 3 degrees) centred on voxel
+ * pos1[k] (host, K x 3, 1-based), evaluated by direct summation in double
+ * precision over the template box — the correlation sum and the local mean and
+ * variance under the mask of search/tom_os3_corr.m:151-176 at that voxel, with
+ * no FFT.  vol_dev: the tomogram (device, volume-sized); cc: K doubles (host).
+ * Uses the plan's template, mask and weight. */
+int tomgpu_match_rescore_fp64_dev(tomgpu_match_plan* plan, const float* vol_dev, const float* eulers,
+                                  const int* pos1, int K, double* cc);
+
 /* One-shot, host buffers (what a MEX gateway calls): plan, upload, set
  * template and volume, run all R angles, download.  maxcc/angidx: volume-sized
  * host arrays; angidx is 0-based (-1 where never updated). */

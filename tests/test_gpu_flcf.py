@@ -83,3 +83,18 @@ def test_exhaustive_128_angle_subset(gpu, oracle):
     ccc, ang = gpu.tom_os3_findTemplate(d["tomo"], d["template"], grid[:24], mask=mask, batch=8)
     idx = np.where(ang > 0, ang - 1, -1).astype(np.int64)
     _compare(ccc, idx, ref_cc, ref_idx, ref_2)
+
+
+@pytest.mark.parametrize("N", [(928, 48, 40), (64, 464, 40), (64, 48, 464)])
+def test_radix29_sizes(gpu, oracle, N):
+    """The 928/464 edges of the full-size workload (radix 16/8/4 x 29), each axis in turn."""
+    rng = np.random.default_rng(sum(N))
+    vol = rng.standard_normal(N).astype(np.float32)
+    T = 16
+    tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
+    mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
+    angles = oracle.av3_angle_grid((0, 0, 0), (90, 90, 90), (90, 90, 90))
+    ref_cc, ref_idx, ref_2 = oracle.find_template(vol, tmpl, mask, angles, keep_second=True)
+    ccc, ang = gpu.tom_os3_findTemplate(vol, tmpl, angles, mask=mask, batch=3)
+    idx = np.where(ang > 0, ang - 1, -1).astype(np.int64)
+    _compare(ccc, idx, ref_cc, ref_idx, ref_2)

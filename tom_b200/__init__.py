@@ -14,6 +14,8 @@ from .tom import (  # noqa: F401
     euler_matrix,
     from_device,
     match_host,
+    pick_peaks,
+    picklist_to_motl,
     to_device,
     tom_av3_angle2index,
     tom_av3_angle_grid,

@@ -81,6 +81,8 @@ _SIGS = {
     "tomgpu_match_init_results_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
     "tomgpu_match_run_dev": (ctypes.c_int, [c_void_p, c_float_p, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p]),
     "tomgpu_match_corr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    "tomgpu_match_rescore_fp64_dev": (ctypes.c_int, [c_void_p, c_void_p, c_float_p, c_int_p, ctypes.c_int,
+                                                     c_double_p]),
     "tomgpu_match_stats_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
     "tomgpu_match": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p, c_void_p, c_float_p,
                                     ctypes.c_int, ctypes.POINTER(MatchParams), c_void_p, c_void_p]),

@@ -575,6 +575,15 @@ int tomgpu_match_corr_dev(tomgpu_match_plan* plan, const float* t, float* cc) {
     return plan->p.corr(t, cc);
 }
 
+int tomgpu_match_rescore_fp64_dev(tomgpu_match_plan* plan, const float* vol, const float* eulers, const int* pos1,
+                                  int K, double* cc) {
+    if (!plan) return TOMGPU_ERR_ARG;
+    if (K < 0 || (K > 0 && (!vol || !eulers || !pos1 || !cc)))
+        return fail(plan->p.ctx, TOMGPU_ERR_ARG, "null pointer or negative count");
+    TG_TRY(use_device(plan->p.ctx));
+    return plan->p.rescore(vol, eulers, pos1, K, cc);
+}
+
 int tomgpu_match_stats_dev(tomgpu_match_plan* plan, float* mean, float* std) {
     if (!plan) return TOMGPU_ERR_ARG;
     if (!plan->p.has_volume) return fail(plan->p.ctx, TOMGPU_ERR_STATE, "no volume set");

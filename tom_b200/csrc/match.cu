@@ -34,6 +34,7 @@
 #include "fft_engine.cuh"
 #include "match.h"
 #include "misc.h"
+#include "rescore.h"
 #include "rotate.h"
 #include "twiddles.h"
 
@@ -861,15 +862,86 @@ int MatchPlan::init_results(float* maxcc, int* angidx) {
 }
 
 // batched full complex 3-D transform of nb volumes [nb][tz][ty][tx]
-cudaError_t c2c3d_batch(float2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st) {
+template <typename C>
+static cudaError_t c2c3d_batch_t(C* data, const int t[3], int nb, int dir, double scale, cudaStream_t st) {
     const long tx = t[0], ty = t[1], tz = t[2];
     cudaError_t e;
     LineGeom gx{1, (int)ty, tx, (int)(tz * nb), tx * ty};
-    if ((e = fft_lines<float2>((int)tx, dir, FFT_C2C, data, data, gx, gx, ty * tz * nb, 1.0, st))) return e;
+    if ((e = fft_lines<C>((int)tx, dir, FFT_C2C, data, data, gx, gx, ty * tz * nb, 1.0, st))) return e;
     LineGeom gy{tx, (int)tx, 1, (int)(tz * nb), tx * ty};
-    if ((e = fft_lines<float2>((int)ty, dir, FFT_C2C, data, data, gy, gy, tx * tz * nb, 1.0, st))) return e;
+    if ((e = fft_lines<C>((int)ty, dir, FFT_C2C, data, data, gy, gy, tx * tz * nb, 1.0, st))) return e;
     LineGeom gz{tx * ty, (int)(tx * ty), 1, nb, tx * ty * tz};
-    return fft_lines<float2>((int)tz, dir, FFT_C2C, data, data, gz, gz, tx * ty * nb, scale, st);
+    return fft_lines<C>((int)tz, dir, FFT_C2C, data, data, gz, gz, tx * ty * nb, scale, st);
+}
+cudaError_t c2c3d_batch(float2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st) {
+    return c2c3d_batch_t<float2>(data, t, nb, dir, scale, st);
+}
+cudaError_t c2c3d_batch64(double2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st) {
+    return c2c3d_batch_t<double2>(data, t, nb, dir, scale, st);
+}
+
+__global__ void k_mulw_c64_batch(double2* __restrict__ a, const float* __restrict__ w, long long n, long long tn) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a[i] = cscale(a[i], (double)w[i % tn]);
+}
+
+int MatchPlan::rescore(const float* vol, const float* eulers, const int* pos1, int K, double* out) {
+    if (!has_template) return fail(ctx, TOMGPU_ERR_STATE, "set the template first");
+    if (K <= 0) return TOMGPU_OK;
+    for (int k = 0; k < K; ++k)
+        for (int d = 0; d < 3; ++d)
+            if (pos1[3 * k + d] < 1 || pos1[3 * k + d] > N[d])
+                return fail(ctx, TOMGPU_ERR_ARG, "candidate position outside the volume");
+    cudaStream_t st = ctx->stream;
+    std::vector<float> mats(9 * (size_t)K);
+    for (int k = 0; k < K; ++k) euler_matrix_host(eulers + 3 * k, mats.data() + 9 * k);
+    std::vector<int> p0(3 * (size_t)K);
+    for (int i = 0; i < 3 * K; ++i) p0[i] = pos1[i] - 1;
+    float *d_m = nullptr, *d_t = nullptr;
+    double *d_t64 = nullptr, *d_out = nullptr;
+    double2* d_c = nullptr;
+    int* d_p = nullptr;
+    const long long n = tn * K;
+    auto cleanup = [&]() {
+        if (d_m) cudaFree(d_m);
+        if (d_t) cudaFree(d_t);
+        if (d_t64) cudaFree(d_t64);
+        if (d_out) cudaFree(d_out);
+        if (d_c) cudaFree(d_c);
+        if (d_p) cudaFree(d_p);
+    };
+    if (cudaMalloc(&d_m, sizeof(float) * 9 * K) || cudaMalloc(&d_t, sizeof(float) * n) ||
+        cudaMalloc(&d_t64, sizeof(double) * n) || cudaMalloc(&d_out, sizeof(double) * K) ||
+        cudaMalloc(&d_p, sizeof(int) * 3 * K) || (has_psf && cudaMalloc(&d_c, sizeof(double2) * n))) {
+        cudaGetLastError();
+        cleanup();
+        return fail(ctx, TOMGPU_ERR_OOM, "rescoring workspace allocation failed");
+    }
+    int rc = TOMGPU_OK;
+    do {
+        cudaError_t e = cudaMemcpyAsync(d_m, mats.data(), sizeof(float) * 9 * K, cudaMemcpyHostToDevice, st);
+        if (!e) e = cudaMemcpyAsync(d_p, p0.data(), sizeof(int) * 3 * K, cudaMemcpyHostToDevice, st);
+        const float center[3] = {(float)((T[0] + 1) / 2), (float)((T[1] + 1) / 2), (float)((T[2] + 1) / 2)};
+        if (!e) e = rotate3d_batch(d_tmpl, d_t, T, d_m, K, center, d_mask, st);
+        if (!e && !has_psf) e = f32_to_f64(d_t, d_t64, n, st);
+        if (!e && has_psf) {
+            e = real_to_c64(d_t, d_c, n, st);
+            if (!e) e = c2c3d_batch64(d_c, T, K, -1, 1.0, st);
+            if (!e) {
+                k_mulw_c64_batch<<<grid_n(n), 256, 0, st>>>(d_c, d_wu, n, tn);
+                e = cudaGetLastError();
+            }
+            if (!e) e = c2c3d_batch64(d_c, T, K, +1, 1.0 / (double)tn, st);
+            if (!e) e = re_c64(d_c, d_t64, n, 1.0, st);
+        }
+        if (!e) e = rescore_fp64(vol, N, d_t64, d_mask, T, d_p, K, msize, tmean, tstd, d_out, st);
+        if (!e) e = cudaMemcpyAsync(out, d_out, sizeof(double) * K, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaStreamSynchronize(st);
+        if (e) rc = cuda_fail(ctx, e, "rescore_fp64");
+        ctx->launches += has_psf ? 11 : 3;
+    } while (0);
+    cleanup();
+    return rc;
 }
 
 }  // namespace tg

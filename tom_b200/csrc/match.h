@@ -20,6 +20,7 @@ cudaError_t launch_c2r_fast(int NH, const float2* H, const float* mu0, const flo
                             int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
                             float* maxcc, int* angidx, cudaStream_t st);
 cudaError_t c2c3d_batch(float2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
+cudaError_t c2c3d_batch64(double2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
 
 struct MatchPlan {
     tomgpu_ctx* ctx = nullptr;
@@ -65,6 +66,7 @@ struct MatchPlan {
     int run(const float* eulers, int R, int index_offset, float* maxcc, int* angidx);
     int corr(const float* t, float* cc);
     int init_results(float* maxcc, int* angidx);
+    int rescore(const float* vol, const float* eulers, const int* pos1, int K, double* out);
 };
 
 }  // namespace tg

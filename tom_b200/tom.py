@@ -479,6 +479,16 @@ class MatchPlan:
     def corr(self, t_dev, out_dev):
         self.ctx.check(lib().tomgpu_match_corr_dev(self.handle, _tptr(t_dev), _tptr(out_dev)))
 
+    def rescore_fp64(self, vol_dev, eulers, pos1):
+        """FP64 direct-sum FLCF of candidates (eulers K x 3 degrees, pos1 K x 3 1-based)."""
+        e = np.ascontiguousarray(np.asarray(eulers, np.float32).reshape(-1, 3))
+        p = np.ascontiguousarray(np.asarray(pos1, np.int32).reshape(-1, 3))
+        out = np.zeros(len(e), np.float64)
+        self.ctx.check(lib().tomgpu_match_rescore_fp64_dev(self.handle, _tptr(vol_dev), e.ctypes.data_as(_lib.c_float_p),
+                                                           p.ctypes.data_as(_lib.c_int_p), len(e),
+                                                           out.ctypes.data_as(_lib.c_double_p)))
+        return out
+
     def stats(self):
         import torch
         x, y, z = self.vol_shape
@@ -486,6 +496,35 @@ class MatchPlan:
         s = torch.empty_like(m)
         self.ctx.check(lib().tomgpu_match_stats_dev(self.handle, _tptr(m), _tptr(s)))
         return m, s
+
+
+def pick_peaks(maxcc_dev, angidx_dev, K, radius, ctx: Context | None = None):
+    """Top-K candidates of a search: K rounds of tom_peak(A, R) on the max-CC
+    volume (first maximum, then zero a ball of radius R), with the angle index
+    recorded at each peak (tom_os3_returnPicklist.m's loop).  Returns
+    (vals[K], pos1[K,3] 1-based [x,y,z], angle index[K] 0-based)."""
+    vals, pos = topk_peaks(maxcc_dev, K, radius, ctx)
+    p0 = pos - 1
+    ok = (pos[:, 0] > 0)
+    idx = np.full(K, -1, np.int64)
+    if ok.any():
+        import torch
+        zz, yy, xx = (torch.as_tensor(p0[ok, 2]), torch.as_tensor(p0[ok, 1]), torch.as_tensor(p0[ok, 0]))
+        idx[ok] = angidx_dev[zz.to(angidx_dev.device), yy.to(angidx_dev.device), xx.to(angidx_dev.device)].cpu().numpy()
+    return vals, pos, idx
+
+
+def picklist_to_motl(vals, pos1, eulers, class_no=0):
+    """MOTL (20 x n) of a pick list, av3/alignment/av3_tomomatch.m:48-70 layout:
+    row 1 CCC, 4 particle number, 8-10 x/y/z (1-based), 17-19 phi/psi/theta, 20 class."""
+    n = len(vals)
+    m = np.zeros((20, n))
+    m[0] = vals
+    m[3] = np.arange(1, n + 1)
+    m[7:10] = np.asarray(pos1, np.float64).T
+    m[16:19] = np.asarray(eulers, np.float64).reshape(-1, 3).T
+    m[19] = class_no
+    return m
 
 
 def match_host(tomo, template, mask, eulers, psf=None, batch: int = 0, ctx: Context | None = None):
