@@ -10,8 +10,8 @@
 //   inv_z_b   16 consecutive y lines per block, 16 threads per line holding
 //             16 values: radix 16 straight from global memory, one block-wide
 //             exchange, radix 16 straight back to global memory.
-//   c2r_w     one warp per x line, the next rotation's tile prefetched with
-//             cp.async while the current one is transformed; running max and
+//   c2r_w     one warp per x line, the next three rotations' tiles in flight
+//             (cp.async) while the current one is transformed; running max and
 //             the FLCF coefficients of the lane's voxels stay in registers.
 #include "ctx.h"
 #include "match.h"
@@ -107,6 +107,8 @@ __global__ void __launch_bounds__(256) k_inv_z_b256(const float2* __restrict__ Q
     }
 }
 
+constexpr int C2R_STAGES = 4;
+
 TG_D void cp_async8(void* smem_dst, const void* gsrc, int bytes) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
@@ -120,10 +122,10 @@ __global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, 
                                                int Nz, int nb, float inv_nm, double c_mean, double inv_m, double mu_t,
                                                int index0, float* __restrict__ maxcc, int* __restrict__ angidx,
                                                const float2* __restrict__ tw_h, const float2* __restrict__ tw_x) {
-    constexpr int YT = 8, NH1 = NH + 1, TS = NH + 2, EPT = NH / 32, NX = 2 * NH;
+    constexpr int YT = 8, NH1 = NH + 1, TS = NH + 2, EPT = NH / 32, NX = 2 * NH, NSTG = C2R_STAGES;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2* tile = reinterpret_cast<float2*>(smem_raw);  // [2][YT][TS]
-    float2* xbuf = tile + 2 * YT * TS;                    // [8][NH]
+    float2* tile = reinterpret_cast<float2*>(smem_raw);  // [NSTG][YT][TS]
+    float2* xbuf = tile + NSTG * YT * TS;                 // [8][NH]
     float2* twh = xbuf + 8 * NH;                          // [NH]
     float2* twx = twh + NH;                               // [NX]
     float* kaps = reinterpret_cast<float*>(twx + NX);    // [nb]
@@ -161,16 +163,20 @@ __global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, 
         }
         cp_async_commit();
     };
-    issue(0, 0);
+    // NSTG-deep pipeline: tiles b+1 .. b+NSTG-1 are in flight while b is
+    // transformed; every iteration commits one group (possibly empty) so that
+    // "all but the newest NSTG-1 groups complete" means tile b has landed.
+#pragma unroll
+    for (int s = 0; s < NSTG - 1; ++s) {
+        if (s < nb) issue(s, s);
+        else cp_async_commit();
+    }
     for (int b = 0; b < nb; ++b) {
-        if (b + 1 < nb) {
-            issue(b + 1, (b + 1) & 1);
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
+        if (b + NSTG - 1 < nb) issue(b + NSTG - 1, (b + NSTG - 1) % NSTG);
+        else cp_async_commit();
+        cp_async_wait<NSTG - 1>();
         __syncthreads();
-        const float2* X = tile + (b & 1) * YT * TS + warp * TS;
+        const float2* X = tile + (b % NSTG) * YT * TS + warp * TS;
         float2 v[EPT];
 #pragma unroll
         for (int i = 0; i < EPT; ++i) {
@@ -241,7 +247,7 @@ static cudaError_t launch_c2r_t(const float2* H, const float* mu0, const float* 
                                 int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
                                 float* maxcc, int* angidx, cudaStream_t st) {
     constexpr int YT = 8, TS = NH + 2;
-    const size_t smem = sizeof(float2) * (2 * YT * TS + 8 * NH + 3 * NH) + sizeof(float) * nb;
+    const size_t smem = sizeof(float2) * (C2R_STAGES * YT * TS + 8 * NH + 3 * NH) + sizeof(float) * nb;
     cudaFuncSetAttribute(k_c2r_w<NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 g((Ny + YT - 1) / YT, Nz);
     k_c2r_w<NH><<<g, 256, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx,
