@@ -238,6 +238,35 @@ int tomgpu_match(tomgpu_ctx* ctx, const float* tomo, const int vol_dims[3], cons
                  const int tmpl_dims[3], const float* mask, const float* psf, const float* eulers,
                  int R, const tomgpu_match_params* params, float* maxcc, int32_t* angidx);
 
+/* ------------------------------------------------- subtomogram alignment --- */
+/* One alignment job of tom_av3_align (av3_new/tom_av3_align.m:1-189) with
+ * filter.Apply = 0.  All volumes are device buffers of size n (x fastest).
+ * wedge_ref == NULL: the 5-7 argument form without wedges; wedge_part == NULL
+ * with wedge_ref set: the 8 argument form (wedge_part = wedge_ref).  mask is
+ * required (pass tom_spheremask(ones) for the reference's default);
+ * mask_ccf == NULL means ones.  Angle ranges are [start increment end] in
+ * degrees, scanned phi outer, psi, theta inner; indices follow
+ * tom_av3_angle2index (phi fastest). */
+typedef struct {
+    int n[3];
+    const float* ref;
+    const float* part;
+    const float* mask;
+    const float* mask_ccf;
+    const float* wedge_ref;
+    const float* wedge_part;
+    float phi[3];
+    float psi[3];
+    float theta[3];
+} tomgpu_align_job;
+
+/* Run n_jobs alignment jobs (any mix of box sizes); per job the outputs of
+ * [angles, shifts, ccf_peak] = tom_av3_align(...): angles (3 floats, degrees),
+ * shifts (3 floats, spline sub-voxel peak minus floor(n/2)+1), ccf_peak
+ * (1 float).  Host output arrays of n_jobs*3, n_jobs*3 and n_jobs floats. */
+int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs, float* angles,
+                         float* shifts, float* ccf_peak);
+
 #ifdef __cplusplus
 }
 #endif

@@ -533,3 +533,54 @@ def tom_corr_norm(a, b, mask, psf1=None, psf2=None):
     a, _, _, n = norm_inside_mask(a, mask)
     b, _, _, _ = norm_inside_mask(b, mask)
     return np.real(np.fft.fftshift(np.fft.ifftn(np.fft.fftn(b) * np.conj(np.fft.fftn(a))))) / n
+
+
+def rotmatrix_double(euler_deg):
+    """tom_angles2rotmatrix (Sptrans/tom_sum_rotation.m): Rz(psi) Rx(theta) Rz(phi) in double."""
+    ph, ps, th = np.deg2rad(np.asarray(euler_deg, np.float64))
+    rz = lambda a: np.array([[np.cos(a), -np.sin(a), 0], [np.sin(a), np.cos(a), 0], [0, 0, 1.0]])
+    rx = np.array([[1, 0, 0], [0, np.cos(th), -np.sin(th)], [0, np.sin(th), np.cos(th)]])
+    return rz(ps) @ rx @ rz(ph)
+
+
+def av3_axis(rng3):
+    """MATLAB start:incr:end of one angle axis."""
+    s, i, e = [float(x) for x in rng3]
+    n = int(np.floor((e - s) / i + 1e-9)) + 1
+    return s + i * np.arange(n)
+
+
+def av3_align(ref, part, phi, psi, theta, mask, mask_ccf, wedge_ref, wedge_part):
+    """[angles shifts ccf_peak] = tom_av3_align(ref,part,phi,psi,theta,mask,filter,mask_ccf,wedge_ref,wedge_part)
+    with filter.Apply = 0 (av3_new/tom_av3_align.m:97-189), FP64 except rot3d (FP32)."""
+    ref = np.asarray(ref, np.float64)
+    part = np.asarray(part, np.float64)
+    n = ref.shape
+    psf_part = np.real(np.fft.ifftn(np.fft.ifftshift(wedge_part)))
+    ccf_max = np.full(n, -2.0)
+    angle_max = np.full(n, -2.0)
+    start = (phi[0], psi[0], theta[0])
+    incr = (phi[1], psi[1], theta[1])
+    end = (phi[2], psi[2], theta[2])
+    for i_phi in av3_axis(phi):
+        for i_psi in av3_axis(psi):
+            for i_theta in av3_axis(theta):
+                R = rotmatrix_double((i_phi, i_psi, i_theta))
+                ref_rot = rotate_matrix(ref, R.astype(np.float32).flatten(order="F")).astype(np.float64)
+                wrot = rotate(wedge_ref, (i_phi, i_psi, i_theta)).astype(np.float64)
+                psf_ref = np.real(np.fft.ifftn(np.fft.ifftshift(wrot)))
+                ref_rot = ref_rot * mask
+                part = part * mask
+                ccf = tom_corr_norm(ref_rot, part, mask, psf_ref, psf_part)
+                new_max = np.where(ccf > ccf_max, ccf, ccf_max)
+                aidx = av3_angle2index((i_phi, i_psi, i_theta), start, incr, end)
+                angle_max = np.where(ccf >= new_max, aidx, angle_max)
+                ccf_max = new_max
+    pos, _ = tom_peak(ccf_max * mask_ccf)
+    ai = angle_max[tuple(p - 1 for p in pos)]
+    angles = av3_index2angle(ai, start, incr, end)
+    rot_ref = rotate(ref, angles).astype(np.float64)
+    ccf_s = tom_corr_norm(rot_ref, part, mask)
+    pos, peak = tom_peak_spline(ccf_s * mask_ccf)
+    shifts = np.array(pos) - (np.floor(np.array(n) / 2) + 1)
+    return angles, shifts, peak, dict(ccf_max=ccf_max, angle_max=angle_max, ccf_s=ccf_s)

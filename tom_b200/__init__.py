@@ -9,6 +9,7 @@ from ._lib import TomGpuError, declared_symbols, lib  # noqa: F401
 from .tom import (  # noqa: F401
     Context,
     MatchPlan,
+    av3_align_batch,
     av3_wedge,
     default_context,
     euler_matrix,
@@ -17,6 +18,7 @@ from .tom import (  # noqa: F401
     pick_peaks,
     picklist_to_motl,
     to_device,
+    tom_av3_align,
     tom_av3_angle2index,
     tom_av3_angle_grid,
     tom_av3_index2angle,

@@ -42,6 +42,13 @@ class MatchParams(ctypes.Structure):
                 ("reserved", ctypes.c_int * 5)]
 
 
+class AlignJob(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int * 3), ("ref", ctypes.c_void_p), ("part", ctypes.c_void_p),
+                ("mask", ctypes.c_void_p), ("mask_ccf", ctypes.c_void_p), ("wedge_ref", ctypes.c_void_p),
+                ("wedge_part", ctypes.c_void_p), ("phi", ctypes.c_float * 3), ("psi", ctypes.c_float * 3),
+                ("theta", ctypes.c_float * 3)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "tomgpu_version": (ctypes.c_char_p, []),
@@ -84,6 +91,8 @@ _SIGS = {
     "tomgpu_match_rescore_fp64_dev": (ctypes.c_int, [c_void_p, c_void_p, c_float_p, c_int_p, ctypes.c_int,
                                                      c_double_p]),
     "tomgpu_match_stats_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    "tomgpu_av3_align_dev": (ctypes.c_int, [c_void_p, ctypes.POINTER(AlignJob), ctypes.c_int, c_float_p, c_float_p,
+                                            c_float_p]),
     "tomgpu_match": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p, c_void_p, c_float_p,
                                     ctypes.c_int, ctypes.POINTER(MatchParams), c_void_p, c_void_p]),
 }

@@ -1,0 +1,420 @@
+// Batched subtomogram alignment with tom_av3_align's semantics
+// (av3_new/tom_av3_align.m:97-189, tom_corr 'norm' of Analysis/tom_corr.m:51-121).
+//
+// Per job (reference, particle, masks, wedges, angle ranges) and per Euler
+// triplet of its scan, in the reference's loop order (phi outer, psi, theta
+// inner):
+//   ref_rot = rot3d(ref, R)            R = tom_angles2rotmatrix, matrix mode
+//   w_rot   = rot3d(wedge_ref, euler)  Euler mode
+//   a = ref_rot*mask (*) psf_part,  b = part*mask (*) psf_ref   (cross-wedging)
+//   a, b normalised inside the mask (mean over the mask, std with n - 1)
+//   ccf = real(fftshift(ifftn(F(b) conj F(a)))) / n
+//   ccf_max = strict max, angle_max = index where ccf >= the updated max
+// The convolutions with the wedge PSFs are products in Fourier space: the
+// spectrum of psf = real(ifftn(ifftshift(w))) is the Hermitian part
+// (W'(k) + W'(-k))/2 of W' = ifftshift(w), for the particle's wedge and for the
+// rotated reference wedge alike.
+// After the scan: first maximum of ccf_max*mask_ccf gives the angle index;
+// the reference rotated by those angles is correlated once more without
+// wedges and tom_peak(.,'spline') of ccf*mask_ccf gives shift and peak.
+//
+// The rotation batch of a job runs as batched template-sized FFTs
+// (fft3d.cu); per-entry statistics are FP64 segmented reductions.
+#include <cfloat>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "ctx.h"
+#include "fft3d.h"
+#include "match.h"
+#include "misc.h"
+#include "peak.h"
+#include "rotate_sample.cuh"
+
+namespace tg {
+
+namespace {
+
+unsigned grid_for(long long n) {
+    long long b = (n + 255) / 256;
+    if (b > 148 * 32) b = 148 * 32;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+TG_D long long shifted(long long v, int nx, int ny, int nz, int sgn) {
+    // sgn = +1: ifftshift source index (i + floor(n/2)); -1: fftshift (i - floor(n/2))
+    const int i = (int)(v % nx), j = (int)((v / nx) % ny), k = (int)(v / ((long long)nx * ny));
+    const int si = pmod(i + sgn * (nx / 2), nx), sj = pmod(j + sgn * (ny / 2), ny), sk = pmod(k + sgn * (nz / 2), nz);
+    return si + (long long)nx * (sj + (long long)ny * sk);
+}
+
+TG_D long long mirrored(long long v, int nx, int ny, int nz) {
+    const int i = (int)(v % nx), j = (int)((v / nx) % ny), k = (int)(v / ((long long)nx * ny));
+    return pmod(-i, nx) + (long long)nx * (pmod(-j, ny) + (long long)ny * pmod(-k, nz));
+}
+
+// A[e] = rot(ref, mref_e) * mask (complex), W[e] = rot(wedge_ref, mw_e)
+__global__ void k_al_rotate(const float* __restrict__ ref, const float* __restrict__ wref,
+                            const float* __restrict__ mask, const float* __restrict__ mref,
+                            const float* __restrict__ mw, int nx, int ny, int nz, float cx, float cy, float cz,
+                            int mask_ref, float2* __restrict__ A, float* __restrict__ W) {
+    const long long nn = (long long)nx * ny * nz;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = blockIdx.y;
+    if (v >= nn) return;
+    const int i = (int)(v % nx), j = (int)((v / nx) % ny), k = (int)(v / ((long long)nx * ny));
+    float m[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) m[q] = mref[9 * e + q];
+    float a = rot_sample(ref, nx, ny, nz, m, cx, cy, cz, i, j, k);
+    if (mask_ref) a = __fmul_rn(a, mask[v]);
+    A[(long long)e * nn + v] = make_float2(a, 0.f);
+    if (W) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q) m[q] = mw[9 * e + q];
+        W[(long long)e * nn + v] = rot_sample(wref, nx, ny, nz, m, cx, cy, cz, i, j, k);
+    }
+}
+
+// A[e][k] *= (W'(k) + W'(-k)) / 2, W' = ifftshift(wedge_part): the spectrum of
+// psf_part = real(ifftn(W'))
+__global__ void k_al_wpart(float2* __restrict__ A, const float* __restrict__ wpart, int nx, int ny, int nz, int E) {
+    const long long nn = (long long)nx * ny * nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn * E; t += (long long)gridDim.x * blockDim.x) {
+        const long long v = t % nn;
+        const float ws = 0.5f * (wpart[shifted(v, nx, ny, nz, +1)] +
+                                 wpart[shifted(mirrored(v, nx, ny, nz), nx, ny, nz, +1)]);
+        A[t] = cscale(A[t], ws);
+    }
+}
+
+// B[e][k] = B0[k] * (W'(k) + W'(-k)) / 2, W' = ifftshift(W[e])
+__global__ void k_al_bside(float2* __restrict__ B, const float2* __restrict__ B0, const float* __restrict__ W, int nx,
+                           int ny, int nz, int E) {
+    const long long nn = (long long)nx * ny * nz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn * E; t += (long long)gridDim.x * blockDim.x) {
+        const long long v = t % nn, e = t / nn;
+        const float* w = W + e * nn;
+        const float ws = 0.5f * (w[shifted(v, nx, ny, nz, +1)] + w[shifted(mirrored(v, nx, ny, nz), nx, ny, nz, +1)]);
+        B[t] = cscale(B0[v], ws);
+    }
+}
+
+// per-entry FP64 sums of norm_inside_mask: pass 0: sum re*m, pass 1: sum over m of (re - mea)^2
+__global__ void __launch_bounds__(256) k_al_stats(const float2* __restrict__ X, const float* __restrict__ mask,
+                                                  long long nn, const double* __restrict__ mea, int pass,
+                                                  double* __restrict__ out) {
+    const int e = blockIdx.y;
+    const float2* x = X + (long long)e * nn;
+    double acc = 0;
+    const double me = pass ? mea[e] : 0.0;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += (long long)gridDim.x * blockDim.x) {
+        if (mask[v] != 0.f) {
+            const double r = (double)x[v].x;
+            acc += pass ? (r - me) * (r - me) : r;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __shared__ double ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < 8; ++w) s += ws[w];
+        atomicAdd(out + e, s);
+    }
+}
+
+__global__ void k_al_mean(const double* __restrict__ s, double* __restrict__ mea, int E, double n) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < E) mea[e] = s[e] / n;
+}
+
+// X[e] = ((re - mea)/st) * (mask != 0), st = sqrt(var_sum / (n - 1))
+__global__ void k_al_normalize(float2* __restrict__ X, const float* __restrict__ mask, long long nn, int E,
+                               const double* __restrict__ mea, const double* __restrict__ var, double n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn * E; t += (long long)gridDim.x * blockDim.x) {
+        const long long v = t % nn, e = t / nn;
+        const double st = sqrt(var[e] / (n - 1.0));
+        const double r = (double)X[t].x;
+        X[t] = make_float2(mask[v] != 0.f ? (float)((r - mea[e]) / st) : 0.f, 0.f);
+    }
+}
+
+// C = B * conj(A)
+__global__ void k_al_cross(float2* __restrict__ B, const float2* __restrict__ A, long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        B[t] = cmulc(B[t], A[t]);
+}
+
+// running max over the E entries in scan order; ccf = real(fftshift(C))/n
+__global__ void k_al_update(const float2* __restrict__ C, int nx, int ny, int nz, int E, double inv_n,
+                            const int* __restrict__ aidx, float* __restrict__ cmax, float* __restrict__ amax) {
+    const long long nn = (long long)nx * ny * nz;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += (long long)gridDim.x * blockDim.x) {
+        const long long src = shifted(v, nx, ny, nz, -1);
+        float m = cmax[v], a = amax[v];
+        for (int e = 0; e < E; ++e) {
+            const float c = (float)((double)C[(long long)e * nn + src].x * inv_n);
+            if (c > m) m = c;
+            if (c >= m) a = (float)aidx[e];
+        }
+        cmax[v] = m;
+        amax[v] = a;
+    }
+}
+
+// single map: out = real(fftshift(C)) / n * mask_ccf
+__global__ void k_al_map(const float2* __restrict__ C, int nx, int ny, int nz, double inv_n,
+                         const float* __restrict__ mccf, float* __restrict__ out) {
+    const long long nn = (long long)nx * ny * nz;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += (long long)gridDim.x * blockDim.x) {
+        const float c = (float)((double)C[shifted(v, nx, ny, nz, -1)].x * inv_n);
+        out[v] = mccf ? c * mccf[v] : c;
+    }
+}
+
+__global__ void k_al_fill(float* __restrict__ a, float* __restrict__ b, long long n, float va, float vb) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        a[t] = va;
+        b[t] = vb;
+    }
+}
+
+__global__ void k_al_mul(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ out, long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        out[t] = b ? a[t] * b[t] : a[t];
+}
+
+__global__ void k_al_r2c_masked(const float* __restrict__ a, const float* __restrict__ m, float2* __restrict__ out,
+                                long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        out[t] = make_float2(m ? a[t] * m[t] : a[t], 0.f);
+}
+
+// matrix of tom_angles2rotmatrix (Sptrans/tom_sum_rotation.m): Rz(psi) Rx(theta) Rz(phi)
+// in double, passed to rot3d's matrix mode as single in column-major order
+void rotmatrix_as_float(double phi, double psi, double theta, float m9[9]) {
+    const double d = 3.14159265358979323846 / 180.0;
+    const double cf = std::cos(phi * d), sf = std::sin(phi * d), cp = std::cos(psi * d), sp = std::sin(psi * d);
+    const double ct = std::cos(theta * d), st = std::sin(theta * d);
+    const double Rzpsi[3][3] = {{cp, -sp, 0}, {sp, cp, 0}, {0, 0, 1}};
+    const double Rx[3][3] = {{1, 0, 0}, {0, ct, -st}, {0, st, ct}};
+    const double Rzphi[3][3] = {{cf, -sf, 0}, {sf, cf, 0}, {0, 0, 1}};
+    double T1[3][3], R[3][3];
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            T1[a][b] = 0;
+            for (int c = 0; c < 3; ++c) T1[a][b] += Rzpsi[a][c] * Rx[c][b];
+        }
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+            R[a][b] = 0;
+            for (int c = 0; c < 3; ++c) R[a][b] += T1[a][c] * Rzphi[c][b];
+        }
+    // column-major: m[0] = R(1,1), m[1] = R(2,1), m[2] = R(3,1), m[3] = R(1,2), ...
+    for (int col = 0; col < 3; ++col)
+        for (int row = 0; row < 3; ++row) m9[3 * col + row] = (float)R[row][col];
+}
+
+std::vector<double> axis_values(const float r[3]) {
+    std::vector<double> v;
+    const double s = r[0], inc = r[1], e = r[2];
+    if (inc == 0) {
+        v.push_back(s);
+        return v;
+    }
+    const long n = (long)std::floor((e - s) / inc + 1e-9) + 1;
+    for (long i = 0; i < n; ++i) v.push_back(s + inc * (double)i);
+    return v;
+}
+
+struct Workspace {
+    float2 *A = nullptr, *B = nullptr, *B0 = nullptr;
+    float *W = nullptr, *cmax = nullptr, *amax = nullptr, *tmp = nullptr, *mats = nullptr;
+    int* aidx = nullptr;
+    double *sums = nullptr, *mea = nullptr, *var = nullptr, *spline = nullptr;
+    unsigned long long* key = nullptr;
+    void release() {
+        void* p[] = {A, B, B0, W, cmax, amax, tmp, mats, aidx, sums, mea, var, spline, key};
+        for (void* q : p)
+            if (q) cudaFree(q);
+    }
+};
+
+}  // namespace
+
+// norm_inside_mask on E complex volumes X (real parts), in place
+static cudaError_t normalize_entries(float2* X, const float* mask, long long nn, int E, double nmask, Workspace& w,
+                                     cudaStream_t st, int64_t* launches) {
+    cudaError_t e = cudaMemsetAsync(w.sums, 0, sizeof(double) * E, st);
+    if (!e) e = cudaMemsetAsync(w.var, 0, sizeof(double) * E, st);
+    dim3 g((unsigned)std::min<long long>((nn + 255) / 256, 64), E);
+    if (!e) {
+        k_al_stats<<<g, 256, 0, st>>>(X, mask, nn, nullptr, 0, w.sums);
+        k_al_mean<<<(E + 127) / 128, 128, 0, st>>>(w.sums, w.mea, E, nmask);
+        k_al_stats<<<g, 256, 0, st>>>(X, mask, nn, w.mea, 1, w.var);
+        k_al_normalize<<<grid_for(nn * E), 256, 0, st>>>(X, mask, nn, E, w.mea, w.var, nmask);
+        e = cudaGetLastError();
+    }
+    *launches += 4;
+    return e;
+}
+
+int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3], float* peak_out,
+              size_t budget_voxels) {
+    const int* n = job.n;
+    const long long nn = (long long)n[0] * n[1] * n[2];
+    cudaStream_t st = ctx->stream;
+    const bool wedges = job.wedge_ref != nullptr;
+    const float* wpart = job.wedge_part ? job.wedge_part : job.wedge_ref;
+    if (!job.ref || !job.part || !job.mask) return fail(ctx, TOMGPU_ERR_ARG, "job needs ref, part and mask");
+    for (int d = 0; d < 3; ++d)
+        if (!fft_length_supported(n[d])) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "box edge not an FFT length");
+    // scan in the reference's loop order
+    std::vector<double> ph = axis_values(job.phi), ps = axis_values(job.psi), th = axis_values(job.theta);
+    struct Ang { double phi, psi, theta; int idx; };
+    std::vector<Ang> scan;
+    const int nph = (int)ph.size(), nps = (int)ps.size();
+    for (size_t a = 0; a < ph.size(); ++a)
+        for (size_t b = 0; b < ps.size(); ++b)
+            for (size_t c = 0; c < th.size(); ++c)
+                scan.push_back({ph[a], ps[b], th[c], (int)(c * nph * nps + b * nph + a)});
+    const int R = (int)scan.size();
+    int E = (int)std::max<long long>(1, std::min<long long>(256, (long long)budget_voxels / nn));
+    E = std::min(E, R);
+    Workspace w;
+    auto A = [&](void** p, size_t b) { return cudaMalloc(p, b) == cudaSuccess; };
+    if (!A((void**)&w.A, sizeof(float2) * nn * E) || !A((void**)&w.B, sizeof(float2) * nn * E) ||
+        !A((void**)&w.B0, sizeof(float2) * nn) || (wedges && !A((void**)&w.W, sizeof(float) * nn * E)) ||
+        !A((void**)&w.cmax, sizeof(float) * nn) || !A((void**)&w.amax, sizeof(float) * nn) ||
+        !A((void**)&w.tmp, sizeof(float) * nn) || !A((void**)&w.mats, sizeof(float) * 18 * E) ||
+        !A((void**)&w.aidx, sizeof(int) * E) || !A((void**)&w.sums, sizeof(double) * E) ||
+        !A((void**)&w.mea, sizeof(double) * E) || !A((void**)&w.var, sizeof(double) * E) ||
+        !A((void**)&w.spline, sizeof(double) * 8) || !A((void**)&w.key, sizeof(unsigned long long))) {
+        cudaGetLastError();
+        w.release();
+        return fail(ctx, TOMGPU_ERR_OOM, "alignment workspace allocation failed");
+    }
+    int rc = TOMGPU_OK;
+    cudaError_t e = cudaSuccess;
+    const float cx = (float)((n[0] + 1) / 2), cy = (float)((n[1] + 1) / 2), cz = (float)((n[2] + 1) / 2);
+    do {
+        // mask size and B0 = F(part*mask) (the loop's part = part .* mask)
+        double nmask = 0;
+        {
+            double* d = w.sums;
+            if ((e = count_nonzero(job.mask, nn, d, st))) break;
+            if ((e = cudaMemcpyAsync(&nmask, d, sizeof(double), cudaMemcpyDeviceToHost, st))) break;
+            if ((e = cudaStreamSynchronize(st))) break;
+        }
+        if (nmask < 2) { rc = fail(ctx, TOMGPU_ERR_ARG, "mask needs at least two voxels"); break; }
+        k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(job.part, wedges ? job.mask : nullptr, w.B0, nn);
+        if ((e = c2c3d<float2>(w.B0, n, -1, 1.0, st))) break;
+        k_al_fill<<<grid_for(nn), 256, 0, st>>>(w.cmax, w.amax, nn, -2.f, -2.f);
+        ctx->launches += 5;
+        std::vector<float> mats(18 * (size_t)E);
+        std::vector<int> aid(E);
+        for (int off = 0; off < R && !e; off += E) {
+            const int nb = std::min(E, R - off);
+            for (int q = 0; q < nb; ++q) {
+                const Ang& g = scan[off + q];
+                rotmatrix_as_float(g.phi, g.psi, g.theta, mats.data() + 9 * q);
+                const float eul[3] = {(float)g.phi, (float)g.psi, (float)g.theta};
+                euler_matrix_host(eul, mats.data() + 9 * E + 9 * q);
+                aid[q] = g.idx;
+            }
+            if ((e = cudaMemcpyAsync(w.mats, mats.data(), sizeof(float) * 18 * E, cudaMemcpyHostToDevice, st))) break;
+            if ((e = cudaMemcpyAsync(w.aidx, aid.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st))) break;
+            dim3 g((unsigned)((nn + 255) / 256), nb);
+            k_al_rotate<<<g, 256, 0, st>>>(job.ref, job.wedge_ref, job.mask, w.mats, w.mats + 9 * E, n[0], n[1], n[2],
+                                           cx, cy, cz, wedges ? 1 : 0, w.A, wedges ? w.W : nullptr);
+            ctx->launches += 1;
+            if (wedges) {
+                // a = ref_rot*mask (*) psf_part
+                if ((e = c2c3d_batch(w.A, n, nb, -1, 1.0, st))) break;
+                k_al_wpart<<<grid_for(nn * nb), 256, 0, st>>>(w.A, wpart, n[0], n[1], n[2], nb);
+                if ((e = c2c3d_batch(w.A, n, nb, +1, 1.0 / (double)nn, st))) break;
+                // b = part*mask (*) psf_ref
+                k_al_bside<<<grid_for(nn * nb), 256, 0, st>>>(w.B, w.B0, w.W, n[0], n[1], n[2], nb);
+                if ((e = c2c3d_batch(w.B, n, nb, +1, 1.0 / (double)nn, st))) break;
+                ctx->launches += 2 + 9;
+            } else {
+                // b = part for every entry
+                for (int q = 0; q < nb; ++q)
+                    k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(job.part, nullptr, w.B + (long long)q * nn, nn);
+                ctx->launches += nb;
+            }
+            if ((e = normalize_entries(w.A, job.mask, nn, nb, nmask, w, st, &ctx->launches))) break;
+            if ((e = normalize_entries(w.B, job.mask, nn, nb, nmask, w, st, &ctx->launches))) break;
+            if ((e = c2c3d_batch(w.A, n, nb, -1, 1.0, st))) break;
+            if ((e = c2c3d_batch(w.B, n, nb, -1, 1.0, st))) break;
+            k_al_cross<<<grid_for(nn * nb), 256, 0, st>>>(w.B, w.A, nn * nb);
+            if ((e = c2c3d_batch(w.B, n, nb, +1, 1.0 / (double)nn, st))) break;
+            k_al_update<<<grid_for(nn), 256, 0, st>>>(w.B, n[0], n[1], n[2], nb, 1.0 / nmask, w.aidx, w.cmax, w.amax);
+            e = cudaGetLastError();
+            ctx->launches += 2 + 9;
+        }
+        if (e) break;
+        // first maximum of ccf_max * mask_ccf
+        k_al_mul<<<grid_for(nn), 256, 0, st>>>(w.cmax, job.mask_ccf, w.tmp, nn);
+        if ((e = argmax_key(w.tmp, nn, w.key, st))) break;
+        unsigned long long key = 0;
+        if ((e = cudaMemcpyAsync(&key, w.key, sizeof key, cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaStreamSynchronize(st))) break;
+        if (!key) { rc = fail(ctx, TOMGPU_ERR_DEVICE, "no correlation peak above -99999"); break; }
+        const long long pv = (long long)(0xFFFFFFFFull - (key & 0xFFFFFFFFull));
+        float ai = 0;
+        if ((e = cudaMemcpy(&ai, w.amax + pv, sizeof(float), cudaMemcpyDeviceToHost))) break;
+        // tom_av3_index2angle
+        const int nth = (int)th.size();
+        (void)nth;
+        const double a3 = std::floor(ai / (double)(nph * nps));
+        const double rest = ai - a3 * nph * nps;
+        const double a2 = std::floor(rest / nph);
+        const double a1 = rest - a2 * nph;
+        const float eul[3] = {(float)(a1 * job.phi[1] + job.phi[0]), (float)(a2 * job.psi[1] + job.psi[0]),
+                              (float)(a3 * job.theta[1] + job.theta[0])};
+        // ccf_s = tom_corr(rot(ref, angles), part, 'norm', mask)
+        float em[9];
+        euler_matrix_host(eul, em);
+        if ((e = cudaMemcpyAsync(w.mats, em, sizeof em, cudaMemcpyHostToDevice, st))) break;
+        int zero = 0;
+        if ((e = cudaMemcpyAsync(w.aidx, &zero, sizeof zero, cudaMemcpyHostToDevice, st))) break;
+        k_al_rotate<<<dim3((unsigned)((nn + 255) / 256), 1), 256, 0, st>>>(job.ref, nullptr, job.mask, w.mats, nullptr,
+                                                                            n[0], n[1], n[2], cx, cy, cz, 0, w.A,
+                                                                            nullptr);
+        k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(job.part, wedges ? job.mask : nullptr, w.B, nn);
+        if ((e = normalize_entries(w.A, job.mask, nn, 1, nmask, w, st, &ctx->launches))) break;
+        if ((e = normalize_entries(w.B, job.mask, nn, 1, nmask, w, st, &ctx->launches))) break;
+        if ((e = c2c3d<float2>(w.A, n, -1, 1.0, st))) break;
+        if ((e = c2c3d<float2>(w.B, n, -1, 1.0, st))) break;
+        k_al_cross<<<grid_for(nn), 256, 0, st>>>(w.B, w.A, nn);
+        if ((e = c2c3d<float2>(w.B, n, +1, 1.0 / (double)nn, st))) break;
+        k_al_map<<<grid_for(nn), 256, 0, st>>>(w.B, n[0], n[1], n[2], 1.0 / nmask, job.mask_ccf, w.tmp);
+        if ((e = argmax_key(w.tmp, nn, w.key, st))) break;
+        if ((e = cudaMemcpyAsync(&key, w.key, sizeof key, cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaStreamSynchronize(st))) break;
+        ctx->launches += 16;
+        if (!key) { rc = fail(ctx, TOMGPU_ERR_DEVICE, "no refinement peak above -99999"); break; }
+        const long long pv2 = (long long)(0xFFFFFFFFull - (key & 0xFFFFFFFFull));
+        const int p0[3] = {(int)(pv2 % n[0]), (int)((pv2 / n[0]) % n[1]), (int)(pv2 / ((long long)n[0] * n[1]))};
+        if ((e = spline_peak(w.tmp, n, p0, w.spline, st))) break;
+        double h[6];
+        if ((e = cudaMemcpyAsync(h, w.spline, sizeof h, cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaStreamSynchronize(st))) break;
+        for (int d = 0; d < 3; ++d) {
+            angles_out[d] = eul[d];
+            shifts_out[d] = (float)(h[d] - (std::floor(n[d] / 2.0) + 1.0));
+        }
+        *peak_out = (float)std::fmax(h[3], std::fmax(h[4], h[5]));
+    } while (0);
+    if (e && !rc) rc = cuda_fail(ctx, e, "av3_align");
+    w.release();
+    return rc;
+}
+
+}  // namespace tg

@@ -600,6 +600,26 @@ int tomgpu_match_stats_dev(tomgpu_match_plan* plan, float* mean, float* std) {
     return TOMGPU_OK;
 }
 
+int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs, float* angles, float* shifts,
+                         float* ccf_peak) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (n_jobs < 0 || (n_jobs > 0 && (!jobs || !angles || !shifts || !ccf_peak)))
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer or negative job count");
+    TG_TRY(use_device(ctx));
+    for (int j = 0; j < n_jobs; ++j) {
+        const tomgpu_align_job& jb = jobs[j];
+        if (!dims_ok(jb.n)) return fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad box size");
+        for (int a = 0; a < 3; ++a) {
+            const float* r = a == 0 ? jb.phi : (a == 1 ? jb.psi : jb.theta);
+            if (r[1] < 0 || (r[1] == 0 && r[2] != r[0]) || r[2] < r[0])
+                return fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad angle range");
+        }
+        const int rc = align_job(ctx, jb, angles + 3 * j, shifts + 3 * j, ccf_peak + j, (size_t)1 << 24);
+        if (rc) return rc;
+    }
+    return TOMGPU_OK;
+}
+
 int tomgpu_match(tomgpu_ctx* ctx, const float* tomo, const int vol[3], const float* tmpl, const int tm[3],
                  const float* mask, const float* psf, const float* eulers, int R, const tomgpu_match_params* params,
                  float* maxcc, int32_t* angidx) {

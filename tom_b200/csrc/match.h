@@ -69,6 +69,9 @@ struct MatchPlan {
     int rescore(const float* vol, const float* eulers, const int* pos1, int K, double* out);
 };
 
+int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3],
+              float* peak_out, size_t budget_voxels);
+
 }  // namespace tg
 
 struct tomgpu_match_plan {

@@ -1,0 +1,49 @@
+// rot3d's per-voxel sampling (Sptrans/tom_rotatec.c:291-399) as an inline
+// device function, shared by the rotation and alignment kernels.  Explicit
+// round-to-nearest intrinsics keep the float operation order of the
+// reference, so results are bit-identical to rot3d.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace tg {
+
+__device__ __forceinline__ float rot_sample(const float* __restrict__ in, int sx, int sy, int sz,
+                                            const float* m, float px, float py, float pz, int i,
+                                            int j, int k) {
+    const float di = (float)(long long)__fsub_rn((float)i, px);
+    const float dj = (float)(long long)__fsub_rn((float)j, py);
+    const float dk = (float)(long long)__fsub_rn((float)k, pz);
+    const float rx = __fadd_rn(__fadd_rn(__fadd_rn(px, __fmul_rn(m[0], di)), __fmul_rn(m[1], dj)),
+                               __fmul_rn(m[2], dk));
+    if (rx < 0.f || rx > (float)(sx - 1)) return 0.f;
+    const float ry = __fadd_rn(__fadd_rn(__fadd_rn(py, __fmul_rn(m[3], di)), __fmul_rn(m[4], dj)),
+                               __fmul_rn(m[5], dk));
+    if (ry < 0.f || ry > (float)(sy - 1)) return 0.f;
+    const float rz = __fadd_rn(__fadd_rn(__fadd_rn(pz, __fmul_rn(m[6], di)), __fmul_rn(m[7], dj)),
+                               __fmul_rn(m[8], dk));
+    if (rz < 0.f || rz > (float)(sz - 1)) return 0.f;
+    const int fx = (int)rx, fy = (int)ry, fz = (int)rz;
+    const float wx = __fsub_rn(rx, (float)fx), wy = __fsub_rn(ry, (float)fy), wz = __fsub_rn(rz, (float)fz);
+    const float ux = __fsub_rn(1.f, wx), uy = __fsub_rn(1.f, wy), uz = __fsub_rn(1.f, wz);
+    const long long sxy = (long long)sx * sy;
+    const long long b = fx + (long long)fy * sx + (long long)fz * sxy;
+    const bool ex = fx == sx - 1, ey = fy == sy - 1, ez = fz == sz - 1;
+    const float v000 = __ldg(in + b);
+    const float v100 = ex ? 0.f : __ldg(in + b + 1);
+    const float v010 = ey ? 0.f : __ldg(in + b + sx);
+    const float v110 = (ex || ey) ? 0.f : __ldg(in + b + sx + 1);
+    const float v001 = ez ? 0.f : __ldg(in + b + sxy);
+    const float v101 = (ex || ez) ? 0.f : __ldg(in + b + sxy + 1);
+    const float v011 = (ey || ez) ? 0.f : __ldg(in + b + sxy + sx);
+    const float v111 = (ex || ey || ez) ? 0.f : __ldg(in + b + sxy + sx + 1);
+    const float a = __fadd_rn(v000, __fmul_rn(__fsub_rn(v100, v000), wx));
+    const float bb = __fadd_rn(__fmul_rn(v010, ux), __fmul_rn(v110, wx));
+    const float c = __fadd_rn(__fmul_rn(v001, ux), __fmul_rn(v101, wx));
+    const float d = __fadd_rn(__fmul_rn(v011, ux), __fmul_rn(v111, wx));
+    const float lo = __fadd_rn(__fmul_rn(a, uy), __fmul_rn(bb, wy));
+    const float hi = __fadd_rn(__fmul_rn(c, uy), __fmul_rn(d, wy));
+    return __fadd_rn(__fmul_rn(lo, uz), __fmul_rn(hi, wz));
+}
+
+
+}  // namespace tg

@@ -605,3 +605,64 @@ def tom_os3_corr(img, template, options=None, ctx: Context | None = None):
     plan.corr(to_device(t, ctx.device), out)
     ctx.synchronize()
     return np.asfortranarray(from_device(out)), options
+
+
+# ------------------------------------------------------ subtomogram alignment
+
+def tom_spheremask_default(shape):
+    """tom_spheremask(ones(n)) with the default radius floor((min(n)-1)/2) (Geom/tom_spheremask.m:41-67)."""
+    shape = tuple(shape)
+    radius = np.floor((min(shape) - 1) / 2)
+    center = [np.floor(s / 2) + 1 for s in shape]
+    g = np.meshgrid(*[np.arange(s, dtype=np.float64) for s in shape], indexing="ij")
+    d = np.sqrt(sum((gi + 1 - c) ** 2 for gi, c in zip(g, center)))
+    m = np.ones(shape, np.float32)
+    m[d >= radius] = 0
+    return m
+
+
+def av3_align_batch(jobs, ctx: Context | None = None):
+    """Run tom_av3_align jobs on the GPU.  Each job is a dict with numpy
+    volumes 'ref', 'part', 'mask' (None: tom_spheremask default), 'mask_ccf'
+    (None: ones), 'wedge_ref', 'wedge_part' (None: no wedges / same as
+    wedge_ref) and angle ranges 'phi', 'psi', 'theta' ([start incr end]).
+    Returns (angles[n,3], shifts[n,3], ccf_peak[n])."""
+    import torch
+    ctx = ctx or default_context()
+    arr = (_lib.AlignJob * len(jobs))()
+    keep = []
+    for j, jb in enumerate(jobs):
+        ref = np.asarray(jb["ref"], np.float32)
+        n = ref.shape
+        mask = jb.get("mask")
+        mask = tom_spheremask_default(n) if mask is None else mask
+        dev = lambda a: None if a is None else to_device(np.asarray(a, np.float32), ctx.device)
+        t = dict(ref=dev(ref), part=dev(jb["part"]), mask=dev(mask), mask_ccf=dev(jb.get("mask_ccf")),
+                 wedge_ref=dev(jb.get("wedge_ref")), wedge_part=dev(jb.get("wedge_part")))
+        keep.append(t)
+        arr[j].n = (ctypes.c_int * 3)(*n)
+        for k in ("ref", "part", "mask", "mask_ccf", "wedge_ref", "wedge_part"):
+            setattr(arr[j], k, t[k].data_ptr() if t[k] is not None else None)
+        arr[j].phi = (ctypes.c_float * 3)(*jb["phi"])
+        arr[j].psi = (ctypes.c_float * 3)(*jb["psi"])
+        arr[j].theta = (ctypes.c_float * 3)(*jb["theta"])
+    angles = np.zeros((len(jobs), 3), np.float32)
+    shifts = np.zeros((len(jobs), 3), np.float32)
+    peaks = np.zeros(len(jobs), np.float32)
+    ctx.check(lib().tomgpu_av3_align_dev(ctx.handle, arr, len(jobs), angles.ctypes.data_as(_lib.c_float_p),
+                                         shifts.ctypes.data_as(_lib.c_float_p), peaks.ctypes.data_as(_lib.c_float_p)))
+    torch.cuda.synchronize(ctx.device)
+    return angles, shifts, peaks
+
+
+def tom_av3_align(ref, part, phi, psi, theta, mask=None, filter=None, mask_ccf=None, wedge_ref=None,
+                  wedge_part=None, ctx: Context | None = None):
+    """[angles shifts ccf_peak] = tom_av3_align(ref,part,phi,psi,theta,mask,filter,mask_ccf,wedge_ref,wedge_part)
+    (av3_new/tom_av3_align.m) on the GPU; filter must be absent or have Apply = 0."""
+    if filter is not None and getattr(filter, "Apply", filter.get("Apply", 0) if isinstance(filter, dict) else 0):
+        raise ValueError("tom_av3_align on the GPU supports filter.Apply = 0 only")
+    if wedge_ref is not None and wedge_part is None:
+        wedge_part = wedge_ref  # the 8-argument form
+    a, s, p = av3_align_batch([dict(ref=ref, part=part, phi=phi, psi=psi, theta=theta, mask=mask,
+                                    mask_ccf=mask_ccf, wedge_ref=wedge_ref, wedge_part=wedge_part)], ctx)
+    return a[0], s[0], float(p[0])
