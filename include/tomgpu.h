@@ -238,6 +238,15 @@ int tomgpu_match(tomgpu_ctx* ctx, const float* tomo, const int vol_dims[3], cons
                  const int tmpl_dims[3], const float* mask, const float* psf, const float* eulers,
                  int R, const tomgpu_match_params* params, float* maxcc, int32_t* angidx);
 
+/* ccf = tom_corr(a, b [, 'norm', mask [, psf1, psf2]]) (Analysis/tom_corr.m:51-121)
+ * on device buffers of size dims: mask == NULL gives the plain form
+ * real(fftshift(ifftn(F(b) conj F(a))))/numel; with a mask, a and b are first
+ * normalised inside it (norm_inside_mask: mean over the mask, std with n - 1)
+ * and the result is divided by the mask size; with psfs, a is convolved with
+ * psf2 and b with psf1 before normalising (cross-wedging). */
+int tomgpu_corr_dev(tomgpu_ctx* ctx, const float* a_dev, const float* b_dev, const int dims[3],
+                    const float* mask_dev, const float* psf1_dev, const float* psf2_dev, float* ccf_dev);
+
 /* ------------------------------------------------- subtomogram alignment --- */
 /* One alignment job of tom_av3_align (av3_new/tom_av3_align.m:1-189) with
  * filter.Apply = 0.  All volumes are device buffers of size n (x fastest).

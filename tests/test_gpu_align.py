@@ -78,3 +78,27 @@ def test_av3_align_batch_mixed_sizes(gpu, oracle):
         assert np.allclose(angles[k], expect[k]), (k, angles[k], expect[k])
         assert np.abs(shifts[k] - np.array([0, 1, -1])).max() < 0.6
         assert peaks[k] > 0.5
+
+
+@pytest.mark.parametrize("form", ["plain", "mask", "psf"])
+def test_tom_corr_forms(gpu, oracle, form):
+    rng = np.random.default_rng(61)
+    n = (32, 24, 40)
+    a = rng.standard_normal(n)
+    b = np.roll(a, (2, -1, 3), axis=(0, 1, 2)) + 0.2 * rng.standard_normal(n)
+    if form == "plain":
+        ref = np.real(np.fft.fftshift(np.fft.ifftn(np.fft.fftn(b) * np.conj(np.fft.fftn(a))))) / a.size
+        got = gpu.tom_corr(a, b)
+    else:
+        mask = oracle.sphere_mask(n, 10).astype(np.float32)
+        if form == "mask":
+            ref = oracle.tom_corr_norm(a.astype(np.float32), b.astype(np.float32), mask)
+            got = gpu.tom_corr(a, b, "norm", mask)
+        else:
+            w = oracle.av3_wedge(n, -50, 50)
+            p1 = np.real(np.fft.ifftn(np.fft.ifftshift(w)))
+            p2 = np.real(np.fft.ifftn(np.fft.ifftshift(oracle.av3_wedge(n, -60, 45))))
+            ref = oracle.tom_corr_norm(a.astype(np.float32), b.astype(np.float32), mask, p1.astype(np.float32),
+                                       p2.astype(np.float32))
+            got = gpu.tom_corr(a, b, "norm", mask, p1, p2)
+    assert np.abs(got - ref).max() <= 1e-4 * np.abs(ref).max()

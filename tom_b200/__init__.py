@@ -23,6 +23,7 @@ from .tom import (  # noqa: F401
     tom_av3_angle_grid,
     tom_av3_index2angle,
     tom_calc_weight_functioninc,
+    tom_corr,
     tom_fourier,
     tom_ifourier,
     tom_os3_angleList,

@@ -91,6 +91,8 @@ _SIGS = {
     "tomgpu_match_rescore_fp64_dev": (ctypes.c_int, [c_void_p, c_void_p, c_float_p, c_int_p, ctypes.c_int,
                                                      c_double_p]),
     "tomgpu_match_stats_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    "tomgpu_corr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int_p, c_void_p, c_void_p, c_void_p,
+                                       c_void_p]),
     "tomgpu_av3_align_dev": (ctypes.c_int, [c_void_p, ctypes.POINTER(AlignJob), ctypes.c_int, c_float_p, c_float_p,
                                             c_float_p]),
     "tomgpu_match": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p, c_void_p, c_float_p,

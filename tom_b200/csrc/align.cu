@@ -264,6 +264,87 @@ static cudaError_t normalize_entries(float2* X, const float* mask, long long nn,
     return e;
 }
 
+namespace {
+__global__ void k_cmul(float2* __restrict__ a, const float2* __restrict__ b, long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        a[t] = cmul(a[t], b[t]);
+}
+__global__ void k_re_keep(float2* __restrict__ a, long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        a[t].y = 0.f;
+}
+}  // namespace
+
+// tom_corr (Analysis/tom_corr.m:51-95): mode 0 plain ccf / numel, mode 1 'norm'
+// with mask (norm_inside_mask, n - 1 std) and optional psfs (a (*) psf2,
+// b (*) psf1 first).  All device buffers of size n; out real.
+int corr_norm(tomgpu_ctx* ctx, const float* a, const float* b, const int n[3], const float* mask, const float* psf1,
+              const float* psf2, float* out) {
+    const long long nn = (long long)n[0] * n[1] * n[2];
+    cudaStream_t st = ctx->stream;
+    for (int d = 0; d < 3; ++d)
+        if (n[d] > 1 && !fft_length_supported(n[d])) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "size not an FFT length");
+    if ((psf1 == nullptr) != (psf2 == nullptr)) return fail(ctx, TOMGPU_ERR_ARG, "give both psfs or none");
+    if (psf1 && !mask) return fail(ctx, TOMGPU_ERR_ARG, "the psf form needs a mask");
+    float2 *A = nullptr, *B = nullptr, *P = nullptr;
+    double *sums = nullptr, *mea = nullptr, *var = nullptr;
+    auto cleanup = [&]() {
+        void* p[] = {A, B, P, sums, mea, var};
+        for (void* q : p)
+            if (q) cudaFree(q);
+    };
+    if (cudaMalloc(&A, sizeof(float2) * nn) || cudaMalloc(&B, sizeof(float2) * nn) ||
+        (psf1 && cudaMalloc(&P, sizeof(float2) * nn)) || cudaMalloc(&sums, 8) || cudaMalloc(&mea, 8) ||
+        cudaMalloc(&var, 8)) {
+        cudaGetLastError();
+        cleanup();
+        return fail(ctx, TOMGPU_ERR_OOM, "tom_corr workspace");
+    }
+    cudaError_t e = cudaSuccess;
+    int rc = TOMGPU_OK;
+    double nmask = (double)nn;
+    do {
+        k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(a, nullptr, A, nn);
+        k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(b, nullptr, B, nn);
+        if (psf1) {
+            // a <- a (*) psf2, b <- b (*) psf1 (real parts kept)
+            if ((e = c2c3d<float2>(A, n, -1, 1.0, st))) break;
+            k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(psf2, nullptr, P, nn);
+            if ((e = c2c3d<float2>(P, n, -1, 1.0, st))) break;
+            k_cmul<<<grid_for(nn), 256, 0, st>>>(A, P, nn);
+            if ((e = c2c3d<float2>(A, n, +1, 1.0 / (double)nn, st))) break;
+            k_re_keep<<<grid_for(nn), 256, 0, st>>>(A, nn);
+            if ((e = c2c3d<float2>(B, n, -1, 1.0, st))) break;
+            k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(psf1, nullptr, P, nn);
+            if ((e = c2c3d<float2>(P, n, -1, 1.0, st))) break;
+            k_cmul<<<grid_for(nn), 256, 0, st>>>(B, P, nn);
+            if ((e = c2c3d<float2>(B, n, +1, 1.0 / (double)nn, st))) break;
+            k_re_keep<<<grid_for(nn), 256, 0, st>>>(B, nn);
+            ctx->launches += 6 + 18;
+        }
+        if (mask) {
+            if ((e = count_nonzero(mask, nn, sums, st))) break;
+            if ((e = cudaMemcpyAsync(&nmask, sums, 8, cudaMemcpyDeviceToHost, st))) break;
+            if ((e = cudaStreamSynchronize(st))) break;
+            if (nmask < 2) { rc = fail(ctx, TOMGPU_ERR_ARG, "mask needs at least two voxels"); break; }
+            Workspace w;
+            w.sums = sums; w.mea = mea; w.var = var;
+            if ((e = normalize_entries(A, mask, nn, 1, nmask, w, st, &ctx->launches))) break;
+            if ((e = normalize_entries(B, mask, nn, 1, nmask, w, st, &ctx->launches))) break;
+        }
+        if ((e = c2c3d<float2>(A, n, -1, 1.0, st))) break;
+        if ((e = c2c3d<float2>(B, n, -1, 1.0, st))) break;
+        k_al_cross<<<grid_for(nn), 256, 0, st>>>(B, A, nn);
+        if ((e = c2c3d<float2>(B, n, +1, 1.0 / (double)nn, st))) break;
+        k_al_map<<<grid_for(nn), 256, 0, st>>>(B, n[0], n[1], n[2], 1.0 / nmask, nullptr, out);
+        e = cudaGetLastError();
+        ctx->launches += 2 + 9 + 2;
+    } while (0);
+    if (e && !rc) rc = cuda_fail(ctx, e, "tom_corr");
+    cleanup();
+    return rc;
+}
+
 int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3], float* peak_out,
               size_t budget_voxels) {
     const int* n = job.n;

@@ -600,6 +600,14 @@ int tomgpu_match_stats_dev(tomgpu_match_plan* plan, float* mean, float* std) {
     return TOMGPU_OK;
 }
 
+int tomgpu_corr_dev(tomgpu_ctx* ctx, const float* a, const float* b, const int dims[3], const float* mask,
+                    const float* psf1, const float* psf2, float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!a || !b || !out || !dims_ok(dims)) return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
+    TG_TRY(use_device(ctx));
+    return corr_norm(ctx, a, b, dims, mask, psf1, psf2, out);
+}
+
 int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs, float* angles, float* shifts,
                          float* ccf_peak) {
     if (!ctx) return TOMGPU_ERR_ARG;

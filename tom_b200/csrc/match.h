@@ -69,6 +69,8 @@ struct MatchPlan {
     int rescore(const float* vol, const float* eulers, const int* pos1, int K, double* out);
 };
 
+int corr_norm(tomgpu_ctx* ctx, const float* a, const float* b, const int n[3], const float* mask, const float* psf1,
+              const float* psf2, float* out);
 int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3],
               float* peak_out, size_t budget_voxels);
 

@@ -158,3 +158,46 @@ CONFIGS = {
     "exhaustive_512x512x256": dict(N=(512, 512, 256), T=40, n_copies=40, n_blobs=8, rho=16, snr=0.1,
                                    max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
 }
+
+
+def make_align_particles(n_particles, seed, sizes=(32, 48, 64, 80, 96), snr=0.05, tilt=(45.0, 65.0),
+                         search_half=15.0, search_step=3.0, max_shift=4):
+    """Subtomogram-alignment workload: each particle a copy of a 6-blob phantom
+    (rendered at its box size) at a seeded Euler, shifted by up to max_shift
+    voxels, plus Gaussian noise at the given SNR, with its own +-tilt missing
+    wedge; the scan covers +-search_half degrees around a seeded start
+    orientation near the truth.  Returns a list of job dicts for
+    tom_b200.av3_align_batch plus the true Eulers and shifts."""
+    rng = np.random.default_rng(seed)
+    jobs, truth = [], []
+    phantoms = {}
+    for p in range(n_particles):
+        n = int(rng.choice(sizes))
+        if n not in phantoms:
+            phantoms[n] = BlobPhantom(np.random.default_rng(seed * 1000 + n), 6, n / 4)
+        ph = phantoms[n]
+        ref = ph.template(n)
+        # true orientation on the scan grid around a seeded start
+        start = np.array([rng.uniform(30, 300), rng.uniform(30, 300), rng.uniform(30, 150)]).round()
+        k = rng.integers(-int(search_half // search_step), int(search_half // search_step) + 1, 3)
+        true_e = start + k * search_step
+        sh = rng.integers(-max_shift, max_shift + 1, 3)
+        part = np.zeros((n, n, n), np.float32, order="F")
+        c = [np.ceil(n / 2) + d for d in sh]
+        ph.render((n, n, n), c, true_e, out=part)
+        var_s = float(np.var(ref[ref > 0.05 * ref.max()])) if ref.max() > 0 else 1.0
+        part = part * np.float32(np.sqrt(snr / var_s)) + rng.standard_normal((n, n, n)).astype(np.float32)
+        a = rng.uniform(*tilt)
+        g = np.meshgrid(*[np.arange(-(n // 2), n - n // 2)] * 3, indexing="ij")
+        with np.errstate(divide="ignore", invalid="ignore"):
+            r = np.abs(g[0]) / np.abs(g[2])
+        w = np.ones((n, n, n), np.float32)
+        w[np.tan(np.deg2rad(90 - a)) > r] = 0
+        part = np.real(np.fft.ifftn(np.fft.fftn(part) * np.fft.ifftshift(w))).astype(np.float32)
+        mask = sphere_mask(n, n / 2 - 2)
+        mccf = sphere_mask(n, max_shift + 1)
+        rngs = [(float(s0 - search_half), float(search_step), float(s0 + search_half)) for s0 in start]
+        jobs.append(dict(ref=ref, part=np.asfortranarray(part), mask=mask, mask_ccf=mccf, wedge_ref=w,
+                         wedge_part=w, phi=rngs[0], psi=rngs[1], theta=rngs[2]))
+        truth.append((true_e, sh))
+    return jobs, truth

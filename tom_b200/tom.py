@@ -621,6 +621,31 @@ def tom_spheremask_default(shape):
     return m
 
 
+def tom_corr(a, b, *args, ctx: Context | None = None):
+    """ccf = tom_corr(a, b) | tom_corr(a, b, 'norm', mask) | tom_corr(a, b, 'norm', mask, psf1, psf2)
+    (Analysis/tom_corr.m) on the GPU; returns a float32 volume [x, y, z]."""
+    import torch
+    ctx = ctx or default_context()
+    A = np.asarray(a, np.float32)
+    mask = psf1 = psf2 = None
+    if args:
+        if args[0] != "norm":
+            raise ValueError("only the 'norm' flag is implemented")
+        if len(args) not in (2, 4):
+            raise ValueError("tom_corr(a, b, 'norm', mask[, psf1, psf2])")
+        mask = args[1]
+        if len(args) == 4:
+            psf1, psf2 = args[2], args[3]
+    dev = lambda x: None if x is None else to_device(np.asarray(x, np.float32), ctx.device)
+    ta, tb_, tm, p1, p2 = dev(A), dev(b), dev(mask), dev(psf1), dev(psf2)
+    out = torch.empty_like(ta)
+    ptr = lambda t: _tptr(t) if t is not None else None
+    ctx.check(lib().tomgpu_corr_dev(ctx.handle, _tptr(ta), _tptr(tb_), _cdims(A.shape), ptr(tm), ptr(p1), ptr(p2),
+                                    _tptr(out)))
+    ctx.synchronize()
+    return np.asfortranarray(from_device(out))
+
+
 def av3_align_batch(jobs, ctx: Context | None = None):
     """Run tom_av3_align jobs on the GPU.  Each job is a dict with numpy
     volumes 'ref', 'part', 'mask' (None: tom_spheremask default), 'mask_ccf'
