@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256) k_inv_z_b256(const float2* __restrict__ Q
     }
 }
 
-constexpr int C2R_STAGES = 4;
+constexpr int C2R_STAGES = 3;
 
 TG_D void cp_async8(void* smem_dst, const void* gsrc, int bytes) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -116,12 +116,21 @@ TG_D void cp_async8(void* smem_dst, const void* gsrc, int bytes) {
 TG_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> TG_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Running maximum without per-voxel coefficients: with gamma >= 0 and
+// mu0 mu_T fixed per voxel, cc_b = (u_b - mu0 mu_T) gamma is a non-decreasing
+// function of u_b = out_b/(N M) + kappa_b, so the batch keeps the best u and
+// its rotation and applies the FLCF formula once, at the read-modify-write.
+// (Rotations whose cc round to the same float but whose u differ may pick a
+// later index than the strict first-wins scan; such voxels have no CC
+// separation between those angles.  gamma = 0 voxels keep the reference's
+// value 0 with the batch's first rotation.)
 template <int NH>
-__global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, const float* __restrict__ mu0,
-                                               const float* __restrict__ gam, const double* __restrict__ tsum, int Ny,
-                                               int Nz, int nb, float inv_nm, double c_mean, double inv_m, double mu_t,
-                                               int index0, float* __restrict__ maxcc, int* __restrict__ angidx,
-                                               const float2* __restrict__ tw_h, const float2* __restrict__ tw_x) {
+__global__ void __launch_bounds__(256, 3) k_c2r_w(const float2* __restrict__ H, const float* __restrict__ mu0,
+                                                  const float* __restrict__ gam, const double* __restrict__ tsum,
+                                                  int Ny, int Nz, int nb, float inv_nm, double c_mean, double inv_m,
+                                                  double mu_t, int index0, float* __restrict__ maxcc,
+                                                  int* __restrict__ angidx, const float2* __restrict__ tw_h,
+                                                  const float2* __restrict__ tw_x) {
     constexpr int YT = 8, NH1 = NH + 1, TS = NH + 2, EPT = NH / 32, NX = 2 * NH, NSTG = C2R_STAGES;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* tile = reinterpret_cast<float2*>(smem_raw);  // [NSTG][YT][TS]
@@ -133,21 +142,12 @@ __global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, 
     const int y0 = blockIdx.x * YT, z = blockIdx.y, y = y0 + warp;
     const bool yok = y < Ny;
     const long long nh1l = NH1;
-    const float mt = (float)mu_t;
-    float m0[EPT][2], g0[EPT][2], bm[EPT][2];
-    int bi[EPT][2];
+    float bu[EPT][2];
+    int bb[EPT][2];
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
-        bm[i][0] = bm[i][1] = -INFINITY;
-        bi[i][0] = bi[i][1] = -1;
-        m0[i][0] = m0[i][1] = g0[i][0] = g0[i][1] = 0.f;
-        if (yok) {
-            const long long v = ((long long)z * Ny + y) * NX + 2 * tgwfft::out_pos<NH>(i, lane);
-            const float2 a = *reinterpret_cast<const float2*>(mu0 + v);
-            const float2 g = *reinterpret_cast<const float2*>(gam + v);
-            m0[i][0] = a.x; m0[i][1] = a.y;
-            g0[i][0] = g.x; g0[i][1] = g.y;
-        }
+        bu[i][0] = bu[i][1] = -INFINITY;
+        bb[i][0] = bb[i][1] = 0;
     }
     tgwfft::stage_table(twh, tw_h, NH);
     tgwfft::stage_table(twx, tw_x, NX);
@@ -191,22 +191,28 @@ __global__ void __launch_bounds__(256, 2) k_c2r_w(const float2* __restrict__ H, 
         const float kap = kaps[b];
 #pragma unroll
         for (int i = 0; i < EPT; ++i) {
-            const float c0 = (fmaf(v[i].x, inv_nm, -m0[i][0] * mt) + kap) * g0[i][0];
-            const float c1 = (fmaf(v[i].y, inv_nm, -m0[i][1] * mt) + kap) * g0[i][1];
-            if (c0 > bm[i][0]) { bm[i][0] = c0; bi[i][0] = index0 + b; }
-            if (c1 > bm[i][1]) { bm[i][1] = c1; bi[i][1] = index0 + b; }
+            const float u0 = fmaf(v[i].x, inv_nm, kap);
+            const float u1 = fmaf(v[i].y, inv_nm, kap);
+            if (u0 > bu[i][0]) { bu[i][0] = u0; bb[i][0] = b; }
+            if (u1 > bu[i][1]) { bu[i][1] = u1; bb[i][1] = b; }
         }
         __syncthreads();
     }
     if (!yok) return;
+    const float mt = (float)mu_t;
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
         const long long v = ((long long)z * Ny + y) * NX + 2 * tgwfft::out_pos<NH>(i, lane);
+        const float2 a = *reinterpret_cast<const float2*>(mu0 + v);
+        const float2 g = *reinterpret_cast<const float2*>(gam + v);
         float2 cur = *reinterpret_cast<float2*>(maxcc + v);
         int2 ci = *reinterpret_cast<int2*>(angidx + v);
         bool ch = false;
-        if (bm[i][0] > cur.x) { cur.x = bm[i][0]; ci.x = bi[i][0]; ch = true; }
-        if (bm[i][1] > cur.y) { cur.y = bm[i][1]; ci.y = bi[i][1]; ch = true; }
+        const float c0 = g.x != 0.f ? (bu[i][0] - a.x * mt) * g.x : 0.f;
+        const float c1 = g.y != 0.f ? (bu[i][1] - a.y * mt) * g.y : 0.f;
+        const int b0 = g.x != 0.f ? bb[i][0] : 0, b1 = g.y != 0.f ? bb[i][1] : 0;
+        if (c0 > cur.x) { cur.x = c0; ci.x = index0 + b0; ch = true; }
+        if (c1 > cur.y) { cur.y = c1; ci.y = index0 + b1; ch = true; }
         if (ch) {
             *reinterpret_cast<float2*>(maxcc + v) = cur;
             *reinterpret_cast<int2*>(angidx + v) = ci;
