@@ -26,13 +26,14 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_w(const float2* __restrict__ 
                                                      const float2* __restrict__ tw_g) {
     constexpr int EPT = NY / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2* tw = reinterpret_cast<float2*>(smem_raw);  // [NY] twiddles
-    float2* xb = tw + NY;                               // [8][NY] exchange
+    float2* tw = reinterpret_cast<float2*>(smem_raw);  // [NY] stage tables
+    float2* xb = tw + NY + 64;                          // [8][NY] exchange
     float2* fs = xb + 8 * NY;                           // [8][NY] F_I columns
     float2* zs = fs + 8 * NY;                           // [8][2][64] template column, double buffered
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const long long col = (long long)blockIdx.x * 8 + warp;
-    tgwfft::stage_table(tw, tw_g, NY);
+    static_assert(tgwfft::WTab<NY>::size <= NY + 64, "stage tables exceed their slot");
+    tgwfft::build_stage_tables<NY>(tw, tw_g);
     float2* buf = xb + warp * NY;
     float2* fw = fs + warp * NY;
     float2* zw = zs + warp * 128;
@@ -135,8 +136,8 @@ __global__ void __launch_bounds__(256, 3) k_c2r_w(const float2* __restrict__ H, 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* tile = reinterpret_cast<float2*>(smem_raw);  // [NSTG][YT][TS]
     float2* xbuf = tile + NSTG * YT * TS;                 // [8][NH]
-    float2* twh = xbuf + 8 * NH;                          // [NH]
-    float2* twx = twh + NH;                               // [NX]
+    float2* twh = xbuf + 8 * NH;                          // [NH + 64] stage tables
+    float2* twx = twh + NH + 64;                          // [NX]
     float* kaps = reinterpret_cast<float*>(twx + NX);    // [nb]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int y0 = blockIdx.x * YT, z = blockIdx.y, y = y0 + warp;
@@ -149,7 +150,8 @@ __global__ void __launch_bounds__(256, 3) k_c2r_w(const float2* __restrict__ H, 
         bu[i][0] = bu[i][1] = -INFINITY;
         bb[i][0] = bb[i][1] = 0;
     }
-    tgwfft::stage_table(twh, tw_h, NH);
+    static_assert(tgwfft::WTab<NH>::size <= NH + 64, "stage tables exceed their slot");
+    tgwfft::build_stage_tables<NH>(twh, tw_h);
     tgwfft::stage_table(twx, tw_x, NX);
     for (int b = threadIdx.x; b < nb; b += blockDim.x) kaps[b] = (float)(c_mean * (tsum[b] * inv_m - mu_t));
     auto issue = [&](int b, int which) {
@@ -200,13 +202,25 @@ __global__ void __launch_bounds__(256, 3) k_c2r_w(const float2* __restrict__ H, 
     }
     if (!yok) return;
     const float mt = (float)mu_t;
+    // every load of the read-modify-write first, then the stores (the loads
+    // would otherwise wait behind stores the compiler cannot disambiguate)
+    float2 av[EPT], gv[EPT], cv[EPT];
+    int2 iv[EPT];
+    const long long row = ((long long)z * Ny + y) * NX;
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
-        const long long v = ((long long)z * Ny + y) * NX + 2 * tgwfft::out_pos<NH>(i, lane);
-        const float2 a = *reinterpret_cast<const float2*>(mu0 + v);
-        const float2 g = *reinterpret_cast<const float2*>(gam + v);
-        float2 cur = *reinterpret_cast<float2*>(maxcc + v);
-        int2 ci = *reinterpret_cast<int2*>(angidx + v);
+        const long long v = row + 2 * tgwfft::out_pos<NH>(i, lane);
+        av[i] = __ldg(reinterpret_cast<const float2*>(mu0 + v));
+        gv[i] = __ldg(reinterpret_cast<const float2*>(gam + v));
+        cv[i] = *reinterpret_cast<const float2*>(maxcc + v);
+        iv[i] = *reinterpret_cast<const int2*>(angidx + v);
+    }
+#pragma unroll
+    for (int i = 0; i < EPT; ++i) {
+        const long long v = row + 2 * tgwfft::out_pos<NH>(i, lane);
+        const float2 a = av[i], g = gv[i];
+        float2 cur = cv[i];
+        int2 ci = iv[i];
         bool ch = false;
         const float c0 = g.x != 0.f ? (bu[i][0] - a.x * mt) * g.x : 0.f;
         const float c1 = g.y != 0.f ? (bu[i][1] - a.y * mt) * g.y : 0.f;
@@ -228,7 +242,7 @@ bool fast_c2r(int NH) { return NH == 128 || NH == 256; }
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
                                long long ncols, int nb, cudaStream_t st) {
     const unsigned g = (unsigned)((ncols + 7) / 8);
-    const size_t smem = sizeof(float2) * (NY * 17 + 8 * 128);
+    const size_t smem = sizeof(float2) * (NY * 17 + 64 + 8 * 128);
     if (NY == 512) {
         cudaFuncSetAttribute(k_corr_y_w<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_corr_y_w<512><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(512));
@@ -253,7 +267,7 @@ static cudaError_t launch_c2r_t(const float2* H, const float* mu0, const float* 
                                 int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
                                 float* maxcc, int* angidx, cudaStream_t st) {
     constexpr int YT = 8, TS = NH + 2;
-    const size_t smem = sizeof(float2) * (C2R_STAGES * YT * TS + 8 * NH + 3 * NH) + sizeof(float) * nb;
+    const size_t smem = sizeof(float2) * (C2R_STAGES * YT * TS + 8 * NH + 3 * NH + 64) + sizeof(float) * nb;
     cudaFuncSetAttribute(k_c2r_w<NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 g((Ny + YT - 1) / YT, Nz);
     k_c2r_w<NH><<<g, 256, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx,

@@ -20,9 +20,11 @@
 // places every half-warp's 16 float2 accesses of every stage of the plans
 // below in 16 distinct bank pairs (checked exhaustively on the host).
 //
-// Twiddles w^(r m) for r < R come from three or four table loads (w^m, w^2m,
-// w^4m, w^8m) and at most three complex products, within a few ulp of the
-// double-precision table.
+// Twiddles: every stage s > 1 (stride NS, radix R) has its own table
+// T_s[r NS + k] = w_(NS R)^(r k) in shared memory, built once per block from
+// the double-precision line table, so a lane reads the R-1 twiddles of its
+// butterfly at consecutive k across the warp (no bank conflicts, no
+// products).
 #pragma once
 #include "fft_engine.cuh"
 
@@ -73,17 +75,48 @@ TG_D void twiddle_powers(const float2* tw, int m, float2* w) {
     }
 }
 
+// Offset of stage s's table (stages numbered from 0; stage 0 needs none) and
+// total size of the per-line stage tables of a plan.
+template <int NS, int... Rs> struct TabSize;
+template <int NS> struct TabSize<NS> { static constexpr int value = 0; };
+template <int NS, int R, int... Rest> struct TabSize<NS, R, Rest...> {
+    static constexpr int value = (NS > 1 ? NS * R : 0) + TabSize<NS * R, Rest...>::value;
+};
+template <int L, int... Rs> constexpr int tab_size(seq<Rs...>) { return TabSize<1, Rs...>::value; }
+template <int L> struct WTab { static constexpr int size = tab_size<L>(typename WPlan<L>::type{}); };
+
+// Build the stage tables of plan L from the line table tw (L entries), all threads of the block.
+template <int L, int NS, int R, int... Rest>
+TG_D void build_tabs_rec(float2* dst, const float2* __restrict__ tw) {
+    if constexpr (NS > 1) {
+        for (int i = threadIdx.x; i < NS * R; i += blockDim.x) {
+            const int r = i / NS, k = i - r * NS;
+            dst[i] = __ldg(tw + (k * r) * (L / (NS * R)));
+        }
+        dst += NS * R;
+    }
+    if constexpr (sizeof...(Rest) > 0) build_tabs_rec<L, NS * R, Rest...>(dst, tw);
+}
+template <int L, int... Rs> TG_D void build_tabs_impl(float2* dst, const float2* __restrict__ tw, seq<Rs...>) {
+    build_tabs_rec<L, 1, Rs...>(dst, tw);
+}
+template <int L> TG_D void build_stage_tables(float2* dst, const float2* __restrict__ tw) {
+    build_tabs_impl<L>(dst, tw, typename WPlan<L>::type{});
+}
+
 template <int L, int R, int NS, int DIR>
-TG_D void wstage(float2* v, const float2* tw, int lane) {
+TG_D void wstage(float2* v, const float2* tab, int lane) {
     constexpr int EPT = L / 32, NB = EPT / R;
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
         if constexpr (NS > 1) {
-            const int j = lane + 32 * q;
-            float2 w[R];
-            twiddle_powers<R, DIR>(tw, (j % NS) * (L / (NS * R)), w);
+            const int k = (lane + 32 * q) % NS;
 #pragma unroll
-            for (int r = 1; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], w[r]);
+            for (int r = 1; r < R; ++r) {
+                float2 w = tab[r * NS + k];
+                if (DIR > 0) w = cconj(w);
+                v[q * R + r] = cmul(v[q * R + r], w);
+            }
         }
         tgfft::dft<R, DIR>(v + q * R, static_cast<const float2*>(nullptr), L / R);  // radices <= 16: no table
     }
@@ -118,15 +151,15 @@ TG_D void wload(float2* v, const float2* buf, int lane) {
 }
 
 template <int L, int DIR, int NS, int R, int... Rest>
-TG_D void wrun(float2* v, float2* buf, const float2* tw, int lane) {
-    wstage<L, R, NS, DIR>(v, tw, lane);
+TG_D void wrun(float2* v, float2* buf, const float2* tab, int lane) {
+    wstage<L, R, NS, DIR>(v, tab, lane);
     if constexpr (sizeof...(Rest) > 0) {
         constexpr int Rn = tgfft::seq_first<Rest...>::value;
         wstore<L, R, NS>(v, buf, lane);
         __syncwarp();
         wload<L, Rn>(v, buf, lane);
         __syncwarp();
-        wrun<L, DIR, NS * R, Rest...>(v, buf, tw, lane);
+        wrun<L, DIR, NS * R, Rest...>(v, buf, NS > 1 ? tab + NS * R : tab, lane);
     }
 }
 
@@ -135,7 +168,8 @@ TG_D void warp_fft_impl(float2* v, float2* buf, const float2* tw, int lane, seq<
     wrun<L, DIR, 1, Rs...>(v, buf, tw, lane);
 }
 
-// In-register transform of one line per warp; buf: L float2 private to the warp.
+// In-register transform of one line per warp; buf: L float2 private to the
+// warp; tabs: the plan's stage tables (build_stage_tables).
 template <int L, int DIR>
 TG_D void warp_fft(float2* v, float2* buf, const float2* tw, int lane) {
     warp_fft_impl<L, DIR>(v, buf, tw, lane, typename WPlan<L>::type{});
