@@ -46,8 +46,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--rot-per-step", type=int, default=64)
-    p.add_argument("--batch", type=int, default=8)
-    p.add_argument("--e2e-rot", type=int, default=512)
+    p.add_argument("--batch", type=int, default=16)
+    p.add_argument("--e2e-rot", type=int, default=1024)
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-seconds", type=float, default=20.0)
     p.add_argument("--no-cpu-baseline", action="store_true")

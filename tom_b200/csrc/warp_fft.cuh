@@ -37,16 +37,13 @@ template <> struct WPlan<512> { typedef seq<8, 8, 8> type; static constexpr int 
 template <> struct WPlan<256> { typedef seq<8, 4, 8> type; static constexpr int R1 = 8, RL = 8; };
 template <> struct WPlan<128> { typedef seq<4, 2, 4, 4> type; static constexpr int R1 = 4, RL = 4; };
 
-TG_D int swz(int p) {
-    const int row = p >> 4;
-    int s = 0;
-    s ^= (row & 1) ? 15 : 0;
-    s ^= (row & 2) ? 14 : 0;
-    s ^= (row & 4) ? 10 : 0;
-    s ^= (row & 8) ? 15 : 0;
-    s ^= (row & 16) ? 13 : 0;
-    return p ^ s;
+__host__ __device__ constexpr int swz(int p) {
+    return p ^ (((p >> 4) & 1 ? 15 : 0) ^ ((p >> 5) & 1 ? 14 : 0) ^ ((p >> 6) & 1 ? 10 : 0) ^
+                ((p >> 7) & 1 ? 15 : 0) ^ ((p >> 8) & 1 ? 13 : 0));
 }
+// swz is linear over GF(2): for bit-disjoint a and c, swz(a + c) = swz(a) ^ swz(c).
+// Exchange positions split into a per-lane part and a compile-time part with
+// disjoint bits (power-of-two plans), so each access costs one XOR.
 
 // w[r] = tw^(r m) (forward sign), conjugated for DIR > 0.  tw is a table of
 // L entries, in shared memory in the hot kernels.
@@ -133,9 +130,9 @@ TG_D void wstore(const float2* v, float2* buf, int lane) {
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
         const int j = lane + 32 * q, k = j % NS;
-        const int base = (j - k) * R + k;
+        const int a = swz((j - k) * R + k);  // bits below NS and from NS*R up
 #pragma unroll
-        for (int r = 0; r < R; ++r) buf[swz(base + r * NS)] = v[q * R + r];
+        for (int r = 0; r < R; ++r) buf[a ^ swz(r * NS)] = v[q * R + r];  // r*NS: the bits between
     }
 }
 
@@ -144,9 +141,9 @@ TG_D void wload(float2* v, const float2* buf, int lane) {
     constexpr int EPT = L / 32, NB = EPT / R;
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
-        const int j = lane + 32 * q;
+        const int a = swz(lane + 32 * q);  // j < L/R
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[q * R + r] = buf[swz(j + r * (L / R))];
+        for (int r = 0; r < R; ++r) v[q * R + r] = buf[a ^ swz(r * (L / R))];
     }
 }
 
