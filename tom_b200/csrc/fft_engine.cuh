@@ -122,6 +122,34 @@ template <int DIR, typename C> TG_D void dft16(C* v) {
         }
 }
 
+// 32-point DFT: two 16-point DFTs of the even and odd samples and a radix-2
+// combination with the 32nd roots of unity.
+template <int DIR, typename C> TG_D void dft32(C* v) {
+    typedef typename CTraits<C>::R Rt;
+    // cos(pi k / 16), k = 0..8
+    const Rt c[9] = {(Rt)1.0, (Rt)0.98078528040323044913, (Rt)0.92387953251128675613, (Rt)0.83146961230254523708,
+                     (Rt)0.70710678118654752440, (Rt)0.55557023301960222474, (Rt)0.38268343236508977173,
+                     (Rt)0.19509032201612826785, (Rt)0.0};
+    C e[16], o[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        e[i] = v[2 * i];
+        o[i] = v[2 * i + 1];
+    }
+    dft16<DIR>(e);
+    dft16<DIR>(o);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        // w = exp(DIR 2 pi i k / 32) = cos(pi k/16) + DIR i sin(pi k/16)
+        const Rt cr = k <= 8 ? c[k] : -c[16 - k];
+        const Rt si = k <= 8 ? c[8 - k] : c[k - 8];
+        const Rt sn = DIR * si;
+        const C t = CTraits<C>::make(o[k].x * cr - o[k].y * sn, o[k].x * sn + o[k].y * cr);
+        v[k] = cadd(e[k], t);
+        v[k + 16] = csub(e[k], t);
+    }
+}
+
 template <int DIR, typename C> TG_D void dft3(C* v) {
     typedef typename CTraits<C>::R Rt;
     const Rt c = (Rt)-0.5, s = (Rt)(DIR * 0.86602540378443864676);
@@ -199,6 +227,7 @@ TG_D void dft(C* v, const C* __restrict__ tw, int q) {
     else if constexpr (R == 5) dft5<DIR>(v);
     else if constexpr (R == 8) dft8<DIR>(v);
     else if constexpr (R == 16) dft16<DIR>(v);
+    else if constexpr (R == 32) dft32<DIR>(v);
     else dft_prime<R, DIR>(v, tw, q);
 }
 
