@@ -16,7 +16,6 @@
 #include "ctx.h"
 #include "match.h"
 #include "twiddles.h"
-#include "hw_fft.cuh"
 #include "warp_fft.cuh"
 
 namespace tg {
@@ -75,71 +74,6 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_w(const float2* __restrict__ 
         float2* nx = zw + ((b + 1) & 1) * 64;
         if (lane < Ty) nx[lane] = n0;
         if (lane + 32 < Ty) nx[lane + 32] = n1;
-        __syncwarp();
-    }
-}
-
-// Half-warp variant for Ny = 512: two columns per warp, 32 values per lane,
-// radix 16 x 32 (one exchange per transform).  F_I is read through L1.
-template <int NY>
-__global__ void __launch_bounds__(256, 2) k_corr_y_h(const float2* __restrict__ fimg, const float2* __restrict__ Z,
-                                                     float2* __restrict__ Q, int Ty, int d0y, long long ncols, int nb,
-                                                     const float2* __restrict__ tw_g) {
-    constexpr int EPT = NY / 16, LINES = 16;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2* tab = reinterpret_cast<float2*>(smem_raw);  // [NY] stage table
-    float2* xb = tab + NY;                              // [LINES][NY] exchange
-    float2* zs = xb + LINES * NY;                       // [LINES][2][64] template column
-    const int l = threadIdx.x & 15, line = threadIdx.x >> 4;
-    const long long col_raw = (long long)blockIdx.x * LINES + line;
-    const bool valid = col_raw < ncols;
-    const long long col = valid ? col_raw : ncols - 1;  // every lane takes part in the exchanges
-    tghfft::build_stage_tables<NY>(tab, tw_g);
-    float2* buf = xb + line * NY;
-    float2* zw = zs + line * 128;
-    {
-        const float2* zc = Z + col * Ty;
-        for (int t = l; t < Ty; t += 16) zw[t] = zc[t];
-    }
-    __syncthreads();
-    const float2* fc = fimg + col * NY;
-    for (int b = 0; b < nb; ++b) {
-        // the next rotation's column: up to 4 values per lane, parked in registers
-        float2 nx[4];
-        const float2* zn = Z + ((long long)(b + 1) * ncols + col) * Ty;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int t = l + 16 * u;
-            nx[u] = (b + 1 < nb && t < Ty) ? zn[t] : make_float2(0.f, 0.f);
-        }
-        const float2* cur = zw + (b & 1) * 64;
-        float2 v[EPT];
-#pragma unroll
-        for (int i = 0; i < EPT; ++i) {
-            const int jy = (tghfft::in_pos<NY>(i, l) - d0y) & (NY - 1);
-            v[i] = jy < Ty ? cur[jy] : make_float2(0.f, 0.f);
-        }
-        tghfft::hfft<NY, -1>(v, buf, tab, l);
-        float2 u[EPT];
-#pragma unroll
-        for (int i = 0; i < EPT; ++i) {
-            constexpr int dummy = 0;
-            (void)dummy;
-            const int o = tghfft::out_index_of_in<NY>(i);
-            u[i] = cmulc(__ldg(fc + tghfft::in_pos<NY>(i, l)), v[o]);
-        }
-        tghfft::hfft<NY, +1>(u, buf, tab, l);
-        if (valid) {
-            float2* qc = Q + ((long long)b * ncols + col) * NY;
-#pragma unroll
-            for (int i = 0; i < EPT; ++i) qc[tghfft::out_pos<NY>(i, l)] = u[i];
-        }
-        float2* zn_s = zw + ((b + 1) & 1) * 64;
-#pragma unroll
-        for (int uu = 0; uu < 4; ++uu) {
-            const int t = l + 16 * uu;
-            if (t < Ty) zn_s[t] = nx[uu];
-        }
         __syncwarp();
     }
 }
@@ -302,19 +236,11 @@ __global__ void __launch_bounds__(256, 3) k_c2r_w(const float2* __restrict__ H, 
 
 // ------------------------------------------------------------- dispatch
 bool fast_corr_y(int NY, int Ty) { return (NY == 256 || NY == 512) && Ty <= 64; }
-static bool half_warp_corr_y = true;  // 512: half-warp lines (radix 16 x 32)
 bool fast_inv_z(int NZ) { return NZ == 256; }
 bool fast_c2r(int NH) { return NH == 128 || NH == 256; }
 
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
                                long long ncols, int nb, cudaStream_t st) {
-    if (NY == 512 && half_warp_corr_y) {
-        const size_t smem_h = sizeof(float2) * (512 + 16 * 512 + 16 * 128);
-        cudaFuncSetAttribute(k_corr_y_h<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_h);
-        k_corr_y_h<512><<<(unsigned)((ncols + 15) / 16), 256, smem_h, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb,
-                                                                            twiddle_table<float2>(512));
-        return cudaGetLastError();
-    }
     const unsigned g = (unsigned)((ncols + 7) / 8);
     const size_t smem = sizeof(float2) * (NY * 17 + 64 + 8 * 128);
     if (NY == 512) {

@@ -155,6 +155,10 @@ CONFIGS = {
     # a reduced volume with the 512x512x256 workload's template, for profiler captures
     "profile_256x256x128": dict(N=(256, 256, 128), T=40, n_copies=10, n_blobs=8, rho=16, snr=0.1,
                                 max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
+    # x edge of the benchmark (the same x-line kernel) on a small y-z plane, for
+    # profiler captures at the benchmark's rotation batch
+    "profile_512x128x64": dict(N=(512, 128, 64), T=40, n_copies=4, n_blobs=8, rho=16, snr=0.1,
+                               max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
     "exhaustive_512x512x256": dict(N=(512, 512, 256), T=40, n_copies=40, n_blobs=8, rho=16, snr=0.1,
                                    max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
 }
