@@ -585,6 +585,7 @@ int MatchPlan::create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batc
         return fail(ctx, TOMGPU_ERR_UNSUPPORTED,
                     "volume/template sizes not supported by the FFT kernels");
     B = batch > 0 ? batch : 8;
+    if (B > 4096) return fail(ctx, TOMGPU_ERR_ARG, "rotation batch above 4096");
     nvox = (long long)N[0] * N[1] * N[2];
     nh1 = N[0] / 2 + 1;
     tn = (long long)T[0] * T[1] * T[2];

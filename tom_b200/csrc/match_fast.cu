@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(256) k_inv_z_b256(const float2* __restrict__ Q
     }
 }
 
-constexpr int C2R_STAGES = 3;
+constexpr int C2R_STAGES = 2;
 
 TG_D void cp_async8(void* smem_dst, const void* gsrc, int bytes) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -126,7 +126,7 @@ template <int N> TG_D void cp_async_wait() { asm volatile("cp.async.wait_group %
 // separation between those angles.  gamma = 0 voxels keep the reference's
 // value 0 with the batch's first rotation.)
 template <int NH>
-__global__ void __launch_bounds__(256, 3) k_c2r_w(const float2* __restrict__ H, const float* __restrict__ mu0,
+__global__ void __launch_bounds__(256, 4) k_c2r_w(const float2* __restrict__ H, const float* __restrict__ mu0,
                                                   const float* __restrict__ gam, const double* __restrict__ tsum,
                                                   int Ny, int Nz, int nb, float inv_nm, double c_mean, double inv_m,
                                                   double mu_t, int index0, float* __restrict__ maxcc,
@@ -144,11 +144,11 @@ __global__ void __launch_bounds__(256, 3) k_c2r_w(const float2* __restrict__ H, 
     const bool yok = y < Ny;
     const long long nh1l = NH1;
     float bu[EPT][2];
-    int bb[EPT][2];
+    unsigned bb[EPT];  // best rotation of the voxel pair, 16 bits each (nb <= 65535)
 #pragma unroll
     for (int i = 0; i < EPT; ++i) {
         bu[i][0] = bu[i][1] = -INFINITY;
-        bb[i][0] = bb[i][1] = 0;
+        bb[i] = 0u;
     }
     static_assert(tgwfft::WTab<NH>::size <= NH + 64, "stage tables exceed their slot");
     tgwfft::build_stage_tables<NH>(twh, tw_h);
@@ -195,8 +195,8 @@ __global__ void __launch_bounds__(256, 3) k_c2r_w(const float2* __restrict__ H, 
         for (int i = 0; i < EPT; ++i) {
             const float u0 = fmaf(v[i].x, inv_nm, kap);
             const float u1 = fmaf(v[i].y, inv_nm, kap);
-            if (u0 > bu[i][0]) { bu[i][0] = u0; bb[i][0] = b; }
-            if (u1 > bu[i][1]) { bu[i][1] = u1; bb[i][1] = b; }
+            if (u0 > bu[i][0]) { bu[i][0] = u0; bb[i] = (bb[i] & 0xFFFF0000u) | (unsigned)b; }
+            if (u1 > bu[i][1]) { bu[i][1] = u1; bb[i] = (bb[i] & 0x0000FFFFu) | ((unsigned)b << 16); }
         }
         __syncthreads();
     }
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(256, 3) k_c2r_w(const float2* __restrict__ H, 
         bool ch = false;
         const float c0 = g.x != 0.f ? (bu[i][0] - a.x * mt) * g.x : 0.f;
         const float c1 = g.y != 0.f ? (bu[i][1] - a.y * mt) * g.y : 0.f;
-        const int b0 = g.x != 0.f ? bb[i][0] : 0, b1 = g.y != 0.f ? bb[i][1] : 0;
+        const int b0 = g.x != 0.f ? (int)(bb[i] & 0xFFFFu) : 0, b1 = g.y != 0.f ? (int)(bb[i] >> 16) : 0;
         if (c0 > cur.x) { cur.x = c0; ci.x = index0 + b0; ch = true; }
         if (c1 > cur.y) { cur.y = c1; ci.y = index0 + b1; ch = true; }
         if (ch) {
