@@ -150,6 +150,21 @@ int tomgpu_weight3d(tomgpu_ctx* ctx, const int dims[3], const double* angles, in
 int tomgpu_wedge_dev(tomgpu_ctx* ctx, const int dims[3], double angle_or_min, double max_angle,
                      int av3, float* out_dev);
 
+/* ------------------------------------------------------- EM-format I/O --- */
+/* Read an EM file (IOfun/tom_emread.m:153-176) into host memory as float
+ * (byte, int16, int32, float and double data; either byte order).  With
+ * out == NULL only dims is filled (size query); capacity is out's length in
+ * floats.  Errors: tomgpu_last_error(NULL). */
+int tomgpu_em_read(const char* path, int dims[3], float* out, size_t capacity);
+/* Write a float volume as an EM file in PC byte order (magic 6 0 0 5,
+ * IOfun/tom_emwrite.m:94-150); comment (may be NULL) fills the 80-char field. */
+int tomgpu_em_write(const char* path, const float* data, const int dims[3], const char* comment);
+
+/* out = real(ifftn(ifftshift(fftshift(fftn(in)) .* w))) in FP64 on the device
+ * (Filtrans/tom_apply_weight_function.m:56-62); w is the centred weight. */
+int tomgpu_apply_weight_dev(tomgpu_ctx* ctx, const float* in_dev, const float* w_dev, const int dims[3],
+                            float* out_dev);
+
 /* ------------------------------------------------------------- FFTs --- */
 /* Replaces fftn / tom_fourier and ifftn / tom_ifourier (Filtrans/tom_fourier.m:44-50,
  * Filtrans/tom_ifourier.m:36-44) on device buffers.  Complex data are

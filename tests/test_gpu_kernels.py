@@ -143,3 +143,20 @@ def test_wedges_vs_oracle(gpu, oracle):
             assert np.array_equal(gpu.tom_wedge(np.zeros(shape), ang), oracle.tom_wedge(shape, ang))
         for mn, mx in ((-60, 60), (-45, 55)):
             assert np.array_equal(gpu.av3_wedge(np.zeros(shape), mn, mx), oracle.av3_wedge(shape, mn, mx))
+
+
+def test_apply_weight_function(gpu, oracle):
+    rng = np.random.default_rng(71)
+    v = rng.standard_normal((24, 20, 32)).astype(np.float32)
+    w = oracle.tom_wedge(v.shape, 30.0)
+    got = gpu.tom_apply_weight_function(v, w)
+    ref = oracle.apply_weight_function(v, w)
+    assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+def test_empty_volume_rule(gpu, oracle):
+    """tom_os3_findTemplate.m: a volume with mean 0 and std 0 is not searched."""
+    T = 16
+    tmpl = np.random.default_rng(1).standard_normal((T, T, T)).astype(np.float32)
+    ccc, ang = gpu.tom_os3_findTemplate(np.zeros((32, 32, 32), np.float32), tmpl, [(0, 0, 0)])
+    assert np.all(ccc == 0) and np.all(ang == -1000)

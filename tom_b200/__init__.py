@@ -22,8 +22,11 @@ from .tom import (  # noqa: F401
     tom_av3_angle2index,
     tom_av3_angle_grid,
     tom_av3_index2angle,
+    tom_apply_weight_function,
     tom_calc_weight_functioninc,
     tom_corr,
+    tom_emread,
+    tom_emwrite,
     tom_fourier,
     tom_ifourier,
     tom_os3_angleList,

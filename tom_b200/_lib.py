@@ -76,6 +76,9 @@ _SIGS = {
     "tomgpu_weight3d": (ctypes.c_int, [c_void_p, c_int_p, c_double_p, ctypes.c_int, ctypes.c_double, c_void_p]),
     "tomgpu_wedge_dev": (ctypes.c_int, [c_void_p, c_int_p, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                         c_void_p]),
+    "tomgpu_em_read": (ctypes.c_int, [ctypes.c_char_p, c_int_p, c_void_p, ctypes.c_size_t]),
+    "tomgpu_em_write": (ctypes.c_int, [ctypes.c_char_p, c_void_p, c_int_p, ctypes.c_char_p]),
+    "tomgpu_apply_weight_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int_p, c_void_p]),
     "tomgpu_fft3d_c2c_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, ctypes.c_int, ctypes.c_int]),
     "tomgpu_fft3d_r2c_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int_p, ctypes.c_int]),
     "tomgpu_fft3d_c2r_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_int_p, ctypes.c_int]),

@@ -455,6 +455,38 @@ int tomgpu_wedge_dev(tomgpu_ctx* ctx, const int dims[3], double a, double b, int
     return TOMGPU_OK;
 }
 
+int tomgpu_apply_weight_dev(tomgpu_ctx* ctx, const float* in, const float* w, const int dims[3], float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!in || !w || !out || !dims_ok(dims)) return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
+    for (int d = 0; d < 3; ++d)
+        if (dims[d] > 1 && !fft_length_supported(dims[d])) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "size not an FFT length");
+    TG_TRY(use_device(ctx));
+    const long long n = numel(dims);
+    double2* c = nullptr;
+    double* r = nullptr;
+    float* ws = nullptr;
+    if (cudaMalloc(&c, sizeof(double2) * n) || cudaMalloc(&r, sizeof(double) * n) || cudaMalloc(&ws, sizeof(float) * n)) {
+        if (c) cudaFree(c);
+        if (r) cudaFree(r);
+        return cuda_fail(ctx, cudaErrorMemoryAllocation, "weight buffers");
+    }
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = ifftshift_real(w, ws, dims, st);
+    if (!e) e = real_to_c64(in, c, n, st);
+    if (!e) e = c2c3d<double2>(c, dims, -1, 1.0, st);
+    if (!e) e = mul_weight_c64(c, ws, n, st);
+    if (!e) e = c2c3d<double2>(c, dims, +1, 1.0 / (double)n, st);
+    if (!e) e = re_c64(c, r, n, 1.0, st);
+    if (!e) e = double_to_float(r, out, n, st);
+    if (!e) e = cudaStreamSynchronize(st);
+    ctx->launches += 10;
+    cudaFree(c);
+    cudaFree(r);
+    cudaFree(ws);
+    if (e) return cuda_fail(ctx, e, "apply_weight");
+    return TOMGPU_OK;
+}
+
 // ----------------------------------------------------------------- FFTs
 static int fft_dims_ok(tomgpu_ctx* ctx, const int dims[3]) {
     if (!dims_ok(dims)) return fail(ctx, TOMGPU_ERR_ARG, "bad dims");

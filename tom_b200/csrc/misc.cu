@@ -227,6 +227,11 @@ cudaError_t mul_weight_c64(double2* a, const float* w, long long n, cudaStream_t
     TG_LAUNCH(k_mul_weight_c64, n, a, w, n);
 }
 cudaError_t re_c64(const double2* a, double* b, long long n, double s, cudaStream_t st) { TG_LAUNCH(k_re_c64, n, a, b, n, s); }
+__global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+cudaError_t double_to_float(const double* a, float* b, long long n, cudaStream_t st) { TG_LAUNCH(k_d2f, n, a, b, n); }
 cudaError_t stats_final(const double* m1, const double* m2, float* mu, float* sig, long long n, cudaStream_t st) {
     TG_LAUNCH(k_stats_final, n, m1, m2, mu, sig, n);
 }

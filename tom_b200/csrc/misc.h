@@ -21,6 +21,7 @@ cudaError_t mul_c64(double2* a, const double2* b, long long n, cudaStream_t st);
 cudaError_t real_to_c64(const float* a, double2* b, long long n, cudaStream_t st);
 cudaError_t mul_weight_c64(double2* a, const float* w, long long n, cudaStream_t st);
 cudaError_t re_c64(const double2* a, double* b, long long n, double s, cudaStream_t st);
+cudaError_t double_to_float(const double* a, float* b, long long n, cudaStream_t st);
 cudaError_t stats_final(const double* m1, const double* m2, float* mu, float* sig, long long n, cudaStream_t st);
 cudaError_t gamma_from_sigma(const float* sig, float* gam, long long n, double tstd, cudaStream_t st);
 cudaError_t place_f64(const float* small, const int t[3], double* big, const int nn[3], const int off[3],

@@ -323,6 +323,36 @@ def tom_os3_sphereMask(template):
     return m, int((m > 0).sum())
 
 
+def tom_apply_weight_function(in_, w_func, ctx: Context | None = None):
+    """out = tom_apply_weight_function(in, w) (Filtrans/tom_apply_weight_function.m:56-62), FP64 on the GPU."""
+    ctx = ctx or default_context()
+    import torch
+    a = np.asarray(in_, np.float32)
+    if a.shape != np.shape(w_func):
+        raise ValueError("volume and weight differ in size")
+    ti, tw = to_device(a, ctx.device), to_device(np.asarray(w_func, np.float32), ctx.device)
+    out = torch.empty_like(ti)
+    ctx.check(lib().tomgpu_apply_weight_dev(ctx.handle, _tptr(ti), _tptr(tw), _cdims(_dims(a)), _tptr(out)))
+    return np.asfortranarray(from_device(out).reshape(a.shape, order="F"))
+
+
+def tom_emread(path):
+    """EM file -> dict(Value=float32 [x,y,z], Header=dict(Size=...)) (IOfun/tom_emread.m)."""
+    d = (ctypes.c_int * 3)()
+    check(lib().tomgpu_em_read(str(path).encode(), d, None, 0))
+    vol = np.zeros(tuple(d), np.float32, order="F")
+    check(lib().tomgpu_em_read(str(path).encode(), d, _ptr(vol), vol.size))
+    return {"Value": vol, "Header": {"Size": tuple(d)}}
+
+
+def tom_emwrite(path, data, comment: str = ""):
+    """Write a float32 EM file (IOfun/tom_emwrite.m), PC byte order."""
+    a = _f32_xfast(np.asarray(data.get("Value") if isinstance(data, dict) else data))
+    if a.ndim == 2:
+        a = a.reshape(a.shape + (1,), order="F")
+    check(lib().tomgpu_em_write(str(path).encode(), _ptr(a), _cdims(a.shape), comment.encode()[:80]))
+
+
 def tom_fourier(a, ctx: Context | None = None):
     """fftn in FP64 on the GPU (Filtrans/tom_fourier.m)."""
     return _fft(a, -1, ctx)
@@ -560,6 +590,10 @@ def tom_os3_findTemplate(volume, template, angle_list, mask=None, psf=None, batc
     t = np.asarray(template, np.float32)
     if mask is None:
         mask, _ = tom_os3_sphereMask(t)
+    if not np.any(vol):
+        # tom_os3_findTemplate.m:221 and :309-313: a volume with mean 0 and
+        # std 0 is not searched; ccc is 0 and the angle map keeps -1000
+        return (np.zeros(vol.shape, np.float32, order="F"), np.full(vol.shape, -1000, np.float32, order="F"))
     plan = MatchPlan(vol.shape, t.shape, batch=batch, ctx=ctx)
     try:
         td, md = to_device(t, ctx.device), to_device(mask, ctx.device)
