@@ -213,6 +213,14 @@ int tomgpu_match_set_volume_dev(tomgpu_match_plan* plan, const float* vol_dev);
 int tomgpu_match_set_template_dev(tomgpu_match_plan* plan, const float* tmpl_dev,
                                   const float* mask_dev, const float* psf_dev);
 
+/* Template and mask taken as given, for tom_os3_corr(img, t) called without
+ * cached statistics (search/tom_os3_corr.m:77-149 with calculationAvailable
+ * false): the template statistics are tom_os3_normUnderMask(t, mask) of this
+ * template, with no tom_norm and no filter.  Then tomgpu_match_corr_dev with
+ * the same template gives tom_os3_corr's map. */
+int tomgpu_match_set_template_raw_dev(tomgpu_match_plan* plan, const float* tmpl_dev,
+                                      const float* mask_dev);
+
 /* Fill maxcc_dev with -1000 and angidx_dev with -1 (findTemplate's initial
  * ccc/angles, :215-218, with 0-based indices). */
 int tomgpu_match_init_results_dev(tomgpu_match_plan* plan, float* maxcc_dev, int32_t* angidx_dev);
@@ -290,6 +298,48 @@ typedef struct {
  * (1 float).  Host output arrays of n_jobs*3, n_jobs*3 and n_jobs floats. */
 int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs, float* angles,
                          float* shifts, float* ccf_peak);
+
+/* ---------------------------------------------------------- peak analysis */
+
+/* tom_os3_analyzePeak(img, peakMap, template, 'PSR')
+ * (Oscar3/matlabPicker/analyze/tom_os3_analyzePeak.m:61-101): the peak map's
+ * local mean and std under tom_os3_sphereMask(template) with a centred
+ * floor(T/4) box zeroed, then (peak - mean)/std where std > 1000 eps(max std),
+ * else 0.  peak_dev/out_dev: map-sized (map_dims, x edge even); tmpl_dims: the
+ * template's size (only its size enters).  FP64 inside. */
+int tomgpu_analyze_psr_dev(tomgpu_ctx* ctx, const float* peak_dev, const int map_dims[3],
+                           const int tmpl_dims[3], float* out_dev);
+
+/* A = tom_os3_corr(t, t) (search/tom_os3_corr.m:77-176, same-size inputs, no
+ * options): the template's autocorrelation FLCF with the default sphere mask,
+ * divided at every voxel.  Template-sized device buffers.  FP64 inside. */
+int tomgpu_template_autocorr_dev(tomgpu_ctx* ctx, const float* t_dev, const int tmpl_dims[3], float* out_dev);
+
+/* tom_os3_analyzePeak(0, peakMap, template, 'Autocorrelation')
+ * (tom_os3_analyzePeak.m:174-190): the FLCF of the peak map with A =
+ * tom_os3_corr(t, t) under mask_dev (options.correlation.mask; NULL =
+ * tom_os3_sphereMask), with A's own statistics. */
+int tomgpu_analyze_autocorr_dev(tomgpu_ctx* ctx, const float* peak_dev, const int map_dims[3],
+                                const float* t_dev, const int tmpl_dims[3], const float* mask_dev,
+                                float* out_dev);
+
+/* tom_os3_bestPeak criteria (options.analysis.ccc / .psr / .autocorr). */
+enum { TOMGPU_ANALYSIS_CCC = 1, TOMGPU_ANALYSIS_PSR = 2, TOMGPU_ANALYSIS_AUTOCORR = 4 };
+
+/* Fill maxcc, psr and autoc with -1000 and angidx with -1. */
+int tomgpu_match_init_analysis_dev(tomgpu_match_plan* plan, float* maxcc_dev, int32_t* angidx_dev,
+                                   float* psr_dev, float* autoc_dev);
+
+/* The search loop of tom_os3_findTemplate.m:255-307 as the reference runs it:
+ * for every rotation the FLCF map, its PSR map and its autocorrelation map
+ * (tom_os3_analyzePeak on the rotated, masked, filtered template), then
+ * tom_os3_bestPeak (search/tom_os3_bestPeak.m:12-47): a voxel takes the
+ * rotation's cc, psr, autocorrelation and index where every criterion in
+ * `flags` (TOMGPU_ANALYSIS_*, at least one) strictly improves.  Several
+ * N-sized FFTs per rotation: the analysis search, not the fast one. */
+int tomgpu_match_run_analysis_dev(tomgpu_match_plan* plan, const float* eulers, int R, int index_offset,
+                                  int flags, float* maxcc_dev, int32_t* angidx_dev, float* psr_dev,
+                                  float* autoc_dev);
 
 #ifdef __cplusplus
 }

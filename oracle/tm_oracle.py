@@ -413,6 +413,130 @@ def find_template_direct_at(volume, template, mask, angles, voxels, psf=None):
 
 
 # ---------------------------------------------------------------------------
+# Peak analysis: PSR and autocorrelation (SOC) maps
+# ---------------------------------------------------------------------------
+
+def psr_mask_box(tshape):
+    """The PSR mask of tom_os3_analyzePeak.m:68,90 inside its template-sized box:
+    tom_os3_sphereMask(template) with a centred box of floor(T/4) voxels per
+    axis zeroed (pasteCenter(mask, 0*sphereMask(zeros(T/4)))).  The N-sized
+    mask is this box pasted at the centre."""
+    box, _ = os3_sphere_mask(tshape)
+    box = np.array(box, np.float64)
+    q = [t // 4 for t in tshape]
+    if min(q) > 0:
+        o = [t // 2 - s // 2 for t, s in zip(tshape, q)]
+        box[o[0]:o[0] + q[0], o[1]:o[1] + q[1], o[2]:o[2] + q[2]] = 0
+    return box
+
+
+def _single_eps(x):
+    """MATLAB eps(single(x)) for x >= 0."""
+    return float(np.spacing(np.float32(x)))
+
+
+def analyze_psr(peak, tshape):
+    """tom_os3_analyzePeak(img, peakMap, template, 'PSR') (analyze/tom_os3_analyzePeak.m:61-101):
+    (peakMap - mean)/std under the PSR mask, 0 where std <= 1000 eps(max std)."""
+    p = np.asarray(peak, np.float64)
+    mean, std, _ = local_stats(p, psr_mask_box(tuple(tshape)))
+    s32 = std.astype(np.float32)
+    tol = 1000 * _single_eps(np.abs(s32).max())
+    res = np.zeros(p.shape)
+    nz = s32 > tol
+    res[nz] = (p - mean)[nz] / s32[nz].astype(np.float64)
+    return res
+
+
+def _hot_threshold(img, std):
+    """The two 'numeric artefact' branches of tom_os3_corr.m:108-127.  The first
+    (tom_norm of the image and template when mean(std) < 0.01) is an affine map
+    of both inputs and leaves the FLCF unchanged; the second marks voxels whose
+    renormalised local std is below 0.05 when the renormalised mean std is
+    still below 0.01.  Returns the threshold on the original std (or None)."""
+    if std.mean() >= 0.01:
+        return None
+    a = np.asarray(img, np.float64)
+    s = a.std()                       # tom_norm's tom_dev std
+    scale = 1.0 / s if s != 0 else 2.0
+    if (std * scale).mean() >= 0.01:
+        return None
+    return 0.05 / scale
+
+
+def os3_corr_same(img, t):
+    """tom_os3_corr(img, template) with no options for same-size inputs
+    (search/tom_os3_corr.m:77-176): default sphere mask, statistics of both
+    inputs under it, res = numerator./denominator at every voxel."""
+    a = np.asarray(img, np.float64)
+    t = np.asarray(t, np.float64)
+    mask, _ = os3_sphere_mask(t.shape)
+    mask = np.asarray(mask, np.float64)
+    mean, std, M = local_stats(a, mask)
+    _, tmean, tstd = norm_under_mask(t, mask)
+    ft = np.fft.rfftn(t * mask)
+    num = np.fft.ifftshift(np.fft.irfftn(np.fft.rfftn(a) * np.conj(ft), s=a.shape, axes=(0, 1, 2))) / M
+    with np.errstate(divide="ignore", invalid="ignore"):
+        res = (num - mean * tmean) / (tstd * std)
+    thr = _hot_threshold(a, std)
+    if thr is not None:
+        res[std < thr] = 0
+    return res
+
+
+def analyze_autocorr(peak, t, mask):
+    """tom_os3_analyzePeak(0, peakMap, template, 'Autocorrelation')
+    (analyze/tom_os3_analyzePeak.m:174-190): the template's autocorrelation
+    A = tom_os3_corr(t, t), then the FLCF of the peak map with A under the
+    correlation mask, with A's own statistics (tom_os3_corr.m, sizes differ)."""
+    A = os3_corr_same(t, t).astype(np.float32).astype(np.float64)
+    p = np.asarray(peak, np.float64)
+    st = FLCF(p, mask)
+    _, am, asd = norm_under_mask(A, mask)
+    res = st.corr(A, am, asd)
+    thr = _hot_threshold(p, st.std)
+    if thr is not None:
+        res[st.std < thr] = 0
+    return res
+
+
+def find_template_analysis(volume, template, mask, angles, psf=None, ccc=True, psr=False, autocorr=False,
+                           margins=False):
+    """tom_os3_findTemplate.m:255-307 with the PSR and autocorrelation maps of
+    every rotation and tom_os3_bestPeak's update (search/tom_os3_bestPeak.m:12-47):
+    a voxel takes the rotation's (cc, psr, soc, index) where every selected
+    criterion strictly improves.  Returns (ccc, idx, psr, soc); idx 0-based,
+    -1 where never updated; ccc/psr/soc -1000 there.  With margins, also the
+    per-voxel smallest |old - new| / (1 + |new|) over all decisions taken on
+    the selected criteria (voxels whose decisions were all clear-cut)."""
+    t, tmean, tstd = prepare_template(template, mask, psf)
+    st = FLCF(volume, mask)
+    out_c = np.full(st.N, -1000.0)
+    out_p = np.full(st.N, -1000.0)
+    out_a = np.full(st.N, -1000.0)
+    idx = np.full(st.N, -1, np.int64)
+    margin = np.full(st.N, np.inf)
+    T = mask.shape
+    for it, ang in enumerate(np.asarray(angles, np.float64).reshape(-1, 3)):
+        tr = rotate(t.astype(np.float32), ang).astype(np.float64) * mask
+        if psf is not None:
+            tr = apply_weight_function(tr, psf)
+        tr = tr.astype(np.float32).astype(np.float64)
+        cc = st.corr(tr, tmean, tstd).astype(np.float32).astype(np.float64)
+        pm = analyze_psr(cc, T)
+        am = analyze_autocorr(cc, tr, mask)
+        upd = np.ones(st.N, bool)
+        for sel, old, new in ((ccc, out_c, cc), (psr, out_p, pm), (autocorr, out_a, am)):
+            if sel:
+                upd &= old < new
+                with np.errstate(invalid="ignore"):
+                    margin = np.minimum(margin, np.abs(old - new) / (1 + np.abs(new)))
+        out_c[upd], out_p[upd], out_a[upd], idx[upd] = cc[upd], pm[upd], am[upd], it
+    res = (out_c, idx, out_p, out_a)
+    return res + (margin,) if margins else res
+
+
+# ---------------------------------------------------------------------------
 # Angles
 # ---------------------------------------------------------------------------
 

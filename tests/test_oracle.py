@@ -129,3 +129,66 @@ def test_angle_grids(oracle):
         a = g0[i]
         assert oracle.av3_angle2index(a, st, inc, en) == i
         assert np.allclose(oracle.av3_index2angle(i, st, inc, en), a)
+
+
+# ------------------------------------------------------------- peak analysis
+
+def _ifftshift_conv_direct(img, big_mask, x):
+    """real(ifftshift(ifftn(fftn(img).*fftn(big_mask))))(x), written out."""
+    N = img.shape
+    s = 0.0
+    for j in np.argwhere(big_mask != 0):
+        q = tuple((x[d] + N[d] // 2 - j[d]) % N[d] for d in range(3))
+        s += big_mask[tuple(j)] * img[q]
+    return s
+
+
+@pytest.mark.parametrize("N", [(12, 10, 14), (11, 13, 9)])
+def test_psr_direct(oracle, N):
+    """PSR of tom_os3_analyzePeak from tom_os3_mean/std written as sums over the
+    pasted N-sized mask (odd and even sizes pin the ifftshift)."""
+    rng = np.random.default_rng(31)
+    pk = rng.standard_normal(N)
+    T = (8, 8, 8)
+    big = oracle.paste_center(N, oracle.psr_mask_box(T))
+    M = (big != 0).sum()
+    res = oracle.analyze_psr(pk, T)
+    box = oracle.psr_mask_box(T)
+    assert box.sum() == oracle.os3_sphere_mask(T)[0].sum() - 8   # 2x2x2 centre box zeroed
+    for x in [(0, 0, 0), (5, 3, 7), (N[0] - 1, N[1] - 1, N[2] - 1)]:
+        m = _ifftshift_conv_direct(pk, big, x) / M
+        e2 = _ifftshift_conv_direct(pk * pk, big, x) / M
+        sd = np.float32(np.sqrt(max(e2 - m * m, 0)))
+        assert abs(res[x] - (pk[x] - m) / float(sd)) < 1e-9 * max(1, abs(res[x]))
+
+
+def test_template_autocorr_direct(oracle):
+    """tom_os3_corr(t, t): 1 at the centre; circular sums elsewhere."""
+    rng = np.random.default_rng(32)
+    T = (8, 8, 8)
+    t = rng.standard_normal(T)
+    A = oracle.os3_corr_same(t, t)
+    c = 4
+    assert abs(A[c, c, c] - 1) < 1e-12
+    S = oracle.os3_sphere_mask(T)[0]
+    M = S.sum()
+    _, tm, ts = oracle.norm_under_mask(t, S)
+    for x in [(0, 0, 0), (2, 5, 7), (7, 1, 3)]:
+        num = sum(t[tuple((x[d] + c + j[d]) % 8 for d in range(3))] * t[tuple(j)] for j in np.argwhere(S != 0)) / M
+        m = _ifftshift_conv_direct(t, S, x) / M
+        e2 = _ifftshift_conv_direct(t * t, S, x) / M
+        assert abs(A[x] - (num - m * tm) / (ts * np.sqrt(e2 - m * m))) < 1e-10
+
+
+def test_analysis_ccc_only_is_find_template(oracle):
+    rng = np.random.default_rng(33)
+    vol = rng.standard_normal((16, 14, 12))
+    T = 8
+    tmpl = rng.standard_normal((T, T, T))
+    mask = oracle.sphere_mask((T, T, T), 3)
+    angles = oracle.av3_angle_grid((0, 0, 0), (90, 90, 90), (270, 90, 90))[:5]
+    c1, i1 = oracle.find_template(vol, tmpl, mask, angles)
+    c2, i2, p2, a2 = oracle.find_template_analysis(vol, tmpl, mask, angles)
+    assert np.array_equal(i1, i2)
+    assert np.abs(c1 - c2).max() < 1e-6
+    assert np.all(np.isfinite(p2)) and np.all(np.isfinite(a2))

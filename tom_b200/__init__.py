@@ -29,10 +29,12 @@ from .tom import (  # noqa: F401
     tom_emwrite,
     tom_fourier,
     tom_ifourier,
+    tom_os3_analyzePeak,
     tom_os3_angleList,
     tom_os3_corr,
     tom_os3_findTemplate,
     tom_os3_sphereMask,
+    tom_os3_template_autocorr,
     tom_peak,
     tom_peakc,
     tom_rotate,

@@ -91,6 +91,14 @@ _SIGS = {
     "tomgpu_match_init_results_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
     "tomgpu_match_run_dev": (ctypes.c_int, [c_void_p, c_float_p, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p]),
     "tomgpu_match_corr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    "tomgpu_match_set_template_raw_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    "tomgpu_match_init_analysis_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tomgpu_match_run_analysis_dev": (ctypes.c_int, [c_void_p, c_float_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                     c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tomgpu_analyze_psr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_int_p, c_void_p]),
+    "tomgpu_template_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p]),
+    "tomgpu_analyze_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p,
+                                                   c_void_p]),
     "tomgpu_match_rescore_fp64_dev": (ctypes.c_int, [c_void_p, c_void_p, c_float_p, c_int_p, ctypes.c_int,
                                                      c_double_p]),
     "tomgpu_match_stats_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),

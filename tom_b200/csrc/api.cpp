@@ -5,6 +5,7 @@
 #include <string>
 #include <vector>
 
+#include "analysis.h"
 #include "ctx.h"
 #include "fft3d.h"
 #include "match.h"
@@ -455,6 +456,49 @@ int tomgpu_wedge_dev(tomgpu_ctx* ctx, const int dims[3], double a, double b, int
     return TOMGPU_OK;
 }
 
+int tomgpu_analyze_psr_dev(tomgpu_ctx* ctx, const float* peak, const int map_dims[3], const int tmpl_dims[3],
+                           float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!peak || !out || !dims_ok(map_dims) || !dims_ok(tmpl_dims))
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
+    TG_TRY(use_device(ctx));
+    PeakAnalysis an;
+    TG_TRY(an.create(ctx, map_dims, tmpl_dims, nullptr));
+    TG_TRY(an.spectra(peak));
+    TG_TRY(an.psr(peak, out));
+    TG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_template_autocorr_dev(tomgpu_ctx* ctx, const float* t, const int tmpl_dims[3], float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!t || !out || !dims_ok(tmpl_dims)) return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
+    TG_TRY(use_device(ctx));
+    // the map-sized part is not used: size it at the template (x edge even for the half spectrum)
+    int nd[3] = {tmpl_dims[0], tmpl_dims[1], tmpl_dims[2]};
+    if (nd[0] % 2) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "template x edge must be even");
+    PeakAnalysis an;
+    TG_TRY(an.create(ctx, nd, tmpl_dims, nullptr));
+    TG_TRY(an.autocorr(t, out));
+    TG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_analyze_autocorr_dev(tomgpu_ctx* ctx, const float* peak, const int map_dims[3], const float* t,
+                                const int tmpl_dims[3], const float* mask, float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!peak || !t || !out || !dims_ok(map_dims) || !dims_ok(tmpl_dims))
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
+    TG_TRY(use_device(ctx));
+    PeakAnalysis an;
+    TG_TRY(an.create(ctx, map_dims, tmpl_dims, mask));
+    TG_TRY(an.autocorr(t, an.tmp_t));
+    TG_TRY(an.spectra(peak));
+    TG_TRY(an.soc(peak, an.tmp_t, out));
+    TG_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TOMGPU_OK;
+}
+
 int tomgpu_apply_weight_dev(tomgpu_ctx* ctx, const float* in, const float* w, const int dims[3], float* out) {
     if (!ctx) return TOMGPU_ERR_ARG;
     if (!in || !w || !out || !dims_ok(dims)) return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
@@ -597,6 +641,33 @@ int tomgpu_match_run_dev(tomgpu_match_plan* plan, const float* eulers, int R, in
         return fail(plan->p.ctx, TOMGPU_ERR_ARG, "result buffers must be 8-byte aligned");
     TG_TRY(use_device(plan->p.ctx));
     return plan->p.run(eulers, R, index_offset, maxcc, angidx);
+}
+
+int tomgpu_match_set_template_raw_dev(tomgpu_match_plan* plan, const float* t, const float* mask) {
+    if (!plan) return TOMGPU_ERR_ARG;
+    if (!t || !mask) return fail(plan->p.ctx, TOMGPU_ERR_ARG, "template and mask are required");
+    TG_TRY(use_device(plan->p.ctx));
+    return plan->p.set_template(t, mask, nullptr, true);
+}
+
+int tomgpu_match_init_analysis_dev(tomgpu_match_plan* plan, float* maxcc, int32_t* angidx, float* psr, float* soc) {
+    if (!plan) return TOMGPU_ERR_ARG;
+    if (!maxcc || !angidx || !psr || !soc) return fail(plan->p.ctx, TOMGPU_ERR_ARG, "null result buffer");
+    TG_TRY(use_device(plan->p.ctx));
+    return analysis_init(plan->p.ctx, plan->p.nvox, maxcc, angidx, psr, soc);
+}
+
+int tomgpu_match_run_analysis_dev(tomgpu_match_plan* plan, const float* eulers, int R, int index_offset, int flags,
+                                  float* maxcc, int32_t* angidx, float* psr, float* soc) {
+    if (!plan) return TOMGPU_ERR_ARG;
+    if (R < 0 || (R > 0 && (!eulers || !maxcc || !angidx || !psr || !soc)) || index_offset < 0)
+        return fail(plan->p.ctx, TOMGPU_ERR_ARG, "null pointer, negative count or offset");
+    if ((flags & 7) == 0 || (flags & ~7))
+        return fail(plan->p.ctx, TOMGPU_ERR_ARG, "flags must select ccc, psr and/or autocorr");
+    TG_TRY(use_device(plan->p.ctx));
+    TG_TRY(plan->p.run_analysis(eulers, R, index_offset, flags, maxcc, angidx, psr, soc));
+    TG_TRY_CUDA(plan->p.ctx, cudaStreamSynchronize(plan->p.ctx->stream));
+    return TOMGPU_OK;
 }
 
 int tomgpu_match_corr_dev(tomgpu_match_plan* plan, const float* t, float* cc) {

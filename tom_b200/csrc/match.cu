@@ -32,6 +32,7 @@
 #include "ctx.h"
 #include "fft3d.h"
 #include "fft_engine.cuh"
+#include "analysis.h"
 #include "match.h"
 #include "misc.h"
 #include "rescore.h"
@@ -549,8 +550,10 @@ static int d0_corr(int N, int T) { return pmod(2 * (N / 2) - T / 2, N); }
 MatchPlan::~MatchPlan() { release(); }
 
 void MatchPlan::release() {
+    delete an;
+    an = nullptr;
     void* ptrs[] = {d_tmpl, d_mask, d_wu, d_fimg, d_mu0, d_sig, d_gam, d_mats, d_t1, d_tc, d_tsum,
-                    d_A, d_Z, d_Q, d_H, d_tmp64};
+                    d_A, d_Z, d_Q, d_H, d_tmp64, d_cc, d_psr, d_soc, d_auto};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     d_tmpl = d_mask = d_wu = nullptr;
@@ -561,6 +564,7 @@ void MatchPlan::release() {
     d_tsum = nullptr;
     d_A = d_Z = d_Q = d_H = nullptr;
     d_tmp64 = nullptr;
+    d_cc = d_psr = d_soc = d_auto = nullptr;
     if (h_mats) cudaFreeHost(h_mats);
     h_mats = nullptr;
     if (ev_mats) cudaEventDestroy(ev_mats);
@@ -634,8 +638,12 @@ int MatchPlan::upload_mats(const float* eulers, int R) {
     return TOMGPU_OK;
 }
 
-int MatchPlan::set_template(const float* tmpl, const float* mask, const float* psf) {
+int MatchPlan::set_template(const float* tmpl, const float* mask, const float* psf, bool raw) {
     cudaStream_t st = ctx->stream;
+    if (an) {  // the peak analysis holds the old mask's spectrum
+        delete an;
+        an = nullptr;
+    }
     TG_TRY_CUDA(ctx, cudaMemcpyAsync(d_mask, mask, sizeof(float) * tn, cudaMemcpyDeviceToDevice, st));
     double* d_red = nullptr;
     TG_TRY(ensure_scratch(ctx, 64));
@@ -647,18 +655,24 @@ int MatchPlan::set_template(const float* tmpl, const float* mask, const float* p
     TG_TRY_CUDA(ctx, cudaStreamSynchronize(st));
     msize = h[0];
     if (msize <= 0) return fail(ctx, TOMGPU_ERR_ARG, "mask has no nonzero voxel");
-    // tom_norm(1e5*(t+1),'mean0+1std'): a = 2e5 t + 2e5 + 100, (a - mean)/std
-    const double s = 2e5, o = 2e5 + 100;
-    TG_TRY_CUDA(ctx, sum_affine_f32(tmpl, tn, s, o, d_red, st));
-    TG_TRY_CUDA(ctx, cudaMemcpyAsync(h, d_red, sizeof(double), cudaMemcpyDeviceToHost, st));
-    TG_TRY_CUDA(ctx, cudaStreamSynchronize(st));
-    const double amean = h[0] / (double)tn;
-    TG_TRY_CUDA(ctx, sum_sqdev_f32(tmpl, tn, s, o, amean, d_red, st));
-    TG_TRY_CUDA(ctx, cudaMemcpyAsync(h, d_red, sizeof(double), cudaMemcpyDeviceToHost, st));
-    TG_TRY_CUDA(ctx, cudaStreamSynchronize(st));
-    const double astd = std::sqrt(h[0] / (double)tn);
-    TG_TRY_CUDA(ctx, normalize_f32(tmpl, d_tmpl, tn, s, o, amean, astd != 0 ? 1.0 / astd : 1.0, st));
-    ctx->launches += 4;
+    if (raw) {
+        // tom_os3_corr without cached statistics: normUnderMask of the given template
+        TG_TRY_CUDA(ctx, cudaMemcpyAsync(d_tmpl, tmpl, sizeof(float) * tn, cudaMemcpyDeviceToDevice, st));
+        psf = nullptr;
+    } else {
+        // tom_norm(1e5*(t+1),'mean0+1std'): a = 2e5 t + 2e5 + 100, (a - mean)/std
+        const double s = 2e5, o = 2e5 + 100;
+        TG_TRY_CUDA(ctx, sum_affine_f32(tmpl, tn, s, o, d_red, st));
+        TG_TRY_CUDA(ctx, cudaMemcpyAsync(h, d_red, sizeof(double), cudaMemcpyDeviceToHost, st));
+        TG_TRY_CUDA(ctx, cudaStreamSynchronize(st));
+        const double amean = h[0] / (double)tn;
+        TG_TRY_CUDA(ctx, sum_sqdev_f32(tmpl, tn, s, o, amean, d_red, st));
+        TG_TRY_CUDA(ctx, cudaMemcpyAsync(h, d_red, sizeof(double), cudaMemcpyDeviceToHost, st));
+        TG_TRY_CUDA(ctx, cudaStreamSynchronize(st));
+        const double astd = std::sqrt(h[0] / (double)tn);
+        TG_TRY_CUDA(ctx, normalize_f32(tmpl, d_tmpl, tn, s, o, amean, astd != 0 ? 1.0 / astd : 1.0, st));
+        ctx->launches += 4;
+    }
     // statistics of the unrotated, filtered template in FP64
     double2* tc64 = nullptr;
     double* tv64 = nullptr;
@@ -845,13 +859,53 @@ int MatchPlan::corr(const float* t, float* cc) {
     TG_TRY_CUDA(ctx, cudaMemsetAsync(d_tsum, 0, sizeof(double), st));
     TG_TRY_CUDA(ctx, launch_spec_x(N[0], d_t1, d_mask, d_A, T, d0_corr(N[0], T[0]), 1, d_tsum, st));
     TG_TRY_CUDA(ctx, launch_spec_z(N[2], d_A, d_Z, T, d0_corr(N[2], T[2]), (int)nh1, 1, st));
+    ctx->launches += 2;
+    return cc_map_tail(cc);
+}
+
+int MatchPlan::cc_map_tail(float* cc) {
+    cudaStream_t st = ctx->stream;
     const long long ncols = nh1 * (long long)N[2];
     TG_TRY_CUDA(ctx, launch_corr_y(N[1], d_fimg, d_Z, d_Q, T[1], d0_corr(N[1], T[1]), ncols, 1, st));
     TG_TRY_CUDA(ctx, launch_inv_z(N[2], d_Q, d_H, N[1], (int)nh1, 1, st));
     const float inv_nm = (float)(1.0 / ((double)nvox * msize));
     TG_TRY_CUDA(ctx, launch_c2r_map(N[0] / 2, d_H, d_mu0, d_gam, d_tsum, N[1], N[2], inv_nm, vmean, 1.0 / msize,
                                     tmean, cc, st));
-    ctx->launches += 5;
+    ctx->launches += 3;
+    return TOMGPU_OK;
+}
+
+// tom_os3_findTemplate.m:255-307 with the PSR and autocorrelation maps of every
+// rotation (tom_os3_analyzePeak) and tom_os3_bestPeak's update for the
+// selected criteria: one rotation at a time, each rotation's maps in FP64.
+int MatchPlan::run_analysis(const float* eulers, int R, int index_offset, int flags, float* maxcc, int* angidx,
+                            float* psr, float* soc) {
+    if (!has_template || !has_volume) return fail(ctx, TOMGPU_ERR_STATE, "template and volume must be set");
+    if (R <= 0) return TOMGPU_OK;
+    if (!an) {
+        an = new (std::nothrow) PeakAnalysis();
+        if (!an) return fail(ctx, TOMGPU_ERR_OOM, "peak-analysis state");
+        int rc = an->create(ctx, N, T, d_mask);
+        if (!rc) rc = alloc((void**)&d_cc, sizeof(float) * nvox);
+        if (!rc) rc = alloc((void**)&d_psr, sizeof(float) * nvox);
+        if (!rc) rc = alloc((void**)&d_soc, sizeof(float) * nvox);
+        if (!rc) rc = alloc((void**)&d_auto, sizeof(float) * tn);
+        if (rc) {
+            delete an;
+            an = nullptr;
+            return rc;
+        }
+    }
+    TG_TRY(upload_mats(eulers, R));
+    for (int r = 0; r < R; ++r) {
+        TG_TRY(prepare_batch(r, 1));          // d_t1: the rotated, masked, filtered template
+        TG_TRY(cc_map_tail(d_cc));
+        TG_TRY(an->autocorr(d_t1, d_auto));
+        TG_TRY(an->spectra(d_cc));
+        TG_TRY(an->psr(d_cc, d_psr));
+        TG_TRY(an->soc(d_cc, d_auto, d_soc));
+        TG_TRY(analysis_update(ctx, d_cc, d_psr, d_soc, nvox, flags, index_offset + r, maxcc, angidx, psr, soc));
+    }
     return TOMGPU_OK;
 }
 

@@ -22,6 +22,8 @@ cudaError_t launch_c2r_fast(int NH, const float2* H, const float* mu0, const flo
 cudaError_t c2c3d_batch(float2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
 cudaError_t c2c3d_batch64(double2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
 
+struct PeakAnalysis;
+
 struct MatchPlan {
     tomgpu_ctx* ctx = nullptr;
     int N[3] = {0, 0, 0}, T[3] = {0, 0, 0};
@@ -53,6 +55,9 @@ struct MatchPlan {
     float2* d_Q = nullptr;
     float2* d_H = nullptr;
     double* d_tmp64 = nullptr;
+    // per-rotation peak analysis (PSR / autocorrelation maps), created on first use
+    PeakAnalysis* an = nullptr;
+    float *d_cc = nullptr, *d_psr = nullptr, *d_soc = nullptr, *d_auto = nullptr;
 
     ~MatchPlan();
     void release();
@@ -60,11 +65,16 @@ struct MatchPlan {
     int create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batch, bool generic);
     int ensure_mats(int R);
     int upload_mats(const float* eulers, int R);
-    int set_template(const float* tmpl, const float* mask, const float* psf);
+    // raw: take the template as given (tom_os3_corr's own statistics) instead
+    // of findTemplate's tom_norm and filter
+    int set_template(const float* tmpl, const float* mask, const float* psf, bool raw = false);
     int set_volume(const float* vol);
     int prepare_batch(int off, int nb);
     int run(const float* eulers, int R, int index_offset, float* maxcc, int* angidx);
     int corr(const float* t, float* cc);
+    int cc_map_tail(float* cc);  // corr_y, inv_z and the FLCF map of the prepared rotation
+    int run_analysis(const float* eulers, int R, int index_offset, int flags, float* maxcc, int* angidx,
+                     float* psr, float* soc);
     int init_results(float* maxcc, int* angidx);
     int rescore(const float* vol, const float* eulers, const int* pos1, int K, double* out);
 };

@@ -118,10 +118,10 @@ struct FVal { const float* a; double s, o; __device__ double operator()(long lon
 struct FSq { const float* a; double s, o, m; __device__ double operator()(long long i) const { double d = (double)a[i] * s + o - m; return d * d; } };
 struct DVal { const double* a; __device__ double operator()(long long i) const { return a[i]; } };
 struct Nz { const float* a; __device__ double operator()(long long i) const { return a[i] != 0.f ? 1.0 : 0.0; } };
-// normUnderMask: mean numerator sum(v*m*(v~=0)), variance numerator
-struct NumMean { const double* v; const float* m; __device__ double operator()(long long i) const { double x = v[i]; return x != 0.0 ? x * (double)m[i] : 0.0; } };
+// normUnderMask (mask = mask~=0 first): mean numerator sum(v*m*(v~=0)), variance numerator
+struct NumMean { const double* v; const float* m; __device__ double operator()(long long i) const { double x = v[i]; return (x != 0.0 && m[i] != 0.f) ? x : 0.0; } };
 struct NumVar { const double* v; const float* m; double mea; __device__ double operator()(long long i) const {
-    const double mk = (double)m[i]; const double t = (mk == 0.0 ? mea : 0.0) + v[i] * mk - mea; return t * t; } };
+    const double mk = m[i] != 0.f ? 1.0 : 0.0; const double t = (mk == 0.0 ? mea : 0.0) + v[i] * mk - mea; return t * t; } };
 
 cudaError_t sum_affine_f32(const float* a, long long n, double s, double o, double* out, cudaStream_t st) {
     return launch_sum(FVal{a, s, o}, n, out, st);

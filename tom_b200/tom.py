@@ -490,8 +490,35 @@ class MatchPlan:
         self.ctx.check(lib().tomgpu_match_set_template_dev(self.handle, _tptr(tmpl_dev), _tptr(mask_dev),
                                                            _tptr(psf_dev) if psf_dev is not None else None))
 
+    def set_template_raw(self, tmpl_dev, mask_dev):
+        """Template statistics of this template as given (tom_os3_corr without cached statistics)."""
+        self._keep = [tmpl_dev, mask_dev]
+        self.ctx.check(lib().tomgpu_match_set_template_raw_dev(self.handle, _tptr(tmpl_dev), _tptr(mask_dev)))
+
     def set_volume(self, vol_dev):
         self.ctx.check(lib().tomgpu_match_set_volume_dev(self.handle, _tptr(vol_dev)))
+
+    def new_analysis_results(self):
+        """(maxcc, angidx, psr, autoc) device buffers, initialised like findTemplate."""
+        import torch
+        x, y, z = self.vol_shape
+        dev = f"cuda:{self.ctx.device}"
+        cc = torch.empty((z, y, x), dtype=torch.float32, device=dev)
+        idx = torch.empty((z, y, x), dtype=torch.int32, device=dev)
+        psr = torch.empty_like(cc)
+        soc = torch.empty_like(cc)
+        self.ctx.check(lib().tomgpu_match_init_analysis_dev(self.handle, _tptr(cc), _tptr(idx), _tptr(psr), _tptr(soc)))
+        return cc, idx, psr, soc
+
+    def run_analysis(self, eulers, maxcc_dev, angidx_dev, psr_dev, autoc_dev, ccc=True, psr=False,
+                     autocorr=False, index_offset: int = 0):
+        """Per-rotation FLCF, PSR and autocorrelation maps with tom_os3_bestPeak's
+        update on the selected criteria (tom_os3_findTemplate's own loop)."""
+        flags = (1 if ccc else 0) | (2 if psr else 0) | (4 if autocorr else 0)
+        e = np.ascontiguousarray(np.asarray(eulers, np.float32).reshape(-1, 3))
+        self.ctx.check(lib().tomgpu_match_run_analysis_dev(self.handle, e.ctypes.data_as(_lib.c_float_p), e.shape[0],
+                                                           int(index_offset), flags, _tptr(maxcc_dev),
+                                                           _tptr(angidx_dev), _tptr(psr_dev), _tptr(autoc_dev)))
 
     def new_results(self):
         import torch
@@ -577,13 +604,20 @@ def match_host(tomo, template, mask, eulers, psf=None, batch: int = 0, ctx: Cont
 
 
 def tom_os3_findTemplate(volume, template, angle_list, mask=None, psf=None, batch: int = 0,
-                         ctx: Context | None = None):
+                         analysis=None, ctx: Context | None = None):
     """[ccc angles] of tom_os3_findTemplate for in-memory inputs (the job/file
     plumbing of the reference is out of scope): template normalised with
     tom_norm(1e5*(t+1),'mean0+1std'), mask = tom_os3_sphereMask(template) when
     not given, psf = optional centred weight.  Returns ccc (float32 [x,y,z],
     -1000 where never updated) and angles (1-based angle-list index as float32,
-    -1000 where never updated), the reference's conventions."""
+    -1000 where never updated), the reference's conventions.
+
+    analysis: None runs the fast search (options.analysis.ccc alone, the
+    only output ccc/angles).  A dict like options.analysis, e.g.
+    {'ccc': 1, 'psr': 1, 'autocorr': 0}, runs the reference's own loop with
+    the PSR and autocorrelation maps of every rotation and tom_os3_bestPeak's
+    update on the selected criteria, and returns (ccc, angles, psr, autoc)
+    (result.ccc/.angles/.psr/.autoc)."""
     ctx = ctx or default_context()
     import torch
     vol = np.asarray(volume, np.float32)
@@ -592,32 +626,83 @@ def tom_os3_findTemplate(volume, template, angle_list, mask=None, psf=None, batc
         mask, _ = tom_os3_sphereMask(t)
     if not np.any(vol):
         # tom_os3_findTemplate.m:221 and :309-313: a volume with mean 0 and
-        # std 0 is not searched; ccc is 0 and the angle map keeps -1000
-        return (np.zeros(vol.shape, np.float32, order="F"), np.full(vol.shape, -1000, np.float32, order="F"))
+        # std 0 is not searched; ccc, psr and autoc are 0 and the angle map keeps -1000
+        z = np.zeros(vol.shape, np.float32, order="F")
+        ang = np.full(vol.shape, -1000, np.float32, order="F")
+        return (z, ang) if analysis is None else (z, ang, z.copy(order="F"), z.copy(order="F"))
     plan = MatchPlan(vol.shape, t.shape, batch=batch, ctx=ctx)
     try:
         td, md = to_device(t, ctx.device), to_device(mask, ctx.device)
         pd = to_device(psf, ctx.device) if psf is not None else None
         plan.set_template(td, md, pd)
         plan.set_volume(to_device(vol, ctx.device))
-        cc, idx = plan.new_results()
-        plan.run(angle_list, cc, idx)
+        if analysis is None:
+            cc, idx = plan.new_results()
+            plan.run(angle_list, cc, idx)
+            extra = ()
+        else:
+            flags = {k: bool(analysis.get(k, 0)) for k in ("ccc", "psr", "autocorr")}
+            if not any(flags.values()):
+                raise ValueError("analysis selects none of ccc, psr, autocorr")
+            cc, idx, pm, am = plan.new_analysis_results()
+            plan.run_analysis(angle_list, cc, idx, pm, am, **flags)
+            extra = (pm, am)
         torch.cuda.synchronize(ctx.device)
         ccc = from_device(cc)
         ang = from_device(idx).astype(np.float32)
         ang = np.where(ang >= 0, ang + 1, -1000).astype(np.float32)
-        return np.asfortranarray(ccc), np.asfortranarray(ang)
+        out = (np.asfortranarray(ccc), np.asfortranarray(ang))
+        return out + tuple(np.asfortranarray(from_device(e)) for e in extra)
     finally:
         plan.close()
+
+
+def tom_os3_analyzePeak(img, peakMap, template, options, ctx: Context | None = None):
+    """res = tom_os3_analyzePeak(img, peakMap, template, options) for
+    options['analysis']['type'] 'PSR' or 'Autocorrelation'
+    (Oscar3/matlabPicker/analyze/tom_os3_analyzePeak.m:61-101,174-190).
+    options['correlation']['mask'] (template-sized) is the mask of the
+    autocorrelation FLCF (tom_os3_sphereMask(template) when absent)."""
+    import torch
+    ctx = ctx or default_context()
+    kind = options["analysis"]["type"]
+    pk = np.asarray(peakMap, np.float32)
+    t = np.asarray(template, np.float32)
+    pd = to_device(pk, ctx.device)
+    out = torch.empty_like(pd)
+    if kind == "PSR":
+        ctx.check(lib().tomgpu_analyze_psr_dev(ctx.handle, _tptr(pd), _cdims(pk.shape), _cdims(t.shape), _tptr(out)))
+    elif kind == "Autocorrelation":
+        mask = options.get("correlation", {}).get("mask")
+        md = to_device(np.asarray(mask, np.float32), ctx.device) if mask is not None else None
+        ctx.check(lib().tomgpu_analyze_autocorr_dev(ctx.handle, _tptr(pd), _cdims(pk.shape),
+                                                    _tptr(to_device(t, ctx.device)), _cdims(t.shape),
+                                                    _tptr(md) if md is not None else None, _tptr(out)))
+    else:
+        raise ValueError("analysis type must be 'PSR' or 'Autocorrelation'")
+    ctx.synchronize()
+    return np.asfortranarray(from_device(out))
+
+
+def tom_os3_template_autocorr(template, ctx: Context | None = None):
+    """tom_os3_corr(template, template) (same-size FLCF, default sphere mask)."""
+    import torch
+    ctx = ctx or default_context()
+    t = np.asarray(template, np.float32)
+    td = to_device(t, ctx.device)
+    out = torch.empty_like(td)
+    ctx.check(lib().tomgpu_template_autocorr_dev(ctx.handle, _tptr(td), _cdims(t.shape), _tptr(out)))
+    ctx.synchronize()
+    return np.asfortranarray(from_device(out))
 
 
 def tom_os3_corr(img, template, options=None, ctx: Context | None = None):
     """FLCF map of one (already rotated, masked, filtered) template against img
     (search/tom_os3_corr.m FLCF branch).  options is a dict that caches the
     search statistics between calls like the reference's options.correlation:
-    keys 'mask' (template-sized), 'templateMean'/'templateSTD' are taken from
-    the plan's template preprocessing of options['template'] when given, else
-    from this template."""
+    keys 'mask' (template-sized); the template statistics are those of
+    findTemplate's preprocessing of options['template'] when given, else
+    tom_os3_normUnderMask of this template (calculationAvailable false)."""
     import torch
     ctx = ctx or default_context()
     options = {} if options is None else options
@@ -630,9 +715,12 @@ def tom_os3_corr(img, template, options=None, ctx: Context | None = None):
     plan = options.get("_plan")
     if plan is None or plan.vol_shape != vol.shape or plan.tmpl_shape != t.shape:
         plan = MatchPlan(vol.shape, t.shape, ctx=ctx)
-        src = options.get("template", t)
-        plan.set_template(to_device(src, ctx.device), to_device(mask, ctx.device),
-                          to_device(options["psf"], ctx.device) if options.get("psf") is not None else None)
+        if options.get("template") is not None:
+            # statistics cached from findTemplate's preprocessed template
+            plan.set_template(to_device(options["template"], ctx.device), to_device(mask, ctx.device),
+                              to_device(options["psf"], ctx.device) if options.get("psf") is not None else None)
+        else:
+            plan.set_template_raw(to_device(t, ctx.device), to_device(mask, ctx.device))
         plan.set_volume(to_device(vol, ctx.device))
         options["_plan"] = plan
     out = torch.empty((vol.shape[2], vol.shape[1], vol.shape[0]), dtype=torch.float32, device=f"cuda:{ctx.device}")
