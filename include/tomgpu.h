@@ -189,7 +189,7 @@ typedef struct {
 /* A matching plan for one volume size and one template size.  It holds the
  * tomogram spectrum, the FP64 local statistics and per-batch workspaces.
  * Volume and template sizes must be FFT lengths the library is built for
- * (8,16,24,32,40,48,64,80,96,128,160,192,232,256,464,512,928 per axis; the
+ * (8,12,16,20,24,32,40,48,64,80,96,128,160,192,232,256,464,512,928 per axis; the
  * template edge along x must keep nx/2 in that list).  params may be NULL. */
 int tomgpu_match_plan_create(tomgpu_ctx* ctx, const int vol_dims[3], const int tmpl_dims[3],
                              const tomgpu_match_params* params, tomgpu_match_plan** out);
@@ -298,6 +298,28 @@ typedef struct {
  * (1 float).  Host output arrays of n_jobs*3, n_jobs*3 and n_jobs floats. */
 int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs, float* angles,
                          float* shifts, float* ccf_peak);
+
+/* One aligned particle for the averaging step of av3_tomomatch. */
+typedef struct {
+    const float* particle;  /* box n, device (after av3_tomomatch's tom_limit(p, -3, 4, 'z')) */
+    const float* wedge;     /* centred wedge weight of its tomogram (av3_wedge), box n, device */
+    float shift[3];         /* tshift, motl rows 11-13 (voxels) */
+    float angles[3];        /* phi, psi, theta, motl rows 17-19 (degrees) */
+} tomgpu_avg_item;
+
+/* The averaging step after alignment (av3/alignment/av3_tomomatch.m:239-249):
+ * for each item in order, average += tom_rotate(tom_shift(particle, -shift),
+ * [-psi -phi -theta]) and wei += 1 where tom_rotate(wedge, [-psi -phi
+ * -theta]) >= 0.5 (the nested tom_limit).  average_dev and wei_dev are device
+ * doubles of box size that accumulate across calls (zero them first). */
+int tomgpu_av3_average_add_dev(tomgpu_ctx* ctx, const int n[3], const tomgpu_avg_item* items, int K,
+                               double* average_dev, double* wei_dev);
+
+/* The weighting that ends an iteration (av3_tomomatch.m:263-265): w = 1./wei
+ * with values above 1e5 set to 0, then real(ifftn(ifftshift(
+ * tom_spheremask(fftshift(fftn(average)).*w, floor(n(1)/2)-3)))).  FP64. */
+int tomgpu_av3_average_final_dev(tomgpu_ctx* ctx, const int n[3], const double* average_dev,
+                                 const double* wei_dev, double* out_dev);
 
 /* ---------------------------------------------------------- peak analysis */
 

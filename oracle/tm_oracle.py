@@ -537,6 +537,60 @@ def find_template_analysis(volume, template, mask, angles, psf=None, ccc=True, p
 
 
 # ---------------------------------------------------------------------------
+# Averaging after alignment
+# ---------------------------------------------------------------------------
+
+def tom_shift(im, delta):
+    """Filtrans/tom_shift.m: Fourier shift by delta (FP64), real part."""
+    im = np.asarray(im, np.float64)
+    dims = im.shape
+    g = np.meshgrid(*[np.arange(-(n // 2), -(n // 2) + n, dtype=np.float64) for n in dims], indexing="ij")
+    d = np.array(delta, np.float64).reshape(3).copy()
+    d[[i for i, n in enumerate(dims) if n == 1]] = 0
+    d = d / np.array(dims, np.float64)
+    x = d[0] * g[0] + d[1] * g[1] + d[2] * g[2]
+    return np.real(np.fft.ifftn(np.fft.fftn(im) * np.exp(-2j * np.pi * np.fft.ifftshift(x))))
+
+
+def tom_limit(a, low, up, mode=None):
+    """Sptrans/tom_limit.m: clamp; 'z': below low -> 0, above up -> up."""
+    a = np.array(a, np.float64, copy=True)
+    if mode == "z":
+        a[a < low] = 0
+        a[a > up] = up
+    else:
+        a[a < low] = low
+        a[a > up] = up
+    return a
+
+
+def av3_average_add(items, shape):
+    """av3/alignment/av3_tomomatch.m:239-249 for (particle, wedge, tshift, [phi psi theta]) items, in order."""
+    avg = np.zeros(shape)
+    wei = np.zeros(shape)
+    for part, wedge, tshift, ang in items:
+        phi, psi, the = ang
+        inv = (-psi, -phi, -the)
+        sh = tom_shift(part, -np.asarray(tshift, np.float64))
+        avg += rotate(sh.astype(np.float32), inv).astype(np.float64)
+        rw = rotate(np.asarray(wedge, np.float32), inv).astype(np.float64)
+        wei += 2 * tom_limit(tom_limit(rw, 0.5, 1, "z"), 0, 0.5)
+    return avg, wei
+
+
+def av3_average_final(avg, wei):
+    """av3_tomomatch.m:263-265: w = 1./wei (above 1e5 -> 0), sphere-masked
+    (radius floor(n/2)-3) spectral weighting of the sum."""
+    with np.errstate(divide="ignore"):
+        w = 1.0 / wei
+    w[w > 100000] = 0
+    lowp = avg.shape[0] // 2 - 3
+    f = np.fft.fftshift(np.fft.fftn(avg)) * w
+    f = f * sphere_mask(avg.shape, lowp, strict=False)
+    return np.real(np.fft.ifftn(np.fft.ifftshift(f)))
+
+
+# ---------------------------------------------------------------------------
 # Angles
 # ---------------------------------------------------------------------------
 

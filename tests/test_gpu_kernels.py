@@ -49,7 +49,7 @@ def test_rotate_batch_with_mask(gpu, oracle):
         assert np.array_equal(got, ref.astype(np.float32))
 
 
-@pytest.mark.parametrize("L", [8, 16, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 232, 256, 464, 512, 928])
+@pytest.mark.parametrize("L", [8, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 232, 256, 464, 512, 928])
 def test_fft_lengths(gpu, L):
     rng = np.random.default_rng(L)
     for shape in [(L, 8, 8), (8, L, 16), (16, 8, L)]:

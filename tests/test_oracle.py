@@ -192,3 +192,20 @@ def test_analysis_ccc_only_is_find_template(oracle):
     assert np.array_equal(i1, i2)
     assert np.abs(c1 - c2).max() < 1e-6
     assert np.all(np.isfinite(p2)) and np.all(np.isfinite(a2))
+
+
+def test_tom_shift_integer(oracle):
+    """tom_shift by whole voxels is a circular shift."""
+    rng = np.random.default_rng(34)
+    a = rng.standard_normal((8, 6, 10))
+    b = oracle.tom_shift(a, (2, -1, 3))
+    assert np.abs(b - np.roll(a, (2, -1, 3), axis=(0, 1, 2))).max() < 1e-12
+
+
+def test_tom_limit(oracle):
+    a = np.array([-4.0, -3.0, 0.5, 4.0, 5.0])
+    assert np.array_equal(oracle.tom_limit(a, -3, 4, "z"), [0, -3, 0.5, 4, 4])
+    assert np.array_equal(oracle.tom_limit(a, -3, 4), [-3, -3, 0.5, 4, 4])
+    # the nested limits of the wedge weight are an indicator of >= 0.5
+    w = np.array([0.0, 0.49, 0.5, 0.7, 1.0])
+    assert np.array_equal(2 * oracle.tom_limit(oracle.tom_limit(w, 0.5, 1, "z"), 0, 0.5), [0, 0, 1, 1, 1])

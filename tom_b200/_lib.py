@@ -49,6 +49,11 @@ class AlignJob(ctypes.Structure):
                 ("theta", ctypes.c_float * 3)]
 
 
+class AvgItem(ctypes.Structure):
+    _fields_ = [("particle", ctypes.c_void_p), ("wedge", ctypes.c_void_p), ("shift", ctypes.c_float * 3),
+                ("angles", ctypes.c_float * 3)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "tomgpu_version": (ctypes.c_char_p, []),
@@ -95,6 +100,9 @@ _SIGS = {
     "tomgpu_match_init_analysis_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "tomgpu_match_run_analysis_dev": (ctypes.c_int, [c_void_p, c_float_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                      c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tomgpu_av3_average_add_dev": (ctypes.c_int, [c_void_p, c_int_p, ctypes.POINTER(AvgItem), ctypes.c_int,
+                                                  c_void_p, c_void_p]),
+    "tomgpu_av3_average_final_dev": (ctypes.c_int, [c_void_p, c_int_p, c_void_p, c_void_p, c_void_p]),
     "tomgpu_analyze_psr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_int_p, c_void_p]),
     "tomgpu_template_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p]),
     "tomgpu_analyze_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p,

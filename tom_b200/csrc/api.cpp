@@ -456,6 +456,29 @@ int tomgpu_wedge_dev(tomgpu_ctx* ctx, const int dims[3], double a, double b, int
     return TOMGPU_OK;
 }
 
+int tomgpu_av3_average_add_dev(tomgpu_ctx* ctx, const int n[3], const tomgpu_avg_item* items, int K, double* avg,
+                               double* wei) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!dims_ok(n) || K < 0 || (K > 0 && !items) || !avg || !wei)
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims or negative count");
+    for (int d = 0; d < 3; ++d)
+        if (!fft_length_supported(n[d])) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "box size not an FFT length");
+    for (int k = 0; k < K; ++k)
+        if (!items[k].particle || !items[k].wedge) return fail(ctx, TOMGPU_ERR_ARG, "item without particle or wedge");
+    if (K == 0) return TOMGPU_OK;
+    TG_TRY(use_device(ctx));
+    return av3_average_add(ctx, n, items, K, avg, wei);
+}
+
+int tomgpu_av3_average_final_dev(tomgpu_ctx* ctx, const int n[3], const double* avg, const double* wei, double* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!dims_ok(n) || !avg || !wei || !out) return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
+    for (int d = 0; d < 3; ++d)
+        if (!fft_length_supported(n[d])) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "box size not an FFT length");
+    TG_TRY(use_device(ctx));
+    return av3_average_final(ctx, n, avg, wei, out);
+}
+
 int tomgpu_analyze_psr_dev(tomgpu_ctx* ctx, const float* peak, const int map_dims[3], const int tmpl_dims[3],
                            float* out) {
     if (!ctx) return TOMGPU_ERR_ARG;

@@ -104,7 +104,7 @@ static cudaError_t dispatch_len(int L, const void* in, void* out, const LineGeom
 #define TG_CASE(N) \
     case N: return launch_lines_t<N, DIR, MODE, C>(in, out, gi, go, nlines, scale, st);
     switch (L) {
-        TG_CASE(8) TG_CASE(16) TG_CASE(24) TG_CASE(32) TG_CASE(40) TG_CASE(48) TG_CASE(64)
+        TG_CASE(8) TG_CASE(12) TG_CASE(16) TG_CASE(20) TG_CASE(24) TG_CASE(32) TG_CASE(40) TG_CASE(48) TG_CASE(64)
         TG_CASE(80) TG_CASE(96) TG_CASE(128) TG_CASE(160) TG_CASE(192) TG_CASE(232)
         TG_CASE(256) TG_CASE(464) TG_CASE(512) TG_CASE(928)
         default: return cudaErrorInvalidValue;
@@ -114,7 +114,7 @@ static cudaError_t dispatch_len(int L, const void* in, void* out, const LineGeom
 
 bool fft_length_supported(int L) {
     switch (L) {
-        case 8: case 16: case 24: case 32: case 40: case 48: case 64: case 80: case 96:
+        case 8: case 12: case 16: case 20: case 24: case 32: case 40: case 48: case 64: case 80: case 96:
         case 128: case 160: case 192: case 232: case 256: case 464: case 512: case 928:
             return true;
         default: return false;

@@ -83,6 +83,8 @@ int corr_norm(tomgpu_ctx* ctx, const float* a, const float* b, const int n[3], c
               const float* psf2, float* out);
 int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3],
               float* peak_out, size_t budget_voxels);
+int av3_average_add(tomgpu_ctx* ctx, const int n[3], const tomgpu_avg_item* items, int K, double* avg, double* wei);
+int av3_average_final(tomgpu_ctx* ctx, const int n[3], const double* avg, const double* wei, double* out);
 
 }  // namespace tg
 

@@ -731,6 +731,102 @@ def tom_os3_corr(img, template, options=None, ctx: Context | None = None):
 
 # ------------------------------------------------------ subtomogram alignment
 
+def av3_average_add(particles, wedges, shifts, angles, average=None, wei=None, ctx: Context | None = None):
+    """Accumulate the averaging step of av3_tomomatch (av3/alignment/av3_tomomatch.m:239-249):
+    average += tom_rotate(tom_shift(p, -shift), [-psi -phi -theta]) and
+    wei += (tom_rotate(wedge, [-psi -phi -theta]) >= 0.5) for each particle in
+    order.  particles/wedges: lists of same-sized volumes ([x,y,z]);
+    shifts: K x 3 (motl rows 11-13); angles: K x 3 phi, psi, theta (rows 17-19).
+    Returns the device sums (float64 tensors [z,y,x]), to pass back in for
+    more particles and to av3_average_final."""
+    import torch
+    ctx = ctx or default_context()
+    K = len(particles)
+    shape = np.shape(particles[0]) if K else np.shape(average)
+    x, y, z = shape
+    dev = f"cuda:{ctx.device}"
+    if average is None:
+        average = torch.zeros((z, y, x), dtype=torch.float64, device=dev)
+        wei = torch.zeros_like(average)
+    if K == 0:
+        return average, wei
+    pd = [to_device(np.asarray(p, np.float32), ctx.device) for p in particles]
+    wcache = {}
+    wd = []
+    for w in wedges:
+        key = id(w)
+        if key not in wcache:
+            wcache[key] = to_device(np.asarray(w, np.float32), ctx.device)
+        wd.append(wcache[key])
+    sh = np.asarray(shifts, np.float32).reshape(K, 3)
+    an = np.asarray(angles, np.float32).reshape(K, 3)
+    items = (_lib.AvgItem * K)()
+    for k in range(K):
+        items[k].particle = _tptr(pd[k])
+        items[k].wedge = _tptr(wd[k])
+        items[k].shift[:] = [float(v) for v in sh[k]]
+        items[k].angles[:] = [float(v) for v in an[k]]
+    ctx.check(lib().tomgpu_av3_average_add_dev(ctx.handle, _cdims(shape), items, K, _tptr(average), _tptr(wei)))
+    return average, wei
+
+
+def av3_average_final(average, wei, ctx: Context | None = None):
+    """The weighting that ends an av3_tomomatch iteration (av3_tomomatch.m:263-265),
+    FP64: returns the new reference ([x,y,z] float64)."""
+    import torch
+    ctx = ctx or default_context()
+    z, y, x = average.shape
+    out = torch.empty_like(average)
+    ctx.check(lib().tomgpu_av3_average_final_dev(ctx.handle, _cdims((x, y, z)), _tptr(average), _tptr(wei),
+                                                 _tptr(out)))
+    ctx.synchronize()
+    return np.asfortranarray(from_device(out))
+
+
+def av3_tomomatch_average(particles, motl, wedgelist, threshold, iclass=0, meanv=None,
+                          ctx: Context | None = None):
+    """The selection and averaging of one av3_tomomatch iteration for an aligned
+    motive list (av3_tomomatch.m:117-118,157-158,239-265).  particles[p] is the
+    volume of motl column p; wedgelist is 3 x W (tomogram number, min and max
+    tilt).  Particles of class 1, 2 or iclass whose CCC (row 1) exceeds
+    threshold * meanv (meanv: mean CCC of those classes, computed from this
+    motl unless given) are averaged and get class 1; the others of those
+    classes get class 2.  Returns (average, wei, motl)."""
+    motl = np.array(motl, np.float64, copy=True)
+    sel = (motl[19] == 1) | (motl[19] == 2) | (motl[19] == iclass)
+    if meanv is None:
+        meanv = float(np.mean(motl[0, sel])) if sel.any() else 0.0
+    wl = np.asarray(wedgelist, np.float64).reshape(3, -1)
+    wedges = {}
+    P, W, S, A = [], [], [], []
+    for p in np.nonzero(sel)[0]:
+        if motl[0, p] > threshold * meanv:
+            itomo = motl[4, p]
+            if itomo not in wedges:
+                col = np.nonzero(wl[0] == itomo)[0][0]
+                wedges[itomo] = av3_wedge(np.zeros(np.shape(particles[p])), wl[1, col], wl[2, col], ctx=ctx)
+            part = np.asarray(particles[p], np.float64)
+            part = np.where(part < -3, 0.0, np.minimum(part, 4.0))   # tom_limit(particle, -3, 4, 'z')
+            P.append(part)
+            W.append(wedges[itomo])
+            S.append(motl[10:13, p])
+            A.append(motl[16:19, p])
+            motl[19, p] = 1
+        else:
+            motl[19, p] = 2
+    avg, wei = av3_average_add(P, W, S, A, ctx=ctx) if P else av3_average_add(
+        [], [], [], [], *_zero_sums(np.shape(particles[0]), ctx), ctx=ctx)
+    return av3_average_final(avg, wei, ctx=ctx), np.asfortranarray(from_device(wei)), motl
+
+
+def _zero_sums(shape, ctx):
+    import torch
+    ctx = ctx or default_context()
+    x, y, z = shape
+    a = torch.zeros((z, y, x), dtype=torch.float64, device=f"cuda:{ctx.device}")
+    return a, torch.zeros_like(a)
+
+
 def tom_spheremask_default(shape):
     """tom_spheremask(ones(n)) with the default radius floor((min(n)-1)/2) (Geom/tom_spheremask.m:41-67)."""
     shape = tuple(shape)
