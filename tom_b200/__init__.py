@@ -10,6 +10,9 @@ from .tom import (  # noqa: F401
     Context,
     MatchPlan,
     av3_align_batch,
+    av3_average_add,
+    av3_average_final,
+    av3_tomomatch_average,
     av3_wedge,
     default_context,
     euler_matrix,
