@@ -321,6 +321,35 @@ int tomgpu_av3_average_add_dev(tomgpu_ctx* ctx, const int n[3], const tomgpu_avg
 int tomgpu_av3_average_final_dev(tomgpu_ctx* ctx, const int n[3], const double* average_dev,
                                  const double* wei_dev, double* out_dev);
 
+/* Wedge of one volume for tomgpu_corr3d_peaks_dev (the WEDGE_REF / WEDGE_PART
+ * forms of tom_mex_corr3d): none ([]), a simple wedge of half-angle
+ * angle_deg (a scalar: tom::SimpleWedge with the cutoff radius
+ * (min(size)-1)/2), or a weight volume (fftshifted, box-sized, device). */
+enum { TOMGPU_WEDGE_NONE = 0, TOMGPU_WEDGE_SIMPLE = 1, TOMGPU_WEDGE_VOLUME = 2 };
+typedef struct {
+    int kind;
+    float angle_deg;
+    const float* volume;
+} tomgpu_wedge_spec;
+
+/* The C++ picker's batched aligner: [out] = tom_mex_corr3d(size, templates,
+ * particles, angles, mask, wedge_ref, wedge_part, 'peak', mask_cc)
+ * (Oscar3/c++Picker/src/mex/tom_mex_corr3d.cpp:53-806 ->
+ * tom::corr3d_batch, src/tom/corr/corr.cpp:1217-1470, with
+ * CorrelationHandlerPeaks, src/tom/corr/correlation_handler.cpp:96-120).
+ * templates / particles: host arrays of nt / np device pointers to box-sized
+ * volumes (n, each axis an FFT length); angles_deg: nang x 3 [phi psi theta]
+ * (host, degrees); mask (device, box) or NULL; wedge_t (nt) / wedge_p (np)
+ * host arrays or NULL; mask_cc: fftshifted peak mask (device) or NULL.
+ * Outputs, host, [particle][template] order (template fastest) like the
+ * MEX's nt x np struct array: peak (3 doubles, 0-based x y z), val (ncc_val,
+ * NaN when no angle gave a peak) and angle_idx (1-based, 0 when none). */
+int tomgpu_corr3d_peaks_dev(tomgpu_ctx* ctx, const int n[3], const float* const* templates, int nt,
+                            const float* const* particles, int np, const double* angles_deg, int nang,
+                            const float* mask, const tomgpu_wedge_spec* wedge_t,
+                            const tomgpu_wedge_spec* wedge_p, const float* mask_cc, double* peak,
+                            double* val, int32_t* angle_idx);
+
 /* ---------------------------------------------------------- peak analysis */
 
 /* tom_os3_analyzePeak(img, peakMap, template, 'PSR')

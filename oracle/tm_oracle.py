@@ -591,6 +591,321 @@ def av3_average_final(avg, wei):
 
 
 # ---------------------------------------------------------------------------
+# The C++ picker's batched aligner (Oscar3/c++Picker): tom_mex_corr3d 'peak'
+# ---------------------------------------------------------------------------
+# Volumes are [x, y, z] arrays (x fastest in memory, Fortran order) like the
+# C++ tom::Volume.  Reduced spectra halve the z axis (the last one), which is
+# what numpy's rfftn/irfftn do on these arrays, and irfftn ignores the
+# imaginary parts of the kz = 0 and kz = nz/2 planes like FFTW's c2r.
+
+CPP_PI = 3.141592653589793238512808959406186204433
+
+
+def cpp_rotmat(phi, theta, psi):
+    """tom_transf_init_rotmat_3d(P, 3, 3, {z, x, z}, {phi, theta, psi})
+    (src/tom/core/transform.c:99-176): P = Rz(phi) Rx(theta) Rz(psi), radians;
+    an angle with angle - floor(angle/(pi/2))*2*pi == 0 is skipped."""
+    P = np.eye(3)
+    for axis, a in ((2, phi), (0, theta), (2, psi)):
+        if a - np.floor(a / (np.pi / 2.0)) * (2.0 * np.pi) == 0.0:
+            continue
+        s, c = np.sin(a), np.cos(a)
+        i, j = (1, 2) if axis == 0 else (0, 1)
+        p0, p1 = P[:, i].copy(), P[:, j].copy()
+        P[:, i] = p0 * c - p1 * s
+        P[:, j] = p0 * s + p1 * c
+    return P
+
+
+def cpp_rotate_coords(shape, phi, psi, theta):
+    """Source coordinates of tom::rotate(src, dst, phi, psi, theta)
+    (include/tom/core/volume_fcn.hpp:206, src/tom/core/volume_fcn.cpp:740-800):
+    src = c + R (dst - c), c = ceil((n-1)/2), as p00*x + (p01*y + (p02*z + p03))."""
+    R = cpp_rotmat(phi, theta, psi)
+    c = np.array([np.ceil((n - 1) / 2.0) for n in shape])
+    t = c - R @ c
+    X, Y, Z = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in shape], indexing="ij")
+    out = []
+    for r in range(3):
+        out.append(R[r, 0] * X + (R[r, 1] * Y + (R[r, 2] * Z + t[r])))
+    return out, R, t
+
+
+def cpp_interp_trilinear(vol, x, y, z):
+    """tom_transf_interpol3d_trilinear_float (src/tom/core/_transform.c:119-262,
+    the active branch): 0 outside [0, n-1]; float weights x - floor(x); the
+    neighbours of an axis are read only where its weight is > 0."""
+    v = np.asarray(vol, np.float32)
+    sx, sy, sz = v.shape
+    out = np.zeros(x.shape, np.float32)
+    ins = (x >= 0) & (y >= 0) & (z >= 0) & (x <= sx - 1) & (y <= sy - 1) & (z <= sz - 1)
+    fx = np.where(ins, x, 0).astype(np.int64)
+    fy = np.where(ins, y, 0).astype(np.int64)
+    fz = np.where(ins, z, 0).astype(np.int64)
+    xo = (np.where(ins, x, 0) - fx).astype(np.float32)
+    yo = (np.where(ins, y, 0) - fy).astype(np.float32)
+    zo = (np.where(ins, z, 0) - fz).astype(np.float32)
+
+    def at(dx, dy, dz):
+        return v[np.minimum(fx + dx, sx - 1), np.minimum(fy + dy, sy - 1), np.minimum(fz + dz, sz - 1)]
+
+    s000 = at(0, 0, 0)
+    s100, s010, s001 = at(1, 0, 0), at(0, 1, 0), at(0, 0, 1)
+    s110, s101, s011, s111 = at(1, 1, 0), at(1, 0, 1), at(0, 1, 1), at(1, 1, 1)
+    f32 = np.float32
+    lx = lambda a, b: (a + (b - a) * xo).astype(f32)
+    ly = lambda a, b: (a + (b - a) * yo).astype(f32)
+    lz = lambda a, b: (a + (b - a) * zo).astype(f32)
+    case = (xo > 0).astype(int) | ((yo > 0).astype(int) << 1) | ((zo > 0).astype(int) << 2)
+    x0yx = (lx(s000, s100) + (lx(s010, s110) - lx(s000, s100)) * yo).astype(f32)
+    r7 = (x0yx + (((lx(s001, s101) + (lx(s011, s111) - lx(s001, s101)) * yo).astype(f32)) - x0yx) * zo).astype(f32)
+    x0y0 = ly(s000, s010)
+    r6 = (x0y0 + ((s001 + (s011 - s001) * yo).astype(f32) - x0y0) * zo).astype(f32)
+    x00x = lx(s000, s100)
+    r5 = (x00x + ((s001 + (s101 - s001) * xo).astype(f32) - x00x) * zo).astype(f32)
+    r3 = (x00x + ((s010 + (s110 - s010) * xo).astype(f32) - x00x) * yo).astype(f32)
+    res = np.select([case == 7, case == 6, case == 5, case == 3, case == 4, case == 2, case == 1],
+                    [r7, r6, r5, r3, lz(s000, s001), ly(s000, s010), lx(s000, s100)], s000)
+    out[ins] = res[ins]
+    return out
+
+
+def cpp_rotate(vol, phi, psi, theta):
+    """tom::rotate(src, dst, phi, psi, theta) with the trilinear interpolation, radians."""
+    (x, y, z), _, _ = cpp_rotate_coords(np.shape(vol), phi, psi, theta)
+    return np.asfortranarray(cpp_interp_trilinear(vol, x, y, z))
+
+
+def ref_transform_lib():
+    lib = _load("libref_transform.so")
+    lib.tom_transf_init_rotmat_3d.argtypes = [_f64p, ctypes.c_size_t, ctypes.c_size_t, _i32p, _f64p]
+    lib.tom_transf_invert.argtypes = [_f64p, _f64p, ctypes.c_int]
+    lib.tom_transf_transf3d_float.argtypes = [
+        _f32p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
+        _f32p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t,
+        _f64p, ctypes.c_int, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]
+    return lib
+
+
+def ref_cpp_rotate(vol, phi, psi, theta):
+    """tom::rotate through the reference's own compiled transform.c: the
+    matrix assembly of volume_fcn.cpp:740-780 written out here, the rotation
+    matrix, the inversion and the transform called from the reference."""
+    lib = ref_transform_lib()
+    v = np.asfortranarray(vol, dtype=np.float32)
+    sx, sy, sz = v.shape
+    P = np.zeros(16)
+    P[15] = 1.0
+    axes = np.array([2, 0, 2], np.int32)
+    ang = np.array([phi, theta, psi], np.float64)
+    lib.tom_transf_init_rotmat_3d(_p(P, _f64p), 4, 3, _p(axes, _i32p), _p(ang, _f64p))
+    lib.tom_transf_invert(_p(P, _f64p), _p(P, _f64p), 4)
+    c = [np.ceil((n - 1) / 2.0) for n in (sx, sy, sz)]
+    for r in range(3):
+        P[4 * r + 3] = c[r] + P[4 * r] * (-c[0]) + P[4 * r + 1] * (-c[1]) + P[4 * r + 2] * (-c[2])
+    out = np.zeros(v.shape, np.float32, order="F")
+    opt = np.zeros(1, np.float64)
+    fn = ctypes.cast(lib.tom_transf_interpol3d_trilinear_float, ctypes.c_void_p)
+    rc = lib.tom_transf_transf3d_float(_p(v, _f32p), sx, sy, sz, sx, sx * sy, _p(out, _f32p), sx, sy, sz, sx,
+                                       sx * sy, _p(P, _f64p), 1, 0.0, fn, opt.ctypes.data_as(ctypes.c_void_p))
+    assert rc == 0
+    return out
+
+
+def cpp_norm_mask(v, mask):
+    """tom::norm_mask(v, mask, NORM_NO_NORM, &variance, false)
+    (src/tom/core/volume_fcn.cpp:172-258): shift to mean 0 under mask != 0,
+    multiply by the mask, shift the masked voxels to mean 0 again; variance =
+    (sum2 - n mean^2) / numel of the masked values."""
+    v = np.asarray(v, np.float64)
+    m = np.asarray(mask, np.float64)
+    inside = m != 0
+    n = inside.sum()
+    mean0 = v[inside].sum() / n
+    w = np.where(inside, (v - mean0) * m, 0.0).astype(np.float32).astype(np.float64)
+    s1, s2 = w[inside].sum(), (w[inside] ** 2).sum()
+    mean1 = s1 / n
+    var = (s2 - n * mean1 * mean1) / v.size
+    if mean1 != 0:
+        w = np.where(inside, w - mean1, w)
+    return w.astype(np.float32), var
+
+
+def cpp_stat(v):
+    """tom::Volume::stat(mean, variance, false): population variance, one pass."""
+    v = np.asarray(v, np.float64)
+    mean = v.sum() / v.size
+    var = ((v * v).sum() - v.size * mean * mean) / v.size
+    return mean, var
+
+
+def cpp_simple_wedge(shape, angle, cutoff, phi=0.0, psi=0.0, theta=0.0, reduced=True):
+    """tom::SimpleWedge::init_wedge_volume (src/tom/core/wedge.cpp:107-180) in
+    float: the frequency k = ((i + ceil(n/2)) mod n) - ceil((n-1)/2) rotated by
+    R(phi, theta, psi) is kept where |R k| <= cutoff and (|z'| < 1e-4 or
+    tan(angle) <= |x'|/|z'|) (cutoff > 0 branch)."""
+    sx, sy, sz = shape
+    f32 = np.float32
+    c = [f32(np.ceil((n - 1) / 2.0)) for n in shape]
+    R = cpp_rotmat(phi, theta, psi)
+    Pd = np.zeros(12)
+    Pd[0:3], Pd[4:7], Pd[8:11] = R[0], R[1], R[2]
+    for r in range(3):
+        Pd[4 * r + 3] = -(Pd[4 * r] * c[0] + Pd[4 * r + 1] * c[1] + Pd[4 * r + 2] * c[2])
+    P = Pd.astype(f32)
+    off = [n // 2 + n % 2 for n in shape]
+    nz = sz // 2 + 1 if reduced else sz
+    xs = ((np.arange(sx) + off[0]) % sx).astype(f32)
+    ys = ((np.arange(sy) + off[1]) % sy).astype(f32)
+    zs = ((np.arange(nz) + off[2]) % sz).astype(f32)
+    X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+    maxdist = f32(np.sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]))
+    tan_a = f32(np.tan(angle))
+    cut = f32(cutoff) if (cutoff > 0 and cutoff < maxdist) else f32(0)
+
+    def row(r, Xv, Yv, Zv):
+        zt = (P[4 * r + 2] * Zv + P[4 * r + 3]).astype(f32)
+        yt = (P[4 * r + 1] * Yv + zt).astype(f32)
+        return (P[4 * r] * Xv + yt).astype(f32)
+
+    x_ = row(0, X, Y, Z)
+    if cut:
+        y_ = row(1, X, Y, Z)
+        z_ = np.abs(row(2, X, Y, Z))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            keep = (np.sqrt((x_ * x_ + y_ * y_ + z_ * z_).astype(f32)) <= cut) & \
+                   ((z_ < f32(1e-4)) | (tan_a <= np.abs(x_) / z_))
+    else:
+        z_ = row(2, X, Y, Z)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            keep = (z_ < f32(1e-4)) | (tan_a <= np.abs(x_) / np.abs(z_))
+    return keep.astype(f32)
+
+
+def cpp_volume_wedge(w, phi=0.0, psi=0.0, theta=0.0):
+    """tom::VolumeWedge::init_wedge_volume (wedge.cpp:330-350): the rotated
+    weight volume, ifftshifted (full grid; the reduced form is its first
+    nz/2+1 z-planes)."""
+    r = cpp_rotate(w, phi, psi, theta)
+    return np.fft.ifftshift(r)
+
+
+def cpp_first_max(v, mask=None):
+    """tom::peak (volume_fcn.cpp:505-540, 890-922): the first voxel of the
+    maximum in x-fastest order, optionally only where mask != 0."""
+    flat = np.asarray(v).ravel(order="F")
+    if mask is not None:
+        mflat = np.asarray(mask).ravel(order="F") != 0
+        cand = np.where(mflat, flat, -np.inf)
+        i = int(np.argmax(cand))
+    else:
+        i = int(np.argmax(flat))
+    return np.unravel_index(i, np.shape(v), order="F"), flat[i]
+
+
+def corr3d_peaks(templates, particles, angles_deg, mask=None, wedge_t=None, wedge_p=None, mask_cc=None):
+    """tom_mex_corr3d(size, templates, particles, angles, mask, wedge_ref,
+    wedge_part, 'peak', mask_cc) -> tom::corr3d_batch
+    (src/mex/tom_mex_corr3d.cpp:700-720, src/tom/corr/corr.cpp:1217-1470) with
+    CorrelationHandlerPeaks (src/tom/corr/correlation_handler.cpp:96-120).
+    wedge_t / wedge_p: per volume None, ('simple', angle_deg) or
+    ('volume', fftshifted weight).  mask_cc is fftshifted.  Returns a dict of
+    arrays indexed [template, particle]: peak (0-based x, y, z), val,
+    angle_idx (0-based, -1 if none) and second (the best value of the other
+    angles, for tie analysis)."""
+    shape = np.shape(particles[0])
+    numel = int(np.prod(shape))
+    nt, npart = len(templates), len(particles)
+    ang = np.asarray(angles_deg, np.float64).reshape(-1, 3) * (CPP_PI / 180.0)
+    cutoff = (min(shape) - 1) // 2
+    lmask = None if mask_cc is None else np.fft.ifftshift(np.asarray(mask_cc))
+
+    def wedge_weight(spec, phi, psi, theta):
+        if spec is None:
+            return None
+        kind, arg = spec
+        if kind == "simple":
+            a = arg * CPP_PI / 180.0
+            if not (a > 0 or cutoff > 0):
+                return None
+            return cpp_simple_wedge(shape, a, cutoff, phi, psi, theta, reduced=True).astype(np.float64)
+        w = np.asarray(arg, np.float64)
+        if np.all(w == 1):
+            return None
+        return cpp_volume_wedge(w.astype(np.float32), phi, psi, theta)[:, :, :shape[2] // 2 + 1].astype(np.float64)
+
+    def var_after(F):
+        r = np.fft.irfftn(F, s=shape, axes=(0, 1, 2)) * numel
+        return (r * r).sum() / numel / (float(numel) * numel)
+
+    # templates: mean 0, std 1 (population), skipped when the variance is 0
+    tn = []
+    for t in templates:
+        m, vv = cpp_stat(t)
+        tn.append(None if not vv else ((np.asarray(t, np.float64) - m) * (1.0 / np.sqrt(vv))).astype(np.float32))
+    # particles: norm_mask or mean removal, spectrum with DC 0
+    pf, pvar = [], []
+    for p in particles:
+        if mask is not None:
+            q, vv = cpp_norm_mask(p, mask)
+        else:
+            m, vv = cpp_stat(p)
+            q = (np.asarray(p, np.float64) - m).astype(np.float32)
+        if not vv:
+            pf.append(None)
+            pvar.append(0.0)
+            continue
+        F = np.fft.rfftn(q.astype(np.float64))
+        F[0, 0, 0] = 0
+        pf.append(F)
+        pvar.append(vv)
+    res = {"peak": np.zeros((nt, npart, 3), np.int64), "val": np.full((nt, npart), np.nan),
+           "angle_idx": np.full((nt, npart), -1, np.int64), "second": np.full((nt, npart), -np.inf)}
+    for ia, (phi, psi, theta) in enumerate(ang):
+        for it in range(nt):
+            if tn[it] is None:
+                continue
+            r = cpp_rotate(tn[it], phi, psi, theta)
+            if mask is not None:
+                r, vt0 = cpp_norm_mask(r, mask)
+            else:
+                m, vt0 = cpp_stat(r)
+                r = (r.astype(np.float32) + np.float32(-m)).astype(np.float32)
+            TF = np.fft.rfftn(r.astype(np.float64))
+            TF[0, 0, 0] = 0
+            wt = wedge_weight(None if wedge_t is None else wedge_t[it], phi, psi, theta)
+            for ip in range(npart):
+                if pf[ip] is None:
+                    continue
+                vp = pvar[ip]
+                PF = pf[ip]
+                if wt is not None:
+                    PF = PF * wt
+                    PF[0, 0, 0] = 0
+                    vp = var_after(PF)
+                TW = TF
+                vt = vt0
+                wp = wedge_weight(None if wedge_p is None else wedge_p[ip], 0.0, 0.0, 0.0)
+                if wp is not None:
+                    TW = TF * wp
+                    TW[0, 0, 0] = 0
+                    vt = var_after(TW)
+                C = TW * np.conj(PF)
+                C[0, 0, 0] = 0
+                cc = np.fft.irfftn(C, s=shape, axes=(0, 1, 2)) * numel / (np.sqrt(vp * vt) * numel * numel)
+                pos, val = cpp_first_max(cc, lmask)
+                if val > res["val"][it, ip] or res["angle_idx"][it, ip] < 0:
+                    if res["angle_idx"][it, ip] >= 0:
+                        res["second"][it, ip] = res["val"][it, ip]
+                    res["val"][it, ip] = val
+                    res["peak"][it, ip] = pos
+                    res["angle_idx"][it, ip] = ia
+                else:
+                    res["second"][it, ip] = max(res["second"][it, ip], val)
+    return res
+
+
+# ---------------------------------------------------------------------------
 # Angles
 # ---------------------------------------------------------------------------
 

@@ -27,7 +27,9 @@ from .tom import (  # noqa: F401
     tom_av3_index2angle,
     tom_apply_weight_function,
     tom_calc_weight_functioninc,
+    cpp_spheremask,
     tom_corr,
+    tom_corr3d,
     tom_emread,
     tom_emwrite,
     tom_fourier,

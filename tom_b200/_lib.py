@@ -54,6 +54,10 @@ class AvgItem(ctypes.Structure):
                 ("angles", ctypes.c_float * 3)]
 
 
+class WedgeSpec(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("angle_deg", ctypes.c_float), ("volume", ctypes.c_void_p)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "tomgpu_version": (ctypes.c_char_p, []),
@@ -103,6 +107,10 @@ _SIGS = {
     "tomgpu_av3_average_add_dev": (ctypes.c_int, [c_void_p, c_int_p, ctypes.POINTER(AvgItem), ctypes.c_int,
                                                   c_void_p, c_void_p]),
     "tomgpu_av3_average_final_dev": (ctypes.c_int, [c_void_p, c_int_p, c_void_p, c_void_p, c_void_p]),
+    "tomgpu_corr3d_peaks_dev": (ctypes.c_int, [c_void_p, c_int_p, ctypes.POINTER(c_void_p), ctypes.c_int,
+                                               ctypes.POINTER(c_void_p), ctypes.c_int, c_double_p, ctypes.c_int,
+                                               c_void_p, ctypes.POINTER(WedgeSpec), ctypes.POINTER(WedgeSpec),
+                                               c_void_p, c_double_p, c_double_p, c_int_p]),
     "tomgpu_analyze_psr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_int_p, c_void_p]),
     "tomgpu_template_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p]),
     "tomgpu_analyze_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p,

@@ -479,6 +479,33 @@ int tomgpu_av3_average_final_dev(tomgpu_ctx* ctx, const int n[3], const double* 
     return av3_average_final(ctx, n, avg, wei, out);
 }
 
+int tomgpu_corr3d_peaks_dev(tomgpu_ctx* ctx, const int n[3], const float* const* templates, int nt,
+                            const float* const* particles, int np, const double* angles_deg, int nang, const float* mask,
+                            const tomgpu_wedge_spec* wedge_t, const tomgpu_wedge_spec* wedge_p, const float* mask_cc,
+                            double* peak, double* val, int32_t* angle_idx) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!dims_ok(n) || nt < 1 || np < 1 || nang < 1 || !templates || !particles || !angles_deg || !peak || !val ||
+        !angle_idx)
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims or empty input");
+    for (int d = 0; d < 3; ++d)
+        if (!fft_length_supported(n[d])) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "box size not an FFT length");
+    for (int t = 0; t < nt; ++t) {
+        if (!templates[t]) return fail(ctx, TOMGPU_ERR_ARG, "null template");
+        if (wedge_t && (wedge_t[t].kind < 0 || wedge_t[t].kind > 2 ||
+                        (wedge_t[t].kind == TOMGPU_WEDGE_VOLUME && !wedge_t[t].volume)))
+            return fail(ctx, TOMGPU_ERR_ARG, "bad template wedge");
+    }
+    for (int p = 0; p < np; ++p) {
+        if (!particles[p]) return fail(ctx, TOMGPU_ERR_ARG, "null particle");
+        if (wedge_p && (wedge_p[p].kind < 0 || wedge_p[p].kind > 2 ||
+                        (wedge_p[p].kind == TOMGPU_WEDGE_VOLUME && !wedge_p[p].volume)))
+            return fail(ctx, TOMGPU_ERR_ARG, "bad particle wedge");
+    }
+    TG_TRY(use_device(ctx));
+    return corr3d_peaks(ctx, n, templates, nt, particles, np, angles_deg, nang, mask, wedge_t, wedge_p, mask_cc, peak,
+                        val, angle_idx);
+}
+
 int tomgpu_analyze_psr_dev(tomgpu_ctx* ctx, const float* peak, const int map_dims[3], const int tmpl_dims[3],
                            float* out) {
     if (!ctx) return TOMGPU_ERR_ARG;

@@ -84,6 +84,9 @@ int corr_norm(tomgpu_ctx* ctx, const float* a, const float* b, const int n[3], c
 int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3],
               float* peak_out, size_t budget_voxels);
 int av3_average_add(tomgpu_ctx* ctx, const int n[3], const tomgpu_avg_item* items, int K, double* avg, double* wei);
+int corr3d_peaks(tomgpu_ctx* ctx, const int n[3], const float* const* templates, int nt, const float* const* particles,
+                 int np, const double* angles_deg, int nang, const float* mask, const tomgpu_wedge_spec* wedge_t,
+                 const tomgpu_wedge_spec* wedge_p, const float* mask_cc, double* peak, double* val, int32_t* angle_idx);
 int av3_average_final(tomgpu_ctx* ctx, const int n[3], const double* avg, const double* wei, double* out);
 
 }  // namespace tg

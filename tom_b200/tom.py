@@ -827,6 +827,89 @@ def _zero_sums(shape, ctx):
     return a, torch.zeros_like(a)
 
 
+def cpp_spheremask(shape, radius):
+    """tom::init_spheremask(mask, radius, 0, 0): 1 where the squared distance
+    from n/2 (integer centre) is <= radius^2, float arithmetic
+    (Oscar3/c++Picker/src/tom/core/volume_fcn.cpp:979-1028)."""
+    f32 = np.float32
+    g = np.meshgrid(*[np.arange(n, dtype=f32) - f32(n // 2) for n in shape], indexing="ij")
+    d2 = (g[0] * g[0] + (g[1] * g[1] + g[2] * g[2])).astype(f32)
+    r = f32(max(radius, 0.0))
+    return np.asfortranarray((d2 <= r * r).astype(f32) if r > 0 else np.zeros(shape, f32))
+
+
+def tom_corr3d(templates, particles, angles, mask=None, wedge_ref=None, wedge_part=None, mask_cc=None,
+               ctx: Context | None = None):
+    """[out] = tom_mex_corr3d(size, templates, particles, angles, mask, wedge_ref,
+    wedge_part, 'peak', mask_cc) (Oscar3/c++Picker/src/mex/tom_mex_corr3d.cpp),
+    the C++ picker's batched aligner on the GPU.
+
+    templates / particles: lists of same-sized volumes [x,y,z]; angles: R x 3
+    [phi psi theta] degrees; mask: None, a radius (tom::init_spheremask) or a
+    volume; wedge_ref / wedge_part: None ([]), one spec for all or a list of
+    specs, a spec being None, an angle in degrees (SimpleWedge) or an
+    fftshifted weight volume; mask_cc: None, a radius or an fftshifted volume.
+    Returns an nt x np object array of dicts with the MEX's fields: peak
+    (0-based [x y z]), ncc_val, angle (degrees), angle_idx (1-based)."""
+    ctx = ctx or default_context()
+    shape = tuple(np.shape(particles[0]))
+    nt, npart = len(templates), len(particles)
+    keep = []
+
+    def dev(a):
+        t = to_device(np.asarray(a, np.float32), ctx.device)
+        keep.append(t)
+        return t
+
+    def vol_or_radius(m):
+        if m is None:
+            return None
+        if np.ndim(m) == 0:
+            return dev(cpp_spheremask(shape, float(m)))
+        return dev(m)
+
+    tp = (ctypes.c_void_p * nt)(*[_tptr(dev(t)).value for t in templates])
+    pp = (ctypes.c_void_p * npart)(*[_tptr(dev(p)).value for p in particles])
+    ang = np.ascontiguousarray(np.asarray(angles, np.float64).reshape(-1, 3))
+    md, mcd = vol_or_radius(mask), vol_or_radius(mask_cc)
+
+    def specs(w, count):
+        if w is None:
+            return None
+        items = list(w) if isinstance(w, (list, tuple)) else [w] * count
+        if len(items) == 1 and count > 1:
+            items = items * count
+        if len(items) != count:
+            raise ValueError("one wedge for all volumes or one per volume")
+        arr = (_lib.WedgeSpec * count)()
+        for i, it in enumerate(items):
+            if it is None:
+                arr[i].kind = 0
+            elif np.ndim(it) == 0:
+                arr[i].kind, arr[i].angle_deg = 1, float(it)
+            else:
+                arr[i].kind, arr[i].volume = 2, _tptr(dev(it))
+        return arr
+
+    wt, wp = specs(wedge_ref, nt), specs(wedge_part, npart)
+    peak = np.zeros((npart, nt, 3), np.float64)
+    val = np.zeros((npart, nt), np.float64)
+    idx = np.zeros((npart, nt), np.int32)
+    ctx.check(lib().tomgpu_corr3d_peaks_dev(ctx.handle, _cdims(shape), tp, nt, pp, npart,
+                                            ang.ctypes.data_as(_lib.c_double_p), len(ang),
+                                            _tptr(md) if md is not None else None, wt, wp,
+                                            _tptr(mcd) if mcd is not None else None,
+                                            peak.ctypes.data_as(_lib.c_double_p), val.ctypes.data_as(_lib.c_double_p),
+                                            idx.ctypes.data_as(_lib.c_int_p)))
+    out = np.empty((nt, npart), dtype=object)
+    for j in range(npart):
+        for i in range(nt):
+            k = int(idx[j, i])
+            out[i, j] = {"peak": peak[j, i].copy(), "ncc_val": float(val[j, i]),
+                         "angle": ang[k - 1].copy() if k > 0 else np.full(3, np.nan), "angle_idx": k}
+    return out
+
+
 def tom_spheremask_default(shape):
     """tom_spheremask(ones(n)) with the default radius floor((min(n)-1)/2) (Geom/tom_spheremask.m:41-67)."""
     shape = tuple(shape)
