@@ -372,7 +372,9 @@ def main():
                 "config": {"workload": args.workload, "tomogram": list(cfg["N"]), "template": cfg["T"],
                            "angles": len(grid), "rot_per_step": rps, "rotation_batch": args.batch,
                            "parallelism": f"angle-partitioned x{world}",
-                           "l2": "inputs larger than L2 (tomogram spectrum 269 MB, per-batch spectra 2.2 GB)"},
+                           "l2": "inputs larger than L2 (tomogram spectrum %d MB, per-batch spectra %.1f GB)" % (
+                               8 * (cfg["N"][0] // 2 + 1) * cfg["N"][1] * cfg["N"][2] // 10**6,
+                               8 * (cfg["N"][0] // 2 + 1) * cfg["N"][1] * cfg["N"][2] * args.batch / 1e9)},
                 "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                              "algorithmic_bytes_per_launch": ab, "avg_launch_ms": avg_s * 1e3},
