@@ -38,6 +38,11 @@ WORKLOAD = "exhaustive_512x512x256"
 METRIC = "TM rot*voxel/s (exhaustive FLCF, 512x512x256 tomogram, 40^3 template)"
 UNIT = "rot*voxel/s"
 
+# DRAM bytes (read + write) per launch of a kernel class at the default batch
+# of 16, from one ncu capture of a smaller volume with the same x edge, scaled
+# by the voxel count (profiles/traffic_c2r_flcf_profile_512x128x64.md).
+TRAFFIC = {"exhaustive_512x512x256": {"c2r_flcf": 16 * (336688128 + 24345856)}}
+
 
 def parse():
     p = argparse.ArgumentParser()
@@ -307,11 +312,7 @@ def main():
     nb = args.batch
     ab = algorithmic_bytes(dom, cfg, nb)
     achieved = ab / avg_s / 1e9 if avg_s > 0 else 0.0
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        with open(tfile) as f:
-            traffic = json.load(f).get(args.workload, {}).get(dom)
+    traffic = TRAFFIC.get(args.workload, {}).get(dom)
     shares = {k: round(v[0] / max(sum(x[0] for x in kt.values()), 1e-9), 4) for k, v in kt.items()}
 
     # accuracy: top-K peaks of the max-CC map rescored in FP64 by direct sums
