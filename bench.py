@@ -312,7 +312,7 @@ def main():
     nb = args.batch
     ab = algorithmic_bytes(dom, cfg, nb)
     achieved = ab / avg_s / 1e9 if avg_s > 0 else 0.0
-    traffic = TRAFFIC.get(args.workload, {}).get(dom)
+    traffic = TRAFFIC.get(args.workload, {}).get(dom) if args.batch == 16 else None
     shares = {k: round(v[0] / max(sum(x[0] for x in kt.values()), 1e-9), 4) for k, v in kt.items()}
 
     # accuracy: top-K peaks of the max-CC map rescored in FP64 by direct sums
