@@ -1,5 +1,6 @@
-"""The register-resident hot kernels (power-of-two sizes) against the generic
-kernels and against FP64 direct sums at sampled voxels, at the benchmark size."""
+"""The register-resident hot kernels (power-of-two sizes and the 928 / 464
+edges) against the generic kernels and against FP64 direct sums at sampled
+voxels, at the benchmark sizes."""
 import numpy as np
 import pytest
 
@@ -20,7 +21,8 @@ def _run(gpu, vol, tmpl, mask, angles, generic, batch):
     return out
 
 
-@pytest.mark.parametrize("workload,n_ang", [("profile_256x256x128", 12), ("exhaustive_512x512x256", 10)])
+@pytest.mark.parametrize("workload,n_ang", [("profile_256x256x128", 12), ("exhaustive_512x512x256", 10),
+                                            ("exhaustive_928x928x464", 6)])
 def test_fast_equals_generic_and_direct_sums(gpu, oracle, workload, n_ang):
     from tom_b200 import synth
     cfg = synth.CONFIGS[workload]
@@ -45,3 +47,19 @@ def test_fast_equals_generic_and_direct_sums(gpu, oracle, workload, n_ang):
     # planted copies are found at their own orientation
     hits = fidx[tuple(d["positions"].astype(int).T)]
     assert (hits == d["euler_index"]).mean() >= 0.8
+
+
+@pytest.mark.parametrize("shape", [(928, 928, 48), (64, 64, 464), (928, 48, 464)])
+def test_928_464_kernels_equal_generic(gpu, oracle, shape):
+    """Each 928 / 464 kernel on its own (the other axes on the generic kernels)."""
+    rng = np.random.default_rng(9)
+    vol = rng.standard_normal(shape).astype(np.float32)
+    T = 48
+    tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
+    mask = oracle.sphere_mask((T, T, T), 23).astype(np.float32)
+    angles = oracle.av3_angle_grid((0, 0, 0), (40, 40, 40), (320, 320, 160))[::97][:5]
+    fcc, fidx = _run(gpu, vol, tmpl, mask, angles, False, 3)
+    gcc, gidx = _run(gpu, vol, tmpl, mask, angles, True, 2)
+    scale = np.abs(gcc).max()
+    assert np.abs(fcc - gcc).max() <= 1e-5 * scale
+    assert (fidx != gidx).mean() < 1e-3

@@ -235,12 +235,13 @@ __global__ void __launch_bounds__(256, 4) k_c2r_w(const float2* __restrict__ H, 
 }
 
 // ------------------------------------------------------------- dispatch
-bool fast_corr_y(int NY, int Ty) { return (NY == 256 || NY == 512) && Ty <= 64; }
-bool fast_inv_z(int NZ) { return NZ == 256; }
-bool fast_c2r(int NH) { return NH == 128 || NH == 256; }
+bool fast_corr_y(int NY, int Ty) { return (NY == 256 || NY == 512 || NY == 928) && Ty <= 64; }
+bool fast_inv_z(int NZ) { return NZ == 256 || NZ == 464; }
+bool fast_c2r(int NH) { return NH == 128 || NH == 256 || NH == 464; }
 
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
                                long long ncols, int nb, cudaStream_t st) {
+    if (NY == 928) return launch_corr_y_p928(fimg, Z, Q, Ty, d0y, ncols, nb, st);
     const unsigned g = (unsigned)((ncols + 7) / 8);
     const size_t smem = sizeof(float2) * (NY * 17 + 64 + 8 * 128);
     if (NY == 512) {
@@ -256,6 +257,7 @@ cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, floa
 }
 
 cudaError_t launch_inv_z_fast(int NZ, const float2* Q, float2* H, int Ny, int nh1, int nb, cudaStream_t st) {
+    if (NZ == 464) return launch_inv_z_p464(Q, H, Ny, nh1, nb, st);
     if (NZ != 256) return cudaErrorInvalidValue;
     dim3 g((Ny + 15) / 16, nh1, nb);
     k_inv_z_b256<<<g, 256, 0, st>>>(Q, H, Ny, nh1, twiddle_table<float2>(256));
@@ -282,6 +284,8 @@ cudaError_t launch_c2r_fast(int NH, const float2* H, const float* mu0, const flo
         return launch_c2r_t<256>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     if (NH == 128)
         return launch_c2r_t<128>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
+    if (NH == 464)
+        return launch_c2r_p464(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     return cudaErrorInvalidValue;
 }
 

@@ -1,0 +1,304 @@
+// Register-resident FLCF kernels for the 928 / 464 edges (the 928x928x464
+// tomogram): y edge 928 = 29 x 32, z edge 464 = 29 x 16, x edge 928 (complex
+// half length 464).  Same arithmetic contract as the generic kernels in
+// match.cu, two-factor Cooley-Tukey instead of the generic engine's three
+// shared-memory passes:
+//
+//   corr_y_p928  one warp per spectrum column: each lane a 29-point DFT of
+//                the samples q + 32 m (in registers), the 928-point twiddle,
+//                one warp-private exchange, 29 lanes a 32-point DFT; the
+//                product with F_I (staged once per column); the inverse the
+//                same way back.  The y samples and the output stay in natural
+//                order, so the global accesses of a lane group are contiguous.
+//   inv_z_p464   16 y lines x 16 threads per block: 29 16-point DFTs per line
+//                straight from global memory, one block exchange, 16 29-point
+//                DFTs per line straight back to global memory.
+//   c2r_p464     8 x lines per block, 16 threads per line: the half-spectrum
+//                unpack, 29 16-point DFTs, a half-warp exchange, 16 29-point
+//                DFTs, the running maximum over the batch in registers and the
+//                FLCF at the read-modify-write (as c2r_w).
+//
+// Index map (inverse; the forward is the conjugate): with n = q + Q m and
+// k = k1 + 29 k2,  y(n) = sum_k1 W29^(m k1) WL^(q k1) sum_k2 Y(k) WQ^(q k2).
+#include "ctx.h"
+#include "match.h"
+#include "pq29.cuh"
+#include "twiddles.h"
+#include "warp_fft.cuh"
+
+namespace tg {
+
+namespace {
+
+tgpq::Cos29 cos29_table() {
+    tgpq::Cos29 t;
+    for (int j = 0; j < 29; ++j) {
+        const double a = 2.0 * M_PI * (double)j / 29.0;
+        t.c[j] = (float)std::cos(a);
+        t.s[j] = (float)std::sin(a);
+    }
+    return t;
+}
+
+constexpr int CY_WARPS = 4, CY_RS = 33;
+
+__global__ void __launch_bounds__(32 * CY_WARPS) k_corr_y_p928(const float2* __restrict__ fimg,
+                                                               const float2* __restrict__ Z, float2* __restrict__ Q,
+                                                               int Ty, int d0y, long long ncols, int nb,
+                                                               const float2* __restrict__ tw_g, tgpq::Cos29 cs) {
+    constexpr int NY = 928, P = 29, RS = CY_RS, WS = 2 * P * RS + 128;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* T = reinterpret_cast<float2*>(smem_raw);  // [29][RS]: W928^(-q k1)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float2* xb = T + P * RS + warp * WS;  // [29][RS] exchange
+    float2* fs = xb + P * RS;         // [29][RS] F_I at k1 + 29 k2
+    float2* zs = fs + P * RS;         // [2][64] template column
+    for (int i = threadIdx.x; i < NY; i += blockDim.x) {
+        const int k1 = i >> 5, q = i & 31;
+        T[k1 * RS + q] = __ldg(tw_g + (q * k1) % NY);
+    }
+    const long long col = (long long)blockIdx.x * CY_WARPS + warp;
+    if (col < ncols) {
+        for (int e = lane; e < NY; e += 32) {
+            const int k2 = e / P, k1 = e - k2 * P;
+            fs[k1 * RS + k2] = fimg[col * NY + e];
+        }
+        const float2* zc = Z + col * Ty;
+        if (lane < Ty) zs[lane] = zc[lane];
+        if (lane + 32 < Ty) zs[lane + 32] = zc[lane + 32];
+    }
+    __syncthreads();
+    if (col >= ncols) return;
+    for (int b = 0; b < nb; ++b) {
+        float2 n0 = make_float2(0.f, 0.f), n1 = make_float2(0.f, 0.f);
+        if (b + 1 < nb) {
+            const float2* zc = Z + ((long long)(b + 1) * ncols + col) * Ty;
+            if (lane < Ty) n0 = zc[lane];
+            if (lane + 32 < Ty) n1 = zc[lane + 32];
+        }
+        const float2* cur = zs + (b & 1) * 64;
+        {
+            float2 v[P];
+#pragma unroll
+            for (int m = 0; m < P; ++m) {
+                int jy = lane + 32 * m - d0y;
+                if (jy < 0) jy += NY;
+                v[m] = jy < Ty ? cur[jy] : make_float2(0.f, 0.f);
+            }
+            tgpq::dft29<-1>(v, cs);
+#pragma unroll
+            for (int k1 = 0; k1 < P; ++k1) xb[k1 * RS + lane] = cmul(v[k1], T[k1 * RS + lane]);
+        }
+        __syncwarp();
+        if (lane < P) {
+            float2 u[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) u[q] = xb[lane * RS + q];
+            tgfft::dft32<-1>(u);
+#pragma unroll
+            for (int k2 = 0; k2 < 32; ++k2) u[k2] = cmulc(fs[lane * RS + k2], u[k2]);
+            tgfft::dft32<+1>(u);
+#pragma unroll
+            for (int q = 0; q < 32; ++q) xb[lane * RS + q] = cmulc(u[q], T[lane * RS + q]);
+        }
+        __syncwarp();
+        {
+            float2 v[P];
+#pragma unroll
+            for (int k1 = 0; k1 < P; ++k1) v[k1] = xb[k1 * RS + lane];
+            tgpq::dft29<+1>(v, cs);
+            float2* qc = Q + ((long long)b * ncols + col) * NY;
+#pragma unroll
+            for (int m = 0; m < P; ++m) qc[lane + 32 * m] = v[m];
+        }
+        float2* nx = zs + ((b + 1) & 1) * 64;
+        if (lane < Ty) nx[lane] = n0;
+        if (lane + 32 < Ty) nx[lane + 32] = n1;
+        __syncwarp();
+    }
+}
+
+constexpr int IZ_LS = 465;
+
+__global__ void __launch_bounds__(256) k_inv_z_p464(const float2* __restrict__ Q, float2* __restrict__ H, int Ny,
+                                                    int nh1, const float2* __restrict__ tw_g, tgpq::Cos29 cs) {
+    constexpr int NZ = 464, P = 29, LS = IZ_LS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* s = reinterpret_cast<float2*>(smem_raw);  // [16][LS]
+    float2* T = s + 16 * LS;                           // [29][16]: W464^(+q k1)
+    for (int i = threadIdx.x; i < P * 16; i += blockDim.x) {
+        const int k1 = i >> 4, q = i & 15;
+        T[i] = cconj(__ldg(tw_g + (q * k1) % NZ));
+    }
+    const int tid = threadIdx.x, l = tid & 15, j = tid >> 4;
+    const int y = blockIdx.x * 16 + l, kx = blockIdx.y, b = blockIdx.z;
+    const bool ok = y < Ny;
+    const long long base = ((long long)b * nh1 + kx) * NZ * Ny;
+    __syncthreads();
+#pragma unroll 1
+    for (int k1 = j; k1 < P; k1 += 16) {
+        float2 u[16];
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2)
+            u[k2] = ok ? Q[base + (long long)(k1 + P * k2) * Ny + y] : make_float2(0.f, 0.f);
+        tgfft::dft16<+1>(u);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) s[l * LS + k1 * 16 + q] = cmul(u[q], T[k1 * 16 + q]);
+    }
+    __syncthreads();
+    float2 v[P];
+#pragma unroll
+    for (int k1 = 0; k1 < P; ++k1) v[k1] = s[l * LS + k1 * 16 + j];
+    tgpq::dft29<+1>(v, cs);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < P; ++m) H[base + (long long)(j + 16 * m) * Ny + y] = v[m];
+    }
+}
+
+TG_D void cp_async8_p(void* smem_dst, const void* gsrc, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
+}
+TG_D void cp_async_commit_p() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+TG_D void cp_async_wait1_p() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+constexpr int C2_YT = 8, C2_TS = 466, C2_XR = 17, C2_XL = 29 * C2_XR;
+
+// The running maximum keeps u = out/(N M) + kappa_b and the batch index of
+// the best rotation per voxel (as k_c2r_w); the FLCF is applied at the
+// read-modify-write.
+__global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_p464(const float2* __restrict__ H, const float* __restrict__ mu0,
+                                                             const float* __restrict__ gam,
+                                                             const double* __restrict__ tsum, int Ny, int Nz, int nb,
+                                                             float inv_nm, double c_mean, double inv_m, double mu_t,
+                                                             int index0, float* __restrict__ maxcc,
+                                                             int* __restrict__ angidx, const float2* __restrict__ tw_h,
+                                                             const float2* __restrict__ tw_x, tgpq::Cos29 cs) {
+    constexpr int NH = 464, NH1 = NH + 1, NX = 2 * NH, P = 29, YT = C2_YT, TS = C2_TS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* tile = reinterpret_cast<float2*>(smem_raw);  // [2][YT][TS]
+    float2* xb = tile + 2 * YT * TS;                      // [YT][29][17] exchange
+    float2* T = xb + YT * C2_XL;                          // [16][32]: W464^(+q k1) at [q][k1]
+    float2* twx = T + 16 * 32;                            // [NH]: W928^(+k)
+    float* kaps = reinterpret_cast<float*>(twx + NH);     // [nb]
+    const int tid = threadIdx.x, line = tid >> 4, q = tid & 15;
+    const int y0 = blockIdx.x * YT, z = blockIdx.y, y = y0 + line;
+    for (int i = tid; i < P * 16; i += blockDim.x) {
+        const int k1 = i >> 4, qq = i & 15;
+        T[qq * 32 + k1] = cconj(__ldg(tw_h + (qq * k1) % NH));
+    }
+    for (int i = tid; i < NH; i += blockDim.x) twx[i] = cconj(__ldg(tw_x + i));
+    for (int b = tid; b < nb; b += blockDim.x) kaps[b] = (float)(c_mean * (tsum[b] * inv_m - mu_t));
+    float bu[P][2];
+    unsigned bb[P];
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        bu[m][0] = bu[m][1] = -INFINITY;
+        bb[m] = 0u;
+    }
+    auto issue = [&](int b, int which) {
+        float2* t = tile + which * YT * TS;
+        const long long hb = (long long)b * NH1 * Nz * Ny;
+        for (int e = tid; e < YT * NH1; e += blockDim.x) {
+            const int kx = e / YT, yl = e - kx * YT;
+            const bool okl = y0 + yl < Ny;
+            const float2* src = H + hb + ((long long)kx * Nz + z) * Ny + (okl ? y0 + yl : 0);
+            cp_async8_p(t + yl * TS + kx, src, okl ? 8 : 0);
+        }
+        cp_async_commit_p();
+    };
+    issue(0, 0);
+    float2* xl = xb + line * C2_XL;
+    for (int b = 0; b < nb; ++b) {
+        if (b + 1 < nb) issue(b + 1, (b + 1) & 1);
+        else cp_async_commit_p();
+        cp_async_wait1_p();
+        __syncthreads();
+        const float2* X = tile + (b & 1) * YT * TS + line * TS;
+        // unpack and the inner 16-point DFTs: k = k1 + 29 k2
+#pragma unroll 1
+        for (int k1 = q; k1 < P; k1 += 16) {
+            float2 u[16];
+#pragma unroll
+            for (int k2 = 0; k2 < 16; ++k2) {
+                const int k = k1 + P * k2;
+                const float2 xa = X[k], xc = cconj(X[NH - k]);
+                const float2 d = cmul(twx[k], csub(xa, xc));
+                u[k2] = cadd(cadd(xa, xc), make_float2(-d.y, d.x));
+            }
+            tgfft::dft16<+1>(u);
+#pragma unroll
+            for (int qq = 0; qq < 16; ++qq) xl[k1 * C2_XR + qq] = cmul(u[qq], T[qq * 32 + k1]);
+        }
+        __syncwarp();
+        float2 v[P];
+#pragma unroll
+        for (int k1 = 0; k1 < P; ++k1) v[k1] = xl[k1 * C2_XR + q];
+        tgpq::dft29<+1>(v, cs);
+        const float kap = kaps[b];
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const float u0 = fmaf(v[m].x, inv_nm, kap);
+            const float u1 = fmaf(v[m].y, inv_nm, kap);
+            if (u0 > bu[m][0]) { bu[m][0] = u0; bb[m] = (bb[m] & 0xFFFF0000u) | (unsigned)b; }
+            if (u1 > bu[m][1]) { bu[m][1] = u1; bb[m] = (bb[m] & 0x0000FFFFu) | ((unsigned)b << 16); }
+        }
+        __syncthreads();  // the tile and the exchange are rewritten next
+    }
+    if (y >= Ny) return;
+    const float mt = (float)mu_t;
+    const long long row = ((long long)z * Ny + y) * NX;
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const long long v = row + 2 * (q + 16 * m);
+        const float2 a = __ldg(reinterpret_cast<const float2*>(mu0 + v));
+        const float2 g = __ldg(reinterpret_cast<const float2*>(gam + v));
+        float2 cur = *reinterpret_cast<const float2*>(maxcc + v);
+        int2 ci = *reinterpret_cast<const int2*>(angidx + v);
+        bool ch = false;
+        const float c0 = g.x != 0.f ? (bu[m][0] - a.x * mt) * g.x : 0.f;
+        const float c1 = g.y != 0.f ? (bu[m][1] - a.y * mt) * g.y : 0.f;
+        const int b0 = g.x != 0.f ? (int)(bb[m] & 0xFFFFu) : 0, b1 = g.y != 0.f ? (int)(bb[m] >> 16) : 0;
+        if (c0 > cur.x) { cur.x = c0; ci.x = index0 + b0; ch = true; }
+        if (c1 > cur.y) { cur.y = c1; ci.y = index0 + b1; ch = true; }
+        if (ch) {
+            *reinterpret_cast<float2*>(maxcc + v) = cur;
+            *reinterpret_cast<int2*>(angidx + v) = ci;
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_corr_y_p928(const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y, long long ncols,
+                               int nb, cudaStream_t st) {
+    const size_t smem = sizeof(float2) * (29 * CY_RS + CY_WARPS * (2 * 29 * CY_RS + 128));
+    cudaFuncSetAttribute(k_corr_y_p928, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const unsigned g = (unsigned)((ncols + CY_WARPS - 1) / CY_WARPS);
+    k_corr_y_p928<<<g, 32 * CY_WARPS, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(928),
+                                                  cos29_table());
+    return cudaGetLastError();
+}
+
+cudaError_t launch_inv_z_p464(const float2* Q, float2* H, int Ny, int nh1, int nb, cudaStream_t st) {
+    const size_t smem = sizeof(float2) * (16 * IZ_LS + 29 * 16);
+    cudaFuncSetAttribute(k_inv_z_p464, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 g((Ny + 15) / 16, nh1, nb);
+    k_inv_z_p464<<<g, 256, smem, st>>>(Q, H, Ny, nh1, twiddle_table<float2>(464), cos29_table());
+    return cudaGetLastError();
+}
+
+cudaError_t launch_c2r_p464(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
+                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
+                            int* angidx, cudaStream_t st) {
+    const size_t smem = sizeof(float2) * (2 * C2_YT * C2_TS + C2_YT * C2_XL + 16 * 32 + 464) + sizeof(float) * nb;
+    cudaFuncSetAttribute(k_c2r_p464, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 g((Ny + C2_YT - 1) / C2_YT, Nz);
+    k_c2r_p464<<<g, 16 * C2_YT, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc,
+                                            angidx, twiddle_table<float2>(464), twiddle_table<float2>(928),
+                                            cos29_table());
+    return cudaGetLastError();
+}
+
+}  // namespace tg
