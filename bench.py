@@ -22,6 +22,7 @@ inside the timed region).
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -41,7 +42,7 @@ UNIT = "rot*voxel/s"
 # DRAM bytes (read + write) per launch of a kernel class at the default batch
 # of 16, from one ncu capture of a smaller volume with the same x edge, scaled
 # by the voxel count (profiles/traffic_c2r_flcf_profile_512x128x64.md).
-TRAFFIC = {"exhaustive_512x512x256": {"c2r_flcf": 16 * (336688128 + 24345856)}}
+TRAFFIC = {"exhaustive_512x512x256": {"c2r_flcf": {16: 16 * (336688128 + 24345856)}}}
 
 
 def parse():
@@ -51,7 +52,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--rot-per-step", type=int, default=64)
-    p.add_argument("--batch", type=int, default=16)
+    p.add_argument("--batch", type=int, default=0,
+                   help="rotation batch; 0 = autotune over 8, 16, 32 before the timed region")
     p.add_argument("--e2e-rot", type=int, default=1024)
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -269,6 +271,16 @@ def main():
     plan.set_template(tb.to_device(d["template"], local), tb.to_device(mask, local))
     vol_dev = tb.to_device(d["tomo"], local)
     plan.set_volume(vol_dev)
+    tune = None
+    if args.batch == 0:
+        e, _ = chunk(grid, 0, world, rank, 64)
+        best, tune = plan.autotune(e, (8, 16, 32))
+        if dist:  # every rank runs the same batch: the smallest of the ranks' choices
+            t = torch.tensor([best], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MIN)
+            if int(t.item()) != best:
+                best, _ = plan.autotune(e, (int(t.item()),))
+        args.batch = best
     cc, idx = plan.new_results()
     rps = args.rot_per_step
 
@@ -312,7 +324,7 @@ def main():
     nb = args.batch
     ab = algorithmic_bytes(dom, cfg, nb)
     achieved = ab / avg_s / 1e9 if avg_s > 0 else 0.0
-    traffic = TRAFFIC.get(args.workload, {}).get(dom) if args.batch == 16 else None
+    traffic = TRAFFIC.get(args.workload, {}).get(dom, {}).get(args.batch)
     shares = {k: round(v[0] / max(sum(x[0] for x in kt.values()), 1e-9), 4) for k, v in kt.items()}
 
     # accuracy: top-K peaks of the max-CC map rescored in FP64 by direct sums
@@ -345,11 +357,13 @@ def main():
             e, _ = chunk(grid, s, world, rank, args.e2e_rot)
             from tom_b200 import _lib
             vol = tomo_h
+            prm = _lib.MatchParams()
+            prm.batch = args.batch
             ectx.check(_lib.lib().tomgpu_match(
                 ectx.handle, vol.ctypes.data, tb.tom._cdims(cfg["N"]), d["template"].ctypes.data,
                 tb.tom._cdims((cfg["T"],) * 3), mask.ctypes.data, None,
                 np.ascontiguousarray(e, np.float32).ctypes.data_as(_lib.c_float_p), len(e),
-                None, cc_h.ctypes.data, idx_h.ctypes.data))
+                ctypes.byref(prm), cc_h.ctypes.data, idx_h.ctypes.data))
         te = time.perf_counter() - t0
         if dist:
             t = torch.tensor([te], device="cuda")
@@ -374,6 +388,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": args.workload, "tomogram": list(cfg["N"]), "template": cfg["T"],
                            "angles": len(grid), "rot_per_step": rps, "rotation_batch": args.batch,
+                           "batch_autotune_ms_per_rotation": tune,
                            "parallelism": f"angle-partitioned x{world}",
                            "l2": "inputs larger than L2 (tomogram spectrum %d MB, per-batch spectra %.1f GB)" % (
                                8 * (cfg["N"][0] // 2 + 1) * cfg["N"][1] * cfg["N"][2] // 10**6,

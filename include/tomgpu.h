@@ -221,6 +221,15 @@ int tomgpu_match_set_template_dev(tomgpu_match_plan* plan, const float* tmpl_dev
 int tomgpu_match_set_template_raw_dev(tomgpu_match_plan* plan, const float* tmpl_dev,
                                       const float* mask_dev);
 
+/* Rotation-batch autotuner: times R rotations of `eulers` (host, R x 3
+ * degrees) for each of the n_cand candidate batch sizes (a candidate whose
+ * work buffers do not fit is skipped), keeps the fastest per rotation for
+ * the plan and returns it in *best (0 if none fitted: the plan keeps its
+ * batch).  ms_per_rot (n_cand floats, or NULL) receives the measured times.
+ * Uses scratch result buffers; needs the template and volume set. */
+int tomgpu_match_autotune(tomgpu_match_plan* plan, const float* eulers, int R, const int* cands, int n_cand,
+                          int* best, float* ms_per_rot);
+
 /* Fill maxcc_dev with -1000 and angidx_dev with -1 (findTemplate's initial
  * ccc/angles, :215-218, with 0-based indices). */
 int tomgpu_match_init_results_dev(tomgpu_match_plan* plan, float* maxcc_dev, int32_t* angidx_dev);

@@ -63,3 +63,26 @@ def test_928_464_kernels_equal_generic(gpu, oracle, shape):
     scale = np.abs(gcc).max()
     assert np.abs(fcc - gcc).max() <= 1e-5 * scale
     assert (fidx != gidx).mean() < 1e-3
+
+
+def test_autotune_keeps_results(gpu, oracle):
+    """The batch autotuner picks a candidate and the plan still finds the same maxima."""
+    import torch
+    rng = np.random.default_rng(10)
+    vol = rng.standard_normal((64, 48, 40)).astype(np.float32)
+    T = 16
+    tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
+    mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
+    angles = oracle.av3_angle_grid((0, 0, 0), (60, 60, 60), (300, 300, 180))[:20]
+    ref_cc, ref_idx = _run(gpu, vol, tmpl, mask, angles, False, 4)
+    plan = gpu.MatchPlan(vol.shape, tmpl.shape, batch=4)
+    plan.set_template(gpu.to_device(tmpl), gpu.to_device(mask))
+    plan.set_volume(gpu.to_device(vol))
+    best, ms = plan.autotune(angles, (2, 5, 8))
+    assert best in (2, 5, 8) and set(ms) == {2, 5, 8}
+    cc, idx = plan.new_results()
+    plan.run(angles, cc, idx)
+    torch.cuda.synchronize()
+    assert np.abs(gpu.from_device(cc) - ref_cc).max() <= 1e-6 * np.abs(ref_cc).max()
+    assert (gpu.from_device(idx) != ref_idx).mean() < 1e-3
+    plan.close()

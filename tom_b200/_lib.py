@@ -100,6 +100,8 @@ _SIGS = {
     "tomgpu_match_init_results_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
     "tomgpu_match_run_dev": (ctypes.c_int, [c_void_p, c_float_p, ctypes.c_int, ctypes.c_int, c_void_p, c_void_p]),
     "tomgpu_match_corr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    "tomgpu_match_autotune": (ctypes.c_int, [c_void_p, c_float_p, ctypes.c_int, c_int_p, ctypes.c_int, c_int_p,
+                                             c_float_p]),
     "tomgpu_match_set_template_raw_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
     "tomgpu_match_init_analysis_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "tomgpu_match_run_analysis_dev": (ctypes.c_int, [c_void_p, c_float_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,

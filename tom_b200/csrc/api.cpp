@@ -693,6 +693,14 @@ int tomgpu_match_run_dev(tomgpu_match_plan* plan, const float* eulers, int R, in
     return plan->p.run(eulers, R, index_offset, maxcc, angidx);
 }
 
+int tomgpu_match_autotune(tomgpu_match_plan* plan, const float* eulers, int R, const int* cands, int n_cand,
+                          int* best, float* ms_per_rot) {
+    if (!plan) return TOMGPU_ERR_ARG;
+    if (!eulers || !cands || R <= 0 || n_cand <= 0) return fail(plan->p.ctx, TOMGPU_ERR_ARG, "bad autotune arguments");
+    TG_TRY(use_device(plan->p.ctx));
+    return plan->p.autotune(eulers, R, cands, n_cand, best, ms_per_rot);
+}
+
 int tomgpu_match_set_template_raw_dev(tomgpu_match_plan* plan, const float* t, const float* mask) {
     if (!plan) return TOMGPU_ERR_ARG;
     if (!t || !mask) return fail(plan->p.ctx, TOMGPU_ERR_ARG, "template and mask are required");

@@ -601,13 +601,7 @@ int MatchPlan::create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batc
     TG_TRY(alloc((void**)&d_mu0, sizeof(float) * nvox));
     TG_TRY(alloc((void**)&d_sig, sizeof(float) * nvox));
     TG_TRY(alloc((void**)&d_gam, sizeof(float) * nvox));
-    TG_TRY(alloc((void**)&d_t1, sizeof(float) * tn * B));
-    TG_TRY(alloc((void**)&d_tc, sizeof(float2) * tn * B));
-    TG_TRY(alloc((void**)&d_tsum, sizeof(double) * B));
-    TG_TRY(alloc((void**)&d_A, sizeof(float2) * nh1 * T[1] * T[2] * B));
-    TG_TRY(alloc((void**)&d_Z, sizeof(float2) * nh1 * N[2] * T[1] * B));
-    TG_TRY(alloc((void**)&d_Q, sizeof(float2) * hs * B));
-    TG_TRY(alloc((void**)&d_H, sizeof(float2) * hs * B));
+    TG_TRY(alloc_batch(B));
     TG_TRY_CUDA(ctx, cudaEventCreateWithFlags(&ev_mats, cudaEventDisableTiming));
     // twiddle tables are built now so that later calls allocate nothing
     const int lens[] = {N[0], N[1], N[2], N[0] / 2, T[0], T[1], T[2]};
@@ -616,6 +610,96 @@ int MatchPlan::create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batc
             return fail(ctx, TOMGPU_ERR_CUDA, "twiddle table allocation failed");
     }
     return TOMGPU_OK;
+}
+
+// The per-batch work buffers (rotated templates, their spectra, Q and H).
+void MatchPlan::free_batch() {
+    void* ptrs[] = {d_t1, d_tc, d_tsum, d_A, d_Z, d_Q, d_H};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    d_t1 = nullptr;
+    d_tc = nullptr;
+    d_tsum = nullptr;
+    d_A = d_Z = d_Q = d_H = nullptr;
+    bytes_held -= batch_bytes;
+    batch_bytes = 0;
+}
+
+int MatchPlan::alloc_batch(int nb) {
+    const long long hs = nh1 * (long long)N[1] * N[2];
+    const int64_t before = bytes_held;
+    int rc = TOMGPU_OK;
+    if (!rc) rc = alloc((void**)&d_t1, sizeof(float) * tn * nb);
+    if (!rc) rc = alloc((void**)&d_tc, sizeof(float2) * tn * nb);
+    if (!rc) rc = alloc((void**)&d_tsum, sizeof(double) * nb);
+    if (!rc) rc = alloc((void**)&d_A, sizeof(float2) * nh1 * T[1] * T[2] * nb);
+    if (!rc) rc = alloc((void**)&d_Z, sizeof(float2) * nh1 * N[2] * T[1] * nb);
+    if (!rc) rc = alloc((void**)&d_Q, sizeof(float2) * hs * nb);
+    if (!rc) rc = alloc((void**)&d_H, sizeof(float2) * hs * nb);
+    batch_bytes = bytes_held - before;
+    if (rc) {
+        free_batch();
+        return rc;
+    }
+    B = nb;
+    return TOMGPU_OK;
+}
+
+// Rotation-batch autotuner: for each candidate batch size the per-batch
+// buffers are re-allocated (a candidate that does not fit is skipped) and R
+// rotations are timed with CUDA events on the context's stream after one
+// untimed batch; the fastest per rotation is kept.  Results go to scratch
+// buffers, so the caller's maxima are untouched.
+int MatchPlan::autotune(const float* eulers, int R, const int* cands, int nc, int* best_out, float* ms_out) {
+    if (!has_template || !has_volume) return fail(ctx, TOMGPU_ERR_STATE, "template and volume must be set");
+    if (R <= 0 || nc <= 0) return fail(ctx, TOMGPU_ERR_ARG, "no rotations or no candidates");
+    cudaStream_t st = ctx->stream;
+    float* cc = nullptr;
+    int* idx = nullptr;
+    if (cudaMalloc(&cc, sizeof(float) * nvox) || cudaMalloc(&idx, sizeof(int) * nvox)) {
+        if (cc) cudaFree(cc);
+        cudaGetLastError();
+        return fail(ctx, TOMGPU_ERR_OOM, "autotune scratch");
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int orig = B;
+    int best = -1;
+    float best_ms = 0.f;
+    int rc = TOMGPU_OK;
+    for (int c = 0; c < nc && !rc; ++c) {
+        const int nb = cands[c];
+        if (nb <= 0 || nb > 4096) continue;
+        free_batch();
+        if (alloc_batch(nb)) {  // does not fit: skip
+            ctx->last_error.clear();
+            continue;
+        }
+        if ((rc = init_results(cc, idx))) break;
+        if ((rc = run(eulers, std::min(R, nb), 0, cc, idx))) break;
+        cudaEventRecord(e0, st);
+        if ((rc = run(eulers, R, 0, cc, idx))) break;
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1)) { rc = cuda_fail(ctx, cudaGetLastError(), "autotune"); break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)R;
+        if (ms_out) ms_out[c] = ms;
+        if (best < 0 || ms < best_ms) {
+            best = nb;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(cc);
+    cudaFree(idx);
+    free_batch();
+    const int keep = best > 0 ? best : orig;
+    if (!rc) rc = alloc_batch(keep);
+    if (best_out) *best_out = best > 0 ? best : 0;
+    return rc;
 }
 
 int MatchPlan::ensure_mats(int R) {

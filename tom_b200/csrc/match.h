@@ -38,6 +38,7 @@ struct MatchPlan {
     bool generic_only = false;  // force the generic kernels (tests compare both paths)
     long long nvox = 0, nh1 = 0, tn = 0;
     int64_t bytes_held = 0;
+    int64_t batch_bytes = 0;
     bool has_template = false, has_volume = false, has_psf = false;
     double msize = 0, tmean = 0, tstd = 0, vmean = 0;
     // template state
@@ -70,6 +71,9 @@ struct MatchPlan {
     void release();
     int alloc(void** p, size_t bytes);
     int create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batch, bool generic);
+    int alloc_batch(int nb);
+    void free_batch();
+    int autotune(const float* eulers, int R, const int* cands, int nc, int* best, float* ms_per_rot);
     int ensure_mats(int R);
     int upload_mats(const float* eulers, int R);
     // raw: take the template as given (tom_os3_corr's own statistics) instead

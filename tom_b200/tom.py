@@ -490,6 +490,18 @@ class MatchPlan:
         self.ctx.check(lib().tomgpu_match_set_template_dev(self.handle, _tptr(tmpl_dev), _tptr(mask_dev),
                                                            _tptr(psf_dev) if psf_dev is not None else None))
 
+    def autotune(self, eulers, candidates=(8, 16, 32)):
+        """Pick the rotation batch with the fastest per-rotation time on these
+        rotations (the plan keeps it); returns (best, {batch: ms per rotation})."""
+        e = np.ascontiguousarray(np.asarray(eulers, np.float32).reshape(-1, 3))
+        c = np.ascontiguousarray(np.asarray(candidates, np.int32))
+        ms = np.zeros(len(c), np.float32)
+        best = ctypes.c_int(0)
+        self.ctx.check(lib().tomgpu_match_autotune(self.handle, e.ctypes.data_as(_lib.c_float_p), e.shape[0],
+                                                   c.ctypes.data_as(_lib.c_int_p), len(c), ctypes.byref(best),
+                                                   ms.ctypes.data_as(_lib.c_float_p)))
+        return best.value, {int(b): float(m) for b, m in zip(c, ms) if m > 0}
+
     def set_template_raw(self, tmpl_dev, mask_dev):
         """Template statistics of this template as given (tom_os3_corr without cached statistics)."""
         self._keep = [tmpl_dev, mask_dev]
