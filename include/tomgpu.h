@@ -359,6 +359,36 @@ int tomgpu_corr3d_peaks_dev(tomgpu_ctx* ctx, const int n[3], const float* const*
                             const tomgpu_wedge_spec* wedge_p, const float* mask_cc, double* peak,
                             double* val, int32_t* angle_idx);
 
+/* ---------------------------------------------------- learned proposer
+ * Training and inference kernels of the candidate proposer (a dilated 3-D
+ * convolutional network, tom_b200/proposer.py); no counterpart in the
+ * reference.  Volumes are [C][Z][Y][X] FP32 device buffers of one sample;
+ * weights [Cout][Cin][27] (taps x fastest), bias [Cout].  Gradient outputs
+ * accumulate (zero them first); loss_dev is one device double that
+ * accumulates. */
+int tomgpu_cnn_conv3d_fwd_dev(tomgpu_ctx* ctx, const float* in, int ci, const int dims[3], const float* w,
+                              const float* b, int co, int dil, int relu, float* out);
+int tomgpu_cnn_conv3d_bwd_data_dev(tomgpu_ctx* ctx, const float* gout, int co, const int dims[3], const float* w,
+                                   int ci, int dil, float* gin);
+int tomgpu_cnn_conv3d_bwd_weight_dev(tomgpu_ctx* ctx, const float* in, int ci, const int dims[3], const float* gout,
+                                     int co, int dil, float* gw, float* gb);
+/* Dense layer over P samples: out[k][p] = b[k] + sum_c W[k][c] F[c][p]. */
+int tomgpu_cnn_dense_fwd_dev(tomgpu_ctx* ctx, const float* W, const float* b, const float* F, int K, int C,
+                             int64_t P, int relu, float* out);
+int tomgpu_cnn_dense_bwd_dev(tomgpu_ctx* ctx, const float* W, const float* F, const float* g, int K, int C,
+                             int64_t P, float* gF, float* gW, float* gb);
+int tomgpu_cnn_relu_bwd_dev(tomgpu_ctx* ctx, float* g, const float* act, int64_t n);
+int tomgpu_cnn_bce_dev(tomgpu_ctx* ctx, const float* logit, const float* target, int64_t n, float pos_weight,
+                       float* grad, double* loss_dev);
+int tomgpu_cnn_softmax_ce_dev(tomgpu_ctx* ctx, const float* logits, const int32_t* labels, int K, int P,
+                              float* grad, double* loss_dev);
+int tomgpu_cnn_adam_dev(tomgpu_ctx* ctx, float* p, const float* g, float* m, float* v, int64_t n, float lr,
+                        float beta1, float beta2, float eps, int step);
+int tomgpu_cnn_gather_dev(tomgpu_ctx* ctx, const float* f, int C, int64_t nv, const int64_t* idx, int P,
+                          float* out);
+int tomgpu_cnn_scatter_add_dev(tomgpu_ctx* ctx, const float* g, int C, int64_t nv, const int64_t* idx, int P,
+                               float* gf);
+
 /* ---------------------------------------------------------- peak analysis */
 
 /* tom_os3_analyzePeak(img, peakMap, template, 'PSR')

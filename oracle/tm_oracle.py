@@ -906,6 +906,70 @@ def corr3d_peaks(templates, particles, angles_deg, mask=None, wedge_t=None, wedg
 
 
 # ---------------------------------------------------------------------------
+# The learned proposer's layers (no reference counterpart): FP64 restatement
+# of the convolution, dense layer and losses, for the gradient checks.
+# ---------------------------------------------------------------------------
+# Volumes [C][Z][Y][X]; weights [Cout][Cin][27], tap t = tx + 3 ty + 9 tz,
+# offset (tx-1, ty-1, tz-1) * dilation, zero padding, "same" size.
+
+def cnn_conv3d(x, w, b, dil):
+    x = np.asarray(x, np.float64)
+    w = np.asarray(w, np.float64)
+    ci, Z, Y, X = x.shape
+    xp = np.pad(x, ((0, 0), (dil, dil), (dil, dil), (dil, dil)))
+    out = np.zeros((w.shape[0], Z, Y, X))
+    for t in range(27):
+        ox, oy, oz = t % 3, (t // 3) % 3, t // 9
+        patch = xp[:, oz * dil:oz * dil + Z, oy * dil:oy * dil + Y, ox * dil:ox * dil + X]
+        out += np.einsum("oc,czyx->ozyx", w[:, :, t], patch)
+    if b is not None:
+        out += np.asarray(b, np.float64)[:, None, None, None]
+    return out
+
+
+def cnn_conv3d_grads(x, w, dil, gout):
+    """(d/dx, d/dw, d/db) of sum(gout * conv3d(x, w, b, dil))."""
+    x = np.asarray(x, np.float64)
+    w = np.asarray(w, np.float64)
+    g = np.asarray(gout, np.float64)
+    ci, Z, Y, X = x.shape
+    xp = np.pad(x, ((0, 0), (dil, dil), (dil, dil), (dil, dil)))
+    gxp = np.zeros_like(xp)
+    gw = np.zeros(w.shape)
+    for t in range(27):
+        ox, oy, oz = t % 3, (t // 3) % 3, t // 9
+        sl = (slice(None), slice(oz * dil, oz * dil + Z), slice(oy * dil, oy * dil + Y), slice(ox * dil, ox * dil + X))
+        gw[:, :, t] = np.einsum("ozyx,czyx->oc", g, xp[sl])
+        gxp[sl] += np.einsum("oc,ozyx->czyx", w[:, :, t], g)
+    gx = gxp[:, dil:dil + Z, dil:dil + Y, dil:dil + X]
+    return gx, gw, g.sum(axis=(1, 2, 3))
+
+
+def cnn_bce(logit, target, pos_weight):
+    z = np.asarray(logit, np.float64)
+    y = np.asarray(target, np.float64)
+    sp_neg = np.log1p(np.exp(-np.abs(z))) + np.maximum(-z, 0)
+    w = np.where(y > 0, pos_weight, 1.0)
+    loss = (w * (y * sp_neg + (1 - y) * (sp_neg + z))).mean()
+    grad = w * (1 / (1 + np.exp(-z)) - y) / z.size
+    return loss, grad
+
+
+def cnn_softmax_ce(logits, labels):
+    """logits [K][P] -> (mean CE, grad)."""
+    l = np.asarray(logits, np.float64)
+    m = l.max(axis=0)
+    e = np.exp(l - m)
+    sm = e / e.sum(axis=0)
+    P = l.shape[1]
+    lab = np.asarray(labels)
+    loss = -np.mean(np.log(sm[lab, np.arange(P)]))
+    g = sm.copy()
+    g[lab, np.arange(P)] -= 1
+    return loss, g / P
+
+
+# ---------------------------------------------------------------------------
 # Angles
 # ---------------------------------------------------------------------------
 

@@ -257,3 +257,48 @@ def test_corr3d_finds_the_rotation(oracle):
     assert res["angle_idx"][0, 0] == 1
     assert tuple(res["peak"][0, 0]) == (0, 0, 0)
     assert res["val"][0, 0] > 0.99
+
+
+# ------------------------------------------------------- learned proposer oracle
+
+def test_cnn_conv_grads_finite_difference(oracle):
+    """The FP64 convolution gradients against central differences."""
+    rng = np.random.default_rng(37)
+    x = rng.standard_normal((2, 5, 6, 7))
+    w = rng.standard_normal((3, 2, 27)) * 0.3
+    b = rng.standard_normal(3)
+    g = rng.standard_normal((3, 5, 6, 7))
+    for dil in (1, 2):
+        gx, gw, gb = oracle.cnn_conv3d_grads(x, w, dil, g)
+        f = lambda xx, ww, bb: float((g * oracle.cnn_conv3d(xx, ww, bb, dil)).sum())
+        h = 1e-6
+        for idx in [(0, 1, 2, 3), (1, 4, 5, 6), (0, 0, 0, 0)]:
+            e = np.zeros_like(x)
+            e[idx] = h
+            assert abs((f(x + e, w, b) - f(x - e, w, b)) / (2 * h) - gx[idx]) < 1e-6
+        for idx in [(0, 1, 13), (2, 0, 0), (1, 1, 26)]:
+            e = np.zeros_like(w)
+            e[idx] = h
+            assert abs((f(x, w + e, b) - f(x, w - e, b)) / (2 * h) - gw[idx]) < 1e-6
+        assert np.allclose(gb, g.sum(axis=(1, 2, 3)))
+
+
+def test_cnn_losses_finite_difference(oracle):
+    rng = np.random.default_rng(38)
+    z = rng.standard_normal(50)
+    y = (rng.random(50) > 0.8).astype(float)
+    loss, g = oracle.cnn_bce(z, y, 5.0)
+    h = 1e-6
+    for i in (0, 7, 33):
+        e = np.zeros(50)
+        e[i] = h
+        fd = (oracle.cnn_bce(z + e, y, 5.0)[0] - oracle.cnn_bce(z - e, y, 5.0)[0]) / (2 * h)
+        assert abs(fd - g[i]) < 1e-8
+    lg = rng.standard_normal((6, 4))
+    lab = np.array([0, 5, 2, 2])
+    loss, g = oracle.cnn_softmax_ce(lg, lab)
+    for idx in [(0, 0), (5, 1), (3, 2)]:
+        e = np.zeros_like(lg)
+        e[idx] = h
+        fd = (oracle.cnn_softmax_ce(lg + e, lab)[0] - oracle.cnn_softmax_ce(lg - e, lab)[0]) / (2 * h)
+        assert abs(fd - g[idx]) < 1e-8

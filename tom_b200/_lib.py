@@ -113,6 +113,28 @@ _SIGS = {
                                                ctypes.POINTER(c_void_p), ctypes.c_int, c_double_p, ctypes.c_int,
                                                c_void_p, ctypes.POINTER(WedgeSpec), ctypes.POINTER(WedgeSpec),
                                                c_void_p, c_double_p, c_double_p, c_int_p]),
+    "tomgpu_cnn_conv3d_fwd_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_void_p, c_void_p,
+                                                 ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p]),
+    "tomgpu_cnn_conv3d_bwd_data_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_void_p,
+                                                      ctypes.c_int, ctypes.c_int, c_void_p]),
+    "tomgpu_cnn_conv3d_bwd_weight_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_void_p,
+                                                        ctypes.c_int, ctypes.c_int, c_void_p, c_void_p]),
+    "tomgpu_cnn_dense_fwd_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int64, ctypes.c_int, c_void_p]),
+    "tomgpu_cnn_dense_bwd_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int64, c_void_p, c_void_p, c_void_p]),
+    "tomgpu_cnn_relu_bwd_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int64]),
+    "tomgpu_cnn_bce_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int64, ctypes.c_float, c_void_p,
+                                          c_void_p]),
+    "tomgpu_cnn_softmax_ce_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, c_void_p,
+                                                 c_void_p]),
+    "tomgpu_cnn_adam_dev": (ctypes.c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64,
+                                           ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                           ctypes.c_int]),
+    "tomgpu_cnn_gather_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int64, c_void_p, ctypes.c_int,
+                                             c_void_p]),
+    "tomgpu_cnn_scatter_add_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int64, c_void_p,
+                                                  ctypes.c_int, c_void_p]),
     "tomgpu_analyze_psr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_int_p, c_void_p]),
     "tomgpu_template_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p]),
     "tomgpu_analyze_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p,

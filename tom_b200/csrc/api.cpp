@@ -835,3 +835,144 @@ int tomgpu_match(tomgpu_ctx* ctx, const float* tomo, const int vol[3], const flo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- learned proposer
+namespace tg {
+cudaError_t cnn_conv_fwd(const float* in, int ci, const int d[3], const float* w, const float* b, int co, int dil,
+                         int relu, float* out, cudaStream_t st);
+cudaError_t cnn_conv_wgrad(const float* in, int ci, const int d[3], const float* gout, int co, int dil, float* gw,
+                           float* gb, cudaStream_t st);
+cudaError_t cnn_flip_weights(const float* w, int co, int ci, float* wt, cudaStream_t st);
+cudaError_t cnn_relu_bwd(float* g, const float* act, long long n, cudaStream_t st);
+cudaError_t cnn_bce(const float* logit, const float* target, long long n, float pw, float* grad, double* loss,
+                    cudaStream_t st);
+cudaError_t cnn_softmax_ce(const float* logits, const int* labels, int K, int P, float* grad, double* loss,
+                           cudaStream_t st);
+cudaError_t cnn_adam(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+                     int step, cudaStream_t st);
+cudaError_t cnn_dense_fwd(const float* W, const float* b, const float* F, int K, int C, long long P, int relu,
+                          float* out, cudaStream_t st);
+cudaError_t cnn_dense_bwd(const float* W, const float* F, const float* g, int K, int C, long long P, float* gF,
+                          float* gW, float* gb, cudaStream_t st);
+cudaError_t cnn_gather(const float* f, int C, long long nv, const long long* idx, int P, float* out, cudaStream_t st);
+cudaError_t cnn_scatter_add(const float* g, int C, long long nv, const long long* idx, int P, float* gf,
+                            cudaStream_t st);
+}  // namespace tg
+
+static bool cnn_ch_ok(int c) { return c == 1 || c == 8 || c == 16 || c == 32 || c == 64; }
+
+int tomgpu_cnn_conv3d_fwd_dev(tomgpu_ctx* ctx, const float* in, int ci, const int dims[3], const float* w,
+                              const float* b, int co, int dil, int relu, float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!in || !w || !out || !dims_ok(dims) || ci < 1 || dil < 1 || dil > 16)
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims, channels or dilation");
+    if (!cnn_ch_ok(co)) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "output channels must be 1, 8, 16, 32 or 64");
+    TG_TRY(use_device(ctx));
+    ctx->launches += 1;
+    TG_TRY_CUDA(ctx, cnn_conv_fwd(in, ci, dims, w, b, co, dil, relu, out, ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_conv3d_bwd_data_dev(tomgpu_ctx* ctx, const float* gout, int co, const int dims[3], const float* w,
+                                   int ci, int dil, float* gin) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!gout || !w || !gin || !dims_ok(dims) || co < 1 || dil < 1 || dil > 16)
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims, channels or dilation");
+    if (!cnn_ch_ok(ci)) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "input channels must be 1, 8, 16, 32 or 64");
+    TG_TRY(use_device(ctx));
+    TG_TRY(ensure_scratch(ctx, sizeof(float) * (size_t)co * ci * 27));
+    float* wt = static_cast<float*>(ctx->scratch);
+    TG_TRY_CUDA(ctx, cnn_flip_weights(w, co, ci, wt, ctx->stream));
+    TG_TRY_CUDA(ctx, cnn_conv_fwd(gout, co, dims, wt, nullptr, ci, dil, 0, gin, ctx->stream));
+    ctx->launches += 2;
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_conv3d_bwd_weight_dev(tomgpu_ctx* ctx, const float* in, int ci, const int dims[3], const float* gout,
+                                     int co, int dil, float* gw, float* gb) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!in || !gout || !gw || !dims_ok(dims) || ci < 1 || co < 1 || dil < 1 || dil > 16)
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims, channels or dilation");
+    TG_TRY(use_device(ctx));
+    ctx->launches += gb ? 2 : 1;
+    TG_TRY_CUDA(ctx, cnn_conv_wgrad(in, ci, dims, gout, co, dil, gw, gb, ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_dense_fwd_dev(tomgpu_ctx* ctx, const float* W, const float* b, const float* F, int K, int C, int64_t P,
+                             int relu, float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!W || !F || !out || K < 1 || C < 1 || P < 1) return fail(ctx, TOMGPU_ERR_ARG, "bad dense layer arguments");
+    TG_TRY(use_device(ctx));
+    ctx->launches += 1;
+    TG_TRY_CUDA(ctx, cnn_dense_fwd(W, b, F, K, C, P, relu, out, ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_dense_bwd_dev(tomgpu_ctx* ctx, const float* W, const float* F, const float* g, int K, int C, int64_t P,
+                             float* gF, float* gW, float* gb) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!W || !F || !g || K < 1 || C < 1 || P < 1) return fail(ctx, TOMGPU_ERR_ARG, "bad dense layer arguments");
+    TG_TRY(use_device(ctx));
+    ctx->launches += 3;
+    TG_TRY_CUDA(ctx, cnn_dense_bwd(W, F, g, K, C, P, gF, gW, gb, ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_relu_bwd_dev(tomgpu_ctx* ctx, float* g, const float* act, int64_t n) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!g || !act || n < 0) return fail(ctx, TOMGPU_ERR_ARG, "null pointer");
+    TG_TRY(use_device(ctx));
+    ctx->launches += 1;
+    TG_TRY_CUDA(ctx, cnn_relu_bwd(g, act, n, ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_bce_dev(tomgpu_ctx* ctx, const float* logit, const float* target, int64_t n, float pos_weight,
+                       float* grad, double* loss_dev) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!logit || !target || !grad || !loss_dev || n < 1) return fail(ctx, TOMGPU_ERR_ARG, "null pointer");
+    TG_TRY(use_device(ctx));
+    ctx->launches += 1;
+    TG_TRY_CUDA(ctx, cnn_bce(logit, target, n, pos_weight, grad, loss_dev, ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_softmax_ce_dev(tomgpu_ctx* ctx, const float* logits, const int32_t* labels, int K, int P, float* grad,
+                              double* loss_dev) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!logits || !labels || !grad || !loss_dev || K < 2 || P < 1) return fail(ctx, TOMGPU_ERR_ARG, "bad arguments");
+    TG_TRY(use_device(ctx));
+    ctx->launches += 1;
+    TG_TRY_CUDA(ctx, cnn_softmax_ce(logits, labels, K, P, grad, loss_dev, ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_adam_dev(tomgpu_ctx* ctx, float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1,
+                        float b2, float eps, int step) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!p || !g || !m || !v || n < 1 || step < 1) return fail(ctx, TOMGPU_ERR_ARG, "bad arguments");
+    TG_TRY(use_device(ctx));
+    ctx->launches += 1;
+    TG_TRY_CUDA(ctx, cnn_adam(p, g, m, v, n, lr, b1, b2, eps, step, ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_gather_dev(tomgpu_ctx* ctx, const float* f, int C, int64_t nv, const int64_t* idx, int P, float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!f || !idx || !out || C < 1 || nv < 1 || P < 1) return fail(ctx, TOMGPU_ERR_ARG, "bad arguments");
+    TG_TRY(use_device(ctx));
+    ctx->launches += 1;
+    TG_TRY_CUDA(ctx, cnn_gather(f, C, nv, reinterpret_cast<const long long*>(idx), P, out, ctx->stream));
+    return TOMGPU_OK;
+}
+
+int tomgpu_cnn_scatter_add_dev(tomgpu_ctx* ctx, const float* g, int C, int64_t nv, const int64_t* idx, int P,
+                               float* gf) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!g || !idx || !gf || C < 1 || nv < 1 || P < 1) return fail(ctx, TOMGPU_ERR_ARG, "bad arguments");
+    TG_TRY(use_device(ctx));
+    ctx->launches += 1;
+    TG_TRY_CUDA(ctx, cnn_scatter_add(g, C, nv, reinterpret_cast<const long long*>(idx), P, gf, ctx->stream));
+    return TOMGPU_OK;
+}
