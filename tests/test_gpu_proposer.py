@@ -108,7 +108,7 @@ def test_refine_equals_exhaustive(gpu, oracle):
     vol = rng.standard_normal(N).astype(np.float32)
     tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
     mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
-    grid = oracle.av3_angle_grid((0, 0, 0), (45, 45, 45), (315, 315, 180))[:40]
+    grid = np.column_stack([rng.uniform(0, 360, 40), rng.uniform(0, 360, 40), rng.uniform(5, 175, 40)])
     cc, idx = pr.search(vol, tmpl, mask, grid)
     torch.cuda.synchronize()
     ccn, idn = gpu.from_device(cc), gpu.from_device(idx)
