@@ -60,6 +60,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--rescore-k", type=int, default=200, help="top-K peaks rescored in FP64 after the timed region")
+    p.add_argument("--learned-train", type=int, default=8, help="training tomograms of the learned_256 workload")
+    p.add_argument("--learned-steps", type=int, default=400, help="timed training steps of the learned_256 workload")
     p.add_argument("--align-particles", type=int, default=40,
                    help="particles timed for --workload align_2048 (extrapolated to 2048)")
     p.add_argument("--workload", default=WORKLOAD,
@@ -214,6 +216,113 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_learned(args):
+    """The learned proposer on a 256^3 tomogram (one 32^3 species, SNR 0.1,
+    +-60 degree wedge): training throughput of the network's own kernels
+    (FLOP/s of forward + backward), and the pruned search (coarse 30 degree
+    search, proposals, fine search in the proposed bins around the proposals)
+    against the exhaustive fine (15 degree) search: time and recall of the
+    exhaustive search's top peaks, with the network's proposals and with the
+    coarse map's own peaks as the candidates."""
+    import torch
+    import tom_b200 as tb
+    from tom_b200 import proposer as pr
+    from tom_b200 import synth
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    ctx = tb.default_context(local)
+    T = 32
+    coarse = tb.tom_av3_angle_grid((0, 0, 0), (30, 30, 30), (330, 330, 180))
+    fine = tb.tom_av3_angle_grid((0, 0, 0), (15, 15, 15), (345, 345, 180))
+    members = pr.bin_members(fine, coarse)
+    ph = synth.BlobPhantom(np.random.default_rng(5), 8, 12)
+    mask = synth.sphere_mask(T, T // 2 - 1)
+
+    def sample(N, n_copies, seed):
+        d = synth.make_tomogram(N, T, n_copies, 8, 12, 0.1, 60, seed=seed, euler_pool=fine,
+                                mask_radius=T // 2 - 1, phantom=ph)
+        ccc, idc = pr.search(d["tomo"], d["template"], mask, coarse, ctx=ctx)
+        return d, ccc, idc
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - t0
+
+    # training set: 128^3 tomograms labelled by the fine search
+    net = pr.ProposerNet(len(coarse), ctx, seed=1)
+    train = []
+    for s in range(args.learned_train):
+        d, ccc, idc = sample((128, 128, 128), 12, 500 + s)
+        ccf, idf = pr.search(d["tomo"], d["template"], mask, fine, ctx=ctx)
+        pos, bins, _ = pr.make_labels(ccf, idf, 12, T / 2, fine, coarse, ctx)
+        train.append((ccc, pos, bins))
+    N = (128, 128, 128)
+
+    def step(i):
+        ccc, pos, bins = train[i % len(train)]
+        x = torch.from_numpy(np.ascontiguousarray(pr.normalise(tb.from_device(ccc).transpose(2, 1, 0)))).to(net.dev)
+        return net.train_step(x, pr.heat_target(N, pos, net.dev), torch.from_numpy(pr.flat_index(pos, N)).to(net.dev),
+                              torch.from_numpy(bins.astype(np.int32)).to(net.dev), pos_weight=200.0, lr=5e-4)
+
+    for i in range(args.warmup):
+        step(i)
+    losses, t_train = timed(lambda: [step(i) for i in range(args.warmup, args.warmup + args.learned_steps)])
+    train_flops = 3 * net.flops_per_voxel() * int(np.prod(N)) * args.learned_steps
+    # test tomogram, 256^3
+    NT = (256, 256, 256)
+    d, ccc, idc = sample(NT, 60, 999)
+    (ccf, idf), t_exh = timed(lambda: pr.search(d["tomo"], d["template"], mask, fine, batch=16, ctx=ctx))
+    K = 60
+    ref_vals, ref_pos, ref_idx = tb.pick_peaks(ccf, idf, K, T / 2, ctx)
+    ref_pos = ref_pos - 1
+    (ccc2, idc2), t_coarse = timed(lambda: pr.search(d["tomo"], d["template"], mask, coarse, batch=16, ctx=ctx))
+    (cpos, _, cbins), t_prop = timed(lambda: pr.propose(net, ccc2, 2 * K, T / 2, 3, ctx))
+    idc_h = tb.from_device(idc2)
+
+    def refine_from(cands, extra_bins):
+        sets = []
+        for c, b in zip(cands, extra_bins):
+            bs = set(int(x) for x in b) | {int(idc_h[c[0], c[1], c[2]])}
+            ids = np.concatenate([members[k] for k in sorted(bs)])
+            sets.append((fine[ids], ids))
+        return pr.refine(d["tomo"], d["template"], mask, cands, sets, ctx=ctx)
+
+    (rpos, rcc, ridx), t_ref = timed(lambda: refine_from(cpos, cbins))
+    _, bpos, _ = tb.pick_peaks(ccc2, idc2, 2 * K, T / 2, ctx)
+    bpos = bpos - 1
+    (bres_pos, bcc, bidx), t_bref = timed(lambda: refine_from(bpos, [[]] * len(bpos)))
+
+    def recall(pos, idx):
+        dd = np.linalg.norm(ref_pos[:, None, :] - np.asarray(pos)[None].astype(float), axis=2)
+        j = np.argmin(dd, axis=1)
+        found = dd[np.arange(len(ref_pos)), j] <= 2
+        same = np.asarray(idx)[j] == ref_idx
+        return float(found.mean()), float((found & same).mean())
+
+    rc, ra = recall(rpos, ridx)
+    bc, ba = recall(bres_pos, bidx)
+    t_pruned = t_coarse + t_prop + t_ref
+    line = {"metric": "learned-pruned search speed-up over the exhaustive fine search (256^3, 32^3 template)",
+            "value": t_exh / t_pruned, "unit": "x", "higher_is_better": True, "n_gpus": 1,
+            "steps": args.learned_steps, "warmup": args.warmup, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "learned_256", "tomogram": list(NT), "template": T, "coarse_angles": len(coarse),
+                       "fine_angles": len(fine), "candidates": 2 * K, "reference_peaks": K,
+                       "train_tomograms": args.learned_train, "train_volume": list(N)},
+            "exhaustive_s": t_exh, "pruned_s": {"coarse": t_coarse, "network": t_prop, "refine": t_ref},
+            "recall_network": {"position": rc, "position_and_angle": ra},
+            "recall_coarse_peaks_without_network": {"position": bc, "position_and_angle": ba,
+                                                    "pruned_s": t_coarse + t_bref},
+            "training": {"flop_per_s": train_flops / t_train, "s_per_step": t_train / args.learned_steps,
+                         "last_loss": losses[-1]},
+            "scaling": "weak", "vs_baseline": None}
+    print(json.dumps(line), flush=True)
+
+
 def run_align(args):
     """Batched uneven subtomogram alignment (2048 particles, edges 32-96, +-15 deg
     at 3 deg = 1331 triplets each, shifts <= 4): a stratified subset is timed and
@@ -255,6 +364,8 @@ def main():
         return run_reference(args)
     if args.workload == "align_2048":
         return run_align(args)
+    if args.workload == "learned_256":
+        return run_learned(args)
     import torch
     import tom_b200 as tb
     world, rank, local = dist_env()
