@@ -53,10 +53,12 @@ __global__ void __launch_bounds__(32 * CY_WARPS) k_corr_y_p928(const float2* __r
     float2* xb = T + P * RS + warp * WS;  // [29][RS] exchange
     float2* fs = xb + P * RS;         // [29][RS] F_I at k1 + 29 k2
     float2* zs = fs + P * RS;         // [2][64] template column
+    float2* w29 = T + P * RS + CY_WARPS * WS;  // [29]: exp(-2 pi i j / 29)
     for (int i = threadIdx.x; i < NY; i += blockDim.x) {
         const int k1 = i >> 5, q = i & 31;
         T[k1 * RS + q] = __ldg(tw_g + (q * k1) % NY);
     }
+    if (threadIdx.x < P) w29[threadIdx.x] = make_float2(cs.c[threadIdx.x], -cs.s[threadIdx.x]);
     const long long col = (long long)blockIdx.x * CY_WARPS + warp;
     if (col < ncols) {
         for (int e = lane; e < NY; e += 32) {
@@ -78,16 +80,24 @@ __global__ void __launch_bounds__(32 * CY_WARPS) k_corr_y_p928(const float2* __r
         }
         const float2* cur = zs + (b & 1) * 64;
         {
-            float2 v[P];
+            // the template column covers Ty <= 64 consecutive y (from d0y, cyclic), so a
+            // lane's samples q + 32 m hold at most two nonzeros: the 29-point DFT of the
+            // lane is two scaled columns of the DFT matrix
+            const int o = (lane - d0y) & 31;  // first window offset with y = lane (mod 32)
+            const float2 a0 = o < Ty ? cur[o] : make_float2(0.f, 0.f);
+            const float2 a1 = o + 32 < Ty ? cur[o + 32] : make_float2(0.f, 0.f);
+            const int m0 = ((d0y + o) % NY - lane) >> 5;
+            const int m1 = m0 == P - 1 ? 0 : m0 + 1;
+            int j0 = 0, j1 = 0;
 #pragma unroll
-            for (int m = 0; m < P; ++m) {
-                int jy = lane + 32 * m - d0y;
-                if (jy < 0) jy += NY;
-                v[m] = jy < Ty ? cur[jy] : make_float2(0.f, 0.f);
+            for (int k1 = 0; k1 < P; ++k1) {
+                const float2 x = cadd(cmul(a0, w29[j0]), cmul(a1, w29[j1]));
+                xb[k1 * RS + lane] = cmul(x, T[k1 * RS + lane]);
+                j0 += m0;
+                j0 -= j0 >= P ? P : 0;
+                j1 += m1;
+                j1 -= j1 >= P ? P : 0;
             }
-            tgpq::dft29<-1>(v, cs);
-#pragma unroll
-            for (int k1 = 0; k1 < P; ++k1) xb[k1 * RS + lane] = cmul(v[k1], T[k1 * RS + lane]);
         }
         __syncwarp();
         if (lane < P) {
@@ -106,10 +116,8 @@ __global__ void __launch_bounds__(32 * CY_WARPS) k_corr_y_p928(const float2* __r
             float2 v[P];
 #pragma unroll
             for (int k1 = 0; k1 < P; ++k1) v[k1] = xb[k1 * RS + lane];
-            tgpq::dft29<+1>(v, cs);
             float2* qc = Q + ((long long)b * ncols + col) * NY;
-#pragma unroll
-            for (int m = 0; m < P; ++m) qc[lane + 32 * m] = v[m];
+            tgpq::dft29_emit<+1>(v, cs, [&](int m, float2 x) { qc[lane + 32 * m] = x; });
         }
         float2* nx = zs + ((b + 1) & 1) * 64;
         if (lane < Ty) nx[lane] = n0;
@@ -120,7 +128,7 @@ __global__ void __launch_bounds__(32 * CY_WARPS) k_corr_y_p928(const float2* __r
 
 constexpr int IZ_LS = 465;
 
-__global__ void __launch_bounds__(256) k_inv_z_p464(const float2* __restrict__ Q, float2* __restrict__ H, int Ny,
+__global__ void __launch_bounds__(256, 3) k_inv_z_p464(const float2* __restrict__ Q, float2* __restrict__ H, int Ny,
                                                     int nh1, const float2* __restrict__ tw_g, tgpq::Cos29 cs) {
     constexpr int NZ = 464, P = 29, LS = IZ_LS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -149,11 +157,10 @@ __global__ void __launch_bounds__(256) k_inv_z_p464(const float2* __restrict__ Q
     float2 v[P];
 #pragma unroll
     for (int k1 = 0; k1 < P; ++k1) v[k1] = s[l * LS + k1 * 16 + j];
-    tgpq::dft29<+1>(v, cs);
-    if (ok) {
-#pragma unroll
-        for (int m = 0; m < P; ++m) H[base + (long long)(j + 16 * m) * Ny + y] = v[m];
-    }
+    float2* hl = H + base + (long long)j * Ny + y;
+    tgpq::dft29_emit<+1>(v, cs, [&](int m, float2 x) {
+        if (ok) hl[(long long)(16 * m) * Ny] = x;
+    });
 }
 
 TG_D void cp_async8_p(void* smem_dst, const void* gsrc, int bytes) {
@@ -168,7 +175,7 @@ constexpr int C2_YT = 8, C2_TS = 466, C2_XR = 17, C2_XL = 29 * C2_XR;
 // The running maximum keeps u = out/(N M) + kappa_b and the batch index of
 // the best rotation per voxel (as k_c2r_w); the FLCF is applied at the
 // read-modify-write.
-__global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_p464(const float2* __restrict__ H, const float* __restrict__ mu0,
+__global__ void __launch_bounds__(16 * C2_YT, 3) k_c2r_p464(const float2* __restrict__ H, const float* __restrict__ mu0,
                                                              const float* __restrict__ gam,
                                                              const double* __restrict__ tsum, int Ny, int Nz, int nb,
                                                              float inv_nm, double c_mean, double inv_m, double mu_t,
@@ -235,15 +242,13 @@ __global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_p464(const float2* __rest
         float2 v[P];
 #pragma unroll
         for (int k1 = 0; k1 < P; ++k1) v[k1] = xl[k1 * C2_XR + q];
-        tgpq::dft29<+1>(v, cs);
         const float kap = kaps[b];
-#pragma unroll
-        for (int m = 0; m < P; ++m) {
-            const float u0 = fmaf(v[m].x, inv_nm, kap);
-            const float u1 = fmaf(v[m].y, inv_nm, kap);
+        tgpq::dft29_emit<+1>(v, cs, [&](int m, float2 x) {
+            const float u0 = fmaf(x.x, inv_nm, kap);
+            const float u1 = fmaf(x.y, inv_nm, kap);
             if (u0 > bu[m][0]) { bu[m][0] = u0; bb[m] = (bb[m] & 0xFFFF0000u) | (unsigned)b; }
             if (u1 > bu[m][1]) { bu[m][1] = u1; bb[m] = (bb[m] & 0x0000FFFFu) | ((unsigned)b << 16); }
-        }
+        });
         __syncthreads();  // the tile and the exchange are rewritten next
     }
     if (y >= Ny) return;
@@ -273,7 +278,7 @@ __global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_p464(const float2* __rest
 
 cudaError_t launch_corr_y_p928(const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y, long long ncols,
                                int nb, cudaStream_t st) {
-    const size_t smem = sizeof(float2) * (29 * CY_RS + CY_WARPS * (2 * 29 * CY_RS + 128));
+    const size_t smem = sizeof(float2) * (29 * CY_RS + CY_WARPS * (2 * 29 * CY_RS + 128) + 32);
     cudaFuncSetAttribute(k_corr_y_p928, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const unsigned g = (unsigned)((ncols + CY_WARPS - 1) / CY_WARPS);
     k_corr_y_p928<<<g, 32 * CY_WARPS, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(928),

@@ -49,4 +49,39 @@ TG_D void dft29(float2* v, const Cos29& t) {
     }
 }
 
+// The same transform without an output array: the inputs are folded in place
+// into x0, the 14 sums and the 14 differences, and each output is handed to
+// emit(k, X[k]) as soon as it is formed (k a compile-time index after
+// unrolling), so the caller stores or consumes it without holding all 29.
+template <int DIR, typename Emit>
+TG_D void dft29_emit(float2* v, const Cos29& t, Emit&& emit) {
+#pragma unroll
+    for (int n = 1; n <= 14; ++n) {
+        const float2 a = v[n], b = v[29 - n];
+        v[n] = cadd(a, b);       // p_n
+        v[29 - n] = csub(a, b);  // m_n
+    }
+    const float2 x0 = v[0];
+    float2 s0 = x0;
+#pragma unroll
+    for (int n = 1; n <= 14; ++n) s0 = cadd(s0, v[n]);
+    emit(0, s0);
+#pragma unroll
+    for (int k = 1; k <= 14; ++k) {
+        float2 re = x0, im = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int n = 1; n <= 14; ++n) {
+            const int j = (n * k) % 29;
+            const float c = t.c[j], s = t.s[j];
+            re.x = fmaf(c, v[n].x, re.x);
+            re.y = fmaf(c, v[n].y, re.y);
+            im.x = fmaf(s, v[29 - n].x, im.x);
+            im.y = fmaf(s, v[29 - n].y, im.y);
+        }
+        const float2 d = DIR > 0 ? make_float2(-im.y, im.x) : make_float2(im.y, -im.x);
+        emit(k, cadd(re, d));
+        emit(29 - k, csub(re, d));
+    }
+}
+
 }  // namespace tgpq

@@ -161,6 +161,11 @@ CONFIGS = {
                                max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
     "exhaustive_512x512x256": dict(N=(512, 512, 256), T=40, n_copies=40, n_blobs=8, rho=16, snr=0.1,
                                    max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
+    # the 928 / 464 kernels on small volumes, for profiler captures
+    "profile_928x928x48": dict(N=(928, 928, 48), T=48, n_copies=20, n_blobs=10, rho=20, snr=0.05,
+                               max_tilt=60, mask_radius=23, angles=((0, 0, 0), (7, 7, 7), (357, 357, 175))),
+    "profile_928x96x464": dict(N=(928, 96, 464), T=48, n_copies=20, n_blobs=10, rho=20, snr=0.05,
+                               max_tilt=60, mask_radius=23, angles=((0, 0, 0), (7, 7, 7), (357, 357, 175))),
     # the full-size tomogram with one of its 48^3 species (52 x 52 x 26 = 70,304 triplets)
     "exhaustive_928x928x464": dict(N=(928, 928, 464), T=48, n_copies=200, n_blobs=10, rho=20, snr=0.05,
                                    max_tilt=60, mask_radius=23, angles=((0, 0, 0), (7, 7, 7), (357, 357, 175))),
