@@ -21,8 +21,8 @@ def _run(gpu, vol, tmpl, mask, angles, generic, batch):
     return out
 
 
-@pytest.mark.parametrize("workload,n_ang", [("profile_256x256x128", 12), ("exhaustive_512x512x256", 10),
-                                            ("exhaustive_928x928x464", 6)])
+@pytest.mark.parametrize("workload,n_ang", [("exhaustive_128", 24), ("profile_256x256x128", 12),
+                                            ("exhaustive_512x512x256", 10), ("exhaustive_928x928x464", 6)])
 def test_fast_equals_generic_and_direct_sums(gpu, oracle, workload, n_ang):
     from tom_b200 import synth
     cfg = synth.CONFIGS[workload]

@@ -235,9 +235,9 @@ __global__ void __launch_bounds__(256, 4) k_c2r_w(const float2* __restrict__ H, 
 }
 
 // ------------------------------------------------------------- dispatch
-bool fast_corr_y(int NY, int Ty) { return (NY == 256 || NY == 512 || NY == 928) && Ty <= 64; }
-bool fast_inv_z(int NZ) { return NZ == 256 || NZ == 464; }
-bool fast_c2r(int NH) { return NH == 128 || NH == 256 || NH == 464; }
+bool fast_corr_y(int NY, int Ty) { return (NY == 128 || NY == 256 || NY == 512 || NY == 928) && Ty <= 64; }
+bool fast_inv_z(int NZ) { return NZ == 128 || NZ == 256 || NZ == 464; }
+bool fast_c2r(int NH) { return NH == 64 || NH == 128 || NH == 256 || NH == 464; }
 
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
                                long long ncols, int nb, cudaStream_t st) {
@@ -250,6 +250,9 @@ cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, floa
     } else if (NY == 256) {
         cudaFuncSetAttribute(k_corr_y_w<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_corr_y_w<256><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(256));
+    } else if (NY == 128) {
+        cudaFuncSetAttribute(k_corr_y_w<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_corr_y_w<128><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(128));
     } else {
         return cudaErrorInvalidValue;
     }
@@ -258,6 +261,7 @@ cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, floa
 
 cudaError_t launch_inv_z_fast(int NZ, const float2* Q, float2* H, int Ny, int nh1, int nb, cudaStream_t st) {
     if (NZ == 464) return launch_inv_z_p464(Q, H, Ny, nh1, nb, st);
+    if (NZ == 128) return launch_inv_z_b128(Q, H, Ny, nh1, nb, st);
     if (NZ != 256) return cudaErrorInvalidValue;
     dim3 g((Ny + 15) / 16, nh1, nb);
     k_inv_z_b256<<<g, 256, 0, st>>>(Q, H, Ny, nh1, twiddle_table<float2>(256));
@@ -284,6 +288,8 @@ cudaError_t launch_c2r_fast(int NH, const float2* H, const float* mu0, const flo
         return launch_c2r_t<256>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     if (NH == 128)
         return launch_c2r_t<128>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
+    if (NH == 64)
+        return launch_c2r_b64(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     if (NH == 464)
         return launch_c2r_p464(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     return cudaErrorInvalidValue;
