@@ -171,7 +171,121 @@ __global__ void __launch_bounds__(256) k_c2r_b64(const float2* __restrict__ H, c
     }
 }
 
+constexpr int CH_YT = 16, CH_TS = 259, CH_XR = 17;
+
+// NH = 256 = 16 (P) x 16 (Q); a half-warp per x line, 16 lines per block
+// (128-byte rows of y per request), two radix-16 stages with one exchange.
+__global__ void __launch_bounds__(256, 2) k_c2r_h256(const float2* __restrict__ H, const float* __restrict__ mu0,
+                                                     const float* __restrict__ gam, const double* __restrict__ tsum,
+                                                     int Ny, int Nz, int nb, float inv_nm, double c_mean, double inv_m,
+                                                     double mu_t, int index0, float* __restrict__ maxcc,
+                                                     int* __restrict__ angidx, const float2* __restrict__ tw_h,
+                                                     const float2* __restrict__ tw_x) {
+    constexpr int NH = 256, NH1 = NH + 1, NX = 2 * NH, P = 16, QN = 16, YT = CH_YT, TS = CH_TS, XR = CH_XR;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* tile = reinterpret_cast<float2*>(smem_raw);  // [2][YT][TS]
+    float2* xb = tile + 2 * YT * TS;                      // [YT][P][XR] exchange
+    float2* T = xb + YT * P * XR;                         // [QN][P]: W256^(+q k1) at [q][k1]
+    float2* twx = T + P * QN;                             // [NH]: W512^(+k)
+    float* kaps = reinterpret_cast<float*>(twx + NH);     // [nb]
+    const int tid = threadIdx.x, line = tid >> 4, j = tid & 15;
+    const int y0 = blockIdx.x * YT, z = blockIdx.y, y = y0 + line;
+    for (int i = tid; i < P * QN; i += blockDim.x) {
+        const int k1 = i >> 4, q = i & 15;
+        T[q * P + k1] = cconj(__ldg(tw_h + (q * k1) % NH));
+    }
+    for (int i = tid; i < NH; i += blockDim.x) twx[i] = cconj(__ldg(tw_x + i));
+    for (int b = tid; b < nb; b += blockDim.x) kaps[b] = (float)(c_mean * (tsum[b] * inv_m - mu_t));
+    float bu[P][2];
+    unsigned bb[P];
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        bu[m][0] = bu[m][1] = -INFINITY;
+        bb[m] = 0u;
+    }
+    auto issue = [&](int b, int which) {
+        float2* t = tile + which * YT * TS;
+        const long long hb = (long long)b * NH1 * Nz * Ny;
+        for (int e = tid; e < YT * NH1; e += blockDim.x) {
+            const int kx = e / YT, yl = e - kx * YT;
+            const bool okl = y0 + yl < Ny;
+            const float2* src = H + hb + ((long long)kx * Nz + z) * Ny + (okl ? y0 + yl : 0);
+            cp_async8_b(t + yl * TS + kx, src, okl ? 8 : 0);
+        }
+        cp_async_commit_b();
+    };
+    issue(0, 0);
+    float2* xl = xb + line * P * XR;
+    for (int b = 0; b < nb; ++b) {
+        if (b + 1 < nb) issue(b + 1, (b + 1) & 1);
+        else cp_async_commit_b();
+        cp_async_wait1_b();
+        __syncthreads();
+        const float2* X = tile + (b & 1) * YT * TS + line * TS;
+        {
+            float2 u[QN];
+#pragma unroll
+            for (int k2 = 0; k2 < QN; ++k2) {
+                const int k = j + P * k2;
+                const float2 xa = X[k], xc = cconj(X[NH - k]);
+                const float2 d = cmul(twx[k], csub(xa, xc));
+                u[k2] = cadd(cadd(xa, xc), make_float2(-d.y, d.x));
+            }
+            tgfft::dft16<+1>(u);
+#pragma unroll
+            for (int q = 0; q < QN; ++q) xl[j * XR + q] = cmul(u[q], T[q * P + j]);
+        }
+        __syncwarp();
+        float2 v[P];
+#pragma unroll
+        for (int k1 = 0; k1 < P; ++k1) v[k1] = xl[k1 * XR + j];
+        tgfft::dft16<+1>(v);
+        const float kap = kaps[b];
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const float u0 = fmaf(v[m].x, inv_nm, kap);
+            const float u1 = fmaf(v[m].y, inv_nm, kap);
+            if (u0 > bu[m][0]) { bu[m][0] = u0; bb[m] = (bb[m] & 0xFFFF0000u) | (unsigned)b; }
+            if (u1 > bu[m][1]) { bu[m][1] = u1; bb[m] = (bb[m] & 0x0000FFFFu) | ((unsigned)b << 16); }
+        }
+        __syncthreads();  // the tile and the exchange are rewritten next
+    }
+    if (y >= Ny) return;
+    const float mt = (float)mu_t;
+    const long long row = ((long long)z * Ny + y) * NX;
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const long long v = row + 2 * (j + QN * m);
+        const float2 a = __ldg(reinterpret_cast<const float2*>(mu0 + v));
+        const float2 g = __ldg(reinterpret_cast<const float2*>(gam + v));
+        float2 cur = *reinterpret_cast<const float2*>(maxcc + v);
+        int2 ci = *reinterpret_cast<const int2*>(angidx + v);
+        bool ch = false;
+        const float c0 = g.x != 0.f ? (bu[m][0] - a.x * mt) * g.x : 0.f;
+        const float c1 = g.y != 0.f ? (bu[m][1] - a.y * mt) * g.y : 0.f;
+        const int b0 = g.x != 0.f ? (int)(bb[m] & 0xFFFFu) : 0, b1 = g.y != 0.f ? (int)(bb[m] >> 16) : 0;
+        if (c0 > cur.x) { cur.x = c0; ci.x = index0 + b0; ch = true; }
+        if (c1 > cur.y) { cur.y = c1; ci.y = index0 + b1; ch = true; }
+        if (ch) {
+            *reinterpret_cast<float2*>(maxcc + v) = cur;
+            *reinterpret_cast<int2*>(angidx + v) = ci;
+        }
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_c2r_h256(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
+                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
+                            int* angidx, cudaStream_t st) {
+    const size_t smem =
+        sizeof(float2) * (2 * CH_YT * CH_TS + CH_YT * 16 * CH_XR + 16 * 16 + 256) + sizeof(float) * nb;
+    cudaFuncSetAttribute(k_c2r_h256, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 g((Ny + CH_YT - 1) / CH_YT, Nz);
+    k_c2r_h256<<<g, 256, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx,
+                                     twiddle_table<float2>(256), twiddle_table<float2>(512));
+    return cudaGetLastError();
+}
 
 cudaError_t launch_inv_z_b128(const float2* Q, float2* H, int Ny, int nh1, int nb, cudaStream_t st) {
     dim3 g((Ny + 31) / 32, nh1, nb);
