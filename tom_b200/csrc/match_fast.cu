@@ -13,8 +13,6 @@
 //   c2r_w     one warp per x line, the next three rotations' tiles in flight
 //             (cp.async) while the current one is transformed; running max and
 //             the FLCF coefficients of the lane's voxels stay in registers.
-#include <cstdlib>
-
 #include "ctx.h"
 #include "match.h"
 #include "twiddles.h"
@@ -237,15 +235,7 @@ __global__ void __launch_bounds__(256, 4) k_c2r_w(const float2* __restrict__ H, 
 }
 
 // ------------------------------------------------------------- dispatch
-// The x edge 512 has two kernels: the half-warp, 16-line k_c2r_h256 (default)
-// and the warp-per-line k_c2r_w<256>; TOMGPU_C2R_W=1 selects the latter.
-static bool c2r_h256_enabled() {
-    static const bool on = [] {
-        const char* e = std::getenv("TOMGPU_C2R_W");
-        return !(e && e[0] == '1');
-    }();
-    return on;
-}
+
 bool fast_corr_y(int NY, int Ty) { return (NY == 128 || NY == 256 || NY == 512 || NY == 928) && Ty <= 64; }
 bool fast_inv_z(int NZ) { return NZ == 128 || NZ == 256 || NZ == 464; }
 bool fast_c2r(int NH) { return NH == 64 || NH == 128 || NH == 256 || NH == 464; }
@@ -295,10 +285,10 @@ static cudaError_t launch_c2r_t(const float2* H, const float* mu0, const float* 
 cudaError_t launch_c2r_fast(int NH, const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny,
                             int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
                             float* maxcc, int* angidx, cudaStream_t st) {
-    if (NH == 256 && c2r_h256_enabled())
-        return launch_c2r_h256(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
+    // x edge 512: the half-warp kernel (k_c2r_h256 measured 20 % faster than the
+    // warp-per-line k_c2r_w<256> on the 512x512x256 search)
     if (NH == 256)
-        return launch_c2r_t<256>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
+        return launch_c2r_h256(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     if (NH == 128)
         return launch_c2r_t<128>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     if (NH == 64)
