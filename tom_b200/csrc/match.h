@@ -31,6 +31,9 @@ cudaError_t launch_inv_z_b128(const float2* Q, float2* H, int Ny, int nh1, int n
 cudaError_t launch_c2r_h256(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
                             int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
                             int* angidx, cudaStream_t st);
+cudaError_t launch_c2r_b128(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
+                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
+                            int* angidx, cudaStream_t st);
 cudaError_t launch_c2r_b64(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
                            int* angidx, cudaStream_t st);

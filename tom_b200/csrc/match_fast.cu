@@ -290,7 +290,7 @@ cudaError_t launch_c2r_fast(int NH, const float2* H, const float* mu0, const flo
     if (NH == 256)
         return launch_c2r_h256(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     if (NH == 128)
-        return launch_c2r_t<128>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
+        return launch_c2r_b128(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     if (NH == 64)
         return launch_c2r_b64(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
     if (NH == 464)

@@ -7,10 +7,12 @@
 //   inv_z_b128  32 y lines x 8 threads per block: 16 8-point DFTs per line
 //               from global memory (32 consecutive y per request), one block
 //               exchange, 8 16-point DFTs per line back to global memory.
-//   c2r_b64     32 x lines per block, 8 threads per line: the half-spectrum
-//               unpack and 8 8-point DFTs, a warp-local exchange, 8 8-point
-//               DFTs; the running maximum over the batch in registers and the
-//               FLCF at the read-modify-write (as c2r_w).
+//   c2r_b8      32 x lines per block, 8 threads per line (x edge 128: 8 x 8;
+//               x edge 256: 16 x 8): the half-spectrum unpack and 8-point
+//               DFTs, a warp-local exchange, 8- or 16-point DFTs; the running
+//               maximum over the batch in registers and the FLCF at the
+//               read-modify-write (as c2r_w).
+//   c2r_h256    x edge 512: a half-warp per line, 16 lines per block, 16 x 16.
 //
 // Index map (inverse): with n = q + Q m and k = k1 + P k2,
 // y(n) = sum_k1 WP^(m k1) WL^(q k1) sum_k2 Y(k) WQ^(q k2).
@@ -69,26 +71,29 @@ TG_D void cp_async8_b(void* smem_dst, const void* gsrc, int bytes) {
 TG_D void cp_async_commit_b() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 TG_D void cp_async_wait1_b() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-constexpr int C1_YT = 32, C1_TS = 65, C1_XR = 9;
+constexpr int C1_YT = 32, C1_XR = 9;
 
-// NH = 64 = 8 (P) x 8 (Q); 8 threads per x line, 32 lines per block
-__global__ void __launch_bounds__(256) k_c2r_b64(const float2* __restrict__ H, const float* __restrict__ mu0,
-                                                 const float* __restrict__ gam, const double* __restrict__ tsum,
-                                                 int Ny, int Nz, int nb, float inv_nm, double c_mean, double inv_m,
-                                                 double mu_t, int index0, float* __restrict__ maxcc,
-                                                 int* __restrict__ angidx, const float2* __restrict__ tw_h,
-                                                 const float2* __restrict__ tw_x) {
-    constexpr int NH = 64, NH1 = NH + 1, NX = 2 * NH, P = 8, QN = 8, YT = C1_YT, TS = C1_TS, XR = C1_XR;
+// Short x lines, 8 threads per line, 32 lines per block: NH = P x 8 with
+// P = 8 (NH 64) or 16 (NH 128, two first-stage tasks per thread).
+template <int NH, int P>
+__global__ void __launch_bounds__(256) k_c2r_b8(const float2* __restrict__ H, const float* __restrict__ mu0,
+                                                const float* __restrict__ gam, const double* __restrict__ tsum,
+                                                int Ny, int Nz, int nb, float inv_nm, double c_mean, double inv_m,
+                                                double mu_t, int index0, float* __restrict__ maxcc,
+                                                int* __restrict__ angidx, const float2* __restrict__ tw_h,
+                                                const float2* __restrict__ tw_x) {
+    constexpr int NH1 = NH + 1, NX = 2 * NH, QN = 8, YT = C1_YT, TS = NH + 1, XR = C1_XR;
+    static_assert(NH == P * QN, "NH = P x 8");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* tile = reinterpret_cast<float2*>(smem_raw);  // [2][YT][TS]
     float2* xb = tile + 2 * YT * TS;                      // [YT][P][XR] exchange
-    float2* T = xb + YT * P * XR;                         // [QN][P]: W64^(+q k1) at [q][k1]
-    float2* twx = T + P * QN;                             // [NH]: W128^(+k)
+    float2* T = xb + YT * P * XR;                         // [QN][P]: W_NH^(+q k1) at [q][k1]
+    float2* twx = T + P * QN;                             // [NH]: W_NX^(+k)
     float* kaps = reinterpret_cast<float*>(twx + NH);     // [nb]
     const int tid = threadIdx.x, line = tid >> 3, j = tid & 7;
     const int y0 = blockIdx.x * YT, z = blockIdx.y, y = y0 + line;
     for (int i = tid; i < P * QN; i += blockDim.x) {
-        const int k1 = i >> 3, q = i & 7;
+        const int k1 = i / QN, q = i - k1 * QN;
         T[q * P + k1] = cconj(__ldg(tw_h + (q * k1) % NH));
     }
     for (int i = tid; i < NH; i += blockDim.x) twx[i] = cconj(__ldg(tw_x + i));
@@ -119,8 +124,9 @@ __global__ void __launch_bounds__(256) k_c2r_b64(const float2* __restrict__ H, c
         cp_async_wait1_b();
         __syncthreads();
         const float2* X = tile + (b & 1) * YT * TS + line * TS;
-        {
-            const int k1 = j;
+#pragma unroll
+        for (int h = 0; h < P / 8; ++h) {
+            const int k1 = j + 8 * h;
             float2 u[QN];
 #pragma unroll
             for (int k2 = 0; k2 < QN; ++k2) {
@@ -137,7 +143,8 @@ __global__ void __launch_bounds__(256) k_c2r_b64(const float2* __restrict__ H, c
         float2 v[P];
 #pragma unroll
         for (int k1 = 0; k1 < P; ++k1) v[k1] = xl[k1 * XR + j];
-        tgfft::dft8<+1>(v);
+        if constexpr (P == 8) tgfft::dft8<+1>(v);
+        else tgfft::dft16<+1>(v);
         const float kap = kaps[b];
 #pragma unroll
         for (int m = 0; m < P; ++m) {
@@ -293,15 +300,28 @@ cudaError_t launch_inv_z_b128(const float2* Q, float2* H, int Ny, int nh1, int n
     return cudaGetLastError();
 }
 
+template <int NH, int P>
+static cudaError_t launch_c2r_b8(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny,
+                                 int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
+                                 float* maxcc, int* angidx, cudaStream_t st) {
+    const size_t smem = sizeof(float2) * (2 * C1_YT * (NH + 1) + C1_YT * P * C1_XR + P * 8 + NH) + sizeof(float) * nb;
+    cudaFuncSetAttribute(k_c2r_b8<NH, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 g((Ny + C1_YT - 1) / C1_YT, Nz);
+    k_c2r_b8<NH, P><<<g, 256, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc,
+                                          angidx, twiddle_table<float2>(NH), twiddle_table<float2>(2 * NH));
+    return cudaGetLastError();
+}
+
 cudaError_t launch_c2r_b64(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
                            int* angidx, cudaStream_t st) {
-    const size_t smem = sizeof(float2) * (2 * C1_YT * C1_TS + C1_YT * 8 * C1_XR + 8 * 8 + 64) + sizeof(float) * nb;
-    cudaFuncSetAttribute(k_c2r_b64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 g((Ny + C1_YT - 1) / C1_YT, Nz);
-    k_c2r_b64<<<g, 256, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx,
-                                    twiddle_table<float2>(64), twiddle_table<float2>(128));
-    return cudaGetLastError();
+    return launch_c2r_b8<64, 8>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
+}
+
+cudaError_t launch_c2r_b128(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
+                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
+                            int* angidx, cudaStream_t st) {
+    return launch_c2r_b8<128, 16>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx, st);
 }
 
 }  // namespace tg
