@@ -11,8 +11,18 @@
 //               x edge 256: 16 x 8): the half-spectrum unpack and 8-point
 //               DFTs, a warp-local exchange, 8- or 16-point DFTs; the running
 //               maximum over the batch in registers and the FLCF at the
-//               read-modify-write (as c2r_w).
+//               read-modify-write.
 //   c2r_h256    x edge 512: a half-warp per line, 16 lines per block, 16 x 16.
+//
+// Running maximum without per-voxel coefficients: with gamma >= 0 and
+// mu0 mu_T fixed per voxel, cc_b = (u_b - mu0 mu_T) gamma is a non-decreasing
+// function of u_b = out_b/(N M) + kappa_b, so the batch keeps the best u and
+// its rotation (16-bit batch indices, two voxels per word) and applies the
+// FLCF formula once, at the read-modify-write.  (Rotations whose cc round to
+// the same float but whose u differ may pick a later index than the strict
+// first-wins scan; such voxels have no CC separation between those angles.
+// gamma = 0 voxels keep the reference's value 0 with the batch's first
+// rotation.)
 //
 // Index map (inverse): with n = q + Q m and k = k1 + P k2,
 // y(n) = sum_k1 WP^(m k1) WL^(q k1) sum_k2 Y(k) WQ^(q k2).

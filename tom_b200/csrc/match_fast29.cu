@@ -16,7 +16,7 @@
 //   c2r_p464     8 x lines per block, 16 threads per line: the half-spectrum
 //                unpack, 29 16-point DFTs, a half-warp exchange, 16 29-point
 //                DFTs, the running maximum over the batch in registers and the
-//                FLCF at the read-modify-write (as c2r_w).
+//                FLCF at the read-modify-write (as c2r_b8).
 //
 // Index map (inverse; the forward is the conjugate): with n = q + Q m and
 // k = k1 + 29 k2,  y(n) = sum_k1 W29^(m k1) WL^(q k1) sum_k2 Y(k) WQ^(q k2).
@@ -173,7 +173,7 @@ TG_D void cp_async_wait1_p() { asm volatile("cp.async.wait_group 1;\n" ::: "memo
 constexpr int C2_YT = 8, C2_TS = 466, C2_XR = 17, C2_XL = 29 * C2_XR;
 
 // The running maximum keeps u = out/(N M) + kappa_b and the batch index of
-// the best rotation per voxel (as k_c2r_w); the FLCF is applied at the
+// the best rotation per voxel (as k_c2r_b8); the FLCF is applied at the
 // read-modify-write.
 __global__ void __launch_bounds__(16 * C2_YT, 3) k_c2r_p464(const float2* __restrict__ H, const float* __restrict__ mu0,
                                                              const float* __restrict__ gam,
