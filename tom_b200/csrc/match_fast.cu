@@ -6,7 +6,10 @@
 //             product with F_I (staged once in shared memory) and the inverse
 //             y-DFT all stay in registers with two warp-private exchanges per
 //             transform (warp_fft.cuh); the next rotation's template values
-//             are fetched while the current one is transformed.
+//             are fetched while the current one is transformed.  y edge 128.
+//   corr_y_s  y edges 256 and 512: as corr_y_w, but the forward y-DFT is
+//             summed straight from the template column's nonzeros into the
+//             inverse transform's register pattern (no exchange).
 //   inv_z_b   16 consecutive y lines per block, 16 threads per line holding
 //             16 values: radix 16 straight from global memory, one block-wide
 //             exchange, radix 16 straight back to global memory.
@@ -78,6 +81,119 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_w(const float2* __restrict__ 
     }
 }
 
+// y edges 256 and 512: the forward y-DFT of the template column straight
+// from its Ty <= 64 nonzeros, with no exchange.  The column holds z[t] at
+// y = (d0y + t) mod NY.  With W_L = exp(-2 pi i / L), t = d + 8 i and
+// k = m + (NY/8) k2:
+//   X(k) = W_NY^(d0y k) sum_d W_8^(d k2) [ W_NY^(d m) sum_i z[d + 8 i] W_(NY/8)^(i m) ].
+// Lane l owns m = l + 32 q (q < NY/256): the bracket is a short sum per
+// residue d, the outer sum one 8-point DFT per m in registers, and the result
+// lands as v[8 q + k2] = X(l + 32 q + (NY/8) k2), the pattern the inverse
+// warp transform starts from.  The phase W_NY^(d0y k) is folded into the
+// staged F_I column (the product is F_I conj(X)).  For NY = 512 the two m of
+// a lane differ by 32, W_64^(32 i) = (-1)^i: even and odd terms are summed
+// once for both.  NI = ceil(Ty / 8) terms per residue.
+template <int NY, int NI>
+__global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ fimg, const float2* __restrict__ Z,
+                                                     float2* __restrict__ Q, int Ty, int d0y, long long ncols, int nb,
+                                                     const float2* __restrict__ tw_g) {
+    constexpr int EPT = NY / 32, NB = EPT / 8;
+    static_assert(tgwfft::WPlan<NY>::RL == 8 && (NB == 1 || NB == 2) && NI >= 1 && NI <= 8, "plan");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* tw = reinterpret_cast<float2*>(smem_raw);  // [NY + 64] stage tables
+    float2* xb = tw + NY + 64;                          // [8][NY] exchange
+    float2* fs = xb + 8 * NY;                           // [8][NY] F_I columns times W_NY^(-d0y k)
+    float2* zs = fs + 8 * NY;                           // [8][2][64] template column, z[t] at (t % 8) * 8 + t / 8
+    float2* lt = zs + 8 * 128;                          // [NI-1][32] W_L8^(i l), then [NB][7][32] W_NY^(d (l + 32 q))
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long col = (long long)blockIdx.x * 8 + warp;
+    static_assert(tgwfft::WTab<NY>::size <= NY + 64, "stage tables exceed their slot");
+    tgwfft::build_stage_tables<NY>(tw, tw_g);
+    constexpr int NW = (NI - 1) * 32, NT = NW + NB * 7 * 32;
+    for (int e = threadIdx.x; e < NT; e += blockDim.x) {
+        int idx;
+        if (e < NW) {
+            idx = 8 * (e / 32 + 1) * (e % 32);
+        } else {
+            const int r = e - NW, q = r / 224, d = (r % 224) / 32 + 1, l = r % 32;
+            idx = d * (l + 32 * q);
+        }
+        lt[e] = __ldg(tw_g + idx % NY);
+    }
+    float2* buf = xb + warp * NY;
+    float2* fw = fs + warp * NY;
+    float2* zw = zs + warp * 128;
+    const int zslot0 = (lane & 7) * 8 + (lane >> 3), zslot1 = zslot0 + 4;  // t = lane, lane + 32
+    if (col < ncols) {
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) {
+            const int p = tgwfft::out_pos<NY>(i, lane);
+            fw[p] = cmulc(fimg[col * NY + p], __ldg(tw_g + (d0y * p) % NY));  // each lane reads only its own
+        }
+        const float2* zc = Z + col * Ty;  // rotation 0
+        zw[zslot0] = lane < Ty ? zc[lane] : make_float2(0.f, 0.f);
+        zw[zslot1] = lane + 32 < Ty ? zc[lane + 32] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();  // the tables; the only block-wide barrier
+    if (col >= ncols) return;
+    for (int b = 0; b < nb; ++b) {
+        // next rotation's column: two loads per lane, parked in registers
+        float2 n0 = make_float2(0.f, 0.f), n1 = make_float2(0.f, 0.f);
+        if (b + 1 < nb) {
+            const float2* zc = Z + ((long long)(b + 1) * ncols + col) * Ty;
+            if (lane < Ty) n0 = zc[lane];
+            if (lane + 32 < Ty) n1 = zc[lane + 32];
+        }
+        const float2* cur = zw + (b & 1) * 64;
+        float2 wi[NI];
+#pragma unroll
+        for (int i = 1; i < NI; ++i) wi[i] = lt[(i - 1) * 32 + lane];
+        float2 v[EPT];
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+            float2 zz[NI + 1];
+#pragma unroll
+            for (int p = 0; p < (NI + 1) / 2; ++p) {
+                const float4 t = reinterpret_cast<const float4*>(cur + d * 8)[p];  // same address in every lane
+                zz[2 * p] = make_float2(t.x, t.y);
+                zz[2 * p + 1] = make_float2(t.z, t.w);
+            }
+            float2 ev = zz[0], od = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int i = 1; i < NI; ++i) {
+                const float2 a = wi[i], c = zz[i];
+                if (NB == 2 && (i & 1)) {
+                    od.x = fmaf(c.x, a.x, fmaf(-c.y, a.y, od.x));
+                    od.y = fmaf(c.x, a.y, fmaf(c.y, a.x, od.y));
+                } else {
+                    ev.x = fmaf(c.x, a.x, fmaf(-c.y, a.y, ev.x));
+                    ev.y = fmaf(c.x, a.y, fmaf(c.y, a.x, ev.y));
+                }
+            }
+            float2 s0 = cadd(ev, od);
+            if (d > 0) s0 = cmul(s0, lt[NW + (d - 1) * 32 + lane]);
+            v[d] = s0;
+            if constexpr (NB == 2) {
+                float2 s1 = csub(ev, od);
+                if (d > 0) s1 = cmul(s1, lt[NW + 224 + (d - 1) * 32 + lane]);
+                v[8 + d] = s1;
+            }
+        }
+        tgfft::dft8<-1>(v);
+        if constexpr (NB == 2) tgfft::dft8<-1>(v + 8);
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) v[i] = cmulc(fw[tgwfft::out_pos<NY>(i, lane)], v[i]);
+        tgwfft::warp_fft<NY, +1>(v, buf, tw, lane);
+        float2* qc = Q + ((long long)b * ncols + col) * NY;
+#pragma unroll
+        for (int i = 0; i < EPT; ++i) qc[tgwfft::out_pos<NY>(i, lane)] = v[i];
+        float2* nx = zw + ((b + 1) & 1) * 64;
+        nx[zslot0] = n0;
+        nx[zslot1] = n1;
+        __syncwarp();
+    }
+}
+
 __global__ void __launch_bounds__(256) k_inv_z_b256(const float2* __restrict__ Q, float2* __restrict__ H, int Ny,
                                                     int nh1, const float2* __restrict__ tw_g) {
     constexpr int NZ = 256, LS = NZ + 1;
@@ -114,18 +230,43 @@ bool fast_corr_y(int NY, int Ty) { return (NY == 128 || NY == 256 || NY == 512 |
 bool fast_inv_z(int NZ) { return NZ == 128 || NZ == 256 || NZ == 464; }
 bool fast_c2r(int NH) { return NH == 64 || NH == 128 || NH == 256 || NH == 464; }
 
+template <int NY, int NI>
+static cudaError_t launch_corr_y_s_ni(const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
+                                      long long ncols, int nb, cudaStream_t st) {
+    const unsigned g = (unsigned)((ncols + 7) / 8);
+    const size_t smem = sizeof(float2) * (NY * 17 + 64 + 8 * 128 + 3 * 7 * 32);
+    cudaFuncSetAttribute(k_corr_y_s<NY, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_corr_y_s<NY, NI><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(NY));
+    return cudaGetLastError();
+}
+
+template <int NY>
+static cudaError_t launch_corr_y_s(const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y, long long ncols,
+                                   int nb, cudaStream_t st) {
+    switch ((Ty + 7) / 8) {
+        case 1: return launch_corr_y_s_ni<NY, 1>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 2: return launch_corr_y_s_ni<NY, 2>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 3: return launch_corr_y_s_ni<NY, 3>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 4: return launch_corr_y_s_ni<NY, 4>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 5: return launch_corr_y_s_ni<NY, 5>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 6: return launch_corr_y_s_ni<NY, 6>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 7: return launch_corr_y_s_ni<NY, 7>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 8: return launch_corr_y_s_ni<NY, 8>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
                                long long ncols, int nb, cudaStream_t st) {
     if (NY == 928) return launch_corr_y_p928(fimg, Z, Q, Ty, d0y, ncols, nb, st);
     const unsigned g = (unsigned)((ncols + 7) / 8);
     const size_t smem = sizeof(float2) * (NY * 17 + 64 + 8 * 128);
-    if (NY == 512) {
-        cudaFuncSetAttribute(k_corr_y_w<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_corr_y_w<512><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(512));
-    } else if (NY == 256) {
-        cudaFuncSetAttribute(k_corr_y_w<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_corr_y_w<256><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(256));
-    } else if (NY == 128) {
+    if (NY == 512 || NY == 256) {
+        if (Ty < 1 || Ty > 64) return cudaErrorInvalidValue;
+        return NY == 512 ? launch_corr_y_s<512>(fimg, Z, Q, Ty, d0y, ncols, nb, st)
+                         : launch_corr_y_s<256>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+    }
+    if (NY == 128) {
         cudaFuncSetAttribute(k_corr_y_w<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_corr_y_w<128><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(128));
     } else {
