@@ -28,6 +28,7 @@
 // y(n) = sum_k1 WP^(m k1) WL^(q k1) sum_k2 Y(k) WQ^(q k2).
 #include "ctx.h"
 #include "match.h"
+#include "tile_copy.cuh"
 #include "twiddles.h"
 #include "warp_fft.cuh"
 
@@ -74,13 +75,6 @@ __global__ void __launch_bounds__(256) k_inv_z_b128(const float2* __restrict__ Q
     }
 }
 
-TG_D void cp_async8_b(void* smem_dst, const void* gsrc, int bytes) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
-}
-TG_D void cp_async_commit_b() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-TG_D void cp_async_wait1_b() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
 constexpr int C1_YT = 32, C1_XR = 9;
 
 // Short x lines, 8 threads per line, 32 lines per block: NH = P x 8 with
@@ -115,23 +109,14 @@ __global__ void __launch_bounds__(256) k_c2r_b8(const float2* __restrict__ H, co
         bu[m][0] = bu[m][1] = -INFINITY;
         bb[m] = 0u;
     }
-    auto issue = [&](int b, int which) {
-        float2* t = tile + which * YT * TS;
-        const long long hb = (long long)b * NH1 * Nz * Ny;
-        for (int e = tid; e < YT * NH1; e += blockDim.x) {
-            const int kx = e / YT, yl = e - kx * YT;
-            const bool okl = y0 + yl < Ny;
-            const float2* src = H + hb + ((long long)kx * Nz + z) * Ny + (okl ? y0 + yl : 0);
-            cp_async8_b(t + yl * TS + kx, src, okl ? 8 : 0);
-        }
-        cp_async_commit_b();
-    };
+    const tgtile::TileCopy<YT, NH1, 256> copy(tile, TS, H, tid, y0, z, Ny, Nz);
+    auto issue = [&](int b, int which) { copy.issue(b, which * (unsigned)(YT * TS * sizeof(float2))); };
     issue(0, 0);
     float2* xl = xb + line * P * XR;
     for (int b = 0; b < nb; ++b) {
         if (b + 1 < nb) issue(b + 1, (b + 1) & 1);
-        else cp_async_commit_b();
-        cp_async_wait1_b();
+        else tgtile::commit();
+        tgtile::wait<1>();
         __syncthreads();
         const float2* X = tile + (b & 1) * YT * TS + line * TS;
 #pragma unroll
@@ -220,23 +205,14 @@ __global__ void __launch_bounds__(256, 2) k_c2r_h256(const float2* __restrict__ 
         bu[m][0] = bu[m][1] = -INFINITY;
         bb[m] = 0u;
     }
-    auto issue = [&](int b, int which) {
-        float2* t = tile + which * YT * TS;
-        const long long hb = (long long)b * NH1 * Nz * Ny;
-        for (int e = tid; e < YT * NH1; e += blockDim.x) {
-            const int kx = e / YT, yl = e - kx * YT;
-            const bool okl = y0 + yl < Ny;
-            const float2* src = H + hb + ((long long)kx * Nz + z) * Ny + (okl ? y0 + yl : 0);
-            cp_async8_b(t + yl * TS + kx, src, okl ? 8 : 0);
-        }
-        cp_async_commit_b();
-    };
+    const tgtile::TileCopy<YT, NH1, 256> copy(tile, TS, H, tid, y0, z, Ny, Nz);
+    auto issue = [&](int b, int which) { copy.issue(b, which * (unsigned)(YT * TS * sizeof(float2))); };
     issue(0, 0);
     float2* xl = xb + line * P * XR;
     for (int b = 0; b < nb; ++b) {
         if (b + 1 < nb) issue(b + 1, (b + 1) & 1);
-        else cp_async_commit_b();
-        cp_async_wait1_b();
+        else tgtile::commit();
+        tgtile::wait<1>();
         __syncthreads();
         const float2* X = tile + (b & 1) * YT * TS + line * TS;
         {
