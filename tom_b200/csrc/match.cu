@@ -889,7 +889,10 @@ int MatchPlan::prepare_batch(int off, int nb) {
     }
     {
         ProfScope ps(ctx, TOMGPU_K_SPEC_Z);
-        TG_TRY_CUDA(ctx, launch_spec_z(N[2], d_A, d_Z, T, d0_corr(N[2], T[2]), (int)nh1, nb, st));
+        if (!generic_only && fast_spec_z(N[2], T[2]))
+            TG_TRY_CUDA(ctx, launch_spec_z_fast(N[2], d_A, d_Z, T[1], T[2], d0_corr(N[2], T[2]), (int)nh1, nb, st));
+        else
+            TG_TRY_CUDA(ctx, launch_spec_z(N[2], d_A, d_Z, T, d0_corr(N[2], T[2]), (int)nh1, nb, st));
     }
     ctx->launches += 2;
     return TOMGPU_OK;

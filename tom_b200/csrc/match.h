@@ -13,6 +13,9 @@ bool match_sizes_supported(const int N[3], const int T[3]);
 bool fast_corr_y(int NY, int Ty);
 bool fast_inv_z(int NZ);
 bool fast_c2r(int NH);
+bool fast_spec_z(int NZ, int Tz);
+cudaError_t launch_spec_z_fast(int NZ, const float2* A, float2* Z, int Ty, int Tz, int d0z, int nh1, int nb,
+                               cudaStream_t st);
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
                                long long ncols, int nb, cudaStream_t st);
 cudaError_t launch_inv_z_fast(int NZ, const float2* Q, float2* H, int Ny, int nh1, int nb, cudaStream_t st);
