@@ -173,10 +173,15 @@ __global__ void __launch_bounds__(256) k_c2r_b8(const float2* __restrict__ H, co
     }
 }
 
-constexpr int CH_YT = 16, CH_TS = 259, CH_XR = 17;
+constexpr int CH_YT = 16, CH_TS = 273, CH_XR = 17, CH_STG = 3;
+static_assert(15 * CH_XR + 15 < CH_TS, "the exchange fits in a tile row");
 
 // NH = 256 = 16 (P) x 16 (Q); a half-warp per x line, 16 lines per block
 // (128-byte rows of y per request), two radix-16 stages with one exchange.
+// Three tiles in flight (the next two rotations load while one is
+// transformed); the exchange reuses the row of the tile being transformed
+// (row stride 273: both the tile and the exchange accesses are conflict-free),
+// so two blocks still fit an SM.
 __global__ void __launch_bounds__(256, 2) k_c2r_h256(const float2* __restrict__ H, const float* __restrict__ mu0,
                                                      const float* __restrict__ gam, const double* __restrict__ tsum,
                                                      int Ny, int Nz, int nb, float inv_nm, double c_mean, double inv_m,
@@ -185,9 +190,8 @@ __global__ void __launch_bounds__(256, 2) k_c2r_h256(const float2* __restrict__ 
                                                      const float2* __restrict__ tw_x) {
     constexpr int NH = 256, NH1 = NH + 1, NX = 2 * NH, P = 16, QN = 16, YT = CH_YT, TS = CH_TS, XR = CH_XR;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float2* tile = reinterpret_cast<float2*>(smem_raw);  // [2][YT][TS]
-    float2* xb = tile + 2 * YT * TS;                      // [YT][P][XR] exchange
-    float2* T = xb + YT * P * XR;                         // [QN][P]: W256^(+q k1) at [q][k1]
+    float2* tile = reinterpret_cast<float2*>(smem_raw);  // [3][YT][TS]: a row is a line, then its exchange [P][XR]
+    float2* T = tile + CH_STG * YT * TS;                  // [QN][P]: W256^(+q k1) at [q][k1]
     float2* twx = T + P * QN;                             // [NH]: W512^(+k)
     float* kaps = reinterpret_cast<float*>(twx + NH);     // [nb]
     const int tid = threadIdx.x, line = tid >> 4, j = tid & 15;
@@ -208,13 +212,17 @@ __global__ void __launch_bounds__(256, 2) k_c2r_h256(const float2* __restrict__ 
     const tgtile::TileCopy<YT, NH1, 256> copy(tile, TS, H, tid, y0, z, Ny, Nz);
     auto issue = [&](int b, int which) { copy.issue(b, which * (unsigned)(YT * TS * sizeof(float2))); };
     issue(0, 0);
-    float2* xl = xb + line * P * XR;
+    if (1 < nb) issue(1, 1);
+    else tgtile::commit();
+    int cur = 0;  // stage of rotation b
     for (int b = 0; b < nb; ++b) {
-        if (b + 1 < nb) issue(b + 1, (b + 1) & 1);
+        const int nxt = cur == 0 ? 2 : cur - 1;  // stage of rotation b + 2
+        if (b + 2 < nb) issue(b + 2, nxt);
         else tgtile::commit();
-        tgtile::wait<1>();
+        tgtile::wait<2>();
         __syncthreads();
-        const float2* X = tile + (b & 1) * YT * TS + line * TS;
+        float2* X = tile + cur * YT * TS + line * TS;
+        float2* xl = X;  // the exchange overwrites the row once the half-warp has read it
         {
             float2 u[QN];
 #pragma unroll
@@ -224,6 +232,7 @@ __global__ void __launch_bounds__(256, 2) k_c2r_h256(const float2* __restrict__ 
                 const float2 d = cmul(twx[k], csub(xa, xc));
                 u[k2] = cadd(cadd(xa, xc), make_float2(-d.y, d.x));
             }
+            __syncwarp();  // every lane of the line has read the row
             tgfft::dft16<+1>(u);
 #pragma unroll
             for (int q = 0; q < QN; ++q) xl[j * XR + q] = cmul(u[q], T[q * P + j]);
@@ -241,7 +250,8 @@ __global__ void __launch_bounds__(256, 2) k_c2r_h256(const float2* __restrict__ 
             if (u0 > bu[m][0]) { bu[m][0] = u0; bb[m] = (bb[m] & 0xFFFF0000u) | (unsigned)b; }
             if (u1 > bu[m][1]) { bu[m][1] = u1; bb[m] = (bb[m] & 0x0000FFFFu) | ((unsigned)b << 16); }
         }
-        __syncthreads();  // the tile and the exchange are rewritten next
+        cur = cur == 2 ? 0 : cur + 1;
+        __syncthreads();  // this stage is loaded again next
     }
     if (y >= Ny) return;
     const float mt = (float)mu_t;
@@ -272,7 +282,7 @@ cudaError_t launch_c2r_h256(const float2* H, const float* mu0, const float* gam,
                             int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
                             int* angidx, cudaStream_t st) {
     const size_t smem =
-        sizeof(float2) * (2 * CH_YT * CH_TS + CH_YT * 16 * CH_XR + 16 * 16 + 256) + sizeof(float) * nb;
+        sizeof(float2) * (CH_STG * CH_YT * CH_TS + 16 * 16 + 256) + sizeof(float) * nb;
     cudaFuncSetAttribute(k_c2r_h256, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 g((Ny + CH_YT - 1) / CH_YT, Nz);
     k_c2r_h256<<<g, 256, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc, angidx,
