@@ -84,13 +84,14 @@ def test_y_column_kernels_every_template_height(gpu, oracle, ny, T):
     assert (fidx != gidx).mean() < 1e-3
 
 
+@pytest.mark.parametrize("nz", [256, 464])
 @pytest.mark.parametrize("T", [8, 12, 20, 32, 48, 64])
-def test_z_spectrum_kernel_every_template_depth(gpu, oracle, T):
-    """The z-edge 256 template-spectrum kernel sums each line's z-DFT from its
-    ceil(Tz / 8) terms per residue: every term count against the generic
-    kernels (x and y edges on the generic kernels)."""
+def test_z_spectrum_kernel_every_template_depth(gpu, oracle, nz, T):
+    """The z-edge 256 / 464 template-spectrum kernels sum each line's z-DFT
+    from its ceil(Tz / 8) terms per residue: every term count against the
+    generic kernels (x and y edges on the generic kernels)."""
     rng = np.random.default_rng(31 + T)
-    vol = rng.standard_normal((64, 80, 256)).astype(np.float32)
+    vol = rng.standard_normal((64, 80, nz)).astype(np.float32)
     tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
     mask = oracle.sphere_mask((T, T, T), T // 2 - 1).astype(np.float32)
     angles = oracle.av3_angle_grid((0, 0, 0), (40, 40, 40), (320, 320, 160))[::83][:5]

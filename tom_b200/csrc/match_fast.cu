@@ -289,16 +289,108 @@ __global__ void __launch_bounds__(256) k_spec_z_s256(const float2* __restrict__ 
     }
 }
 
+// z edge 464 (NZ = 8 x 58): as k_spec_z_s256 with two m per lane.  With
+// L8 = NZ / 8, t = d + 8 i and kz = m + L8 k2:
+//   X(kz) = W_NZ^(d0z kz) sum_d W_8^(d k2) [ W_NZ^(d m) sum_i z[d + 8 i] W_L8^(i m) ],
+// lane l owns m = l + 32 q (q < ceil(L8 / 32), m < L8): NI terms per
+// residue, one 8-point DFT per m, the phase W_NZ^(d0z kz) per output.  Eight
+// y lines per block; the block's lines are loaded and stored through shared
+// memory in 64-byte runs of y.
+template <int NZ, int NI>
+__global__ void __launch_bounds__(256, 3) k_spec_z_s(const float2* __restrict__ A, float2* __restrict__ Z, int Ty,
+                                                  int Tz, int d0z, int nh1, const float2* __restrict__ tw_g) {
+    constexpr int L8 = NZ / 8, MB = (L8 + 31) / 32, OS = 9, PER = NI - 1 + 7;
+    static_assert(NZ % 8 == 0 && MB <= 2 && NI >= 1 && NI <= 8, "plan");
+    __shared__ __align__(16) float2 lt[2 * 14 * 32];  // [q][NI-1][32] W_L8^(i m), then [q][7][32] W_NZ^(d m)
+    __shared__ __align__(16) float2 zs[8 * 64];       // [line][slot]: z[t] at (t % 8) * 8 + t / 8
+    __shared__ __align__(16) float2 ob[NZ * OS];      // [kz][line]
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int jy0 = blockIdx.x * 8, kx = blockIdx.y, b = blockIdx.z;
+    for (int e = tid; e < MB * PER * 32; e += 256) {
+        const int q = e / (PER * 32), r = (e / 32) % PER, m = (e % 32) + 32 * q;
+        const int idx = r < NI - 1 ? 8 * (r + 1) * m : (r - (NI - 1) + 1) * m;
+        lt[e] = __ldg(tw_g + idx % NZ);
+    }
+    const long long abase = ((long long)b * nh1 + kx) * Tz * Ty;
+    for (int i = tid; i < 64 * 8; i += 256) {
+        const int t = i >> 3, li = i & 7;
+        float2 v = make_float2(0.f, 0.f);
+        if (t < Tz && jy0 + li < Ty) v = A[abase + (long long)t * Ty + jy0 + li];
+        zs[li * 64 + (t & 7) * 8 + (t >> 3)] = v;
+    }
+    __syncthreads();
+    const float2* zw = zs + w * 64;
+    auto line_sums = [&](int q) {
+        const int m = lane + 32 * q;
+        const float2* lq = lt + q * PER * 32;
+        float2 wi[NI];
+#pragma unroll
+        for (int i = 1; i < NI; ++i) wi[i] = lq[(i - 1) * 32 + lane];
+        float2 v[8];
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+            float2 zz[NI + 1];
+#pragma unroll
+            for (int p = 0; p < (NI + 1) / 2; ++p) {
+                const float4 t = reinterpret_cast<const float4*>(zw + d * 8)[p];  // same address in every lane
+                zz[2 * p] = make_float2(t.x, t.y);
+                zz[2 * p + 1] = make_float2(t.z, t.w);
+            }
+            float2 acc = zz[0];
+#pragma unroll
+            for (int i = 1; i < NI; ++i) {
+                const float2 a = wi[i], c = zz[i];
+                acc.x = fmaf(c.x, a.x, fmaf(-c.y, a.y, acc.x));
+                acc.y = fmaf(c.x, a.y, fmaf(c.y, a.x, acc.y));
+            }
+            if (d > 0) acc = cmul(acc, lq[(NI - 1 + d - 1) * 32 + lane]);
+            v[d] = acc;
+        }
+        tgfft::dft8<-1>(v);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; ++k2) {
+            const int kz = m + L8 * k2;
+            ob[kz * OS + w] = cmul(v[k2], __ldg(tw_g + (d0z * kz) % NZ));
+        }
+    };
+    line_sums(0);
+    if constexpr (MB == 2) {
+        if (lane + 32 < L8) line_sums(1);
+    }
+    __syncthreads();
+    const long long zbase = ((long long)b * nh1 + kx) * NZ * Ty;
+    for (int i = tid; i < NZ * 8; i += 256) {
+        const int kz = i >> 3, li = i & 7;
+        if (jy0 + li < Ty) Z[zbase + (long long)kz * Ty + jy0 + li] = ob[kz * OS + li];
+    }
+}
+
 // ------------------------------------------------------------- dispatch
 
 bool fast_corr_y(int NY, int Ty) { return (NY == 128 || NY == 256 || NY == 512 || NY == 928) && Ty <= 64; }
 bool fast_inv_z(int NZ) { return NZ == 128 || NZ == 256 || NZ == 464; }
 bool fast_c2r(int NH) { return NH == 64 || NH == 128 || NH == 256 || NH == 464; }
-bool fast_spec_z(int NZ, int Tz) { return NZ == 256 && Tz >= 1 && Tz <= 64; }
+bool fast_spec_z(int NZ, int Tz) { return (NZ == 256 || NZ == 464) && Tz >= 1 && Tz <= 64; }
+
+template <int NZ>
+static cudaError_t launch_spec_z_nz(const float2* A, float2* Z, int Ty, int Tz, int d0z, int nh1, int nb,
+                                    cudaStream_t st) {
+    const dim3 g((Ty + 7) / 8, nh1, nb);
+    const float2* tw = twiddle_table<float2>(NZ);
+    switch ((Tz + 7) / 8) {
+#define C_(n) \
+    case n: k_spec_z_s<NZ, n><<<g, 256, 0, st>>>(A, Z, Ty, Tz, d0z, nh1, tw); break;
+        C_(1) C_(2) C_(3) C_(4) C_(5) C_(6) C_(7) C_(8)
+#undef C_
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launch_spec_z_fast(int NZ, const float2* A, float2* Z, int Ty, int Tz, int d0z, int nh1, int nb,
                                cudaStream_t st) {
     if (!fast_spec_z(NZ, Tz)) return cudaErrorInvalidValue;
+    if (NZ == 464) return launch_spec_z_nz<464>(A, Z, Ty, Tz, d0z, nh1, nb, st);
     const dim3 g((Ty + 7) / 8, nh1, nb);
     const float2* tw = twiddle_table<float2>(256);
     switch ((Tz + 7) / 8) {
