@@ -51,6 +51,9 @@ int tomgpu_ctx_destroy(tomgpu_ctx* ctx);
  * as void*); NULL selects the CUDA legacy default stream. */
 int tomgpu_ctx_set_stream(tomgpu_ctx* ctx, void* cuda_stream);
 int tomgpu_ctx_synchronize(tomgpu_ctx* ctx);
+/* Release the device memory that tomgpu_match keeps in the context between
+ * calls (no counterpart in the reference: TOM plans nothing across calls). */
+int tomgpu_ctx_trim(tomgpu_ctx* ctx);
 /* Device kernel launches issued by this context since creation. */
 int64_t tomgpu_ctx_launch_count(const tomgpu_ctx* ctx);
 
@@ -265,7 +268,11 @@ int tomgpu_match_rescore_fp64_dev(tomgpu_match_plan* plan, const float* vol_dev,
 
 /* One-shot, host buffers (what a MEX gateway calls): plan, upload, set
  * template and volume, run all R angles, download.  maxcc/angidx: volume-sized
- * host arrays; angidx is 0-based (-1 where never updated). */
+ * host arrays; angidx is 0-based (-1 where never updated).  The plan and the
+ * device copies of the arguments stay in the context for the next call with
+ * the same sizes, psf presence and params (a search split over several calls,
+ * or one template after another), so such a call allocates nothing;
+ * tomgpu_ctx_trim releases them. */
 int tomgpu_match(tomgpu_ctx* ctx, const float* tomo, const int vol_dims[3], const float* tmpl,
                  const int tmpl_dims[3], const float* mask, const float* psf, const float* eulers,
                  int R, const tomgpu_match_params* params, float* maxcc, int32_t* angidx);

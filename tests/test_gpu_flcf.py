@@ -98,3 +98,34 @@ def test_radix29_sizes(gpu, oracle, N):
     ccc, ang = gpu.tom_os3_findTemplate(vol, tmpl, angles, mask=mask, batch=3)
     idx = np.where(ang > 0, ang - 1, -1).astype(np.int64)
     _compare(ccc, idx, ref_cc, ref_idx, ref_2)
+
+
+def test_match_host_reuses_context_state(gpu, oracle):
+    """tomgpu_match keeps its plan and device buffers in the context between
+    calls with the same sizes: a second call (other template, other angles),
+    a call with other sizes and a call after tomgpu_ctx_trim all equal calls
+    on fresh contexts."""
+    rng = np.random.default_rng(21)
+    T = 16
+    mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
+    vol_a = rng.standard_normal((48, 40, 32)).astype(np.float32)
+    vol_b = rng.standard_normal((40, 48, 32)).astype(np.float32)
+    t1 = rng.standard_normal((T, T, T)).astype(np.float32)
+    t2 = rng.standard_normal((T, T, T)).astype(np.float32)
+    grid = oracle.av3_angle_grid((0, 0, 0), (60, 60, 60), (300, 300, 180))
+    calls = [(vol_a, t1, grid[:12]), (vol_a, t2, grid[12:30]), (vol_b, t1, grid[:7]), (vol_b, t2, grid[30:41])]
+    ctx = gpu.Context(0)
+    try:
+        for i, (v, t, e) in enumerate(calls):
+            if i == 3:
+                ctx.check(gpu._lib.lib().tomgpu_ctx_trim(ctx.handle))
+            got_cc, got_idx = gpu.match_host(v, t, mask, e, batch=4, ctx=ctx)
+            fresh = gpu.Context(0)
+            try:
+                ref_cc, ref_idx = gpu.match_host(v, t, mask, e, batch=4, ctx=fresh)
+            finally:
+                fresh.close()
+            assert np.array_equal(got_cc, ref_cc), i
+            assert np.array_equal(got_idx, ref_idx), i
+    finally:
+        ctx.close()

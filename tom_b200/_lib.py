@@ -67,6 +67,7 @@ _SIGS = {
     "tomgpu_ctx_destroy": (ctypes.c_int, [c_void_p]),
     "tomgpu_ctx_set_stream": (ctypes.c_int, [c_void_p, c_void_p]),
     "tomgpu_ctx_synchronize": (ctypes.c_int, [c_void_p]),
+    "tomgpu_ctx_trim": (ctypes.c_int, [c_void_p]),
     "tomgpu_ctx_launch_count": (ctypes.c_int64, [c_void_p]),
     "tomgpu_ctx_profile": (ctypes.c_int, [c_void_p, ctypes.c_int]),
     "tomgpu_ctx_profile_read": (ctypes.c_int, [c_void_p, ctypes.c_int, c_double_p, ctypes.POINTER(ctypes.c_int64)]),

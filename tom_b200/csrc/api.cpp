@@ -14,6 +14,33 @@
 #include "rotate.h"
 #include "twiddles.h"
 
+// tomgpu_match's state kept in the context between calls
+struct MatchCache {
+    tomgpu_match_plan* plan = nullptr;
+    int vol[3] = {0, 0, 0}, tm[3] = {0, 0, 0};
+    tomgpu_match_params prm{};
+    bool psf = false;
+    float *d_vol = nullptr, *d_t = nullptr, *d_m = nullptr, *d_p = nullptr, *d_cc = nullptr;
+    int* d_i = nullptr;
+
+    bool same(const int v[3], const int t[3], const tomgpu_match_params& p, bool has_psf) const {
+        for (int d = 0; d < 3; ++d)
+            if (vol[d] != v[d] || tm[d] != t[d]) return false;
+        return has_psf == psf && std::memcmp(&prm, &p, sizeof(p)) == 0;
+    }
+    ~MatchCache() {
+        void* ptrs[] = {d_vol, d_t, d_m, d_p, d_cc, d_i};
+        for (void* q : ptrs)
+            if (q) cudaFree(q);
+        tomgpu_match_plan_destroy(plan);
+    }
+};
+
+static void drop_match_cache(tomgpu_ctx* ctx) {
+    delete static_cast<MatchCache*>(ctx->match_cache);
+    ctx->match_cache = nullptr;
+}
+
 namespace tg {
 
 static thread_local std::string g_create_error;
@@ -170,6 +197,7 @@ int tomgpu_ctx_destroy(tomgpu_ctx* ctx) {
     if (!ctx) return TOMGPU_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drop_match_cache(ctx);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_err) cudaFree(ctx->d_err);
     for (auto& p : ctx->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
@@ -789,6 +817,14 @@ int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jo
     return TOMGPU_OK;
 }
 
+int tomgpu_ctx_trim(tomgpu_ctx* ctx) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    TG_TRY(use_device(ctx));
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drop_match_cache(ctx);
+    return TOMGPU_OK;
+}
+
 int tomgpu_match(tomgpu_ctx* ctx, const float* tomo, const int vol[3], const float* tmpl, const int tm[3],
                  const float* mask, const float* psf, const float* eulers, int R, const tomgpu_match_params* params,
                  float* maxcc, int32_t* angidx) {
@@ -796,41 +832,55 @@ int tomgpu_match(tomgpu_ctx* ctx, const float* tomo, const int vol[3], const flo
     if (!tomo || !tmpl || !mask || !maxcc || !angidx || (R > 0 && !eulers) || R < 0 || !dims_ok(vol) || !dims_ok(tm))
         return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
     TG_TRY(use_device(ctx));
-    tomgpu_match_plan* plan = nullptr;
-    TG_TRY(tomgpu_match_plan_create(ctx, vol, tm, params, &plan));
+    tomgpu_match_params prm{};
+    if (params) prm = *params;
+    MatchCache* mc = static_cast<MatchCache*>(ctx->match_cache);
+    if (mc && !mc->same(vol, tm, prm, psf != nullptr)) {
+        cudaStreamSynchronize(ctx->stream);
+        drop_match_cache(ctx);
+        mc = nullptr;
+    }
     const long long nv = numel(vol), nt = numel(tm);
-    float *d_vol = nullptr, *d_t = nullptr, *d_m = nullptr, *d_p = nullptr, *d_cc = nullptr;
-    int* d_i = nullptr;
+    if (!mc) {
+        mc = new MatchCache();
+        for (int d = 0; d < 3; ++d) { mc->vol[d] = vol[d]; mc->tm[d] = tm[d]; }
+        mc->prm = prm;
+        mc->psf = psf != nullptr;
+        int rc = tomgpu_match_plan_create(ctx, vol, tm, params, &mc->plan);
+        if (!rc && (cudaMalloc(&mc->d_vol, sizeof(float) * nv) || cudaMalloc(&mc->d_t, sizeof(float) * nt) ||
+                    cudaMalloc(&mc->d_m, sizeof(float) * nt) || (psf && cudaMalloc(&mc->d_p, sizeof(float) * nt)) ||
+                    cudaMalloc(&mc->d_cc, sizeof(float) * nv) || cudaMalloc(&mc->d_i, sizeof(int) * nv))) {
+            cudaGetLastError();
+            rc = cuda_fail(ctx, cudaErrorMemoryAllocation, "match buffers");
+        }
+        if (rc) {
+            delete mc;
+            return rc;
+        }
+        ctx->match_cache = mc;
+    }
+    tomgpu_match_plan* plan = mc->plan;
     int rc = TOMGPU_OK;
     cudaStream_t st = ctx->stream;
     do {
-        if (cudaMalloc(&d_vol, sizeof(float) * nv) || cudaMalloc(&d_t, sizeof(float) * nt) ||
-            cudaMalloc(&d_m, sizeof(float) * nt) || (psf && cudaMalloc(&d_p, sizeof(float) * nt)) ||
-            cudaMalloc(&d_cc, sizeof(float) * nv) || cudaMalloc(&d_i, sizeof(int) * nv)) {
-            rc = cuda_fail(ctx, cudaErrorMemoryAllocation, "match buffers");
-            break;
-        }
-        cudaError_t e = cudaMemcpyAsync(d_vol, tomo, sizeof(float) * nv, cudaMemcpyHostToDevice, st);
-        if (!e) e = cudaMemcpyAsync(d_t, tmpl, sizeof(float) * nt, cudaMemcpyHostToDevice, st);
-        if (!e) e = cudaMemcpyAsync(d_m, mask, sizeof(float) * nt, cudaMemcpyHostToDevice, st);
-        if (!e && psf) e = cudaMemcpyAsync(d_p, psf, sizeof(float) * nt, cudaMemcpyHostToDevice, st);
+        cudaError_t e = cudaMemcpyAsync(mc->d_vol, tomo, sizeof(float) * nv, cudaMemcpyHostToDevice, st);
+        if (!e) e = cudaMemcpyAsync(mc->d_t, tmpl, sizeof(float) * nt, cudaMemcpyHostToDevice, st);
+        if (!e) e = cudaMemcpyAsync(mc->d_m, mask, sizeof(float) * nt, cudaMemcpyHostToDevice, st);
+        if (!e && psf) e = cudaMemcpyAsync(mc->d_p, psf, sizeof(float) * nt, cudaMemcpyHostToDevice, st);
         if (e) { rc = cuda_fail(ctx, e, "upload"); break; }
-        if ((rc = tomgpu_match_set_template_dev(plan, d_t, d_m, d_p))) break;
-        if ((rc = tomgpu_match_set_volume_dev(plan, d_vol))) break;
-        if ((rc = tomgpu_match_init_results_dev(plan, d_cc, d_i))) break;
-        if ((rc = tomgpu_match_run_dev(plan, eulers, R, 0, d_cc, d_i))) break;
-        e = cudaMemcpyAsync(maxcc, d_cc, sizeof(float) * nv, cudaMemcpyDeviceToHost, st);
-        if (!e) e = cudaMemcpyAsync(angidx, d_i, sizeof(int) * nv, cudaMemcpyDeviceToHost, st);
+        if ((rc = tomgpu_match_set_template_dev(plan, mc->d_t, mc->d_m, mc->d_p))) break;
+        if ((rc = tomgpu_match_set_volume_dev(plan, mc->d_vol))) break;
+        if ((rc = tomgpu_match_init_results_dev(plan, mc->d_cc, mc->d_i))) break;
+        if ((rc = tomgpu_match_run_dev(plan, eulers, R, 0, mc->d_cc, mc->d_i))) break;
+        e = cudaMemcpyAsync(maxcc, mc->d_cc, sizeof(float) * nv, cudaMemcpyDeviceToHost, st);
+        if (!e) e = cudaMemcpyAsync(angidx, mc->d_i, sizeof(int) * nv, cudaMemcpyDeviceToHost, st);
         if (!e) e = cudaStreamSynchronize(st);
         if (e) { rc = cuda_fail(ctx, e, "download"); break; }
     } while (0);
-    if (d_vol) cudaFree(d_vol);
-    if (d_t) cudaFree(d_t);
-    if (d_m) cudaFree(d_m);
-    if (d_p) cudaFree(d_p);
-    if (d_cc) cudaFree(d_cc);
-    if (d_i) cudaFree(d_i);
-    tomgpu_match_plan_destroy(plan);
+    if (rc) {  // leave nothing half-set for the next call
+        cudaStreamSynchronize(st);
+        drop_match_cache(ctx);
+    }
     return rc;
 }
 

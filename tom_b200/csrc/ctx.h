@@ -18,6 +18,9 @@ struct tomgpu_ctx {
     // small scratch for reductions (peak keys, partial sums)
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
+    // tomgpu_match's plan and device buffers, kept for the next call with the
+    // same sizes and parameters (released by tomgpu_ctx_trim and at destroy)
+    void* match_cache = nullptr;
     // kernel-class timers (tomgpu_ctx_profile)
     bool prof = false;
     struct Pending { int kind; cudaEvent_t a, b; };
