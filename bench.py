@@ -335,7 +335,11 @@ def run_align(args):
     torch.cuda.set_device(local)
     jobs, truth = synth.make_align_particles(args.align_particles, seed=77)
     ctx = tb.default_context(local)
-    tb.av3_align_batch(jobs[:1], ctx)  # warm-up
+    # warm-up: one particle of every box size (twiddle tables, first launches)
+    first = {}
+    for j in jobs:
+        first.setdefault(j["ref"].shape, j)
+    tb.av3_align_batch(list(first.values()), ctx)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     angles, shifts, peaks = tb.av3_align_batch(jobs, ctx)

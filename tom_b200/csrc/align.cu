@@ -247,6 +247,18 @@ struct Workspace {
 
 }  // namespace
 
+// The alignment workspace of one tomgpu_av3_align_dev call: grown to the
+// largest job, reused by the following jobs.
+struct AlignScratch {
+    Workspace w;
+    size_t cap[14] = {0};
+    void release() {
+        w.release();
+        w = Workspace();
+        for (size_t& c : cap) c = 0;
+    }
+};
+
 // norm_inside_mask on E complex volumes X (real parts), in place
 static cudaError_t normalize_entries(float2* X, const float* mask, long long nn, int E, double nmask, Workspace& w,
                                      cudaStream_t st, int64_t* launches) {
@@ -346,7 +358,7 @@ int corr_norm(tomgpu_ctx* ctx, const float* a, const float* b, const int n[3], c
 }
 
 int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3], float* peak_out,
-              size_t budget_voxels) {
+              size_t budget_voxels, AlignScratch* scratch) {
     const int* n = job.n;
     const long long nn = (long long)n[0] * n[1] * n[2];
     cudaStream_t st = ctx->stream;
@@ -367,17 +379,29 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
     const int R = (int)scan.size();
     int E = (int)std::max<long long>(1, std::min<long long>(256, (long long)budget_voxels / nn));
     E = std::min(E, R);
-    Workspace w;
-    auto A = [&](void** p, size_t b) { return cudaMalloc(p, b) == cudaSuccess; };
-    if (!A((void**)&w.A, sizeof(float2) * nn * E) || !A((void**)&w.B, sizeof(float2) * nn * E) ||
-        !A((void**)&w.B0, sizeof(float2) * nn) || (wedges && !A((void**)&w.W, sizeof(float) * nn * E)) ||
-        !A((void**)&w.cmax, sizeof(float) * nn) || !A((void**)&w.amax, sizeof(float) * nn) ||
-        !A((void**)&w.tmp, sizeof(float) * nn) || !A((void**)&w.mats, sizeof(float) * 18 * E) ||
-        !A((void**)&w.aidx, sizeof(int) * E) || !A((void**)&w.sums, sizeof(double) * E) ||
-        !A((void**)&w.mea, sizeof(double) * E) || !A((void**)&w.var, sizeof(double) * E) ||
-        !A((void**)&w.spline, sizeof(double) * 8) || !A((void**)&w.key, sizeof(unsigned long long))) {
+    AlignScratch local;
+    AlignScratch& sc = scratch ? *scratch : local;
+    Workspace& w = sc.w;
+    // grow-only buffers, kept for the next job of the call
+    size_t* cap = sc.cap;
+    auto G = [&](int i, void** p, size_t b) {
+        if (b <= cap[i]) return true;
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        cap[i] = 0;
+        if (cudaMalloc(p, b) != cudaSuccess) return false;
+        cap[i] = b;
+        return true;
+    };
+    if (!G(0, (void**)&w.A, sizeof(float2) * nn * E) || !G(1, (void**)&w.B, sizeof(float2) * nn * E) ||
+        !G(2, (void**)&w.B0, sizeof(float2) * nn) || (wedges && !G(3, (void**)&w.W, sizeof(float) * nn * E)) ||
+        !G(4, (void**)&w.cmax, sizeof(float) * nn) || !G(5, (void**)&w.amax, sizeof(float) * nn) ||
+        !G(6, (void**)&w.tmp, sizeof(float) * nn) || !G(7, (void**)&w.mats, sizeof(float) * 18 * R) ||
+        !G(8, (void**)&w.aidx, sizeof(int) * R) || !G(9, (void**)&w.sums, sizeof(double) * E) ||
+        !G(10, (void**)&w.mea, sizeof(double) * E) || !G(11, (void**)&w.var, sizeof(double) * E) ||
+        !G(12, (void**)&w.spline, sizeof(double) * 8) || !G(13, (void**)&w.key, sizeof(unsigned long long))) {
         cudaGetLastError();
-        w.release();
+        sc.release();
         return fail(ctx, TOMGPU_ERR_OOM, "alignment workspace allocation failed");
     }
     int rc = TOMGPU_OK;
@@ -397,22 +421,25 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
         if ((e = c2c3d<float2>(w.B0, n, -1, 1.0, st))) break;
         k_al_fill<<<grid_for(nn), 256, 0, st>>>(w.cmax, w.amax, nn, -2.f, -2.f);
         ctx->launches += 5;
-        std::vector<float> mats(18 * (size_t)E);
-        std::vector<int> aid(E);
+        // every rotation's matrices and angle index, uploaded once: [R] matrix-mode
+        // matrices, then [R] Euler-mode matrices
+        std::vector<float> mats(18 * (size_t)R);
+        std::vector<int> aid(R);
+        for (int q = 0; q < R; ++q) {
+            const Ang& g = scan[q];
+            rotmatrix_as_float(g.phi, g.psi, g.theta, mats.data() + 9 * q);
+            const float eul[3] = {(float)g.phi, (float)g.psi, (float)g.theta};
+            euler_matrix_host(eul, mats.data() + 9 * (size_t)R + 9 * q);
+            aid[q] = g.idx;
+        }
+        if ((e = cudaMemcpyAsync(w.mats, mats.data(), sizeof(float) * 18 * R, cudaMemcpyHostToDevice, st))) break;
+        if ((e = cudaMemcpyAsync(w.aidx, aid.data(), sizeof(int) * R, cudaMemcpyHostToDevice, st))) break;
         for (int off = 0; off < R && !e; off += E) {
             const int nb = std::min(E, R - off);
-            for (int q = 0; q < nb; ++q) {
-                const Ang& g = scan[off + q];
-                rotmatrix_as_float(g.phi, g.psi, g.theta, mats.data() + 9 * q);
-                const float eul[3] = {(float)g.phi, (float)g.psi, (float)g.theta};
-                euler_matrix_host(eul, mats.data() + 9 * E + 9 * q);
-                aid[q] = g.idx;
-            }
-            if ((e = cudaMemcpyAsync(w.mats, mats.data(), sizeof(float) * 18 * E, cudaMemcpyHostToDevice, st))) break;
-            if ((e = cudaMemcpyAsync(w.aidx, aid.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, st))) break;
             dim3 g((unsigned)((nn + 255) / 256), nb);
-            k_al_rotate<<<g, 256, 0, st>>>(job.ref, job.wedge_ref, job.mask, w.mats, w.mats + 9 * E, n[0], n[1], n[2],
-                                           cx, cy, cz, wedges ? 1 : 0, w.A, wedges ? w.W : nullptr);
+            k_al_rotate<<<g, 256, 0, st>>>(job.ref, job.wedge_ref, job.mask, w.mats + 9 * off,
+                                           w.mats + 9 * (size_t)R + 9 * off, n[0], n[1], n[2], cx, cy, cz,
+                                           wedges ? 1 : 0, w.A, wedges ? w.W : nullptr);
             ctx->launches += 1;
             if (wedges) {
                 // a = ref_rot*mask (*) psf_part
@@ -435,7 +462,8 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
             if ((e = c2c3d_batch(w.B, n, nb, -1, 1.0, st))) break;
             k_al_cross<<<grid_for(nn * nb), 256, 0, st>>>(w.B, w.A, nn * nb);
             if ((e = c2c3d_batch(w.B, n, nb, +1, 1.0 / (double)nn, st))) break;
-            k_al_update<<<grid_for(nn), 256, 0, st>>>(w.B, n[0], n[1], n[2], nb, 1.0 / nmask, w.aidx, w.cmax, w.amax);
+            k_al_update<<<grid_for(nn), 256, 0, st>>>(w.B, n[0], n[1], n[2], nb, 1.0 / nmask, w.aidx + off, w.cmax,
+                                                      w.amax);
             e = cudaGetLastError();
             ctx->launches += 2 + 9;
         }
@@ -494,8 +522,16 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
         *peak_out = (float)std::fmax(h[3], std::fmax(h[4], h[5]));
     } while (0);
     if (e && !rc) rc = cuda_fail(ctx, e, "av3_align");
-    w.release();
+    if (!scratch) local.release();
     return rc;
+}
+
+AlignScratch* align_scratch_new() { return new AlignScratch(); }
+
+void align_scratch_free(AlignScratch* s) {
+    if (!s) return;
+    s->release();
+    delete s;
 }
 
 }  // namespace tg

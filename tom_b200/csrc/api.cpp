@@ -803,18 +803,24 @@ int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jo
     if (n_jobs < 0 || (n_jobs > 0 && (!jobs || !angles || !shifts || !ccf_peak)))
         return fail(ctx, TOMGPU_ERR_ARG, "null pointer or negative job count");
     TG_TRY(use_device(ctx));
-    for (int j = 0; j < n_jobs; ++j) {
+    AlignScratch* scratch = align_scratch_new();
+    int rc = TOMGPU_OK;
+    for (int j = 0; j < n_jobs && !rc; ++j) {
         const tomgpu_align_job& jb = jobs[j];
-        if (!dims_ok(jb.n)) return fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad box size");
-        for (int a = 0; a < 3; ++a) {
+        if (!dims_ok(jb.n)) {
+            rc = fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad box size");
+            break;
+        }
+        for (int a = 0; a < 3 && !rc; ++a) {
             const float* r = a == 0 ? jb.phi : (a == 1 ? jb.psi : jb.theta);
             if (r[1] < 0 || (r[1] == 0 && r[2] != r[0]) || r[2] < r[0])
-                return fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad angle range");
+                rc = fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad angle range");
         }
-        const int rc = align_job(ctx, jb, angles + 3 * j, shifts + 3 * j, ccf_peak + j, (size_t)1 << 24);
-        if (rc) return rc;
+        if (!rc) rc = align_job(ctx, jb, angles + 3 * j, shifts + 3 * j, ccf_peak + j, (size_t)1 << 24, scratch);
     }
-    return TOMGPU_OK;
+    cudaStreamSynchronize(ctx->stream);
+    align_scratch_free(scratch);
+    return rc;
 }
 
 int tomgpu_ctx_trim(tomgpu_ctx* ctx) {

@@ -106,8 +106,12 @@ struct MatchPlan {
 
 int corr_norm(tomgpu_ctx* ctx, const float* a, const float* b, const int n[3], const float* mask, const float* psf1,
               const float* psf2, float* out);
+// scratch: workspace reused across jobs (align_scratch_new), or NULL for a private one
+struct AlignScratch;
+AlignScratch* align_scratch_new();
+void align_scratch_free(AlignScratch* s);
 int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3],
-              float* peak_out, size_t budget_voxels);
+              float* peak_out, size_t budget_voxels, AlignScratch* scratch);
 int av3_average_add(tomgpu_ctx* ctx, const int n[3], const tomgpu_avg_item* items, int K, double* avg, double* wei);
 int corr3d_peaks(tomgpu_ctx* ctx, const int n[3], const float* const* templates, int nt, const float* const* particles,
                  int np, const double* angles_deg, int nang, const float* mask, const tomgpu_wedge_spec* wedge_t,
