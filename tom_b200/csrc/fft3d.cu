@@ -29,8 +29,16 @@ __global__ void __launch_bounds__(256) k_fft_lines(const void* in, void* out,
     constexpr int NL = LineCfg<L>::NL, NT = LineCfg<L>::NT, LS = LineCfg<L>::LS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
+    // element offsets of the block's lines (one division per line, not per element)
+    __shared__ long offs_i[NL], offs_o[NL];
     const int tid = threadIdx.x;
     const long line0 = (long)blockIdx.x * NL;
+    for (int l = tid; l < NL; l += NT) {
+        const long gl = line0 + l;
+        offs_i[l] = (gl % gi.cnt0) * gi.s0 + (gl / gi.cnt0) * gi.s1;
+        offs_o[l] = (gl % go.cnt0) * go.s0 + (gl / go.cnt0) * go.s1;
+    }
+    __syncthreads();
     const Rt* rin = reinterpret_cast<const Rt*>(in);
     const C* cin = reinterpret_cast<const C*>(in);
 
@@ -41,7 +49,7 @@ __global__ void __launch_bounds__(256) k_fft_lines(const void* in, void* out,
         const long gl = line0 + l;
         C v = CTraits<C>::make(0, 0);
         if (gl < nlines) {
-            const long off = (gl % gi.cnt0) * gi.s0 + (gl / gi.cnt0) * gi.s1;
+            const long off = offs_i[l];
             if (MODE == FFT_R2C) {
                 v = CTraits<C>::make(rin[off + e * gi.es], 0);
             } else if (MODE == FFT_C2R) {
@@ -65,7 +73,7 @@ __global__ void __launch_bounds__(256) k_fft_lines(const void* in, void* out,
         else { e = i / NL; l = i - e * NL; }
         const long gl = line0 + l;
         if (gl >= nlines) continue;
-        const long off = (gl % go.cnt0) * go.s0 + (gl / go.cnt0) * go.s1;
+        const long off = offs_o[l];
         const C v = s[l * LS + e];
         if (MODE == FFT_R2C) {
             if (e <= L / 2) cout[off + e * go.es] = cscale(v, sc);
