@@ -50,21 +50,16 @@ TG_D long long shifted(long long v, int nx, int ny, int nz, int sgn) {
     return si + (long long)nx * (sj + (long long)ny * sk);
 }
 
-TG_D long long mirrored(long long v, int nx, int ny, int nz) {
-    const int i = (int)(v % nx), j = (int)((v / nx) % ny), k = (int)(v / ((long long)nx * ny));
-    return pmod(-i, nx) + (long long)nx * (pmod(-j, ny) + (long long)ny * pmod(-k, nz));
-}
-
 // A[e] = rot(ref, mref_e) * mask (complex), W[e] = rot(wedge_ref, mw_e)
 __global__ void k_al_rotate(const float* __restrict__ ref, const float* __restrict__ wref,
                             const float* __restrict__ mask, const float* __restrict__ mref,
                             const float* __restrict__ mw, int nx, int ny, int nz, float cx, float cy, float cz,
                             int mask_ref, float2* __restrict__ A, float* __restrict__ W) {
-    const long long nn = (long long)nx * ny * nz;
-    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nn = nx * ny * nz;  // boxes hold fewer than 2^31 voxels
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const int e = blockIdx.y;
     if (v >= nn) return;
-    const int i = (int)(v % nx), j = (int)((v / nx) % ny), k = (int)(v / ((long long)nx * ny));
+    const int i = v % nx, t = v / nx, j = t % ny, k = t / ny;
     float m[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) m[q] = mref[9 * e + q];
@@ -80,25 +75,52 @@ __global__ void k_al_rotate(const float* __restrict__ ref, const float* __restri
 
 // A[e][k] *= (W'(k) + W'(-k)) / 2, W' = ifftshift(wedge_part): the spectrum of
 // psf_part = real(ifftn(W'))
+// The two source voxels of (W'(k) + W'(-k)) / 2 with W' = ifftshift(W):
+// ifftshift(v) and ifftshift(-v) (all boxes hold fewer than 2^31 voxels).
+TG_D void wedge_pair(int v, int nx, int ny, int nz, int& s1, int& s2) {
+    const int i = v % nx, t = v / nx, j = t % ny, k = t / ny;
+    const int hx = nx / 2, hy = ny / 2, hz = nz / 2;
+    const int a1 = i + hx < nx ? i + hx : i + hx - nx, b1 = j + hy < ny ? j + hy : j + hy - ny,
+              c1 = k + hz < nz ? k + hz : k + hz - nz;
+    const int mi = i ? nx - i : 0, mj = j ? ny - j : 0, mk = k ? nz - k : 0;
+    const int a2 = mi + hx < nx ? mi + hx : mi + hx - nx, b2 = mj + hy < ny ? mj + hy : mj + hy - ny,
+              c2 = mk + hz < nz ? mk + hz : mk + hz - nz;
+    s1 = a1 + nx * (b1 + ny * c1);
+    s2 = a2 + nx * (b2 + ny * c2);
+}
+
+// A[e][k] *= (W'(k) + W'(-k)) / 2, W' = ifftshift(wedge_part): the spectrum of
+// psf_part; the weight is the same for every entry, so one thread per voxel
+// applies it to the AL_EG entries of its group (blockIdx.y)
+constexpr int AL_EG = 16;
 __global__ void k_al_wpart(float2* __restrict__ A, const float* __restrict__ wpart, int nx, int ny, int nz, int E) {
-    const long long nn = (long long)nx * ny * nz;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn * E; t += (long long)gridDim.x * blockDim.x) {
-        const long long v = t % nn;
-        const float ws = 0.5f * (wpart[shifted(v, nx, ny, nz, +1)] +
-                                 wpart[shifted(mirrored(v, nx, ny, nz), nx, ny, nz, +1)]);
-        A[t] = cscale(A[t], ws);
+    const int nn = nx * ny * nz;
+    const int e0 = blockIdx.y * AL_EG, e1 = min(E, e0 + AL_EG);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += gridDim.x * blockDim.x) {
+        int s1, s2;
+        wedge_pair(v, nx, ny, nz, s1, s2);
+        const float ws = 0.5f * (wpart[s1] + wpart[s2]);
+        for (int e = e0; e < e1; ++e) {
+            float2* a = A + (long long)e * nn + v;
+            *a = cscale(*a, ws);
+        }
     }
 }
 
-// B[e][k] = B0[k] * (W'(k) + W'(-k)) / 2, W' = ifftshift(W[e])
+// B[e][k] = B0[k] * (W'(k) + W'(-k)) / 2, W' = ifftshift(W[e]); the index pair
+// is computed once per voxel for the AL_EG entries of the group
 __global__ void k_al_bside(float2* __restrict__ B, const float2* __restrict__ B0, const float* __restrict__ W, int nx,
                            int ny, int nz, int E) {
-    const long long nn = (long long)nx * ny * nz;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn * E; t += (long long)gridDim.x * blockDim.x) {
-        const long long v = t % nn, e = t / nn;
-        const float* w = W + e * nn;
-        const float ws = 0.5f * (w[shifted(v, nx, ny, nz, +1)] + w[shifted(mirrored(v, nx, ny, nz), nx, ny, nz, +1)]);
-        B[t] = cscale(B0[v], ws);
+    const int nn = nx * ny * nz;
+    const int e0 = blockIdx.y * AL_EG, e1 = min(E, e0 + AL_EG);
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += gridDim.x * blockDim.x) {
+        int s1, s2;
+        wedge_pair(v, nx, ny, nz, s1, s2);
+        const float2 b0 = B0[v];
+        for (int e = e0; e < e1; ++e) {
+            const float* w = W + (long long)e * nn;
+            B[(long long)e * nn + v] = cscale(b0, 0.5f * (w[s1] + w[s2]));
+        }
     }
 }
 
@@ -444,10 +466,10 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
             if (wedges) {
                 // a = ref_rot*mask (*) psf_part
                 if ((e = c2c3d_batch(w.A, n, nb, -1, 1.0, st))) break;
-                k_al_wpart<<<grid_for(nn * nb), 256, 0, st>>>(w.A, wpart, n[0], n[1], n[2], nb);
+                k_al_wpart<<<dim3(grid_for(nn), (nb + AL_EG - 1) / AL_EG), 256, 0, st>>>(w.A, wpart, n[0], n[1], n[2], nb);
                 if ((e = c2c3d_batch(w.A, n, nb, +1, 1.0 / (double)nn, st))) break;
                 // b = part*mask (*) psf_ref
-                k_al_bside<<<grid_for(nn * nb), 256, 0, st>>>(w.B, w.B0, w.W, n[0], n[1], n[2], nb);
+                k_al_bside<<<dim3(grid_for(nn), (nb + AL_EG - 1) / AL_EG), 256, 0, st>>>(w.B, w.B0, w.W, n[0], n[1], n[2], nb);
                 if ((e = c2c3d_batch(w.B, n, nb, +1, 1.0 / (double)nn, st))) break;
                 ctx->launches += 2 + 9;
             } else {
