@@ -15,10 +15,31 @@
 
 namespace tg {
 
-template <int L> struct LineCfg {
+// Skew and line pitch of the shared-memory lines, per length and element
+// size, chosen by counting the bank-conflict wavefronts of every load, stage
+// and store of k_fft_lines (x pass and two strided passes) for each candidate
+// and kept where the measured pass time agreed (96 with 8-byte elements
+// measured no faster skewed and stays unskewed):
+// {L, SK, LS for 8-byte elements, SK, LS for 16-byte elements}.
+struct LineLayout { int L, sk8, ls8, sk16, ls16; };
+constexpr LineLayout kLineLayouts[] = {
+    {8, 0, 9, 0, 9},       {12, 0, 19, 0, 19},    {16, 0, 17, 0, 17},    {20, 0, 21, 2, 25},
+    {24, 3, 27, 3, 27},    {32, 0, 35, 3, 37},    {40, 3, 45, 3, 45},    {48, 4, 51, 4, 51},
+    {64, 4, 69, 3, 73},    {80, 4, 85, 4, 85},    {96, 0, 97, 3, 109},  {128, 4, 137, 3, 145},
+    {160, 4, 170, 3, 181}, {192, 4, 206, 3, 217}, {256, 4, 274, 4, 273}, {512, 4, 548, 3, 578}};
+constexpr LineLayout line_layout(int L) {
+    for (const LineLayout& x : kLineLayouts)
+        if (x.L == L) return x;
+    return {L, 0, L + 1, 0, L + 1};  // the radix-29 lengths: unskewed
+}
+
+template <int L, typename C> struct LineCfg {
     static constexpr int NL = (2048 / L) < 1 ? 1 : ((2048 / L) > 64 ? 64 : (2048 / L));
     static constexpr int NT = 256;
-    static constexpr int LS = L + 1;
+    static constexpr bool W16 = sizeof(C) == 16;
+    static constexpr int SK = W16 ? line_layout(L).sk16 : line_layout(L).sk8;
+    static constexpr int LS = W16 ? line_layout(L).ls16 : line_layout(L).ls8;
+    static_assert(LS >= tgfft::skew<SK>(L - 1) + 1, "line pitch holds the skewed line");
 };
 
 template <int L, int DIR, int MODE, typename C>
@@ -26,7 +47,7 @@ __global__ void __launch_bounds__(256) k_fft_lines(const void* in, void* out,
                                                    LineGeom gi, LineGeom go, const C* __restrict__ tw,
                                                    double scale, long nlines) {
     typedef typename CTraits<C>::R Rt;
-    constexpr int NL = LineCfg<L>::NL, NT = LineCfg<L>::NT, LS = LineCfg<L>::LS;
+    constexpr int NL = LineCfg<L, C>::NL, NT = LineCfg<L, C>::NT, LS = LineCfg<L, C>::LS, SK = LineCfg<L, C>::SK;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s = reinterpret_cast<C*>(smem_raw);
     // element offsets of the block's lines (one division per line, not per element)
@@ -59,10 +80,10 @@ __global__ void __launch_bounds__(256) k_fft_lines(const void* in, void* out,
                 v = cin[off + e * gi.es];
             }
         }
-        s[l * LS + e] = v;
+        s[l * LS + tgfft::skew<SK>(e)] = v;
     }
     __syncthreads();
-    tgfft::smem_fft<L, DIR, NL, NT, LS, C>(s, tw, tid);
+    tgfft::smem_fft<L, DIR, NL, NT, LS, C, SK>(s, tw, tid);
 
     Rt* rout = reinterpret_cast<Rt*>(out);
     C* cout = reinterpret_cast<C*>(out);
@@ -74,7 +95,7 @@ __global__ void __launch_bounds__(256) k_fft_lines(const void* in, void* out,
         const long gl = line0 + l;
         if (gl >= nlines) continue;
         const long off = offs_o[l];
-        const C v = s[l * LS + e];
+        const C v = s[l * LS + tgfft::skew<SK>(e)];
         if (MODE == FFT_R2C) {
             if (e <= L / 2) cout[off + e * go.es] = cscale(v, sc);
         } else if (MODE == FFT_C2R) {
@@ -88,7 +109,8 @@ __global__ void __launch_bounds__(256) k_fft_lines(const void* in, void* out,
 template <int L, int DIR, int MODE, typename C>
 static cudaError_t launch_lines_t(const void* in, void* out, const LineGeom& gi, const LineGeom& go,
                                   long nlines, double scale, cudaStream_t st) {
-    constexpr int NL = LineCfg<L>::NL, NT = LineCfg<L>::NT, LS = LineCfg<L>::LS;
+    constexpr int NL = LineCfg<L, C>::NL, LS = LineCfg<L, C>::LS;
+    constexpr int NT = LineCfg<L, C>::NT;
     const size_t smem = (size_t)NL * LS * sizeof(C);
     auto kern = k_fft_lines<L, DIR, MODE, C>;
     static unsigned attr_mask = 0;  // one bit per device: attribute already raised

@@ -232,7 +232,12 @@ TG_D void dft(C* v, const C* __restrict__ tw, int q) {
 }
 
 // ------------------------------------------------------------ one stage
-template <int L, int R, int NS, int DIR, int NL, int NT, int LS, typename C>
+// Position of element p of a line in shared memory: p + (p >> SK) (one
+// padding slot every 2^SK elements, SK = 0: none), which spreads the
+// power-of-two strides of the Stockham stages over the banks.
+template <int SK> TG_HD constexpr int skew(int p) { return SK ? p + (p >> SK) : p; }
+
+template <int L, int R, int NS, int DIR, int NL, int NT, int LS, typename C, int SK = 0>
 TG_D void stage(C* s, const C* __restrict__ tw, int tid) {
     constexpr int NBL = L / R;
     constexpr int NB = NL * NBL;
@@ -243,9 +248,9 @@ TG_D void stage(C* s, const C* __restrict__ tw, int tid) {
         const int b = tid + q * NT;
         if (NB % NT == 0 || b < NB) {
             const int line = b / NBL, j = b - line * NBL;
-            const C* src = s + line * LS + j;
+            const C* src = s + line * LS;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[q][r] = src[r * NBL];
+            for (int r = 0; r < R; ++r) v[q][r] = src[skew<SK>(j + r * NBL)];
             if (NS > 1) {
                 const int k = j % NS;
 #pragma unroll
@@ -265,30 +270,32 @@ TG_D void stage(C* s, const C* __restrict__ tw, int tid) {
         if (NB % NT == 0 || b < NB) {
             const int line = b / NBL, j = b - line * NBL;
             const int k = j % NS;
-            C* dst = s + line * LS + (j - k) * R + k;
+            C* dst = s + line * LS;
+            const int p0 = (j - k) * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) dst[r * NS] = v[q][r];
+            for (int r = 0; r < R; ++r) dst[skew<SK>(p0 + r * NS)] = v[q][r];
         }
     }
     __syncthreads();
 }
 
-template <int L, int DIR, int NL, int NT, int LS, typename C, int NS, int R, int... Rest>
+template <int L, int DIR, int NL, int NT, int LS, typename C, int SK, int NS, int R, int... Rest>
 TG_D void run_stages(C* s, const C* __restrict__ tw, int tid) {
-    stage<L, R, NS, DIR, NL, NT, LS>(s, tw, tid);
-    if constexpr (sizeof...(Rest) > 0) run_stages<L, DIR, NL, NT, LS, C, NS * R, Rest...>(s, tw, tid);
+    stage<L, R, NS, DIR, NL, NT, LS, C, SK>(s, tw, tid);
+    if constexpr (sizeof...(Rest) > 0) run_stages<L, DIR, NL, NT, LS, C, SK, NS * R, Rest...>(s, tw, tid);
 }
 
-template <int L, int DIR, int NL, int NT, int LS, typename C, int... Rs>
+template <int L, int DIR, int NL, int NT, int LS, typename C, int SK, int... Rs>
 TG_D void smem_fft_impl(C* s, const C* __restrict__ tw, int tid, seq<Rs...>) {
-    run_stages<L, DIR, NL, NT, LS, C, 1, Rs...>(s, tw, tid);
+    run_stages<L, DIR, NL, NT, LS, C, SK, 1, Rs...>(s, tw, tid);
 }
 
-// Transform NL lines in shared memory.  The caller must have synchronised
-// after filling s; the routine ends with a barrier.
-template <int L, int DIR, int NL, int NT, int LS, typename C>
+// Transform NL lines in shared memory (line i at s + i LS, element p at
+// skew<SK>(p) within it).  The caller must have synchronised after filling
+// s; the routine ends with a barrier.
+template <int L, int DIR, int NL, int NT, int LS, typename C, int SK = 0>
 TG_D void smem_fft(C* s, const C* __restrict__ tw, int tid) {
-    smem_fft_impl<L, DIR, NL, NT, LS, C>(s, tw, tid, typename Radices<L>::type{});
+    smem_fft_impl<L, DIR, NL, NT, LS, C, SK>(s, tw, tid, typename Radices<L>::type{});
 }
 
 }  // namespace tgfft
