@@ -18,8 +18,11 @@
 // the reference rotated by those angles is correlated once more without
 // wedges and tom_peak(.,'spline') of ccf*mask_ccf gives shift and peak.
 //
-// The rotation batch of a job runs as batched template-sized FFTs
-// (fft3d.cu); per-entry statistics are FP64 segmented reductions.
+// The rotation batch of a job runs as batched template-sized real-to-half
+// and half-to-real FFTs (fft3d.cu): every volume of the scan is real and every
+// spectral factor (the Hermitian wedge parts, F(b) conj F(a)) keeps Hermitian
+// symmetry, so the half spectrum carries the whole computation.  Per-entry
+// statistics are FP64 segmented reductions.
 #include <cfloat>
 #include <cmath>
 #include <string>
@@ -54,7 +57,7 @@ TG_D long long shifted(long long v, int nx, int ny, int nz, int sgn) {
 __global__ void k_al_rotate(const float* __restrict__ ref, const float* __restrict__ wref,
                             const float* __restrict__ mask, const float* __restrict__ mref,
                             const float* __restrict__ mw, int nx, int ny, int nz, float cx, float cy, float cz,
-                            int mask_ref, float2* __restrict__ A, float* __restrict__ W) {
+                            int mask_ref, float* __restrict__ Ar, float2* __restrict__ A, float* __restrict__ W) {
     const int nn = nx * ny * nz;  // boxes hold fewer than 2^31 voxels
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const int e = blockIdx.y;
@@ -65,7 +68,8 @@ __global__ void k_al_rotate(const float* __restrict__ ref, const float* __restri
     for (int q = 0; q < 9; ++q) m[q] = mref[9 * e + q];
     float a = rot_sample(ref, nx, ny, nz, m, cx, cy, cz, i, j, k);
     if (mask_ref) a = __fmul_rn(a, mask[v]);
-    A[(long long)e * nn + v] = make_float2(a, 0.f);
+    if (Ar) Ar[(long long)e * nn + v] = a;
+    else A[(long long)e * nn + v] = make_float2(a, 0.f);
     if (W) {
 #pragma unroll
         for (int q = 0; q < 9; ++q) m[q] = mw[9 * e + q];
@@ -73,8 +77,6 @@ __global__ void k_al_rotate(const float* __restrict__ ref, const float* __restri
     }
 }
 
-// A[e][k] *= (W'(k) + W'(-k)) / 2, W' = ifftshift(wedge_part): the spectrum of
-// psf_part = real(ifftn(W'))
 // The two source voxels of (W'(k) + W'(-k)) / 2 with W' = ifftshift(W):
 // ifftshift(v) and ifftshift(-v) (all boxes hold fewer than 2^31 voxels).
 TG_D void wedge_pair(int v, int nx, int ny, int nz, int& s1, int& s2) {
@@ -89,38 +91,101 @@ TG_D void wedge_pair(int v, int nx, int ny, int nz, int& s1, int& s2) {
     s2 = a2 + nx * (b2 + ny * c2);
 }
 
-// A[e][k] *= (W'(k) + W'(-k)) / 2, W' = ifftshift(wedge_part): the spectrum of
-// psf_part; the weight is the same for every entry, so one thread per voxel
-// applies it to the AL_EG entries of its group (blockIdx.y)
+// A[e][k] *= (W'(k) + W'(-k)) / 2 with W' = ifftshift(wedge_part) (the
+// spectrum of psf_part), and B[e][k] = B0[k] (W'(k) + W'(-k)) / 2 with
+// W' = ifftshift(W[e]), on half spectra ((nx/2+1) ny nz per entry): half
+// index h is the full-grid frequency kx + nx (ky + ny kz) with kx <= nx/2.
+// The index pair is computed once per frequency for the AL_EG entries of the
+// block's group (blockIdx.y).
 constexpr int AL_EG = 16;
-__global__ void k_al_wpart(float2* __restrict__ A, const float* __restrict__ wpart, int nx, int ny, int nz, int E) {
-    const int nn = nx * ny * nz;
+__global__ void k_al_wpart_h(float2* __restrict__ A, const float* __restrict__ wpart, int nx, int ny, int nz, int E) {
+    const int nh = nx / 2 + 1, nhn = nh * ny * nz;
     const int e0 = blockIdx.y * AL_EG, e1 = min(E, e0 + AL_EG);
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += gridDim.x * blockDim.x) {
+    for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < nhn; h += gridDim.x * blockDim.x) {
+        const int kx = h % nh, t = h / nh;
         int s1, s2;
-        wedge_pair(v, nx, ny, nz, s1, s2);
+        wedge_pair(kx + nx * t, nx, ny, nz, s1, s2);
         const float ws = 0.5f * (wpart[s1] + wpart[s2]);
         for (int e = e0; e < e1; ++e) {
-            float2* a = A + (long long)e * nn + v;
+            float2* a = A + (long long)e * nhn + h;
             *a = cscale(*a, ws);
         }
     }
 }
 
-// B[e][k] = B0[k] * (W'(k) + W'(-k)) / 2, W' = ifftshift(W[e]); the index pair
-// is computed once per voxel for the AL_EG entries of the group
-__global__ void k_al_bside(float2* __restrict__ B, const float2* __restrict__ B0, const float* __restrict__ W, int nx,
-                           int ny, int nz, int E) {
-    const int nn = nx * ny * nz;
+__global__ void k_al_bside_h(float2* __restrict__ B, const float2* __restrict__ B0, const float* __restrict__ W,
+                             int nx, int ny, int nz, int E) {
+    const int nh = nx / 2 + 1, nhn = nh * ny * nz, nn = nx * ny * nz;
     const int e0 = blockIdx.y * AL_EG, e1 = min(E, e0 + AL_EG);
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += gridDim.x * blockDim.x) {
+    for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < nhn; h += gridDim.x * blockDim.x) {
+        const int kx = h % nh, t = h / nh;
         int s1, s2;
-        wedge_pair(v, nx, ny, nz, s1, s2);
-        const float2 b0 = B0[v];
+        wedge_pair(kx + nx * t, nx, ny, nz, s1, s2);
+        const float2 b0 = B0[h];
         for (int e = e0; e < e1; ++e) {
             const float* w = W + (long long)e * nn;
-            B[(long long)e * nn + v] = cscale(b0, 0.5f * (w[s1] + w[s2]));
+            B[(long long)e * nhn + h] = cscale(b0, 0.5f * (w[s1] + w[s2]));
         }
+    }
+}
+
+// the particle in every entry (no wedges)
+__global__ void k_al_bcast(float* __restrict__ B, const float* __restrict__ part, int nn, int E) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < (long long)nn * E;
+         t += (long long)gridDim.x * blockDim.x)
+        B[t] = part[t % nn];
+}
+
+// per-entry FP64 sums of norm_inside_mask on real volumes: pass 0: sum x m,
+// pass 1: sum over m of (x - mea)^2
+__global__ void __launch_bounds__(256) k_al_stats_r(const float* __restrict__ X, const float* __restrict__ mask,
+                                                    long long nn, const double* __restrict__ mea, int pass,
+                                                    double* __restrict__ out) {
+    const int e = blockIdx.y;
+    const float* x = X + (long long)e * nn;
+    double acc = 0;
+    const double me = pass ? mea[e] : 0.0;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += (long long)gridDim.x * blockDim.x) {
+        if (mask[v] != 0.f) {
+            const double r = (double)x[v];
+            acc += pass ? (r - me) * (r - me) : r;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __shared__ double ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0;
+        for (int k = 0; k < 8; ++k) sum += ws[k];
+        atomicAdd(out + e, sum);
+    }
+}
+
+__global__ void k_al_normalize_r(float* __restrict__ X, const float* __restrict__ mask, long long nn, int E,
+                                 const double* __restrict__ mea, const double* __restrict__ var, double n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nn * E; t += (long long)gridDim.x * blockDim.x) {
+        const long long v = t % nn, e = t / nn;
+        const double st = sqrt(var[e] / (n - 1.0));
+        X[t] = mask[v] != 0.f ? (float)(((double)X[t] - mea[e]) / st) : 0.f;
+    }
+}
+
+// running max over the E entries in scan order; ccf = fftshift(C) / n, C real
+__global__ void k_al_update_r(const float* __restrict__ C, int nx, int ny, int nz, int E, double inv_n,
+                              const int* __restrict__ aidx, float* __restrict__ cmax, float* __restrict__ amax) {
+    const long long nn = (long long)nx * ny * nz;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += (long long)gridDim.x * blockDim.x) {
+        const long long src = shifted(v, nx, ny, nz, -1);
+        float m = cmax[v], a = amax[v];
+        for (int e = 0; e < E; ++e) {
+            const float c = (float)((double)C[(long long)e * nn + src] * inv_n);
+            if (c > m) m = c;
+            if (c >= m) a = (float)aidx[e];
+        }
+        cmax[v] = m;
+        amax[v] = a;
     }
 }
 
@@ -170,23 +235,6 @@ __global__ void k_al_normalize(float2* __restrict__ X, const float* __restrict__
 __global__ void k_al_cross(float2* __restrict__ B, const float2* __restrict__ A, long long n) {
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
         B[t] = cmulc(B[t], A[t]);
-}
-
-// running max over the E entries in scan order; ccf = real(fftshift(C))/n
-__global__ void k_al_update(const float2* __restrict__ C, int nx, int ny, int nz, int E, double inv_n,
-                            const int* __restrict__ aidx, float* __restrict__ cmax, float* __restrict__ amax) {
-    const long long nn = (long long)nx * ny * nz;
-    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += (long long)gridDim.x * blockDim.x) {
-        const long long src = shifted(v, nx, ny, nz, -1);
-        float m = cmax[v], a = amax[v];
-        for (int e = 0; e < E; ++e) {
-            const float c = (float)((double)C[(long long)e * nn + src].x * inv_n);
-            if (c > m) m = c;
-            if (c >= m) a = (float)aidx[e];
-        }
-        cmax[v] = m;
-        amax[v] = a;
-    }
 }
 
 // single map: out = real(fftshift(C)) / n * mask_ccf
@@ -255,13 +303,14 @@ std::vector<double> axis_values(const float r[3]) {
 }
 
 struct Workspace {
-    float2 *A = nullptr, *B = nullptr, *B0 = nullptr;
+    float2 *A = nullptr, *B = nullptr, *B0 = nullptr;  // the scan: half spectra; the refinement: complex
+    float *Ar = nullptr, *Br = nullptr;                // the scan's real volumes
     float *W = nullptr, *cmax = nullptr, *amax = nullptr, *tmp = nullptr, *mats = nullptr;
     int* aidx = nullptr;
     double *sums = nullptr, *mea = nullptr, *var = nullptr, *spline = nullptr;
     unsigned long long* key = nullptr;
     void release() {
-        void* p[] = {A, B, B0, W, cmax, amax, tmp, mats, aidx, sums, mea, var, spline, key};
+        void* p[] = {A, B, B0, Ar, Br, W, cmax, amax, tmp, mats, aidx, sums, mea, var, spline, key};
         for (void* q : p)
             if (q) cudaFree(q);
     }
@@ -273,7 +322,7 @@ struct Workspace {
 // largest job, reused by the following jobs.
 struct AlignScratch {
     Workspace w;
-    size_t cap[14] = {0};
+    size_t cap[16] = {0};
     void release() {
         w.release();
         w = Workspace();
@@ -292,6 +341,23 @@ static cudaError_t normalize_entries(float2* X, const float* mask, long long nn,
         k_al_mean<<<(E + 127) / 128, 128, 0, st>>>(w.sums, w.mea, E, nmask);
         k_al_stats<<<g, 256, 0, st>>>(X, mask, nn, w.mea, 1, w.var);
         k_al_normalize<<<grid_for(nn * E), 256, 0, st>>>(X, mask, nn, E, w.mea, w.var, nmask);
+        e = cudaGetLastError();
+    }
+    *launches += 4;
+    return e;
+}
+
+// norm_inside_mask on E real volumes X, in place
+static cudaError_t normalize_entries_r(float* X, const float* mask, long long nn, int E, double nmask, Workspace& w,
+                                       cudaStream_t st, int64_t* launches) {
+    cudaError_t e = cudaMemsetAsync(w.sums, 0, sizeof(double) * E, st);
+    if (!e) e = cudaMemsetAsync(w.var, 0, sizeof(double) * E, st);
+    dim3 g((unsigned)std::min<long long>((nn + 255) / 256, 64), E);
+    if (!e) {
+        k_al_stats_r<<<g, 256, 0, st>>>(X, mask, nn, nullptr, 0, w.sums);
+        k_al_mean<<<(E + 127) / 128, 128, 0, st>>>(w.sums, w.mea, E, nmask);
+        k_al_stats_r<<<g, 256, 0, st>>>(X, mask, nn, w.mea, 1, w.var);
+        k_al_normalize_r<<<grid_for(nn * E), 256, 0, st>>>(X, mask, nn, E, w.mea, w.var, nmask);
         e = cudaGetLastError();
     }
     *launches += 4;
@@ -415,7 +481,10 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
         cap[i] = b;
         return true;
     };
-    if (!G(0, (void**)&w.A, sizeof(float2) * nn * E) || !G(1, (void**)&w.B, sizeof(float2) * nn * E) ||
+    const long long nhn = (long long)(n[0] / 2 + 1) * n[1] * n[2];  // one half spectrum
+    const long long ncx = std::max<long long>(nn, nhn * E);         // complex slots: E half spectra or one volume
+    if (!G(0, (void**)&w.A, sizeof(float2) * ncx) || !G(1, (void**)&w.B, sizeof(float2) * ncx) ||
+        !G(14, (void**)&w.Ar, sizeof(float) * nn * E) || !G(15, (void**)&w.Br, sizeof(float) * nn * E) ||
         !G(2, (void**)&w.B0, sizeof(float2) * nn) || (wedges && !G(3, (void**)&w.W, sizeof(float) * nn * E)) ||
         !G(4, (void**)&w.cmax, sizeof(float) * nn) || !G(5, (void**)&w.amax, sizeof(float) * nn) ||
         !G(6, (void**)&w.tmp, sizeof(float) * nn) || !G(7, (void**)&w.mats, sizeof(float) * 18 * R) ||
@@ -439,8 +508,9 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
             if ((e = cudaStreamSynchronize(st))) break;
         }
         if (nmask < 2) { rc = fail(ctx, TOMGPU_ERR_ARG, "mask needs at least two voxels"); break; }
-        k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(job.part, wedges ? job.mask : nullptr, w.B0, nn);
-        if ((e = c2c3d<float2>(w.B0, n, -1, 1.0, st))) break;
+        // B0: half spectrum of part (* mask where wedges are given)
+        k_al_mul<<<grid_for(nn), 256, 0, st>>>(job.part, wedges ? job.mask : nullptr, w.Br, nn);
+        if ((e = r2c3d_batch<float2>(w.Br, w.B0, n, 1, st))) break;
         k_al_fill<<<grid_for(nn), 256, 0, st>>>(w.cmax, w.amax, nn, -2.f, -2.f);
         ctx->launches += 5;
         // every rotation's matrices and angle index, uploaded once: [R] matrix-mode
@@ -461,31 +531,31 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
             dim3 g((unsigned)((nn + 255) / 256), nb);
             k_al_rotate<<<g, 256, 0, st>>>(job.ref, job.wedge_ref, job.mask, w.mats + 9 * off,
                                            w.mats + 9 * (size_t)R + 9 * off, n[0], n[1], n[2], cx, cy, cz,
-                                           wedges ? 1 : 0, w.A, wedges ? w.W : nullptr);
+                                           wedges ? 1 : 0, w.Ar, nullptr, wedges ? w.W : nullptr);
             ctx->launches += 1;
+            const dim3 gh(grid_for(nhn), (nb + AL_EG - 1) / AL_EG);
             if (wedges) {
                 // a = ref_rot*mask (*) psf_part
-                if ((e = c2c3d_batch(w.A, n, nb, -1, 1.0, st))) break;
-                k_al_wpart<<<dim3(grid_for(nn), (nb + AL_EG - 1) / AL_EG), 256, 0, st>>>(w.A, wpart, n[0], n[1], n[2], nb);
-                if ((e = c2c3d_batch(w.A, n, nb, +1, 1.0 / (double)nn, st))) break;
+                if ((e = r2c3d_batch<float2>(w.Ar, w.A, n, nb, st))) break;
+                k_al_wpart_h<<<gh, 256, 0, st>>>(w.A, wpart, n[0], n[1], n[2], nb);
+                if ((e = c2r3d_batch<float2>(w.A, w.Ar, n, nb, 1.0 / (double)nn, st))) break;
                 // b = part*mask (*) psf_ref
-                k_al_bside<<<dim3(grid_for(nn), (nb + AL_EG - 1) / AL_EG), 256, 0, st>>>(w.B, w.B0, w.W, n[0], n[1], n[2], nb);
-                if ((e = c2c3d_batch(w.B, n, nb, +1, 1.0 / (double)nn, st))) break;
+                k_al_bside_h<<<gh, 256, 0, st>>>(w.B, w.B0, w.W, n[0], n[1], n[2], nb);
+                if ((e = c2r3d_batch<float2>(w.B, w.Br, n, nb, 1.0 / (double)nn, st))) break;
                 ctx->launches += 2 + 9;
             } else {
                 // b = part for every entry
-                for (int q = 0; q < nb; ++q)
-                    k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(job.part, nullptr, w.B + (long long)q * nn, nn);
-                ctx->launches += nb;
+                k_al_bcast<<<grid_for(nn * nb), 256, 0, st>>>(w.Br, job.part, (int)nn, nb);
+                ctx->launches += 1;
             }
-            if ((e = normalize_entries(w.A, job.mask, nn, nb, nmask, w, st, &ctx->launches))) break;
-            if ((e = normalize_entries(w.B, job.mask, nn, nb, nmask, w, st, &ctx->launches))) break;
-            if ((e = c2c3d_batch(w.A, n, nb, -1, 1.0, st))) break;
-            if ((e = c2c3d_batch(w.B, n, nb, -1, 1.0, st))) break;
-            k_al_cross<<<grid_for(nn * nb), 256, 0, st>>>(w.B, w.A, nn * nb);
-            if ((e = c2c3d_batch(w.B, n, nb, +1, 1.0 / (double)nn, st))) break;
-            k_al_update<<<grid_for(nn), 256, 0, st>>>(w.B, n[0], n[1], n[2], nb, 1.0 / nmask, w.aidx + off, w.cmax,
-                                                      w.amax);
+            if ((e = normalize_entries_r(w.Ar, job.mask, nn, nb, nmask, w, st, &ctx->launches))) break;
+            if ((e = normalize_entries_r(w.Br, job.mask, nn, nb, nmask, w, st, &ctx->launches))) break;
+            if ((e = r2c3d_batch<float2>(w.Ar, w.A, n, nb, st))) break;
+            if ((e = r2c3d_batch<float2>(w.Br, w.B, n, nb, st))) break;
+            k_al_cross<<<grid_for(nhn * nb), 256, 0, st>>>(w.B, w.A, nhn * nb);
+            if ((e = c2r3d_batch<float2>(w.B, w.Br, n, nb, 1.0 / (double)nn, st))) break;
+            k_al_update_r<<<grid_for(nn), 256, 0, st>>>(w.Br, n[0], n[1], n[2], nb, 1.0 / nmask, w.aidx + off,
+                                                        w.cmax, w.amax);
             e = cudaGetLastError();
             ctx->launches += 2 + 9;
         }
@@ -516,8 +586,8 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
         int zero = 0;
         if ((e = cudaMemcpyAsync(w.aidx, &zero, sizeof zero, cudaMemcpyHostToDevice, st))) break;
         k_al_rotate<<<dim3((unsigned)((nn + 255) / 256), 1), 256, 0, st>>>(job.ref, nullptr, job.mask, w.mats, nullptr,
-                                                                            n[0], n[1], n[2], cx, cy, cz, 0, w.A,
-                                                                            nullptr);
+                                                                            n[0], n[1], n[2], cx, cy, cz, 0, nullptr,
+                                                                            w.A, nullptr);
         k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(job.part, wedges ? job.mask : nullptr, w.B, nn);
         if ((e = normalize_entries(w.A, job.mask, nn, 1, nmask, w, st, &ctx->launches))) break;
         if ((e = normalize_entries(w.B, job.mask, nn, 1, nmask, w, st, &ctx->launches))) break;

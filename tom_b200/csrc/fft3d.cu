@@ -213,6 +213,43 @@ cudaError_t c2c3d(C* data, const int n[3], int dir, double scale, cudaStream_t s
     return cudaSuccess;
 }
 
+// E volumes one after another (real: nx ny nz each, half: (nx/2+1) ny nz
+// each): the batch joins z in the line geometry of every pass.
+template <typename C>
+cudaError_t r2c3d_batch(const void* real_in, C* half_out, const int n[3], int E, cudaStream_t st) {
+    const long nx = n[0], ny = n[1], nz = n[2], nh = nx / 2 + 1;
+    cudaError_t e;
+    LineGeom gi{1, (int)ny, nx, (int)(nz * E), nx * ny};
+    LineGeom go{1, (int)ny, nh, (int)(nz * E), nh * ny};
+    if ((e = fft_lines<C>((int)nx, -1, FFT_R2C, real_in, half_out, gi, go, ny * nz * E, 1.0, st))) return e;
+    LineGeom gy{nh, (int)nh, 1, (int)(nz * E), nh * ny};
+    if (ny > 1 && (e = fft_lines<C>((int)ny, -1, FFT_C2C, half_out, half_out, gy, gy, nh * nz * E, 1.0, st)))
+        return e;
+    LineGeom gz{nh * ny, (int)(nh * ny), 1, E, nh * ny * nz};
+    if (nz > 1 && (e = fft_lines<C>((int)nz, -1, FFT_C2C, half_out, half_out, gz, gz, nh * ny * E, 1.0, st)))
+        return e;
+    return cudaSuccess;
+}
+
+template <typename C>
+cudaError_t c2r3d_batch(C* half_inout, void* real_out, const int n[3], int E, double scale, cudaStream_t st) {
+    const long nx = n[0], ny = n[1], nz = n[2], nh = nx / 2 + 1;
+    cudaError_t e;
+    LineGeom gz{nh * ny, (int)(nh * ny), 1, E, nh * ny * nz};
+    if (nz > 1 &&
+        (e = fft_lines<C>((int)nz, +1, FFT_C2C, half_inout, half_inout, gz, gz, nh * ny * E, 1.0, st)))
+        return e;
+    LineGeom gy{nh, (int)nh, 1, (int)(nz * E), nh * ny};
+    if (ny > 1 &&
+        (e = fft_lines<C>((int)ny, +1, FFT_C2C, half_inout, half_inout, gy, gy, nh * nz * E, 1.0, st)))
+        return e;
+    LineGeom gi{1, (int)ny, nh, (int)(nz * E), nh * ny};
+    LineGeom go{1, (int)ny, nx, (int)(nz * E), nx * ny};
+    return fft_lines<C>((int)nx, +1, FFT_C2R, half_inout, real_out, gi, go, ny * nz * E, scale, st);
+}
+
+template cudaError_t r2c3d_batch<float2>(const void*, float2*, const int[3], int, cudaStream_t);
+template cudaError_t c2r3d_batch<float2>(float2*, void*, const int[3], int, double, cudaStream_t);
 template cudaError_t r2c3d<float2>(const void*, float2*, const int[3], cudaStream_t);
 template cudaError_t r2c3d<double2>(const void*, double2*, const int[3], cudaStream_t);
 template cudaError_t c2r3d<float2>(float2*, void*, const int[3], double, cudaStream_t);

@@ -30,5 +30,10 @@ template <typename C> cudaError_t r2c3d(const void* real_in, C* half_out, const 
 template <typename C>
 cudaError_t c2r3d(C* half_inout, void* real_out, const int n[3], double scale, cudaStream_t st);
 template <typename C> cudaError_t c2c3d(C* data, const int n[3], int dir, double scale, cudaStream_t st);
+// E volumes stored one after another (FP32)
+template <typename C>
+cudaError_t r2c3d_batch(const void* real_in, C* half_out, const int n[3], int E, cudaStream_t st);
+template <typename C>
+cudaError_t c2r3d_batch(C* half_inout, void* real_out, const int n[3], int E, double scale, cudaStream_t st);
 
 }  // namespace tg
