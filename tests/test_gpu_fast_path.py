@@ -65,13 +65,14 @@ def test_928_464_kernels_equal_generic(gpu, oracle, shape):
     assert (fidx != gidx).mean() < 1e-3
 
 
-@pytest.mark.parametrize("ny", [256, 512])
+@pytest.mark.parametrize("ny", [128, 256, 512])
 @pytest.mark.parametrize("T", [8, 12, 20, 32, 48, 64])
 def test_y_column_kernels_every_template_height(gpu, oracle, ny, T):
     """The y-edge 256 / 512 column kernels sum the template's forward y-DFT
-    from its nonzeros, ceil(Ty / 8) terms per residue: every term count a
-    template edge (an FFT length) reaches, against the generic kernels (x and
-    z edges on the generic kernels)."""
+    from its nonzeros, ceil(Ty / 8) terms per residue (the y-edge 128 kernel
+    transforms the template column in full): every term count a template
+    edge (an FFT length) reaches, against the generic kernels (x and z edges
+    on the generic kernels)."""
     rng = np.random.default_rng(11 + T)
     vol = rng.standard_normal((64, ny, 80)).astype(np.float32)
     tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
