@@ -230,35 +230,59 @@ def refine(vol, template, mask, centres, angle_sets, window=2, batch=8, ctx=None
     edge L >= T + 2 window + 1 (an FFT length), with the centre's own angle
     list; the best CC within +-window voxels of the centre.  The crop holds
     every voxel the FLCF at those positions reads, so the values equal the
-    full-volume search's there.  Returns (positions, cc, fine angle index)."""
+    full-volume search's there.  The tomogram stays on the device; crops,
+    results and the window maxima are device tensors on the context's stream
+    (one result buffer pair for all centres), read back once at the end.
+    Returns (positions, cc, fine angle index)."""
     import torch
     ctx = ctx or default_context()
+    dev = f"cuda:{ctx.device}"
     vol = np.asarray(vol, np.float32)
+    shape = vol.shape
     T = np.shape(template)[0]
     need = T + 2 * window + 1
     L = next(n for n in (16, 24, 32, 40, 48, 64, 80, 96, 128) if n >= need)
     half = L // 2
+    centres = np.asarray(centres, np.int64).reshape(-1, 3)
+    n = len(centres)
     plan = MatchPlan((L, L, L), np.shape(template), batch=batch, ctx=ctx)
-    plan.set_template(to_device(template, ctx.device), to_device(mask, ctx.device))
-    out_pos, out_cc, out_idx = [], [], []
-    for c, angs in zip(np.asarray(centres, np.int64).reshape(-1, 3), angle_sets):
-        sl = [np.arange(c[d] - half, c[d] - half + L) % vol.shape[d] for d in range(3)]
-        crop = np.asfortranarray(vol[np.ix_(sl[0], sl[1], sl[2])])
-        plan.set_volume(to_device(crop, ctx.device))
+    try:
+        plan.set_template(to_device(template, ctx.device), to_device(mask, ctx.device))
+        vt = torch.from_numpy(np.ascontiguousarray(vol.transpose(2, 1, 0))).to(dev)  # [z][y][x]
+        ar = torch.arange(L, device=dev)
         cc, idx = plan.new_results()
-        grid, ids = angs
-        plan.run(grid, cc, idx)
+        crop = torch.empty((L, L, L), dtype=torch.float32, device=dev)
+        w0, w1 = half - window, half + window + 1
+        best_v = torch.empty(n, dtype=torch.float32, device=dev)
+        best_k = torch.empty(n, dtype=torch.int64, device=dev)
+        best_i = torch.empty(n, dtype=torch.int32, device=dev)
+        for q, (c, angs) in enumerate(zip(centres, angle_sets)):
+            zi, yi, xi = [(ar + int(c[d] - half)) % shape[d] for d in (2, 1, 0)]
+            crop.copy_(vt.index_select(0, zi).index_select(1, yi).index_select(2, xi))
+            plan.set_volume(crop)
+            plan.init_results(cc, idx)
+            grid, _ = angs
+            plan.run(grid, cc, idx)
+            # window maxima, flattened x-slowest (the order of an [x][y][z] array)
+            wv = cc[w0:w1, w0:w1, w0:w1].permute(2, 1, 0).reshape(-1)
+            wi = idx[w0:w1, w0:w1, w0:w1].permute(2, 1, 0).reshape(-1)
+            k = torch.argmax(wv)
+            best_v[q] = wv[k]
+            best_k[q] = k
+            best_i[q] = wi[k]
         torch.cuda.synchronize(ctx.device)
-        w = from_device(cc)[half - window:half + window + 1, half - window:half + window + 1,
-                            half - window:half + window + 1]
-        wi = from_device(idx)[half - window:half + window + 1, half - window:half + window + 1,
-                              half - window:half + window + 1]
-        k = np.unravel_index(int(np.argmax(w)), w.shape)
-        out_pos.append([(c[d] + k[d] - window) % vol.shape[d] for d in range(3)])
-        out_cc.append(float(w[k]))
-        out_idx.append(int(ids[wi[k]]) if wi[k] >= 0 else -1)
-    plan.close()
-    return np.array(out_pos), np.array(out_cc), np.array(out_idx)
+        vals, ks, locs = best_v.cpu().numpy(), best_k.cpu().numpy(), best_i.cpu().numpy()
+    finally:
+        plan.close()
+    w = 2 * window + 1
+    out_pos, out_idx = [], []
+    for q, (c, angs) in enumerate(zip(centres, angle_sets)):
+        kx, ky, kz = np.unravel_index(int(ks[q]), (w, w, w))
+        out_pos.append([(c[0] + kx - window) % shape[0], (c[1] + ky - window) % shape[1],
+                        (c[2] + kz - window) % shape[2]])
+        ids = angs[1]
+        out_idx.append(int(ids[locs[q]]) if locs[q] >= 0 else -1)
+    return np.array(out_pos), np.asarray(vals, np.float64), np.array(out_idx)
 
 
 def bin_members(fine_grid, coarse_grid):

@@ -540,6 +540,10 @@ class MatchPlan:
         self.ctx.check(lib().tomgpu_match_init_results_dev(self.handle, _tptr(cc), _tptr(idx)))
         return cc, idx
 
+    def init_results(self, maxcc_dev, angidx_dev):
+        """Reset result buffers of the volume's size (-1000 / -1), as new_results."""
+        self.ctx.check(lib().tomgpu_match_init_results_dev(self.handle, _tptr(maxcc_dev), _tptr(angidx_dev)))
+
     def run(self, eulers, maxcc_dev, angidx_dev, index_offset: int = 0):
         e = np.ascontiguousarray(np.asarray(eulers, np.float32).reshape(-1, 3))
         self.ctx.check(lib().tomgpu_match_run_dev(self.handle, e.ctypes.data_as(_lib.c_float_p), e.shape[0],
