@@ -1,6 +1,6 @@
 """FLCF matching parity on the GPU against the FP64 oracle.
 
-Tolerance: |cc_gpu - cc_oracle| <= 1e-4 * max|cc_oracle|
+Tolerance (the parity bar): |cc_gpu - cc_oracle| <= 1e-4 * max|cc_oracle|
 over every voxel, and identical angle indices wherever the oracle's best CC
 beats its runner-up by more than that tolerance."""
 import numpy as np
