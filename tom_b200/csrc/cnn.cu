@@ -9,10 +9,11 @@
 // swapped (the host passes the re-arranged weights); the weight gradient is a
 // reduction over voxels per (co, ci, tap).
 //
-// conv_fwd: one block per output tile of 4 x 8 x 8 voxels and all output
-// channels (<= 64); per input channel the tile plus its halo is staged in
-// shared memory and every thread applies the 27 taps of its voxel to all
-// output channels (27 x Cout multiply-adds per staged value read 27 times).
+// conv_fwd (k_conv_fwd2): one block per 32 x 8 x 4 output tile and group of
+// up to 16 output channels; per input channel the tile plus its halo is
+// staged in shared memory and every thread applies the 27 taps to its 4
+// voxels and the group's channels (4 x 16 multiply-adds per tap for 4 staged
+// values and 4 float4 weight reads).
 #include <cstdint>
 
 #include "common.cuh"
@@ -22,54 +23,94 @@ namespace tg {
 
 namespace {
 
-constexpr int TX = 8, TY = 8, TZ = 4, CONV_THREADS = TX * TY * TZ, MAX_CO = 64;
+// Register-blocked forward convolution: a 32 x 8 x 4 output tile per block,
+// each thread 4 voxels along y (lanes along x, so every shared-memory read of
+// a warp is 32 consecutive floats) for a group of up to 16 output channels
+// (the group is blockIdx.z / ztiles).  Per input channel the tile and its halo
+// are staged row by row (one division per row), the group's weights tap-major
+// so that a tap's channel weights are read as float4.
+constexpr int FX = 32, FY = 8, FZ = 4, FR = 4, FCG = 16;
 
 template <int CO>
-__global__ void __launch_bounds__(CONV_THREADS) k_conv_fwd(const float* __restrict__ in, int ci_n, int nx, int ny,
-                                                           int nz, const float* __restrict__ w,
-                                                           const float* __restrict__ bias, int dil, int relu,
-                                                           float* __restrict__ out) {
-    extern __shared__ float sm[];
-    const int hx = TX + 2 * dil, hy = TY + 2 * dil, hz = TZ + 2 * dil;
-    float* tile = sm;                       // [hz][hy][hx]
-    float* ws = sm + hz * hy * hx;          // [CO][27] weights of the current input channel
-    const int tx = threadIdx.x % TX, ty = (threadIdx.x / TX) % TY, tz = threadIdx.x / (TX * TY);
-    const int bx = blockIdx.x * TX, by = blockIdx.y * TY, bz = blockIdx.z * TZ;
-    const int x = bx + tx, y = by + ty, z = bz + tz;
+__global__ void __launch_bounds__(256) k_conv_fwd2(const float* __restrict__ in, int ci_n, int nx, int ny, int nz,
+                                                   const float* __restrict__ w, const float* __restrict__ bias,
+                                                   int dil, int relu, float* __restrict__ out, int ztiles) {
+    constexpr int CG = CO < FCG ? CO : FCG;
+    extern __shared__ __align__(16) float smf[];
+    const int hx = FX + 2 * dil, hy = FY + 2 * dil, hz = FZ + 2 * dil;
+    float* tile = smf;                                // [hz][hy][hx]
+    float* ws = smf + ((hz * hy * hx + 3) & ~3);      // [27][CG]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int ty = (tid >> 5) & 1, tz = tid >> 6;
+    const int g = blockIdx.z / ztiles, zt = blockIdx.z - g * ztiles;
+    const int bx = blockIdx.x * FX, by = blockIdx.y * FY, bz = zt * FZ, c0 = g * CG;
     const long long nv = (long long)nx * ny * nz;
-    float acc[CO];
+    float acc[FR][CG];
 #pragma unroll
-    for (int c = 0; c < CO; ++c) acc[c] = 0.f;
-    const int ht = hz * hy * hx;
+    for (int r = 0; r < FR; ++r)
+#pragma unroll
+        for (int c = 0; c < CG; ++c) acc[r][c] = 0.f;
+    const int rows = hz * hy;
     for (int ci = 0; ci < ci_n; ++ci) {
         const float* src = in + (long long)ci * nv;
-        for (int i = threadIdx.x; i < ht; i += CONV_THREADS) {
-            const int ix = i % hx, iy = (i / hx) % hy, iz = i / (hx * hy);
-            const int gx = bx + ix - dil, gy = by + iy - dil, gz = bz + iz - dil;
-            const bool ok = gx >= 0 && gx < nx && gy >= 0 && gy < ny && gz >= 0 && gz < nz;
-            tile[i] = ok ? __ldg(src + ((long long)gz * ny + gy) * nx + gx) : 0.f;
+        for (int row = warp; row < rows; row += 8) {
+            const int iz = row / hy, iy = row - iz * hy;
+            const int gy = by + iy - dil, gz = bz + iz - dil;
+            const bool rok = gy >= 0 && gy < ny && gz >= 0 && gz < nz;
+            const float* srow = src + ((long long)gz * ny + gy) * nx;
+            for (int ix = lane; ix < hx; ix += 32) {
+                const int gx = bx + ix - dil;
+                tile[row * hx + ix] = (rok && gx >= 0 && gx < nx) ? __ldg(srow + gx) : 0.f;
+            }
         }
-        for (int i = threadIdx.x; i < CO * 27; i += CONV_THREADS) {
-            const int c = i / 27, t = i - c * 27;
-            ws[i] = __ldg(w + ((long long)c * ci_n + ci) * 27 + t);
+        for (int i = tid; i < 27 * CG; i += 256) {
+            const int t = i / CG, c = i - t * CG;
+            ws[i] = __ldg(w + ((long long)(c0 + c) * ci_n + ci) * 27 + t);
         }
         __syncthreads();
 #pragma unroll
         for (int t = 0; t < 27; ++t) {
             const int ox = (t % 3) * dil, oy = ((t / 3) % 3) * dil, oz = (t / 9) * dil;
-            const float v = tile[((tz + oz) * hy + (ty + oy)) * hx + (tx + ox)];
+            const float* trow = tile + ((tz + oz) * hy + (ty * FR + oy)) * hx + lane + ox;
+            float v[FR];
 #pragma unroll
-            for (int c = 0; c < CO; ++c) acc[c] = fmaf(ws[c * 27 + t], v, acc[c]);
+            for (int r = 0; r < FR; ++r) v[r] = trow[r * hx];
+            if constexpr (CG % 4 == 0) {
+                const float4* wr = reinterpret_cast<const float4*>(ws + t * CG);
+#pragma unroll
+                for (int c4 = 0; c4 < CG / 4; ++c4) {
+                    const float4 wv = wr[c4];
+#pragma unroll
+                    for (int r = 0; r < FR; ++r) {
+                        acc[r][4 * c4] = fmaf(wv.x, v[r], acc[r][4 * c4]);
+                        acc[r][4 * c4 + 1] = fmaf(wv.y, v[r], acc[r][4 * c4 + 1]);
+                        acc[r][4 * c4 + 2] = fmaf(wv.z, v[r], acc[r][4 * c4 + 2]);
+                        acc[r][4 * c4 + 3] = fmaf(wv.w, v[r], acc[r][4 * c4 + 3]);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < CG; ++c) {
+                    const float wv = ws[t * CG + c];
+#pragma unroll
+                    for (int r = 0; r < FR; ++r) acc[r][c] = fmaf(wv, v[r], acc[r][c]);
+                }
+            }
         }
         __syncthreads();
     }
-    if (x < nx && y < ny && z < nz) {
+    const int x = bx + lane, z = bz + tz;
+    if (x >= nx || z >= nz) return;
+#pragma unroll
+    for (int r = 0; r < FR; ++r) {
+        const int y = by + ty * FR + r;
+        if (y >= ny) continue;
         const long long o = ((long long)z * ny + y) * nx + x;
 #pragma unroll
-        for (int c = 0; c < CO; ++c) {
-            float r = acc[c] + (bias ? __ldg(bias + c) : 0.f);
-            if (relu) r = fmaxf(r, 0.f);
-            out[(long long)c * nv + o] = r;
+        for (int c = 0; c < CG; ++c) {
+            float res = acc[r][c] + (bias ? __ldg(bias + c0 + c) : 0.f);
+            if (relu) res = fmaxf(res, 0.f);
+            out[(long long)(c0 + c) * nv + o] = res;
         }
     }
 }
@@ -272,11 +313,14 @@ unsigned gridn(long long n) {
 template <int CO>
 cudaError_t launch_fwd(const float* in, int ci, const int d[3], const float* w, const float* b, int dil, int relu,
                        float* out, cudaStream_t st) {
-    const size_t smem = sizeof(float) * ((size_t)(TX + 2 * dil) * (TY + 2 * dil) * (TZ + 2 * dil) + CO * 27);
+    constexpr int CG = CO < FCG ? CO : FCG, NG = CO / CG;
+    const size_t tile = (size_t)(FX + 2 * dil) * (FY + 2 * dil) * (FZ + 2 * dil);
+    const size_t smem = sizeof(float) * (((tile + 3) & ~(size_t)3) + 27 * CG);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
-    cudaFuncSetAttribute(k_conv_fwd<CO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 g((d[0] + TX - 1) / TX, (d[1] + TY - 1) / TY, (d[2] + TZ - 1) / TZ);
-    k_conv_fwd<CO><<<g, CONV_THREADS, smem, st>>>(in, ci, d[0], d[1], d[2], w, b, dil, relu, out);
+    cudaFuncSetAttribute(k_conv_fwd2<CO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int ztiles = (d[2] + FZ - 1) / FZ;
+    dim3 g((d[0] + FX - 1) / FX, (d[1] + FY - 1) / FY, ztiles * NG);
+    k_conv_fwd2<CO><<<g, 256, smem, st>>>(in, ci, d[0], d[1], d[2], w, b, dil, relu, out, ztiles);
     return cudaGetLastError();
 }
 
