@@ -49,7 +49,7 @@ TRAFFIC = {"exhaustive_512x512x256": {"c2r_flcf": {16: 16 * (336639232 + 2224768
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--steps", type=int, default=30)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--rot-per-step", type=int, default=64)
@@ -94,36 +94,57 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    INTERVAL_MS = 50
+
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host time, csv line)
+        self.window = None
 
     def start(self):
+        """Start sampling and return once the first sample has arrived (at
+        most 5 s), so that the timed region that follows is covered."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.INTERVAL_MS)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t_end = time.time() + 5.0
+        while not self.lines and time.time() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self, t0, t1):
+        """Host-time window of the timed region (from before its first launch
+        to after the synchronize that ends it)."""
+        self.window = (t0, t1)
 
     def stop(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        # one more interval, so that a sample taken just before the window closed is read
+        time.sleep(2 * self.INTERVAL_MS / 1e3)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
+        lines = self.lines
+        if self.window:
+            inside = [x for x in lines if self.window[0] <= x[0] <= self.window[1]]
+            # a timed region shorter than one interval keeps the samples nearest to it
+            lines = inside or sorted(lines, key=lambda x: abs(x[0] - 0.5 * sum(self.window)))[:2]
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for _, ln in lines:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -136,7 +157,8 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "interval_ms": self.INTERVAL_MS}
 
 
 def make_workload(name=WORKLOAD):
@@ -418,11 +440,13 @@ def main():
     ctx.profile(True)
     l0 = ctx.launches
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0 = time.time()
     ev0.record()
     for s in range(args.warmup, args.warmup + args.steps):
         step(s)
     ev1.record()
     torch.cuda.synchronize()
+    clocks.mark(h0, time.time())
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launches - l0
     kt = ctx.kernel_times()
