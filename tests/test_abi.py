@@ -22,6 +22,8 @@ def test_exports_every_declared_symbol():
     raw = ctypes.CDLL(L.LIB_PATH)
     missing = [n for n in names if not hasattr(raw, n)]
     assert not missing, missing
+    # the ctypes binding declares a signature for exactly these entry points
+    assert set(L._SIGS) == set(names)
 
 
 def test_status_strings_and_version():
@@ -65,3 +67,43 @@ def test_host_matrix_equals_oracle(oracle):
         if rng.random() < 0.5:
             e = (rng.random(3) * 360).astype(np.float32)
         assert np.array_equal(tom_b200.euler_matrix(e), oracle.euler_matrix(e))
+
+
+_NULL_CALLS = r'''
+import ctypes, json, sys
+sys.path.insert(0, sys.argv[1])
+from tom_b200 import _lib
+L = _lib.lib()
+out = {}
+for name, (res, args) in _lib._SIGS.items():
+    if res is ctypes.c_char_p:
+        continue
+    vals = [0 if a in (ctypes.c_int, ctypes.c_int64, ctypes.c_size_t) else
+            0.0 if a in (ctypes.c_float, ctypes.c_double) else None for a in args]
+    out[name] = getattr(L, name)(*vals)
+print(json.dumps(out))
+'''
+
+
+def test_every_entry_point_rejects_null_arguments():
+    """Each entry point called with NULL handles and pointers and zero sizes
+    returns TOMGPU_ERR_ARG (the destroy calls, like free, accept NULL; the
+    counters read 0), and none of them crashes the process.  The calls run in
+    a child process so that a crash fails this test instead of the session."""
+    import json
+    import subprocess
+    import sys
+    L = _lib()
+    p = subprocess.run([sys.executable, "-c", _NULL_CALLS, ROOT], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    got = json.loads(p.stdout.strip().splitlines()[-1])
+    accept_null = {"tomgpu_ctx_destroy", "tomgpu_match_plan_destroy"}
+    counters = {"tomgpu_ctx_launch_count", "tomgpu_match_plan_bytes"}
+    assert set(got) == {n for n in L._SIGS if L._SIGS[n][0] is not ctypes.c_char_p}
+    for name, st in got.items():
+        if name in accept_null:
+            assert st == L.TOMGPU_OK, name
+        elif name in counters:
+            assert st == 0, name
+        else:
+            assert st == L.TOMGPU_ERR_ARG, (name, st)
