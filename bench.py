@@ -205,7 +205,8 @@ def cpu_baseline(d, mask, grid, seconds):
     nvox = int(np.prod(d["tomo"].shape))
     return {"value": n * nvox / tn, "unit": UNIT, "cores": cpu.workers,
             "kind": "reference" if cpu.use_ref else "port",
-            "sample": f"{n} of 24624 triplets on the full 512x512x256 tomogram ({tn:.1f} s; rotation by the "
+            "sample": f"{n} of {len(grid)} triplets on the full {'x'.join(map(str, d['tomo'].shape))} tomogram "
+                      f"({tn:.1f} s; rotation by the "
                       f"reference's compiled rot3d, FP32 pocketfft rfftn/irfftn on {cpu.workers} threads, "
                       "numpy FLCF + max)"}
 
@@ -234,7 +235,7 @@ def run_reference(args):
                        "tomogram": list(cfg["N"]), "template": cfg["T"]},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu.workers,
                              "kind": "reference" if cpu.use_ref else "port",
-                             "sample": f"{args.steps} steps x {rps} triplet of the 24624-triplet grid"},
+                             "sample": f"{args.steps} steps x {rps} triplet of the {len(grid)}-triplet grid"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
