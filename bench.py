@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--rot-per-step", type=int, default=64)
     p.add_argument("--batch", type=int, default=0,
-                   help="rotation batch; 0 = autotune over 8, 16, 32 before the timed region")
+                   help="rotation batch; 0 = autotune over 8, 16, 32, 64 before the timed region")
     p.add_argument("--e2e-rot", type=int, default=1024)
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -417,7 +417,7 @@ def main():
     tune = None
     if args.batch == 0:
         e, _ = chunk(grid, 0, world, rank, 64)
-        best, tune = plan.autotune(e, (8, 16, 32))
+        best, tune = plan.autotune(e, (8, 16, 32, 64))
         if dist:  # every rank runs the same batch: the smallest of the ranks' choices
             t = torch.tensor([best], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MIN)

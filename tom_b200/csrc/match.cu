@@ -625,6 +625,13 @@ void MatchPlan::free_batch() {
     batch_bytes = 0;
 }
 
+int64_t MatchPlan::batch_need(int nb) const {
+    const long long hs = nh1 * (long long)N[1] * N[2];
+    return (int64_t)nb * ((int64_t)sizeof(float) * tn + (int64_t)sizeof(float2) * tn + (int64_t)sizeof(double) +
+                          (int64_t)sizeof(float2) * nh1 * T[1] * T[2] + (int64_t)sizeof(float2) * nh1 * N[2] * T[1] +
+                          2 * (int64_t)sizeof(float2) * hs);
+}
+
 int MatchPlan::alloc_batch(int nb) {
     const long long hs = nh1 * (long long)N[1] * N[2];
     const int64_t before = bytes_held;
@@ -646,7 +653,8 @@ int MatchPlan::alloc_batch(int nb) {
 }
 
 // Rotation-batch autotuner: for each candidate batch size the per-batch
-// buffers are re-allocated (a candidate that does not fit is skipped) and R
+// buffers are re-allocated (a candidate whose buffers would leave less than
+// 2 GiB of the device free, or whose allocation fails, is skipped) and R
 // rotations are timed with CUDA events on the context's stream after one
 // untimed batch; the fastest per rotation is kept.  Results go to scratch
 // buffers, so the caller's maxima are untouched.
@@ -671,6 +679,13 @@ int MatchPlan::autotune(const float* eulers, int R, const int* cands, int nc, in
     for (int c = 0; c < nc && !rc; ++c) {
         const int nb = cands[c];
         if (nb <= 0 || nb > 4096) continue;
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot)) {
+            rc = cuda_fail(ctx, cudaGetLastError(), "autotune memory query");
+            break;
+        }
+        // the current batch buffers come back with free_batch
+        if (batch_need(nb) + (int64_t(2) << 30) > (int64_t)fr + batch_bytes) continue;
         free_batch();
         if (alloc_batch(nb)) {  // does not fit: skip
             ctx->last_error.clear();

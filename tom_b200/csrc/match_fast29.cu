@@ -23,6 +23,7 @@
 #include "ctx.h"
 #include "match.h"
 #include "pq29.cuh"
+#include "tile_copy.cuh"
 #include "twiddles.h"
 #include "warp_fft.cuh"
 
@@ -163,13 +164,6 @@ __global__ void __launch_bounds__(256, 3) k_inv_z_p464(const float2* __restrict_
     });
 }
 
-TG_D void cp_async8_p(void* smem_dst, const void* gsrc, int bytes) {
-    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(bytes) : "memory");
-}
-TG_D void cp_async_commit_p() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-TG_D void cp_async_wait1_p() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-
 constexpr int C2_YT = 8, C2_TS = 466, C2_XR = 17, C2_XL = 29 * C2_XR;
 
 // The running maximum keeps u = out/(N M) + kappa_b and the batch index of
@@ -211,16 +205,16 @@ __global__ void __launch_bounds__(16 * C2_YT, 3) k_c2r_p464(const float2* __rest
             const int kx = e / YT, yl = e - kx * YT;
             const bool okl = y0 + yl < Ny;
             const float2* src = H + hb + ((long long)kx * Nz + z) * Ny + (okl ? y0 + yl : 0);
-            cp_async8_p(t + yl * TS + kx, src, okl ? 8 : 0);
+            tgtile::cp_async8((unsigned)__cvta_generic_to_shared(t + yl * TS + kx), src, okl ? 8 : 0);
         }
-        cp_async_commit_p();
+        tgtile::commit();
     };
     issue(0, 0);
     float2* xl = xb + line * C2_XL;
     for (int b = 0; b < nb; ++b) {
         if (b + 1 < nb) issue(b + 1, (b + 1) & 1);
-        else cp_async_commit_p();
-        cp_async_wait1_p();
+        else tgtile::commit();
+        tgtile::wait<1>();
         __syncthreads();
         const float2* X = tile + (b & 1) * YT * TS + line * TS;
         // unpack and the inner 16-point DFTs: k = k1 + 29 k2
