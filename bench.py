@@ -484,6 +484,12 @@ def main():
                    "max_rel_err": float(err.max() / np.abs(fp64).max()),
                    "note": "FP32 spectral max-CC at the top-K peaks vs FP64 direct-sum FLCF at the same angle"}
 
+    # the device-resident plan is done: its batch buffers (up to ~100 GB at
+    # 928^2 x 464) are released before the end-to-end call builds its own
+    plan.close()
+    del cc, idx, vol_dev
+    torch.cuda.empty_cache()
+
     # end to end through the one-shot C-ABI call with pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -544,7 +550,6 @@ def main():
                 "kernel_share": shares, "fp64_rescore": rescore,
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
         print(json.dumps(line), flush=True)
-    plan.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

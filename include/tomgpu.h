@@ -183,7 +183,8 @@ int tomgpu_fft3d_c2r_dev(tomgpu_ctx* ctx, void* half_dev, void* real_dev, const 
 
 /* ---------------------------------------------------- FLCF matching --- */
 typedef struct {
-    int batch;          /* rotations per batch; 0 = default (8) */
+    int batch;          /* rotations per batch; 0 = the largest of 64, 32, 16 whose
+                           per-batch buffers fit in half the free device memory, else 8 */
     int wedge_fp64;     /* reserved, 0 */
     int path;           /* 0: fastest kernels for the sizes; 1: generic kernels only */
     int reserved[5];

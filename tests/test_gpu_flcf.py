@@ -129,3 +129,36 @@ def test_match_host_reuses_context_state(gpu, oracle):
             assert np.array_equal(got_idx, ref_idx), i
     finally:
         ctx.close()
+
+
+def test_default_batch_is_sized_from_free_memory(gpu, oracle):
+    """With batch 0 a plan takes the largest of 64 / 32 / 16 rotations whose
+    buffers fit in half the free device memory: for a small volume that is
+    64 (the plan holds what an explicit batch of 64 holds), and its search
+    finds the maxima of a search with batch 8 (the batches group the running
+    maximum differently, so near-ties may round apart: the autotune test's
+    bars)."""
+    import torch
+    rng = np.random.default_rng(17)
+    T = 16
+    vol = rng.standard_normal((48, 40, 32)).astype(np.float32)
+    tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
+    mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
+    angles = oracle.av3_angle_grid((0, 0, 0), (60, 60, 60), (300, 300, 180))[:70]
+    p64 = gpu.MatchPlan(vol.shape, tmpl.shape, batch=64)
+    b64 = p64.bytes
+    p64.close()
+    out = {}
+    for batch in (0, 8):
+        plan = gpu.MatchPlan(vol.shape, tmpl.shape, batch=batch)
+        if batch == 0:
+            assert plan.bytes == b64
+        plan.set_template(gpu.to_device(tmpl), gpu.to_device(mask))
+        plan.set_volume(gpu.to_device(vol))
+        cc, idx = plan.new_results()
+        plan.run(angles, cc, idx)
+        torch.cuda.synchronize()
+        out[batch] = gpu.from_device(cc).copy(), gpu.from_device(idx).copy()
+        plan.close()
+    assert np.abs(out[0][0] - out[8][0]).max() <= 1e-6 * np.abs(out[8][0]).max()
+    assert (out[0][1] != out[8][1]).mean() < 1e-3

@@ -588,8 +588,7 @@ int MatchPlan::create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batc
     if (!match_sizes_supported(N, T))
         return fail(ctx, TOMGPU_ERR_UNSUPPORTED,
                     "volume/template sizes not supported by the FFT kernels");
-    B = batch > 0 ? batch : 8;
-    if (B > 4096) return fail(ctx, TOMGPU_ERR_ARG, "rotation batch above 4096");
+    if (batch > 4096) return fail(ctx, TOMGPU_ERR_ARG, "rotation batch above 4096");
     nvox = (long long)N[0] * N[1] * N[2];
     nh1 = N[0] / 2 + 1;
     tn = (long long)T[0] * T[1] * T[2];
@@ -601,7 +600,7 @@ int MatchPlan::create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batc
     TG_TRY(alloc((void**)&d_mu0, sizeof(float) * nvox));
     TG_TRY(alloc((void**)&d_sig, sizeof(float) * nvox));
     TG_TRY(alloc((void**)&d_gam, sizeof(float) * nvox));
-    TG_TRY(alloc_batch(B));
+    TG_TRY(alloc_batch(batch > 0 ? batch : default_batch()));
     TG_TRY_CUDA(ctx, cudaEventCreateWithFlags(&ev_mats, cudaEventDisableTiming));
     // twiddle tables are built now so that later calls allocate nothing
     const int lens[] = {N[0], N[1], N[2], N[0] / 2, T[0], T[1], T[2]};
@@ -623,6 +622,20 @@ void MatchPlan::free_batch() {
     d_A = d_Z = d_Q = d_H = nullptr;
     bytes_held -= batch_bytes;
     batch_bytes = 0;
+}
+
+// Without a requested batch: the largest of 64, 32 and 16 rotations whose
+// buffers take at most half of the device memory free at this point (the
+// rest is left to the caller), else 8.
+int MatchPlan::default_batch() const {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        return 8;
+    }
+    for (int nb : {64, 32, 16})
+        if (batch_need(nb) <= (int64_t)(fr / 2)) return nb;
+    return 8;
 }
 
 int64_t MatchPlan::batch_need(int nb) const {
