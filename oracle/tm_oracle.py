@@ -218,6 +218,47 @@ def tom_norm_mean0_1std(a):
     return (a - m) / s if s != 0 else a - m
 
 
+def tom_dev(a, mask=None):
+    """(mean, max, min, std) of Analysis/tom_dev.m:57-60: in double, over the
+    voxels where mask > 0 (all without a mask), std with the 1/n normalisation."""
+    a = np.asarray(a, np.float64)
+    v = a[np.asarray(mask) > 0] if mask is not None else a.ravel()
+    return v.mean(), v.max(), v.min(), v.std()
+
+
+def tom_norm(a, scf="mean0+1std", mask=None):
+    """Sptrans/tom_norm.m:79-153, every branch: 'mean0+1std' (after a -> 2a + 100,
+    :83-85), 'phase', '1std' / '2std' / '3std' (tom_limit about the mean),
+    'oscar' (3std limit + 100, then phase-normalised) and a number scf (the
+    range [min, max] mapped to [0, scf]; a / scf for a constant input; a when
+    the mean already equals scf).  Statistics from tom_dev, inside the mask
+    when one is given."""
+    a = np.asarray(a, np.float64)
+    if isinstance(scf, str) and scf == "mean0+1std":
+        a = a * 2 + 100
+    mea, ma, mi, st = tom_dev(a, mask)
+    if isinstance(scf, str):
+        if scf == "phase":
+            return (a - mea) / (mea + 1e-12)
+        if scf in ("1std", "2std", "3std"):
+            k = float(scf[0])
+            return tom_limit(a, mea - k * st, mea + k * st) - mea
+        if scf == "mean0+1std":
+            return (a - mea) / st if st != 0 else a - mea
+        if scf == "oscar":
+            m2, _, _, s2 = tom_dev(a)
+            c = tom_limit(a, m2 - 3 * s2, m2 + 3 * s2) - m2 + 100
+            mc = tom_dev(c, mask)[0]
+            return (c - mc) / (mc + 1e-12)
+        raise ValueError("Only numbers and keyword 'phase', '2std' , '3std' or 'mean0+1std' allowed.")
+    if st != 0 and mea != scf:
+        s = a - mi
+        return scf * s / s.max()
+    if st == 0 and mea != scf:
+        return a / scf
+    return a
+
+
 def os3_sphere_mask(shape):
     """tom_os3_sphereMask(template): radius floor(min/2)-1, centre floor(n/2)+1 (1-based),
     zero where distance >= radius; non-cubic input -> all ones."""

@@ -75,6 +75,52 @@ def test_tom_fourier_kat():
     assert np.isclose(c[0, 1], np.conj(expect[0, 3])) and np.isclose(c[1, 1], np.conj(expect[3, 3]))
 
 
+def test_tom_norm_kat(oracle):
+    """Sptrans/tom_norm.m:29-43: c = tom_norm(a, 10) maps [min, max] = [0, 19]
+    to [0, 10].  23 of the 25 printed values are the map's values truncated
+    to 3 decimals; two are print slips: the input 8 prints as 4.210 five times and once (row 5,
+    column 2) as 4.219, and the input 2 prints as 1.056 where 10 * 2 / 19 =
+    1.0526 is the value of the same linear map that fits the other 23."""
+    a = np.array([[10, 1, 19, 8, 5], [12, 9, 17, 10, 10], [3, 3, 2, 0, 8], [15, 8, 0, 7, 8],
+                  [0, 8, 6, 15, 8]], float)
+    printed = np.array([[5.263, 0.526, 10.00, 4.210, 2.631], [6.315, 4.736, 8.947, 5.263, 5.263],
+                        [1.578, 1.578, 1.056, 0, 4.210], [7.894, 4.210, 0, 3.684, 4.210],
+                        [0, 4.219, 3.157, 7.894, 4.210]])
+    c = oracle.tom_norm(a, 10)
+    slips = np.zeros(a.shape, bool)
+    slips[2, 2] = slips[4, 1] = True
+    # the printed values are truncated to 3 decimals (7.8947 -> 7.894, 4.7368 -> 4.736)
+    d = c[~slips] - printed[~slips]
+    assert np.all((d > -1e-12) & (d < 1e-3))
+    assert np.isclose(c[4, 1], 4.2105, atol=1e-4) and np.isclose(c[2, 2], 1.0526, atol=1e-4)
+    # the constant and the already-scaled cases of the same branch (:142-147)
+    assert np.array_equal(oracle.tom_norm(np.full((3, 3), 4.0), 2), np.full((3, 3), 2.0))
+    b = np.array([1.0, 2.0, 3.0])
+    assert np.array_equal(oracle.tom_norm(b, 2), b)
+
+
+def test_tom_norm_branches(oracle):
+    """The string branches of tom_norm against their definitions, and the
+    'mean0+1std' branch against the restatement the template statistics use."""
+    rng = np.random.default_rng(4)
+    a = rng.standard_normal((6, 5, 4)) * 3 + 1
+    assert np.allclose(oracle.tom_norm(a, "mean0+1std"), oracle.tom_norm_mean0_1std(a), rtol=0, atol=1e-12)
+    assert np.allclose(oracle.tom_norm(a), oracle.tom_norm_mean0_1std(a), rtol=0, atol=1e-12)
+    m, s = a.mean(), a.std()
+    assert np.allclose(oracle.tom_norm(a, "phase"), (a - m) / (m + 1e-12))
+    for k in (1, 2, 3):
+        assert np.allclose(oracle.tom_norm(a, f"{k}std"), np.clip(a, m - k * s, m + k * s) - m)
+    mask = np.zeros(a.shape)
+    mask[1:4, 1:4, 1:3] = 1
+    v = a[mask > 0]
+    mm, ms = v.mean(), v.std()
+    assert np.allclose(oracle.tom_norm(a, "2std", mask), np.clip(a, mm - 2 * ms, mm + 2 * ms) - mm)
+    c = np.clip(a, m - 3 * s, m + 3 * s) - m + 100
+    assert np.allclose(oracle.tom_norm(a, "oscar"), (c - c.mean()) / (c.mean() + 1e-12))
+    with pytest.raises(ValueError):
+        oracle.tom_norm(a, "4std")
+
+
 def test_rotation_axis_conventions(oracle):
     """Sptrans/tom_rotate.m:59-61: X axis ~ phi=0 psi=0 the=a; Y ~ phi=270 psi=90 the=a; Z ~ phi=a."""
     for a in (20.0, 37.0, 90.0):
