@@ -19,8 +19,6 @@ cross-entropy).
 """
 from __future__ import annotations
 
-import ctypes
-
 import numpy as np
 
 from . import _lib
