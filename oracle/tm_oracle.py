@@ -322,9 +322,12 @@ def norm_under_mask(vol, mask):
     m = mask != 0
     n = m.sum()
     v = np.asarray(vol, np.float64)
-    mea = ((v * m) * (v != 0)).sum() / n
-    st = np.sqrt(((((~m) * mea) + (v * m) - mea) ** 2).sum() / n)
-    return ((v - mea) / st) * m, mea, st
+    # a NaN or Inf anywhere in vol (the unguarded same-size division of
+    # tom_os3_corr.m:172-176) makes both statistics NaN, as in MATLAB (NaN * 0 = NaN)
+    with np.errstate(invalid="ignore"):
+        mea = ((v * m) * (v != 0)).sum() / n
+        st = np.sqrt(((((~m) * mea) + (v * m) - mea) ** 2).sum() / n)
+        return ((v - mea) / st) * m, mea, st
 
 
 def paste_center(shape, small):
@@ -362,8 +365,12 @@ class FLCF:
         self.fimage = np.fft.rfftn(np.asarray(volume, np.float64))
 
     def corr(self, t, tmean, tstd):
-        """search/tom_os3_corr.m:151-176 for one (already rotated/modified) template."""
-        p = paste_center(self.N, np.asarray(t, np.float64) * self.mask)
+        """search/tom_os3_corr.m:151-176 for one (already rotated/modified) template.
+        A template holding NaN (an autocorrelation map from the same-size
+        branch) gives NaN numerators and denominators, and the denominator
+        rule then leaves 0 at every voxel, as the reference's res(nonzero)."""
+        with np.errstate(invalid="ignore"):
+            p = paste_center(self.N, np.asarray(t, np.float64) * self.mask)
         ft = np.fft.rfftn(p)
         num = np.fft.ifftshift(np.fft.irfftn(self.fimage * np.conj(ft), s=self.N, axes=(0, 1, 2))) / self.M
         num = num - self.mean * tmean
