@@ -78,9 +78,10 @@ def test_tom_fourier_kat():
 def test_tom_norm_kat(oracle):
     """Sptrans/tom_norm.m:29-43: c = tom_norm(a, 10) maps [min, max] = [0, 19]
     to [0, 10].  23 of the 25 printed values are the map's values truncated
-    to 3 decimals; two are print slips: the input 8 prints as 4.210 five times and once (row 5,
-    column 2) as 4.219, and the input 2 prints as 1.056 where 10 * 2 / 19 =
-    1.0526 is the value of the same linear map that fits the other 23."""
+    to 3 decimals; two are print slips: the input 8 prints as 4.210 five
+    times and once (row 5, column 2) as 4.219, and the input 2 prints as
+    1.056 where 10 * 2 / 19 = 1.0526 is the value of the same linear map that
+    fits the other 23."""
     a = np.array([[10, 1, 19, 8, 5], [12, 9, 17, 10, 10], [3, 3, 2, 0, 8], [15, 8, 0, 7, 8],
                   [0, 8, 6, 15, 8]], float)
     printed = np.array([[5.263, 0.526, 10.00, 4.210, 2.631], [6.315, 4.736, 8.947, 5.263, 5.263],
@@ -348,3 +349,20 @@ def test_cnn_losses_finite_difference(oracle):
         e[idx] = h
         fd = (oracle.cnn_softmax_ce(lg + e, lab)[0] - oracle.cnn_softmax_ce(lg - e, lab)[0]) / (2 * h)
         assert abs(fd - g[idx]) < 1e-8
+
+
+def test_constant_template_rule(oracle):
+    """A constant template: tom_norm(...,'mean0+1std') leaves zeros
+    (Sptrans/tom_norm.m:114-119 with std 0), its std under the mask is 0, so
+    every FLCF denominator is 0 and tom_os3_corr.m:169-176 leaves 0 at every
+    voxel; tom_os3_bestPeak's strict update then keeps the first angle
+    everywhere (ccc 0, angle index 0)."""
+    rng = np.random.default_rng(12)
+    vol = rng.standard_normal((12, 10, 8))
+    tmpl = np.full((6, 6, 6), 3.0)
+    mask = oracle.sphere_mask((6, 6, 6), 2.5)
+    angles = oracle.av3_angle_grid((0, 0, 0), (30, 30, 30), (330, 330, 180))[:7]
+    t, tmean, tstd = oracle.prepare_template(tmpl, mask)
+    assert not t.any() and tmean == 0 and tstd == 0
+    ccc, idx = oracle.find_template(vol, tmpl, mask, angles)
+    assert not ccc.any() and not idx.any()
