@@ -380,14 +380,20 @@ def _fft(a, direction, ctx):
 # ---------------------------------------------------------------- angles
 
 def _rotmatrix(phi, psi, theta):
-    """tom_angles2rotmatrix (Sptrans/tom_sum_rotation.m): Rz(psi) Rx(theta) Rz(phi), double."""
-    ph, ps, th = np.deg2rad([phi, psi, theta])
+    """tom_angles2rotmatrix (Sptrans/tom_sum_rotation.m): Rz(psi) Rx(theta) Rz(phi), double,
+    with the reference's degree conversion a .* pi ./ 180 (in that order)."""
+    ph, ps, th = (np.asarray([phi, psi, theta], np.float64) * np.pi) / 180
     rz = lambda a: np.array([[np.cos(a), -np.sin(a), 0], [np.sin(a), np.cos(a), 0], [0, 0, 1]])
     rx = np.array([[1, 0, 0], [0, np.cos(th), -np.sin(th)], [0, np.sin(th), np.cos(th)]])
     return rz(ps) @ rx @ rz(ph)
 
 
 def _os3_axis(start, inc, end):
+    """One axis of tom_os3_angleList (search/tom_os3_angleList.m, dim 2).
+    start < end: start:inc:end mod 360.  Otherwise the reference walks
+    start+1:inc:end+359 into a result preallocated with
+    floor((360+end-start)/inc)+1 zeros, so when the walk is one step shorter
+    (e.g. 300 -> 60 by 30: 301 331 1 31) the list keeps a trailing 0."""
     if start < end:
         vals = []
         i = start
@@ -400,7 +406,8 @@ def _os3_axis(start, inc, end):
     while i <= end + 360 - 1 + 1e-9:
         vals.append(np.mod(i, 360))
         i += inc
-    return vals
+    size = int(np.floor((360 + end - start) / inc)) + 1
+    return vals + [0.0] * max(0, size - len(vals))
 
 
 def tom_os3_angleList(start, increment, end, dedup=True):
