@@ -72,6 +72,44 @@ def test_key_packing_order():
     assert np.all(np.diff(k[order]) >= 0)
 
 
+def _bestpeak_merge(parts):
+    """The checker: merge [(cc, idx), ...] in rank order with tom_os3_bestPeak's
+    rule (search/tom_os3_bestPeak.m:42-47: a strictly larger CC replaces, so on
+    equal CC the earlier rank's, i.e. earlier angle's, pair stays)."""
+    cc = parts[0][0].astype(np.float32).copy()
+    idx = parts[0][1].astype(np.int32).copy()
+    for c, i in parts[1:]:
+        better = c > cc
+        cc = np.where(better, c, cc)
+        idx = np.where(better, i, idx)
+    return cc, idx
+
+
+def test_key_max_merge_is_the_bestpeak_merge():
+    """One elementwise MAX over the ranks' packed keys (what the all-reduce
+    computes) equals the rank-order bestPeak merge, with CCs quantised so
+    ranks tie often, signed zeros, and voxels a rank never updated."""
+    from tom_b200 import shard
+    rng = np.random.default_rng(8)
+    n, world, n_angles = 4000, 4, 1000
+    parts = []
+    for r in range(world):
+        lo, hi = shard.angle_slice(n_angles, world, r)
+        cc = (np.round(rng.standard_normal(n) * 4) / 8).astype(np.float32)
+        cc[rng.random(n) < 0.05] = -0.0
+        idx = rng.integers(lo, hi, n).astype(np.int32)
+        unset = rng.random(n) < 0.02
+        cc[unset], idx[unset] = -1000.0, -1
+        parts.append((cc, idx))
+    keys = np.max(np.stack([shard.pack_keys(torch.from_numpy(c), torch.from_numpy(i)).numpy() for c, i in parts]),
+                  axis=0)
+    c2, i2 = shard.unpack_keys(torch.from_numpy(keys))
+    ref_cc, ref_idx = _bestpeak_merge(parts)
+    assert np.array_equal(c2.numpy(), np.where(ref_cc == 0, 0, ref_cc).astype(np.float32))
+    # where every rank left -1000 / -1 the merge keeps -1; elsewhere the indices agree
+    assert np.array_equal(i2.numpy(), ref_idx)
+
+
 def test_angle_slices_cover_exactly():
     from tom_b200 import shard
     for n in (1, 7, 1008, 24624):

@@ -14,8 +14,6 @@ performs it.
 """
 from __future__ import annotations
 
-import numpy as np
-
 
 def angle_slice(n_angles: int, world: int, rank: int):
     """Contiguous slice [lo, hi) of the angle list for `rank`."""
@@ -57,14 +55,3 @@ def merge_results(cc, idx, group=None):
     keys = pack_keys(cc, idx)
     dist.all_reduce(keys, op=dist.ReduceOp.MAX, group=group)
     return unpack_keys(keys)
-
-
-def merge_numpy(parts):
-    """Reference merge of [(cc, idx), ...] in rank order with the bestPeak rule."""
-    cc = np.full_like(parts[0][0], -np.inf, dtype=np.float64)
-    idx = np.full(parts[0][1].shape, -1, np.int64)
-    for c, i in parts:
-        better = (c > cc) | ((c == cc) & (i < idx) & (i >= 0))
-        cc = np.where(better, c, cc)
-        idx = np.where(better, i, idx)
-    return cc, idx
