@@ -724,10 +724,25 @@ int MatchPlan::autotune(const float* eulers, int R, const int* cands, int nc, in
     cudaFree(cc);
     cudaFree(idx);
     free_batch();
+    // the batch buffers come back after an error too, so the plan stays usable;
+    // the first error's status and message are the ones reported
     const int keep = best > 0 ? best : orig;
-    if (!rc) rc = alloc_batch(keep);
+    const std::string first = ctx->last_error;
+    const int rc2 = alloc_batch(keep);
+    if (!rc) rc = rc2;
+    else if (rc2) ctx->last_error = first;
     if (best_out) *best_out = best > 0 ? best : 0;
     return rc;
+}
+
+// Template, volume and the rotation-batch buffers (which a failed
+// re-allocation in the autotuner can leave absent) before any batch work.
+int MatchPlan::check_ready() {
+    if (!has_template || !has_volume) return fail(ctx, TOMGPU_ERR_STATE, "template and volume must be set");
+    if (!d_t1 || !d_A || !d_Z || !d_Q || !d_H)
+        return fail(ctx, TOMGPU_ERR_STATE,
+                    "the plan has no rotation-batch buffers (their re-allocation failed): destroy and re-create it");
+    return TOMGPU_OK;
 }
 
 int MatchPlan::ensure_mats(int R) {
@@ -927,7 +942,7 @@ int MatchPlan::prepare_batch(int off, int nb) {
 }
 
 int MatchPlan::run(const float* eulers, int R, int index_offset, float* maxcc, int* angidx) {
-    if (!has_template || !has_volume) return fail(ctx, TOMGPU_ERR_STATE, "template and volume must be set");
+    if (int rc = check_ready()) return rc;
     if (R <= 0) return TOMGPU_OK;
     cudaStream_t st = ctx->stream;
     TG_TRY(upload_mats(eulers, R));
@@ -966,7 +981,7 @@ int MatchPlan::run(const float* eulers, int R, int index_offset, float* maxcc, i
 }
 
 int MatchPlan::corr(const float* t, float* cc) {
-    if (!has_template || !has_volume) return fail(ctx, TOMGPU_ERR_STATE, "template and volume must be set");
+    if (int rc = check_ready()) return rc;
     cudaStream_t st = ctx->stream;
     // the given template is already rotated, masked and filtered: S and the
     // spectrum come from t * mask (tom_os3_corr.m:151)
@@ -995,7 +1010,7 @@ int MatchPlan::cc_map_tail(float* cc) {
 // selected criteria: one rotation at a time, each rotation's maps in FP64.
 int MatchPlan::run_analysis(const float* eulers, int R, int index_offset, int flags, float* maxcc, int* angidx,
                             float* psr, float* soc) {
-    if (!has_template || !has_volume) return fail(ctx, TOMGPU_ERR_STATE, "template and volume must be set");
+    if (int rc = check_ready()) return rc;
     if (R <= 0) return TOMGPU_OK;
     if (!an) {
         an = new (std::nothrow) PeakAnalysis();

@@ -88,6 +88,7 @@ struct MatchPlan {
     int alloc_batch(int nb);
     int64_t batch_need(int nb) const;  // bytes alloc_batch(nb) allocates
     int default_batch() const;
+    int check_ready();
     void free_batch();
     int autotune(const float* eulers, int R, const int* cands, int nc, int* best, float* ms_per_rot);
     int ensure_mats(int R);
