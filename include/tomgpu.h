@@ -201,11 +201,14 @@ int tomgpu_match_plan_destroy(tomgpu_match_plan* plan);
 /* Bytes of device memory the plan holds. */
 int64_t tomgpu_match_plan_bytes(const tomgpu_match_plan* plan);
 
-/* Once per tomogram (tom_os3_findTemplate.m:243-245; statistics/tom_os3_mean.m:49-62,
- * statistics/tom_os3_std.m:48-67): the tomogram spectrum and the local mean and
- * standard deviation under the mask, accumulated in FP64.  The mask must be
- * given first (tomgpu_match_set_template) or here: mask_dev (template-sized)
- * may be NULL when a template is already set. */
+/* Once per tomogram and template (tom_os3_findTemplate.m:243-245;
+ * statistics/tom_os3_mean.m:49-62, statistics/tom_os3_std.m:48-67): the
+ * tomogram spectrum and the local mean and standard deviation under the mask,
+ * accumulated in FP64, and the FLCF denominators with the template's std.
+ * The template and mask must be set first (tomgpu_match_set_template_dev or
+ * _raw_dev).  A later template with the same mask keeps the volume (its
+ * denominators follow the new template); one with another mask unsets it,
+ * and runs return TOMGPU_ERR_STATE until the volume is set again. */
 int tomgpu_match_set_volume_dev(tomgpu_match_plan* plan, const float* vol_dev);
 
 /* Template, mask and optional weight (psf) volume, template-sized, device
@@ -213,7 +216,8 @@ int tomgpu_match_set_volume_dev(tomgpu_match_plan* plan, const float* vol_dev);
  * 'mean0+1std') (tom_os3_findTemplate.m:157) and the unrotated, filtered
  * template statistics (tom_os3_normUnderMask on tom_os3_modifyImage,
  * :233-234).  psf_dev is the centred weight of tom_apply_weight_function
- * (NULL: no filter).  Must precede tomgpu_match_set_volume_dev. */
+ * (NULL: no filter).  Must precede tomgpu_match_set_volume_dev; a volume set
+ * before it stays set when the mask is the same and is unset otherwise. */
 int tomgpu_match_set_template_dev(tomgpu_match_plan* plan, const float* tmpl_dev,
                                   const float* mask_dev, const float* psf_dev);
 

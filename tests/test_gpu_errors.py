@@ -122,3 +122,50 @@ def test_match_host_errors_and_empty_angle_list(gpu, oracle):
     finally:
         fresh.close()
     assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+
+
+def test_template_change_after_the_volume(gpu, oracle):
+    """The volume's local statistics are made with the mask and its FLCF
+    denominators with the template's std.  A new template with the same mask
+    keeps the volume (the denominators follow the template): the search equals
+    a fresh plan's.  A new mask unsets the volume: a run reports
+    TOMGPU_ERR_STATE before launching anything, and with the volume set again
+    the search equals a fresh plan's."""
+    import torch
+    L = gpu._lib
+    vol, tmpl, mask, angles = _inputs(oracle)
+    tmpl2 = np.random.default_rng(9).standard_normal(tmpl.shape).astype(np.float32)
+    mask2 = oracle.sphere_mask(tmpl.shape, tmpl.shape[0] // 2 - 2).astype(np.float32)
+
+    def results(plan, cc, idx):
+        plan.init_results(cc, idx)
+        plan.run(angles, cc, idx)
+        torch.cuda.synchronize()
+        return gpu.from_device(cc).copy(), gpu.from_device(idx).copy()
+
+    ctx = gpu.Context(0)
+    try:
+        plan = gpu.MatchPlan(vol.shape, tmpl.shape, batch=4, ctx=ctx)
+        plan.set_template(gpu.to_device(tmpl), gpu.to_device(mask))
+        vd = gpu.to_device(vol)
+        plan.set_volume(vd)
+        cc, idx = plan.new_results()
+        plan.set_template(gpu.to_device(tmpl2), gpu.to_device(mask))  # same mask
+        same_mask = results(plan, cc, idx)
+        plan.set_template(gpu.to_device(tmpl), gpu.to_device(mask2))  # another mask
+        with pytest.raises(gpu.TomGpuError) as e:
+            plan.run(angles, cc, idx)
+        assert e.value.status == L.TOMGPU_ERR_STATE
+        plan.set_volume(vd)
+        new_mask = results(plan, cc, idx)
+        plan.close()
+    finally:
+        ctx.close()
+    fresh = gpu.Context(0)
+    try:
+        ref1 = _search(gpu, fresh, vol, tmpl2, mask, angles)
+        ref2 = _search(gpu, fresh, vol, tmpl, mask2, angles)
+    finally:
+        fresh.close()
+    for got, ref in ((same_mask, ref1), (new_mask, ref2)):
+        assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])

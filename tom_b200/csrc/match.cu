@@ -767,6 +767,17 @@ int MatchPlan::upload_mats(const float* eulers, int R) {
 
 int MatchPlan::set_template(const float* tmpl, const float* mask, const float* psf, bool raw) {
     cudaStream_t st = ctx->stream;
+    // The volume's local mean and std are made with the mask, its FLCF
+    // denominators (gamma) with the template's std: with the same mask the
+    // volume stays set and gamma is recomputed at the end; a new mask unsets
+    // the volume.  A template that fails half-way leaves the plan unset.
+    std::vector<float> m((size_t)tn);
+    TG_TRY_CUDA(ctx, cudaMemcpyAsync(m.data(), mask, sizeof(float) * tn, cudaMemcpyDeviceToHost, st));
+    TG_TRY_CUDA(ctx, cudaStreamSynchronize(st));
+    const bool keep_volume =
+        has_volume && h_mask.size() == m.size() && std::memcmp(h_mask.data(), m.data(), sizeof(float) * tn) == 0;
+    has_template = false;
+    has_volume = false;
     if (an) {  // the peak analysis holds the old mask's spectrum
         delete an;
         an = nullptr;
@@ -836,10 +847,12 @@ int MatchPlan::set_template(const float* tmpl, const float* mask, const float* p
     cudaFree(tc64);
     cudaFree(tv64);
     if (rc) return rc;
+    h_mask.swap(m);
     has_template = true;
-    if (has_volume) {
+    if (keep_volume) {
         TG_TRY_CUDA(ctx, gamma_from_sigma(d_sig, d_gam, nvox, tstd, st));
         ctx->launches += 1;
+        has_volume = true;
     }
     return TOMGPU_OK;
 }

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "ctx.h"
 
 namespace tg {
@@ -54,6 +56,7 @@ struct MatchPlan {
     int64_t bytes_held = 0;
     int64_t batch_bytes = 0;
     bool has_template = false, has_volume = false, has_psf = false;
+    std::vector<float> h_mask;  // host copy of the mask the volume statistics were made with
     double msize = 0, tmean = 0, tstd = 0, vmean = 0;
     // template state
     float* d_tmpl = nullptr;  // tom_norm'ed template
