@@ -108,7 +108,7 @@ int tomgpu_peak_dev(tomgpu_ctx* ctx, const float* v_dev, const int dims[3], floa
 
 /* K peaks by repeated [c val M] = tom_peak(A, R) (Analysis/tom_peak.m:203-279):
  * each round takes the first maximum and zeroes the ball of radius R around
- * it.  work_dev: a scratch copy of A is made internally (A is not modified).
+ * it.  The search zeroes balls in an internal scratch copy; v_dev is not modified.
  * vals: K floats, pos1: K x 3 ints (1-based). */
 int tomgpu_topk_dev(tomgpu_ctx* ctx, const float* v_dev, const int dims[3], int K, double radius,
                     float* vals, int* pos1);
