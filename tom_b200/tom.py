@@ -460,7 +460,9 @@ class MatchPlan:
 
     Tensors are torch CUDA float32, shaped (z, y, x).  Usage mirrors
     tom_os3_findTemplate: set_template (template, mask, optional psf) ->
-    set_volume -> init_results -> run(eulers) [repeat] -> results.
+    set_volume -> init_results -> run(eulers) [repeat] -> results.  A later
+    set_template with the same mask keeps the volume; after one with another
+    mask, set_volume again (run raises TomGpuError TOMGPU_ERR_STATE until then).
     """
 
     def __init__(self, vol_shape_xyz, tmpl_shape_xyz, batch: int = 0, ctx: Context | None = None,
