@@ -17,7 +17,9 @@ Rank 0 prints one JSON line.  `value` is rot*voxel/s of the timed region
 (device time, CUDA events, max over ranks); `e2e` is the same metric through
 the one-shot C-ABI call tomgpu_match with pinned host buffers (upload of the
 tomogram, FP64 statistics, the search, download of max-CC and angle index
-inside the timed region).
+inside the timed region).  Before the timed region the rotation batch is
+autotuned over 8, 16, 32 and 64 (those that fit); the device-resident plan is
+released before the end-to-end leg builds its own.
 """
 from __future__ import annotations
 
