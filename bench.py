@@ -534,8 +534,10 @@ def main():
         cpu = cpu_baseline(d, mask, grid, args.cpu_seconds)
 
     if rank == 0:
-        metric = METRIC if args.workload == WORKLOAD else "TM rot*voxel/s (exhaustive FLCF, %s tomogram, %d^3 template)" % (
-            "x".join(str(v) for v in cfg["N"]), cfg["T"])
+        metric = METRIC
+        if args.workload != WORKLOAD:
+            metric = "TM rot*voxel/s (exhaustive FLCF, %s tomogram, %d^3 template)" % (
+                "x".join(str(v) for v in cfg["N"]), cfg["T"])
         line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",

@@ -566,9 +566,9 @@ class MatchPlan:
         e = np.ascontiguousarray(np.asarray(eulers, np.float32).reshape(-1, 3))
         p = np.ascontiguousarray(np.asarray(pos1, np.int32).reshape(-1, 3))
         out = np.zeros(len(e), np.float64)
-        self.ctx.check(lib().tomgpu_match_rescore_fp64_dev(self.handle, _tptr(vol_dev), e.ctypes.data_as(_lib.c_float_p),
-                                                           p.ctypes.data_as(_lib.c_int_p), len(e),
-                                                           out.ctypes.data_as(_lib.c_double_p)))
+        self.ctx.check(lib().tomgpu_match_rescore_fp64_dev(
+            self.handle, _tptr(vol_dev), e.ctypes.data_as(_lib.c_float_p), p.ctypes.data_as(_lib.c_int_p), len(e),
+            out.ctypes.data_as(_lib.c_double_p)))
         return out
 
     def stats(self):
