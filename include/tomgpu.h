@@ -48,7 +48,9 @@ const char* tomgpu_last_error(const tomgpu_ctx* ctx);
 int tomgpu_ctx_create(int device, tomgpu_ctx** out);
 int tomgpu_ctx_destroy(tomgpu_ctx* ctx);
 /* Issue all further work of this context on an existing cudaStream_t (passed
- * as void*); NULL selects the CUDA legacy default stream. */
+ * as void*); NULL selects the CUDA legacy default stream.  Work already
+ * queued on the previous stream completes before the new stream's next work
+ * (an event wait on the device; the call does not block the host). */
 int tomgpu_ctx_set_stream(tomgpu_ctx* ctx, void* cuda_stream);
 int tomgpu_ctx_synchronize(tomgpu_ctx* ctx);
 /* Release the device memory that tomgpu_match keeps in the context between

@@ -209,7 +209,18 @@ int tomgpu_ctx_destroy(tomgpu_ctx* ctx) {
 
 int tomgpu_ctx_set_stream(tomgpu_ctx* ctx, void* s) {
     if (!ctx) return TOMGPU_ERR_ARG;
-    ctx->stream = static_cast<cudaStream_t>(s);
+    cudaStream_t ns = static_cast<cudaStream_t>(s);
+    if (ns == ctx->stream) return TOMGPU_OK;
+    TG_TRY(use_device(ctx));
+    // work already queued on the previous stream completes before any work
+    // issued on the new one: an event wait on the device, the host does not block
+    cudaEvent_t ev = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (!e) e = cudaEventRecord(ev, ctx->stream);
+    if (!e) e = cudaStreamWaitEvent(ns, ev, 0);
+    if (ev) cudaEventDestroy(ev);
+    if (e) return cuda_fail(ctx, e, "stream switch");
+    ctx->stream = ns;
     return TOMGPU_OK;
 }
 
