@@ -219,3 +219,14 @@ def test_match_plan_engine_layout_and_resume(oracle, job, reference, tmp_path):
     assert info["resumed_at"] == 15
     assert cc.dtype == np.float32 and idx.dtype == np.int32 and cc.shape == vol.shape
     assert np.array_equal(cc, reference[0]) and np.array_equal(idx, reference[1])
+
+
+def test_checkpointed_find_template_empty_volume(tmp_path):
+    """tom_os3_findTemplate.m:221 and :309-313: an empty volume is not searched
+    (ccc 0, angles -1000), so no device and no checkpoint are needed."""
+    from tom_b200.checkpoint import find_template_checkpointed
+    path = str(tmp_path / "ck.npz")
+    ccc, ang, info = find_template_checkpointed(np.zeros((12, 10, 8), np.float32), np.ones((6, 6, 6)),
+                                                np.zeros((4, 3)), path)
+    assert ccc.shape == (12, 10, 8) and not ccc.any() and (ang == -1000).all()
+    assert info["chunks_run"] == 0 and not os.path.exists(path)

@@ -246,7 +246,6 @@ def find_template_checkpointed(volume, template, angle_list, path, mask=None, ps
     (angles 1-based as float32, -1000 where never updated) and the resume
     record of run_checkpointed."""
     from .tom import MatchPlan, default_context, tom_os3_sphereMask, to_device
-    ctx = ctx or default_context()
     vol = np.asarray(volume, np.float32)
     t = np.asarray(template, np.float32)
     if mask is None:
@@ -258,6 +257,7 @@ def find_template_checkpointed(volume, template, angle_list, path, mask=None, ps
                 {"resumed_at": 0, "chunks_run": 0, "checkpoints": 0})
     key = {"tomogram_crc32": _crc32(vol), "template_shape": list(t.shape), "template_crc32": _crc32(t),
            "mask_crc32": _crc32(mask), "psf_crc32": None if psf is None else _crc32(np.asarray(psf, np.float32))}
+    ctx = ctx or default_context()
     plan = MatchPlan(vol.shape, t.shape, batch=batch, ctx=ctx)
     try:
         plan.set_template(to_device(t, ctx.device), to_device(mask, ctx.device),
