@@ -19,6 +19,12 @@ def pytest_configure(config):
         subprocess.run(["make", "-C", ORACLE, "oracle"], check=False, capture_output=True)
 
 
+# host-side tests of the library's C++ (no GPU needed) skip, like the ABI
+# tests, where libtomgpu.so has not been built
+needs_library = pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "tom_b200", "libtomgpu.so")),
+                                   reason="libtomgpu.so not built (python -m tom_b200.build_ext)")
+
+
 @pytest.fixture(scope="session")
 def oracle():
     import tm_oracle

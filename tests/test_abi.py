@@ -5,6 +5,8 @@ import os
 
 import pytest
 
+from conftest import needs_library
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -57,6 +59,7 @@ def test_context_creation_reports_missing_device():
     assert b"device" in L.lib().tomgpu_last_error(None)
 
 
+@needs_library
 def test_host_matrix_equals_oracle(oracle):
     """tomgpu_euler_matrix (host C++) equals the oracle's restatement bit for bit."""
     import numpy as np

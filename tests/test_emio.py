@@ -4,6 +4,10 @@ meets.  Host-only: runs without a GPU."""
 import numpy as np
 import pytest
 
+from conftest import needs_library
+
+pytestmark = needs_library
+
 
 def _header(magic, dims, comment=b""):
     h = bytearray(512)

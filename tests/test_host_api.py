@@ -3,6 +3,7 @@ their index conventions, the mask builders and the motive-list layout,
 against the reference's definitions and the oracle."""
 import numpy as np
 
+from conftest import needs_library
 from tom_b200 import tom
 
 
@@ -43,6 +44,7 @@ def test_os3_angle_list_dedup():
         assert np.abs(tom._rotmatrix(*a) - tom._rotmatrix(*kept[i])).max() < 1e-9
 
 
+@needs_library
 def test_rotmatrix_is_the_zxz_matrix():
     """Rz(psi) Rx(theta) Rz(phi) (Sptrans/tom_sum_rotation.m) against the
     float32 matrix of tom_rotatec (rm.. order: column-major rows of R)."""
