@@ -42,8 +42,8 @@ METRIC = "TM rot*voxel/s (exhaustive FLCF, 512x512x256 tomogram, 40^3 template)"
 UNIT = "rot*voxel/s"
 
 # DRAM bytes (read + write) per launch of a kernel class at a rotation batch,
-# from one ncu capture of a smaller volume with the same x edge, scaled by the
-# voxel count (profiles/traffic_c2r_flcf_profile_512x128x64.md).
+# from one ncu capture of a 512x128x64 volume (the same x edge), scaled by the
+# voxel count of the 512x512x256 tomogram.
 TRAFFIC = {"exhaustive_512x512x256": {"c2r_flcf": {16: 16 * (336639232 + 22247680),
                                                   32: 16 * (606162432 + 24264960)}}}
 

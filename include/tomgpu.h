@@ -121,17 +121,20 @@ int tomgpu_peak_radius_dev(tomgpu_ctx* ctx, float* v_dev, const int dims[3], dou
                            int pos1[3]);
 
 /* Allocation-free variant of tomgpu_topk_dev, for callers that must not
- * allocate device memory at the time they search peaks (during CUDA graph
- * capture, under a host framework that owns the device memory, in loops that
- * may not risk an allocation failure).  No context: work is issued on
- * `stream` (NULL = legacy default stream); v_dev is the volume, vals_dev (K
- * floats) and pos1_dev (K x 3 ints, 1-based) are device outputs.  The scratch
- * lives in file-scope device arrays: at most 16,777,216 voxels (64 MiB, held on
- * every GPU where the library's code is loaded until exit); larger volumes
- * return TOMGPU_ERR_UNSUPPORTED.  The first call on a device sets the scratch
- * up and must precede any stream capture on that device.  Calls share the
- * scratch: calls that overlap on the GPU race.  Errors: tomgpu_last_error(NULL).
- * This entry point has no counterpart in the reference. */
+ * allocate device memory at the time they search peaks (under a host
+ * framework that owns the device memory, such as a MEX next to gpuArray data,
+ * or in loops that may not risk an allocation failure).  No context: work is
+ * issued on `stream` (NULL = legacy default stream); v_dev is the volume,
+ * vals_dev (K floats) and pos1_dev (K x 3 ints, 1-based) are device outputs.
+ * The scratch lives in file-scope device arrays: at most 16,777,216 voxels
+ * (64 MiB, held on every GPU where the library's code is loaded until exit);
+ * larger volumes return TOMGPU_ERR_UNSUPPORTED.  The first call on a device
+ * sets the scratch up (looks up its device address) and should come before
+ * any stream capture on that device; the address is kept for the life of the
+ * process, so do not call this entry point again after cudaDeviceReset.
+ * Calls share the scratch: calls that overlap on the GPU race.  Errors:
+ * tomgpu_last_error(NULL).  This entry point has no counterpart in the
+ * reference. */
 int tomgpu_topk_noalloc_dev(void* stream, const float* v_dev, const int dims[3], int K, double radius,
                             float* vals_dev, int* pos1_dev);
 

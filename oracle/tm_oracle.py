@@ -57,7 +57,7 @@ def _load(name):
         path = os.path.join(REF_DIR, name)
         if not os.path.exists(path):
             raise FileNotFoundError(
-                f"{path} missing: run `make -C oracle` (reference libraries need the reference sources)")
+                f"{path} missing: run `make -C oracle oracle` (reference libraries: `make -C oracle ref REF=<TOM source tree>`)")
         _LIBS[name] = ctypes.CDLL(path)
     return _LIBS[name]
 

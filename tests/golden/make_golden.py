@@ -1,6 +1,6 @@
 """Generate tests/golden/reference_c.npz: outputs of the reference's own C
 routines, compiled from its sources into oracle/_ref by oracle/Makefile
-(`make -C oracle ref`, which needs the reference tree), on seeded inputs:
+(`make -C oracle ref REF=<TOM source tree>`), on seeded inputs:
 
 * rot3d (Sptrans/tom_rotatec.c:146-401): Euler and matrix mode, table and
   free angles, default and explicit centres, cubic and non-cubic volumes;
@@ -27,7 +27,7 @@ TABLE = [0, 30, 45, 60, 90, 120, 135, 150, 180, 210, 225, 240, 270, 300, 315, 33
 def main():
     import tm_oracle as O
     if not O.ref_available():
-        raise SystemExit("oracle/_ref not built: run `make -C oracle ref` with the reference sources present")
+        raise SystemExit("oracle/_ref not built: run `make -C oracle ref REF=<TOM source tree>`")
     rng = np.random.default_rng(2024)
     out = {}
     # rot3d

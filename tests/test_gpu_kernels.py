@@ -127,6 +127,27 @@ def test_topk_matches_oracle(gpu, oracle):
         assert tuple(pos[k]) == c and vals[k] == np.float32(v)
 
 
+def test_topk_radius_beyond_the_volume_and_rejected_radii(gpu, oracle):
+    """A radius beyond the volume's diagonal zeroes the whole volume after the
+    first peak (the zeroing box is clamped to the volume on each axis), so the
+    later rounds find 0 at (1, 1, 1), as tom_peak does on the zeroed matrix;
+    a radius far beyond the int range behaves the same.  Negative, NaN and
+    infinite radii are rejected before anything is launched."""
+    rng = np.random.default_rng(16)
+    vol = rng.standard_normal((20, 17, 12)).astype(np.float32)
+    diag = float(np.sqrt(20 ** 2 + 17 ** 2 + 12 ** 2))
+    for radius in (diag + 5.0, 1e6, 3e9):
+        vals, pos = gpu.topk_peaks(gpu.to_device(vol), 4, radius)
+        ref = oracle.topk_peaks(vol, 4, radius)
+        for k, (c, v) in enumerate(ref):
+            assert tuple(pos[k]) == c and vals[k] == np.float32(v), (radius, k)
+        assert list(vals[1:]) == [0.0, 0.0, 0.0] and all(tuple(p) == (1, 1, 1) for p in pos[1:])
+    for bad in (float("inf"), float("nan"), -1.0):
+        with pytest.raises(gpu.TomGpuError) as e:
+            gpu.topk_peaks(gpu.to_device(vol), 3, bad)
+        assert e.value.status == gpu._lib.TOMGPU_ERR_ARG, bad
+
+
 def test_weight3d_vs_reference(gpu, oracle):
     for dims, ang, th in [((16, 12, 10), [[0, 0, 0, 0], [-60, -20, 20, 60]], 16),
                           ((32, 32, 32), np.vstack([np.zeros(41), np.arange(-60, 61, 3)]), 64)]:

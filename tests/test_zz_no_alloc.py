@@ -1,9 +1,10 @@
 """The allocation-free top-K entry point (tomgpu_topk_noalloc_dev) gives the same
 peaks as the allocating tomgpu_topk_dev, on two calls in a row.
 
-Callers that cannot allocate device memory when they need peaks (inside CUDA
-graph capture, under a framework that owns the device memory) use this entry
-point; its scratch is a fixed 2^24-voxel device array.  The file name sorts
+Callers that cannot allocate device memory when they need peaks (under a
+framework that owns the device memory, in loops that may not risk an
+allocation failure) use this entry point; its scratch is a fixed 2^24-voxel
+device array.  The file name sorts
 last so a run that stops at the first failure has already run the rest."""
 import ctypes
 
@@ -55,3 +56,6 @@ def test_noalloc_topk_rejects_oversized_volume(gpu):
     st = lib.tomgpu_topk_noalloc_dev(None, _tptr(small), _cdims((512, 512, 256)), 4, 2.0, _tptr(vals), _tptr(pos))
     assert st == _lib.TOMGPU_ERR_UNSUPPORTED
     assert b"16777216" in lib.tomgpu_last_error(None)
+    for bad in (float("inf"), float("nan")):
+        st = lib.tomgpu_topk_noalloc_dev(None, _tptr(small), _cdims((2, 2, 2)), 4, bad, _tptr(vals), _tptr(pos))
+        assert st == _lib.TOMGPU_ERR_ARG, bad

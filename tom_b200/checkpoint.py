@@ -44,6 +44,19 @@ FORMAT = "tomgpu-search-checkpoint-1"
 RETRIES = 10
 
 
+
+def _fsync_dir(d: str) -> None:
+    """Flush a directory entry (the rename of a new checkpoint) to disk, so a
+    power loss after save() returns does not bring back the older checkpoint.
+    POSIX only: elsewhere directories cannot be opened and this does nothing."""
+    if os.name != "posix":
+        return
+    fd = os.open(d, os.O_RDONLY)
+    try:
+        os.fsync(fd)
+    finally:
+        os.close(fd)
+
 class CheckpointMismatch(RuntimeError):
     """The checkpoint on disk belongs to another search."""
 
@@ -125,6 +138,7 @@ class SearchCheckpoint:
                 if meta["cursor"] != int(cursor):
                     raise CheckpointCorrupt(f"{tmp}: cursor read back wrong")
                 os.replace(tmp, self.path)
+                _fsync_dir(os.path.dirname(os.path.abspath(self.path)))
                 return
             except (OSError, CheckpointCorrupt) as e:
                 last = e

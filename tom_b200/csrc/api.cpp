@@ -353,8 +353,8 @@ int tomgpu_peak(tomgpu_ctx* ctx, const float* v, const int dims[3], float* val, 
 int tomgpu_topk_dev(tomgpu_ctx* ctx, const float* v, const int dims[3], int K, double radius, float* vals,
                     int* pos1) {
     if (!ctx) return TOMGPU_ERR_ARG;
-    if (!v || !vals || !pos1 || !dims_ok(dims) || K < 0 || radius < 0)
-        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims, K or radius");
+    if (!v || !vals || !pos1 || !dims_ok(dims) || K < 0 || !(radius >= 0) || std::isinf(radius))
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims, K or radius (negative, NaN or infinite)");
     const long long n = numel(dims);
     if (n > 0xFFFFFFFFll) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "more than 2^32 voxels");
     if (K == 0) return TOMGPU_OK;
@@ -387,8 +387,8 @@ int tomgpu_topk_dev(tomgpu_ctx* ctx, const float* v, const int dims[3], int K, d
 
 int tomgpu_peak_radius_dev(tomgpu_ctx* ctx, float* v, const int dims[3], double radius, float* val, int pos1[3]) {
     if (!ctx) return TOMGPU_ERR_ARG;
-    if (!v || !val || !pos1 || !dims_ok(dims) || radius < 0)
-        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims or radius");
+    if (!v || !val || !pos1 || !dims_ok(dims) || !(radius >= 0) || std::isinf(radius))
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims or radius (negative, NaN or infinite)");
     if (numel(dims) > 0xFFFFFFFFll) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "more than 2^32 voxels");
     TG_TRY(use_device(ctx));
     TG_TRY(ensure_scratch(ctx, 64 + 4 * sizeof(int)));

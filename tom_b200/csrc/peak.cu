@@ -9,6 +9,9 @@
 // atomicMax per block reduce the keys.
 #include "peak.h"
 
+#include <algorithm>
+#include <cmath>
+
 namespace tg {
 
 __device__ __forceinline__ unsigned long long peak_key(float v, unsigned idx) {
@@ -58,11 +61,15 @@ __global__ void __launch_bounds__(256) k_argmax(const float* __restrict__ v, lon
     }
 }
 
-// Zero the ball of radius r around the peak recorded in *key and append the
-// peak (value, 1-based position) to the output lists.  One thread per voxel of
-// the (2r+1)^3 box.
+// Zero the ball of radius R around the peak recorded in *key and append the
+// peak (value, 1-based position) to the output lists.  The ball's bounding box
+// [p - r, p + r] (r = floor(R)) is clamped on each axis to the volume, as the
+// reference clamps its sub-block (Analysis/tom_peak.m:218-270); the launch
+// covers w = min(2r + 1, n) positions per axis, which always hold the clamped
+// range, and the distance test uses R^2 in double.  One thread per position.
 __global__ void k_zero_ball(float* __restrict__ v, int sx, int sy, int sz, const unsigned long long* key,
-                            int r, double r2, float* __restrict__ vals, int* __restrict__ pos, int k) {
+                            int r, double r2, int wx, int wy, int wz, float* __restrict__ vals,
+                            int* __restrict__ pos, int k) {
     const unsigned long long kk = *key;
     if (kk == 0ull) {  // nothing above the start value left
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -75,7 +82,6 @@ __global__ void k_zero_ball(float* __restrict__ v, int sx, int sy, int sz, const
     const int px = (int)(idx % (unsigned)sx);
     const int py = (int)((idx / (unsigned)sx) % (unsigned)sy);
     const int pz = (int)(idx / ((unsigned)sx * (unsigned)sy));
-    const int w = 2 * r + 1;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t == 0) {
         vals[k] = key_value(kk);
@@ -83,12 +89,14 @@ __global__ void k_zero_ball(float* __restrict__ v, int sx, int sy, int sz, const
         pos[3 * k + 1] = py + 1;
         pos[3 * k + 2] = pz + 1;
     }
-    if (t >= (long long)w * w * w) return;
-    const int dx = (int)(t % w) - r, dy = (int)((t / w) % w) - r, dz = (int)(t / ((long long)w * w)) - r;
-    const int x = px + dx, y = py + dy, z = pz + dz;
-    if (x < 0 || y < 0 || z < 0 || x >= sx || y >= sy || z >= sz) return;
-    if ((double)dx * dx + (double)dy * dy + (double)dz * dz <= r2)
-        v[x + (long long)sx * (y + (long long)sy * z)] = 0.f;
+    if (t >= (long long)wx * wy * wz) return;
+    // r <= max(n) keeps p +- r inside the int range
+    const int x = max(px - r, 0) + (int)(t % wx);
+    const int y = max(py - r, 0) + (int)((t / wx) % wy);
+    const int z = max(pz - r, 0) + (int)(t / ((long long)wx * wy));
+    if (x > min(px + r, sx - 1) || y > min(py + r, sy - 1) || z > min(pz + r, sz - 1)) return;
+    const double dx = x - px, dy = y - py, dz = z - pz;
+    if (dx * dx + dy * dy + dz * dz <= r2) v[x + (long long)sx * (y + (long long)sy * z)] = 0.f;
 }
 
 // tom_intpeak per axis: parabola through the 3 neighbours (a 3-point
@@ -132,14 +140,19 @@ cudaError_t argmax_key(const float* v, long long n, unsigned long long* d_key, c
 
 cudaError_t topk_rounds(float* work, const int dims[3], int K, double radius, unsigned long long* d_key,
                         float* d_vals, int* d_pos, cudaStream_t st, int64_t* launches) {
+    if (!(radius >= 0) || std::isinf(radius)) return cudaErrorInvalidValue;  // callers reject these first
     const long long n = (long long)dims[0] * dims[1] * dims[2];
-    const int r = radius > 0 ? (int)radius : 0;
-    const long long box = (long long)(2 * r + 1) * (2 * r + 1) * (2 * r + 1);
+    const int nmax = std::max(dims[0], std::max(dims[1], dims[2]));
+    // beyond the largest edge the clamped box is the whole volume on every axis
+    const int r = radius > (double)nmax ? nmax : (int)radius;
+    const int wx = std::min(2 * r + 1, dims[0]), wy = std::min(2 * r + 1, dims[1]), wz = std::min(2 * r + 1, dims[2]);
+    const long long box = (long long)wx * wy * wz;  // at most n <= 2^32 voxels
+    const unsigned blocks = (unsigned)((box + 255) / 256);
     for (int k = 0; k < K; ++k) {
         cudaError_t e = argmax_key(work, n, d_key, st);
         if (e) return e;
-        k_zero_ball<<<(unsigned)((box + 255) / 256), 256, 0, st>>>(work, dims[0], dims[1], dims[2], d_key, r,
-                                                                   radius * radius, d_vals, d_pos, k);
+        k_zero_ball<<<blocks, 256, 0, st>>>(work, dims[0], dims[1], dims[2], d_key, r, radius * radius, wx, wy, wz,
+                                            d_vals, d_pos, k);
         if ((e = cudaGetLastError())) return e;
         *launches += 2;
     }

@@ -1,22 +1,23 @@
 // Top-K peak search that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc at the moment they need peaks: code that
-// runs while a stream is being captured into a CUDA graph (allocation is not a
-// capturable operation), callers inside a host framework that owns the
-// device's memory through its own pool and forbids outside allocations (a
-// MATLAB MEX running next to gpuArray data, a serving process with a fixed
-// memory budget), and real-time loops that must not risk an allocation
-// failure mid-run.  For them this variant of tomgpu_topk_dev keeps its scratch
-// — a working copy of the volume that the peak rounds zero in place, and the
-// 64-bit arg-max key — in file-scope __device__ arrays, so every call uses
-// memory that already exists.
+// Some callers cannot call cudaMalloc at the moment they need peaks: callers
+// inside a host framework that owns the device's memory through its own pool
+// and forbids outside allocations (a MATLAB MEX running next to gpuArray
+// data, a serving process with a fixed memory budget), and real-time loops
+// that must not risk an allocation failure mid-run.  For them this variant of
+// tomgpu_topk_dev keeps its scratch — a working copy of the volume that the
+// peak rounds zero in place, and the 64-bit arg-max key — in file-scope
+// __device__ arrays, so every call uses memory that already exists.
 //
 // Limits and sharing: the working copy holds at most 2^24 voxels (64 MiB); the
 // arrays exist on every GPU where this code is loaded, until the process
 // exits.  All calls share them, so calls that overlap on the GPU (different
 // streams or host threads without ordering) race and corrupt each other.  The
-// first call on a device looks up the arrays' device addresses and must come
-// before any stream capture on that device.
+// first call on a device looks up the arrays' device addresses and should come
+// before any stream capture on that device.  The addresses are kept for the
+// life of the process: after cudaDeviceReset (which ends the context that held
+// the arrays) this entry point must not be called again in that process.
+#include <cmath>
 #include <mutex>
 #include <string>
 
@@ -65,8 +66,8 @@ int scratch_for_device(int dev, float** work, unsigned long long** key) {
 extern "C" int tomgpu_topk_noalloc_dev(void* stream, const float* v_dev, const int dims[3], int K, double radius,
                                        float* vals_dev, int* pos1_dev) {
     using namespace tg;
-    if (!v_dev || !dims || !vals_dev || !pos1_dev || K < 0 || !(radius >= 0))
-        return fail(nullptr, TOMGPU_ERR_ARG, "null pointer, negative K or bad radius");
+    if (!v_dev || !dims || !vals_dev || !pos1_dev || K < 0 || !(radius >= 0) || std::isinf(radius))
+        return fail(nullptr, TOMGPU_ERR_ARG, "null pointer, negative K or bad radius (negative, NaN or infinite)");
     if (dims[0] <= 0 || dims[1] <= 0 || dims[2] <= 0) return fail(nullptr, TOMGPU_ERR_ARG, "bad dims");
     const long long n = (long long)dims[0] * dims[1] * dims[2];
     if (n > kNoAllocMaxVoxels)
