@@ -57,12 +57,17 @@ def parse():
     p.add_argument("--rot-per-step", type=int, default=64)
     p.add_argument("--batch", type=int, default=0,
                    help="rotation batch; 0 = autotune over 8, 16, 32, 64 before the timed region")
+    p.add_argument("--path", type=int, default=0, choices=[0, 1, 2],
+                   help="kernel path of the plan: 0 fastest (TMA x-line tiles at the 512 x edge), 1 generic, "
+                        "2 as 0 with cp.async x-line tiles")
     p.add_argument("--e2e-rot", type=int, default=1024)
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-seconds", type=float, default=20.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--rescore-k", type=int, default=200, help="top-K peaks rescored in FP64 after the timed region")
+    p.add_argument("--rescore-k", type=int, default=None,
+                   help="top-K peaks rescored in FP64 after the timed region (default 200; 1000 for the "
+                        "928x928x464 workload)")
     p.add_argument("--learned-train", type=int, default=8, help="training tomograms of the learned_256 workload")
     p.add_argument("--learned-steps", type=int, default=400, help="timed training steps of the learned_256 workload")
     p.add_argument("--align-particles", type=int, default=40,
@@ -412,7 +417,7 @@ def main():
     cfg, grid, d, mask = make_workload(args.workload)
     nvox = int(np.prod(cfg["N"]))
     ctx = tb.default_context(local)
-    plan = tb.MatchPlan(cfg["N"], (cfg["T"],) * 3, batch=args.batch, ctx=ctx)
+    plan = tb.MatchPlan(cfg["N"], (cfg["T"],) * 3, batch=args.batch, ctx=ctx, path=args.path)
     plan.set_template(tb.to_device(d["template"], local), tb.to_device(mask, local))
     vol_dev = tb.to_device(d["tomo"], local)
     plan.set_volume(vol_dev)
@@ -476,6 +481,8 @@ def main():
 
     # accuracy: top-K peaks of the max-CC map rescored in FP64 by direct sums
     rescore = None
+    if args.rescore_k is None:
+        args.rescore_k = 1000 if args.workload == "exhaustive_928x928x464" else 200
     if args.rescore_k > 0 and rank == 0:
         K = args.rescore_k
         vals, pos, aidx = tb.pick_peaks(cc, idx, K, cfg["T"] / 2, ctx)
@@ -512,6 +519,7 @@ def main():
             vol = tomo_h
             prm = _lib.MatchParams()
             prm.batch = args.batch
+            prm.path = args.path
             ectx.check(_lib.lib().tomgpu_match(
                 ectx.handle, vol.ctypes.data, tb.tom._cdims(cfg["N"]), d["template"].ctypes.data,
                 tb.tom._cdims((cfg["T"],) * 3), mask.ctypes.data, None,
@@ -543,6 +551,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": args.workload, "tomogram": list(cfg["N"]), "template": cfg["T"],
                            "angles": len(grid), "rot_per_step": rps, "rotation_batch": args.batch,
+                           "kernel_path": args.path,
                            "batch_autotune_ms_per_rotation": tune,
                            "parallelism": f"angle-partitioned x{world}",
                            "l2": "inputs larger than L2 (tomogram spectrum %d MB, per-batch spectra %.1f GB)" % (
@@ -552,6 +561,9 @@ def main():
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                              "algorithmic_bytes_per_launch": ab, "avg_launch_ms": avg_s * 1e3},
                 "kernel_share": shares, "fp64_rescore": rescore,
+                "seconds_per_search": {"device": len(grid) * nvox * world / value,
+                                       "e2e": len(grid) * nvox * world / e2e["value"] if e2e else None,
+                                       "note": "the whole angle grid at this rate, one template"},
                 "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk}
         print(json.dumps(line), flush=True)
     if dist:

@@ -22,7 +22,7 @@ extern "C" {
 typedef enum {
     TOMGPU_OK = 0,
     TOMGPU_ERR_ARG = 1,         /* invalid argument: null pointer, size, mode */
-    TOMGPU_ERR_UNSUPPORTED = 2, /* size the kernels are not built for (FFT length) */
+    TOMGPU_ERR_UNSUPPORTED = 2, /* size beyond the FFT line limits or another fixed limit */
     TOMGPU_ERR_OOM = 3,         /* device allocation failed */
     TOMGPU_ERR_CUDA = 4,        /* CUDA runtime error (details: tomgpu_last_error) */
     TOMGPU_ERR_STATE = 5,       /* call order: e.g. run before a volume is set */
@@ -191,15 +191,20 @@ typedef struct {
     int batch;          /* rotations per batch; 0 = the largest of 64, 32, 16 whose
                            per-batch buffers fit in half the free device memory, else 8 */
     int wedge_fp64;     /* reserved, 0 */
-    int path;           /* 0: fastest kernels for the sizes; 1: generic kernels only */
+    int path;           /* 0: fastest kernels for the sizes; 1: generic kernels only;
+                           2: as 0, but the x-line kernel of the 512 x edge loads its tiles
+                           with per-thread cp.async instead of TMA (for comparison) */
     int reserved[5];
 } tomgpu_match_params;
 
 /* A matching plan for one volume size and one template size.  It holds the
  * tomogram spectrum, the FP64 local statistics and per-batch workspaces.
- * Volume and template sizes must be FFT lengths the library is built for
- * (8,12,16,20,24,32,40,48,64,80,96,128,160,192,232,256,464,512,928 per axis; the
- * template edge along x must keep nx/2 in that list).  params may be NULL. */
+ * Any volume and template edges (odd ones included) within the FFT line
+ * limits: every edge up to 3528 voxels, and edges whose prime factors are all
+ * in {2,3,5,7,11,13} up to 7150; the template no larger than the volume on any
+ * axis.  Edges 128, 256, 464, 512, 928 (and others of the compiled list) run
+ * dedicated kernels, every other edge the run-time line engine.  Outside
+ * these limits: TOMGPU_ERR_UNSUPPORTED.  params may be NULL. */
 int tomgpu_match_plan_create(tomgpu_ctx* ctx, const int vol_dims[3], const int tmpl_dims[3],
                              const tomgpu_match_params* params, tomgpu_match_plan** out);
 int tomgpu_match_plan_destroy(tomgpu_match_plan* plan);
@@ -375,6 +380,16 @@ int tomgpu_corr3d_peaks_dev(tomgpu_ctx* ctx, const int n[3], const float* const*
                             const float* mask, const tomgpu_wedge_spec* wedge_t,
                             const tomgpu_wedge_spec* wedge_p, const float* mask_cc, double* peak,
                             double* val, int32_t* angle_idx);
+
+/* tomgpu_corr3d_peaks_dev with every volume (templates, particles, mask,
+ * wedge volumes, mask_cc) in host memory: the form the tom_mex_corr3d
+ * gateway calls (Oscar3/c++Picker/src/mex/tom_mex_corr3d.cpp:53-806, whose
+ * volumes are MATLAB arrays or EM files read on the host).  The volumes are
+ * copied to the device for the call; outputs as tomgpu_corr3d_peaks_dev. */
+int tomgpu_corr3d_peaks(tomgpu_ctx* ctx, const int n[3], const float* const* templates, int nt,
+                        const float* const* particles, int np, const double* angles_deg, int nang,
+                        const float* mask, const tomgpu_wedge_spec* wedge_t, const tomgpu_wedge_spec* wedge_p,
+                        const float* mask_cc, double* peak, double* val, int32_t* angle_idx);
 
 /* ---------------------------------------------------- learned proposer
  * Training and inference kernels of the candidate proposer (a dilated 3-D

@@ -63,3 +63,55 @@ def test_corr3d_recovers_rotation(gpu, oracle):
     assert out[0, 0]["angle_idx"] == 3
     assert tuple(out[0, 0]["peak"].astype(int)) == (0, 0, 0)
     assert out[0, 0]["ncc_val"] > 0.95
+
+
+def test_corr3d_host_entry_point_equals_device_one(gpu, oracle):
+    """tomgpu_corr3d_peaks (the host-volume form the tom_mex_corr3d gateway
+    calls) gives the device form's results bit for bit, with a mask, wedge
+    volumes for the templates, simple wedges for the particles and a peak mask."""
+    import ctypes
+    from tom_b200 import _lib
+    from tom_b200.tom import _cdims
+    n = (20, 18, 16)
+    temps, parts, rng = _data(63, n, 2, 3)
+    angles = rng.uniform(-180, 180, (4, 3))
+    mask = gpu.cpp_spheremask(n, 7)
+    mcc = gpu.cpp_spheremask(n, 3)
+    w1 = oracle.av3_wedge(n, -60, 60).astype(np.float32)
+    ref = gpu.tom_corr3d(temps, parts, angles, mask=mask, wedge_ref=w1, wedge_part=[40.0, None, 55.0], mask_cc=mcc)
+    host = [np.asfortranarray(np.asarray(v, np.float32)) for v in temps + parts + [mask, mcc, w1]]
+    ptr = lambda a: ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+    tp = (ctypes.c_void_p * 2)(*[ptr(h).value for h in host[:2]])
+    pp = (ctypes.c_void_p * 3)(*[ptr(h).value for h in host[2:5]])
+    wt = (_lib.WedgeSpec * 2)()
+    for i in range(2):
+        wt[i].kind, wt[i].volume = 2, ptr(host[7])
+    wp = (_lib.WedgeSpec * 3)()
+    wp[0].kind, wp[0].angle_deg = 1, 40.0
+    wp[1].kind = 0
+    wp[2].kind, wp[2].angle_deg = 1, 55.0
+    ang = np.ascontiguousarray(angles, np.float64)
+    peak = np.zeros((3, 2, 3), np.float64)
+    val = np.zeros((3, 2), np.float64)
+    idx = np.zeros((3, 2), np.int32)
+    ctx = gpu.default_context()
+    ctx.check(_lib.lib().tomgpu_corr3d_peaks(ctx.handle, _cdims(n), tp, 2, pp, 3, ang.ctypes.data_as(_lib.c_double_p),
+                                             len(ang), ptr(host[5]), wt, wp, ptr(host[6]),
+                                             peak.ctypes.data_as(_lib.c_double_p), val.ctypes.data_as(_lib.c_double_p),
+                                             idx.ctypes.data_as(_lib.c_int_p)))
+    for i in range(2):
+        for j in range(3):
+            r = ref[i, j]
+            assert idx[j, i] == r["angle_idx"] and val[j, i] == r["ncc_val"]
+            assert np.array_equal(peak[j, i], r["peak"])
+
+
+def test_corr3d_odd_box(gpu, oracle):
+    """An odd box (the FFT lengths 25, 21 and 19, 19 through Bluestein)."""
+    n = (25, 21, 19)
+    temps, parts, rng = _data(64, n, 1, 2)
+    angles = rng.uniform(-180, 180, (4, 3))
+    out = gpu.tom_corr3d(temps, parts, angles, mask=gpu.cpp_spheremask(n, 8), wedge_ref=30.0, wedge_part=45.0)
+    ref = oracle.corr3d_peaks(temps, parts, angles, mask=gpu.cpp_spheremask(n, 8), wedge_t=[("simple", 30.0)],
+                              wedge_p=[("simple", 45.0)] * 2)
+    _compare(out, ref)

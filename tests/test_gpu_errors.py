@@ -35,9 +35,9 @@ def _search(gpu, ctx, vol, tmpl, mask, angles):
 def test_unsupported_sizes_and_bad_batch(gpu, oracle):
     L = gpu._lib
     cases = [
-        ((100, 64, 64), (16, 16, 16), 4, L.TOMGPU_ERR_UNSUPPORTED, "not supported"),  # 100: no kernel length
+        ((3637, 64, 64), (16, 16, 16), 4, L.TOMGPU_ERR_UNSUPPORTED, "not supported"),  # beyond the line limits
         ((32, 32, 32), (48, 48, 48), 4, L.TOMGPU_ERR_UNSUPPORTED, "not supported"),  # template > volume
-        ((48, 40, 32), (17, 16, 16), 4, L.TOMGPU_ERR_UNSUPPORTED, "not supported"),  # 17: no template length
+        ((48, 40, 32), (17, 16, 49), 4, L.TOMGPU_ERR_UNSUPPORTED, "not supported"),  # template > volume in z
         ((48, 40, 32), (16, 16, 16), 5000, L.TOMGPU_ERR_ARG, "batch"),
     ]
     vol, tmpl, mask, angles = _inputs(oracle)
@@ -107,7 +107,7 @@ def test_match_host_errors_and_empty_angle_list(gpu, oracle):
     vol, tmpl, mask, angles = _inputs(oracle)
     ctx = gpu.Context(0)
     try:
-        bad = np.zeros((100, 64, 64), np.float32)
+        bad = np.zeros((3637, 8, 8), np.float32)  # an edge beyond the FFT line limits
         with pytest.raises(gpu.TomGpuError) as e:
             gpu.match_host(bad, tmpl, mask, angles, batch=4, ctx=ctx)
         assert e.value.status == L.TOMGPU_ERR_UNSUPPORTED

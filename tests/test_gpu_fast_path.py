@@ -124,3 +124,36 @@ def test_autotune_keeps_results(gpu, oracle):
     assert np.abs(gpu.from_device(cc) - ref_cc).max() <= 1e-6 * np.abs(ref_cc).max()
     assert (gpu.from_device(idx) != ref_idx).mean() < 1e-3
     plan.close()
+
+
+@pytest.mark.parametrize("shape,batch", [((512, 40, 24), 5), ((512, 64, 32), 16), ((512, 512, 8), 3)])
+def test_tma_x_lines_equal_cp_async_x_lines(gpu, oracle, shape, batch):
+    """The 512 x edge's x-line kernel with TMA tile loads (the default) gives
+    the cp.async kernel's results bit for bit (the same arithmetic; a y edge
+    that is not a multiple of 16 exercises the TMA's zero fill), and meets the
+    oracle's parity bar."""
+    import torch
+    rng = np.random.default_rng(shape[1])
+    vol = rng.standard_normal(shape).astype(np.float32)
+    T = 16
+    tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
+    mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
+    angles = oracle.av3_angle_grid((0, 0, 0), (30, 30, 30), (330, 330, 180))[:11]
+    out = {}
+    for path in (0, 2):
+        plan = gpu.MatchPlan(vol.shape, tmpl.shape, batch=batch, path=path)
+        plan.set_template(gpu.to_device(tmpl), gpu.to_device(mask))
+        plan.set_volume(gpu.to_device(vol))
+        cc, idx = plan.new_results()
+        plan.run(angles, cc, idx)
+        plan.ctx.synchronize()
+        torch.cuda.synchronize()
+        out[path] = gpu.from_device(cc).copy(), gpu.from_device(idx).copy()
+        plan.close()
+    assert np.array_equal(out[0][0], out[2][0]) and np.array_equal(out[0][1], out[2][1])
+    if shape[1] <= 64:
+        ref_cc, ref_idx, ref_2 = oracle.find_template(vol, tmpl, mask, angles, keep_second=True)
+        scale = np.abs(ref_cc).max()
+        assert np.abs(out[0][0] - ref_cc).max() <= REL * scale
+        sep = (ref_cc - ref_2) > 2 * REL * scale
+        assert np.array_equal(out[0][1][sep], ref_idx[sep])

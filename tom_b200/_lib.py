@@ -114,6 +114,10 @@ _SIGS = {
                                                ctypes.POINTER(c_void_p), ctypes.c_int, c_double_p, ctypes.c_int,
                                                c_void_p, ctypes.POINTER(WedgeSpec), ctypes.POINTER(WedgeSpec),
                                                c_void_p, c_double_p, c_double_p, c_int_p]),
+    "tomgpu_corr3d_peaks": (ctypes.c_int, [c_void_p, c_int_p, ctypes.POINTER(c_void_p), ctypes.c_int,
+                                           ctypes.POINTER(c_void_p), ctypes.c_int, c_double_p, ctypes.c_int,
+                                           c_void_p, ctypes.POINTER(WedgeSpec), ctypes.POINTER(WedgeSpec),
+                                           c_void_p, c_double_p, c_double_p, c_int_p]),
     "tomgpu_cnn_conv3d_fwd_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_void_p, c_void_p,
                                                  ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p]),
     "tomgpu_cnn_conv3d_bwd_data_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_void_p,

@@ -337,7 +337,6 @@ int PeakAnalysis::create(tomgpu_ctx* c, const int vol[3], const int tm[3], const
     for (int d = 0; d < 3; ++d)
         if (!fft_length_supported(N[d]) || !fft_length_supported(T[d]) || T[d] > N[d])
             return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "peak-analysis sizes not supported by the FFT kernels");
-    if (N[0] % 2) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "the map's x edge must be even");
     nvox = (long long)N[0] * N[1] * N[2];
     hs = (long long)(N[0] / 2 + 1) * N[1] * N[2];
     tn = (long long)T[0] * T[1] * T[2];

@@ -545,6 +545,70 @@ int tomgpu_corr3d_peaks_dev(tomgpu_ctx* ctx, const int n[3], const float* const*
                         val, angle_idx);
 }
 
+int tomgpu_corr3d_peaks(tomgpu_ctx* ctx, const int n[3], const float* const* templates, int nt,
+                        const float* const* particles, int np, const double* angles_deg, int nang, const float* mask,
+                        const tomgpu_wedge_spec* wedge_t, const tomgpu_wedge_spec* wedge_p, const float* mask_cc,
+                        double* peak, double* val, int32_t* angle_idx) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!dims_ok(n) || nt < 1 || np < 1 || nang < 1 || !templates || !particles || !angles_deg || !peak || !val ||
+        !angle_idx)
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer, bad dims or empty input");
+    for (int t = 0; t < nt; ++t)
+        if (!templates[t]) return fail(ctx, TOMGPU_ERR_ARG, "null template");
+    for (int p = 0; p < np; ++p)
+        if (!particles[p]) return fail(ctx, TOMGPU_ERR_ARG, "null particle");
+    TG_TRY(use_device(ctx));
+    // every host volume (templates, particles, masks, wedge volumes) goes into
+    // one device buffer; the device entry point then gets pointers into it
+    const long long nv = numel(n);
+    std::vector<const float*> src;
+    for (int t = 0; t < nt; ++t) src.push_back(templates[t]);
+    for (int p = 0; p < np; ++p) src.push_back(particles[p]);
+    const int i_mask = mask ? (int)src.size() : -1;
+    if (mask) src.push_back(mask);
+    const int i_mcc = mask_cc ? (int)src.size() : -1;
+    if (mask_cc) src.push_back(mask_cc);
+    std::vector<tomgpu_wedge_spec> wt, wp;
+    std::vector<int> wt_i, wp_i;
+    auto wedges = [&](const tomgpu_wedge_spec* w, int cnt, std::vector<tomgpu_wedge_spec>& out,
+                      std::vector<int>& at) -> bool {
+        if (!w) return true;
+        for (int i = 0; i < cnt; ++i) {
+            if (w[i].kind < 0 || w[i].kind > 2 || (w[i].kind == TOMGPU_WEDGE_VOLUME && !w[i].volume)) return false;
+            out.push_back(w[i]);
+            at.push_back(w[i].kind == TOMGPU_WEDGE_VOLUME ? (int)src.size() : -1);
+            if (w[i].kind == TOMGPU_WEDGE_VOLUME) src.push_back(w[i].volume);
+        }
+        return true;
+    };
+    if (!wedges(wedge_t, nt, wt, wt_i)) return fail(ctx, TOMGPU_ERR_ARG, "bad template wedge");
+    if (!wedges(wedge_p, np, wp, wp_i)) return fail(ctx, TOMGPU_ERR_ARG, "bad particle wedge");
+    float* d = nullptr;
+    if (cudaMalloc(&d, sizeof(float) * nv * src.size()) != cudaSuccess)
+        return cuda_fail(ctx, cudaErrorMemoryAllocation, "corr3d input buffer");
+    int rc = TOMGPU_OK;
+    for (size_t i = 0; i < src.size() && !rc; ++i) {
+        cudaError_t e = cudaMemcpyAsync(d + nv * i, src[i], sizeof(float) * nv, cudaMemcpyHostToDevice, ctx->stream);
+        if (e) rc = cuda_fail(ctx, e, "corr3d upload");
+    }
+    if (!rc) {
+        std::vector<const float*> tp(nt), pp(np);
+        for (int t = 0; t < nt; ++t) tp[t] = d + nv * t;
+        for (int p = 0; p < np; ++p) pp[p] = d + nv * (nt + p);
+        for (size_t i = 0; i < wt.size(); ++i)
+            if (wt_i[i] >= 0) wt[i].volume = d + nv * wt_i[i];
+        for (size_t i = 0; i < wp.size(); ++i)
+            if (wp_i[i] >= 0) wp[i].volume = d + nv * wp_i[i];
+        rc = tomgpu_corr3d_peaks_dev(ctx, n, tp.data(), nt, pp.data(), np, angles_deg, nang,
+                                     i_mask >= 0 ? d + nv * i_mask : nullptr, wedge_t ? wt.data() : nullptr,
+                                     wedge_p ? wp.data() : nullptr, i_mcc >= 0 ? d + nv * i_mcc : nullptr, peak, val,
+                                     angle_idx);
+    }
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    return rc;
+}
+
 int tomgpu_analyze_psr_dev(tomgpu_ctx* ctx, const float* peak, const int map_dims[3], const int tmpl_dims[3],
                            float* out) {
     if (!ctx) return TOMGPU_ERR_ARG;
@@ -563,9 +627,8 @@ int tomgpu_template_autocorr_dev(tomgpu_ctx* ctx, const float* t, const int tmpl
     if (!ctx) return TOMGPU_ERR_ARG;
     if (!t || !out || !dims_ok(tmpl_dims)) return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
     TG_TRY(use_device(ctx));
-    // the map-sized part is not used: size it at the template (x edge even for the half spectrum)
+    // the map-sized part is not used: size it at the template
     int nd[3] = {tmpl_dims[0], tmpl_dims[1], tmpl_dims[2]};
-    if (nd[0] % 2) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "template x edge must be even");
     PeakAnalysis an;
     TG_TRY(an.create(ctx, nd, tmpl_dims, nullptr));
     TG_TRY(an.autocorr(t, out));
@@ -625,8 +688,9 @@ static int fft_dims_ok(tomgpu_ctx* ctx, const int dims[3]) {
     if (!dims_ok(dims)) return fail(ctx, TOMGPU_ERR_ARG, "bad dims");
     for (int d = 0; d < 3; ++d)
         if (dims[d] > 1 && !fft_length_supported(dims[d]))
-            return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "FFT length " + std::to_string(dims[d]) + " not built");
-    if (!fft_length_supported(dims[0])) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "x length not built");
+            return fail(ctx, TOMGPU_ERR_UNSUPPORTED,
+                        "FFT length " + std::to_string(dims[d]) +
+                            " beyond the line limits (every length up to 3528; {2,3,5,7,11,13}-smooth up to 7150)");
     return TOMGPU_OK;
 }
 
@@ -676,9 +740,11 @@ int tomgpu_match_plan_create(tomgpu_ctx* ctx, const int vol[3], const int tm[3],
     if (!out || !dims_ok(vol) || !dims_ok(tm)) return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
     *out = nullptr;
     if (params && params->batch < 0) return fail(ctx, TOMGPU_ERR_ARG, "negative batch");
+    if (params && (params->path < 0 || params->path > 2)) return fail(ctx, TOMGPU_ERR_ARG, "path is 0, 1 or 2");
     TG_TRY(use_device(ctx));
     tomgpu_match_plan* p = new tomgpu_match_plan();
     int rc = p->p.create(ctx, vol, tm, params ? params->batch : 0, params ? params->path == 1 : false);
+    p->p.no_tma = params && params->path == 2;
     if (rc) {
         delete p;
         return rc;

@@ -9,8 +9,10 @@
 // template-sized wedge filter, and the tom_fourier entry points.
 #include "fft3d.h"
 #include "fft_engine.cuh"
+#include "fft_rt.cuh"
 #include "twiddles.h"
 
+#include <algorithm>
 #include <cstdio>
 
 namespace tg {
@@ -128,6 +130,101 @@ static cudaError_t launch_lines_t(const void* in, void* out, const LineGeom& gi,
     return cudaGetLastError();
 }
 
+// Lines of any length: the run-time engine (fft_rt.cuh), NL lines per block
+// in two ping-pong buffers of pitch LS.
+constexpr int kRtMaxLines = 64;
+
+template <int DIR, int MODE, typename C>
+__global__ void __launch_bounds__(256) k_fft_lines_rt(const void* in, void* out, LineGeom gi, LineGeom go,
+                                                      tgrt::Plan p, tgrt::Tabs<C> tabs, int NL, int LS,
+                                                      double scale, long nlines) {
+    typedef typename CTraits<C>::R Rt;
+    constexpr int NT = 256;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s = reinterpret_cast<C*>(smem_raw);
+    C* s2 = s + (size_t)NL * LS;
+    __shared__ long offs_i[kRtMaxLines], offs_o[kRtMaxLines];
+    const int tid = threadIdx.x;
+    const int L = p.L;
+    const long line0 = (long)blockIdx.x * NL;
+    for (int l = tid; l < NL; l += NT) {
+        const long gl = line0 + l;
+        offs_i[l] = (gl % gi.cnt0) * gi.s0 + (gl / gi.cnt0) * gi.s1;
+        offs_o[l] = (gl % go.cnt0) * go.s0 + (gl / go.cnt0) * go.s1;
+    }
+    __syncthreads();
+    const Rt* rin = reinterpret_cast<const Rt*>(in);
+    const C* cin = reinterpret_cast<const C*>(in);
+    for (int i = tid; i < NL * L; i += NT) {
+        int l, e;
+        if (gi.es == 1) { l = i / L; e = i - l * L; }
+        else { e = i / NL; l = i - e * NL; }
+        const long gl = line0 + l;
+        C v = CTraits<C>::make(0, 0);
+        if (gl < nlines) {
+            const long off = offs_i[l];
+            if (MODE == FFT_R2C) v = CTraits<C>::make(rin[off + e * gi.es], 0);
+            else if (MODE == FFT_C2R) v = e <= L / 2 ? cin[off + e * gi.es] : cconj(cin[off + (L - e) * gi.es]);
+            else v = cin[off + e * gi.es];
+        }
+        s[l * LS + e] = v;
+    }
+    __syncthreads();
+    const C* res = tgrt::fft<DIR>(s, s2, p, tabs, NL, LS, tid, NT);
+    Rt* rout = reinterpret_cast<Rt*>(out);
+    C* cout = reinterpret_cast<C*>(out);
+    const Rt sc = (Rt)scale;
+    for (int i = tid; i < NL * L; i += NT) {
+        int l, e;
+        if (go.es == 1) { l = i / L; e = i - l * L; }
+        else { e = i / NL; l = i - e * NL; }
+        const long gl = line0 + l;
+        if (gl >= nlines) continue;
+        const long off = offs_o[l];
+        const C v = res[l * LS + e];
+        if (MODE == FFT_R2C) {
+            if (e <= L / 2) cout[off + e * go.es] = cscale(v, sc);
+        } else if (MODE == FFT_C2R) {
+            rout[off + e * go.es] = v.x * sc;
+        } else {
+            cout[off + e * go.es] = cscale(v, sc);
+        }
+    }
+}
+
+// Lines per block for a run-time plan: as many as fit a 48 KB budget (at
+// least one, at most 64 and at most the number of lines).
+static int rt_lines_per_block(int LS, size_t elem, long nlines) {
+    const size_t per = 2 * (size_t)LS * elem;
+    long nl = (long)std::max<size_t>(1, (48 * 1024) / per);
+    nl = std::min<long>(nl, kRtMaxLines);
+    nl = std::min<long>(nl, std::max<long>(nlines, 1));
+    return (int)nl;
+}
+
+template <int DIR, int MODE, typename C>
+static cudaError_t launch_lines_rt(int L, const void* in, void* out, const LineGeom& gi, const LineGeom& go,
+                                   long nlines, double scale, cudaStream_t st) {
+    tgrt::Plan p;
+    if (!rt_plan(L, (int)sizeof(C), &p)) return cudaErrorInvalidValue;
+    tgrt::Tabs<C> tabs;
+    if (!rt_tabs<C>(p, &tabs)) return cudaErrorMemoryAllocation;
+    if (nlines <= 0) return cudaSuccess;
+    const int LS = tgrt::pitch(p);
+    const int NL = rt_lines_per_block(LS, sizeof(C), nlines);
+    const size_t smem = 2 * (size_t)NL * LS * sizeof(C);
+    auto kern = k_fft_lines_rt<DIR, MODE, C>;
+    // above 40 KB the kernel's static arrays could take the block past the
+    // 48 KB a launch gets without opting in
+    if (smem > 40 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e) return e;
+    }
+    const long blocks = (nlines + NL - 1) / NL;
+    kern<<<(unsigned)blocks, 256, smem, st>>>(in, out, gi, go, p, tabs, NL, LS, scale, nlines);
+    return cudaGetLastError();
+}
+
 template <int DIR, int MODE, typename C>
 static cudaError_t dispatch_len(int L, const void* in, void* out, const LineGeom& gi, const LineGeom& go,
                                 long nlines, double scale, cudaStream_t st) {
@@ -136,19 +233,18 @@ static cudaError_t dispatch_len(int L, const void* in, void* out, const LineGeom
     switch (L) {
         TG_CASE(8) TG_CASE(12) TG_CASE(16) TG_CASE(20) TG_CASE(24) TG_CASE(32) TG_CASE(40) TG_CASE(48) TG_CASE(64)
         TG_CASE(80) TG_CASE(96) TG_CASE(128) TG_CASE(160) TG_CASE(192) TG_CASE(232)
-        TG_CASE(256) TG_CASE(464) TG_CASE(512) TG_CASE(928)
-        default: return cudaErrorInvalidValue;
+        TG_CASE(256) TG_CASE(464) TG_CASE(512) TG_CASE(928) TG_CASE(1024)
+        default: return launch_lines_rt<DIR, MODE, C>(L, in, out, gi, go, nlines, scale, st);
     }
 #undef TG_CASE
 }
 
+// Every length whose run-time plan fits one block in FP64 (the set-up
+// transforms run in FP64): every L up to 3528, and beyond that the lengths
+// whose prime factors are all in {2, 3, 5, 7, 11, 13}, up to 7150.
 bool fft_length_supported(int L) {
-    switch (L) {
-        case 8: case 12: case 16: case 20: case 24: case 32: case 40: case 48: case 64: case 80: case 96:
-        case 128: case 160: case 192: case 232: case 256: case 464: case 512: case 928:
-            return true;
-        default: return false;
-    }
+    tgrt::Plan p;
+    return rt_plan(L, (int)sizeof(double2), &p);
 }
 
 template <typename C>

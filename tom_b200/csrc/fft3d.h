@@ -2,6 +2,9 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "twiddles.h"
+#include "fft_plan.h"
+
 namespace tg {
 
 enum { FFT_C2C = 0, FFT_R2C = 1, FFT_C2R = 2 };
@@ -16,6 +19,7 @@ struct LineGeom {
     long s1;
 };
 
+// Any line length the library transforms (compile-time or run-time plan).
 bool fft_length_supported(int L);
 
 // One batched FFT of length L along lines (in and out may alias: each block

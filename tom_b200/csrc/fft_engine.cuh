@@ -20,7 +20,7 @@ template <int... Rs> struct seq {};
 template <int A, int... Rs> struct seq_first { static constexpr int value = A; };
 
 // Radix plans: odd radices last so that every stride NS before them is a power
-// of two.  Only lengths listed here are supported (the host checks).
+// of two.  Other lengths run on the run-time engine (fft_rt.cuh).
 template <int L> struct Radices;
 template <> struct Radices<8> { typedef seq<8> type; };
 template <> struct Radices<12> { typedef seq<4, 3> type; };
@@ -41,6 +41,7 @@ template <> struct Radices<256> { typedef seq<16, 16> type; };
 template <> struct Radices<464> { typedef seq<16, 29> type; };
 template <> struct Radices<512> { typedef seq<8, 8, 8> type; };
 template <> struct Radices<928> { typedef seq<8, 4, 29> type; };
+template <> struct Radices<1024> { typedef seq<16, 8, 8> type; };
 
 template <typename C> TG_D C ldtw(const C* tw, int m) { return __ldg(tw + m); }
 

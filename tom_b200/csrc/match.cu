@@ -404,8 +404,8 @@ template <typename K> static void raise_smem(K kern, size_t smem) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-#define TG_HOT_LENGTHS(X) X(16) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256) X(464) X(512) X(928)
-#define TG_HALF_LENGTHS(X) X(8) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(232) X(256) X(464)
+#define TG_HOT_LENGTHS(X) X(16) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256) X(464) X(512) X(928) X(1024)
+#define TG_HALF_LENGTHS(X) X(8) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(232) X(256) X(464) X(512)
 
 static bool hot_len(int L) {
     switch (L) {
@@ -427,13 +427,22 @@ static bool half_len(int L) {
     }
 }
 
+// Any volume and template edge MATLAB's fftn takes, within the line-length
+// limits of the FFT engines (fft_length_supported; lengths without a
+// compile-time kernel run on match_rt.cu's kernels); the template no larger
+// than the volume.
 bool match_sizes_supported(const int N[3], const int T[3]) {
-    for (int d = 0; d < 3; ++d)
-        if (!hot_len(N[d]) || T[d] > N[d] || T[d] < 1) return false;
-    if (N[0] % 2 || !half_len(N[0] / 2)) return false;
-    if (!fft_length_supported(T[0]) || !fft_length_supported(T[1]) || !fft_length_supported(T[2])) return false;
+    for (int d = 0; d < 3; ++d) {
+        if (T[d] < 1 || T[d] > N[d]) return false;
+        if (!fft_length_supported(N[d]) || !fft_length_supported(T[d])) return false;
+        if (!hot_len(N[d]) && !match_rt_length_ok(N[d])) return false;
+    }
+    if (!(N[0] % 2 == 0 && half_len(N[0] / 2)) && !match_rt_length_ok(N[0])) return false;
     return true;
 }
+
+// the x edges the compile-time c2r kernels (half-length packing) cover
+static bool c2r_compiled(int NX) { return NX % 2 == 0 && half_len(NX / 2); }
 
 static cudaError_t launch_spec_x(int NX, const float* t2, const float* mask, float2* A, const int T[3], int d0x,
                                  int nb, double* tsum, cudaStream_t st) {
@@ -450,7 +459,7 @@ static cudaError_t launch_spec_x(int NX, const float* t2, const float* mask, flo
     }
         TG_HOT_LENGTHS(C_)
 #undef C_
-        default: return cudaErrorInvalidValue;
+        default: return launch_spec_x_rt(NX, t2, mask, A, T, d0x, nb, tsum, st);
     }
 }
 
@@ -467,7 +476,7 @@ static cudaError_t launch_spec_z(int NZ, const float2* A, float2* Z, const int T
     }
         TG_HOT_LENGTHS(C_)
 #undef C_
-        default: return cudaErrorInvalidValue;
+        default: return launch_spec_z_rt(NZ, A, Z, T, d0z, nh1, nb, st);
     }
 }
 
@@ -485,7 +494,7 @@ static cudaError_t launch_corr_y(int NY, const float2* fimg, const float2* Z, fl
     }
         TG_HOT_LENGTHS(C_)
 #undef C_
-        default: return cudaErrorInvalidValue;
+        default: return launch_corr_y_rt(NY, fimg, Z, Q, Ty, d0y, ncols, nb, st);
     }
 }
 
@@ -501,7 +510,7 @@ static cudaError_t launch_inv_z(int NZ, const float2* Q, float2* H, int Ny, int 
     }
         TG_HOT_LENGTHS(C_)
 #undef C_
-        default: return cudaErrorInvalidValue;
+        default: return launch_inv_z_rt(NZ, Q, H, Ny, nh1, nb, st);
     }
 }
 
@@ -605,7 +614,13 @@ int MatchPlan::create(tomgpu_ctx* c, const int vol[3], const int tm[3], int batc
     // twiddle tables are built now so that later calls allocate nothing
     const int lens[] = {N[0], N[1], N[2], N[0] / 2, T[0], T[1], T[2]};
     for (int L : lens) {
-        if (!twiddle_table<float2>(L) || !twiddle_table<double2>(L))
+        if (L < 1) continue;
+        tgrt::Plan p32, p64;
+        tgrt::Tabs<float2> t32;
+        tgrt::Tabs<double2> t64;
+        if (!twiddle_table<float2>(L) || !twiddle_table<double2>(L) ||
+            (rt_plan(L, (int)sizeof(float2), &p32) && !rt_tabs<float2>(p32, &t32)) ||
+            (rt_plan(L, (int)sizeof(double2), &p64) && !rt_tabs<double2>(p64, &t64)))
             return fail(ctx, TOMGPU_ERR_CUDA, "twiddle table allocation failed");
     }
     return TOMGPU_OK;
@@ -693,8 +708,8 @@ int MatchPlan::autotune(const float* eulers, int R, const int* cands, int nc, in
         const int nb = cands[c];
         if (nb <= 0 || nb > 4096) continue;
         size_t fr = 0, tot = 0;
-        if (cudaMemGetInfo(&fr, &tot)) {
-            rc = cuda_fail(ctx, cudaGetLastError(), "autotune memory query");
+        if (cudaError_t e_ = cudaMemGetInfo(&fr, &tot)) {
+            rc = cuda_fail(ctx, e_, "autotune memory query");
             break;
         }
         // the current batch buffers come back with free_batch
@@ -709,7 +724,7 @@ int MatchPlan::autotune(const float* eulers, int R, const int* cands, int nc, in
         cudaEventRecord(e0, st);
         if ((rc = run(eulers, R, 0, cc, idx))) break;
         cudaEventRecord(e1, st);
-        if (cudaEventSynchronize(e1)) { rc = cuda_fail(ctx, cudaGetLastError(), "autotune"); break; }
+        if (cudaError_t e_ = cudaEventSynchronize(e1)) { rc = cuda_fail(ctx, e_, "autotune"); break; }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         ms /= (float)R;
@@ -823,24 +838,24 @@ int MatchPlan::set_template(const float* tmpl, const float* mask, const float* p
     has_psf = psf != nullptr;
     do {
         if (has_psf) {
-            if (ifftshift_real(psf, d_wu, T, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "ifftshift"); break; }
+            if (cudaError_t e_ = ifftshift_real(psf, d_wu, T, st)) { rc = cuda_fail(ctx, e_, "ifftshift"); break; }
             real_to_c64(d_tmpl, tc64, tn, st);
-            if (c2c3d<double2>(tc64, T, -1, 1.0, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "fft"); break; }
+            if (cudaError_t e_ = c2c3d<double2>(tc64, T, -1, 1.0, st)) { rc = cuda_fail(ctx, e_, "fft"); break; }
             mul_weight_c64(tc64, d_wu, tn, st);
-            if (c2c3d<double2>(tc64, T, +1, 1.0 / (double)tn, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "ifft"); break; }
+            if (cudaError_t e_ = c2c3d<double2>(tc64, T, +1, 1.0 / (double)tn, st)) { rc = cuda_fail(ctx, e_, "ifft"); break; }
             re_c64(tc64, tv64, tn, 1.0, st);
             ctx->launches += 10;
         } else {
             affine_f32_to_f64(d_tmpl, tv64, tn, 1.0, 0.0, st);
             ctx->launches += 1;
         }
-        if (norm_under_mask_sums(tv64, d_mask, tn, d_red, nullptr, 0, 0, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "sum"); break; }
+        if (cudaError_t e_ = norm_under_mask_sums(tv64, d_mask, tn, d_red, nullptr, 0, 0, st)) { rc = cuda_fail(ctx, e_, "sum"); break; }
         cudaMemcpyAsync(h, d_red, sizeof(double), cudaMemcpyDeviceToHost, st);
         cudaStreamSynchronize(st);
         tmean = h[0] / msize;
-        if (norm_under_mask_sums(tv64, d_mask, tn, nullptr, d_red, tmean, 1, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "sum"); break; }
+        if (cudaError_t e_ = norm_under_mask_sums(tv64, d_mask, tn, nullptr, d_red, tmean, 1, st)) { rc = cuda_fail(ctx, e_, "sum"); break; }
         cudaMemcpyAsync(h, d_red, sizeof(double), cudaMemcpyDeviceToHost, st);
-        if (cudaStreamSynchronize(st)) { rc = cuda_fail(ctx, cudaGetLastError(), "sync"); break; }
+        if (cudaError_t e_ = cudaStreamSynchronize(st)) { rc = cuda_fail(ctx, e_, "sync"); break; }
         tstd = std::sqrt(h[0] / msize);
         ctx->launches += 2;
     } while (0);
@@ -889,28 +904,28 @@ int MatchPlan::set_volume(const float* vol) {
     do {
         const int T0[3] = {T[0], T[1], T[2]};
         // I0 = I - c and its spectrum
-        if (affine_f32_to_f64(vol, v64, nvox, 1.0, -vmean, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "affine"); break; }
-        if (r2c3d<double2>(v64, f1, N, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "r2c"); break; }
+        if (cudaError_t e_ = affine_f32_to_f64(vol, v64, nvox, 1.0, -vmean, st)) { rc = cuda_fail(ctx, e_, "affine"); break; }
+        if (cudaError_t e_ = r2c3d<double2>(v64, f1, N, st)) { rc = cuda_fail(ctx, e_, "r2c"); break; }
         {
             long long n = hs;
             k_pack_fimg<<<grid_n(n), 256, 0, st>>>(f1, d_fimg, (int)nh1, N[1], N[2]);
         }
         // spectrum of I0^2
-        if (square_f64(v64, nvox, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "square"); break; }
-        if (r2c3d<double2>(v64, f2, N, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "r2c"); break; }
+        if (cudaError_t e_ = square_f64(v64, nvox, st)) { rc = cuda_fail(ctx, e_, "square"); break; }
+        if (cudaError_t e_ = r2c3d<double2>(v64, f2, N, st)) { rc = cuda_fail(ctx, e_, "r2c"); break; }
         // mask placed at (j - floor(T/2)) mod N: convolution kernel of tom_os3_mean / tom_os3_std
-        if (cudaMemsetAsync(v64, 0, sizeof(double) * nvox, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "memset"); break; }
+        if (cudaError_t e_ = cudaMemsetAsync(v64, 0, sizeof(double) * nvox, st)) { rc = cuda_fail(ctx, e_, "memset"); break; }
         const int off[3] = {-(T[0] / 2), -(T[1] / 2), -(T[2] / 2)};
-        if (place_f64(d_mask, T0, v64, N, off, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "place"); break; }
-        if (r2c3d<double2>(v64, fm, N, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "r2c"); break; }
+        if (cudaError_t e_ = place_f64(d_mask, T0, v64, N, off, st)) { rc = cuda_fail(ctx, e_, "place"); break; }
+        if (cudaError_t e_ = r2c3d<double2>(v64, fm, N, st)) { rc = cuda_fail(ctx, e_, "r2c"); break; }
         const double sc = 1.0 / ((double)nvox * msize);
         mul_c64(f1, fm, hs, st);
-        if (c2r3d<double2>(f1, v64, N, sc, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "c2r"); break; }
+        if (cudaError_t e_ = c2r3d<double2>(f1, v64, N, sc, st)) { rc = cuda_fail(ctx, e_, "c2r"); break; }
         mul_c64(f2, fm, hs, st);
-        if (c2r3d<double2>(f2, m2, N, sc, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "c2r"); break; }
-        if (stats_final(v64, m2, d_mu0, d_sig, nvox, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "stats"); break; }
-        if (gamma_from_sigma(d_sig, d_gam, nvox, tstd, st)) { rc = cuda_fail(ctx, cudaGetLastError(), "gamma"); break; }
-        if (cudaStreamSynchronize(st)) { rc = cuda_fail(ctx, cudaGetLastError(), "sync"); break; }
+        if (cudaError_t e_ = c2r3d<double2>(f2, m2, N, sc, st)) { rc = cuda_fail(ctx, e_, "c2r"); break; }
+        if (cudaError_t e_ = stats_final(v64, m2, d_mu0, d_sig, nvox, st)) { rc = cuda_fail(ctx, e_, "stats"); break; }
+        if (cudaError_t e_ = gamma_from_sigma(d_sig, d_gam, nvox, tstd, st)) { rc = cuda_fail(ctx, e_, "gamma"); break; }
+        if (cudaError_t e_ = cudaStreamSynchronize(st)) { rc = cuda_fail(ctx, e_, "sync"); break; }
         ctx->launches += 4 * 3 + 3 * 2 + 8;
     } while (0);
     cleanup();
@@ -981,12 +996,18 @@ int MatchPlan::run(const float* eulers, int R, int index_offset, float* maxcc, i
         }
         {
             ProfScope ps(ctx, TOMGPU_K_C2R_FLCF);
-            if (!generic_only && fast_c2r(N[0] / 2))
+            if (!generic_only && !no_tma && N[0] == 512 && N[1] % 2 == 0 && tma_c2r_available())
+                TG_TRY_CUDA(ctx, launch_c2r_t256(d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean, 1.0 / msize,
+                                                 tmean, index_offset + off, maxcc, angidx, ctx->d_err, st));
+            else if (!generic_only && N[0] % 2 == 0 && fast_c2r(N[0] / 2))
                 TG_TRY_CUDA(ctx, launch_c2r_fast(N[0] / 2, d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean,
                                                  1.0 / msize, tmean, index_offset + off, maxcc, angidx, st));
-            else
+            else if (c2r_compiled(N[0]))
                 TG_TRY_CUDA(ctx, launch_c2r_flcf(N[0] / 2, d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean,
                                                  1.0 / msize, tmean, index_offset + off, maxcc, angidx, st));
+            else
+                TG_TRY_CUDA(ctx, launch_c2r_flcf_rt(N[0], d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean,
+                                                    1.0 / msize, tmean, index_offset + off, maxcc, angidx, st));
         }
         ctx->launches += 3;
     }
@@ -1012,8 +1033,12 @@ int MatchPlan::cc_map_tail(float* cc) {
     TG_TRY_CUDA(ctx, launch_corr_y(N[1], d_fimg, d_Z, d_Q, T[1], d0_corr(N[1], T[1]), ncols, 1, st));
     TG_TRY_CUDA(ctx, launch_inv_z(N[2], d_Q, d_H, N[1], (int)nh1, 1, st));
     const float inv_nm = (float)(1.0 / ((double)nvox * msize));
-    TG_TRY_CUDA(ctx, launch_c2r_map(N[0] / 2, d_H, d_mu0, d_gam, d_tsum, N[1], N[2], inv_nm, vmean, 1.0 / msize,
-                                    tmean, cc, st));
+    if (c2r_compiled(N[0]))
+        TG_TRY_CUDA(ctx, launch_c2r_map(N[0] / 2, d_H, d_mu0, d_gam, d_tsum, N[1], N[2], inv_nm, vmean, 1.0 / msize,
+                                        tmean, cc, st));
+    else
+        TG_TRY_CUDA(ctx, launch_c2r_map_rt(N[0], d_H, d_mu0, d_gam, d_tsum, N[1], N[2], inv_nm, vmean, 1.0 / msize,
+                                           tmean, cc, st));
     ctx->launches += 3;
     return TOMGPU_OK;
 }

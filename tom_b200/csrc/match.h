@@ -11,6 +11,22 @@ namespace tg {
 
 bool match_sizes_supported(const int N[3], const int T[3]);
 
+// the stages on the run-time line engine for edges without compiled kernels
+// (match_rt.cu); the c2r kernels take the x edge itself, which may be odd
+bool match_rt_length_ok(int L);
+cudaError_t launch_spec_x_rt(int NX, const float* t2, const float* mask, float2* A, const int T[3], int d0x, int nb,
+                             double* tsum, cudaStream_t st);
+cudaError_t launch_spec_z_rt(int NZ, const float2* A, float2* Z, const int T[3], int d0z, int nh1, int nb,
+                             cudaStream_t st);
+cudaError_t launch_corr_y_rt(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
+                             long long ncols, int nb, cudaStream_t st);
+cudaError_t launch_inv_z_rt(int NZ, const float2* Q, float2* H, int Ny, int nh1, int nb, cudaStream_t st);
+cudaError_t launch_c2r_flcf_rt(int NX, const float2* H, const float* mu0, const float* gam, const double* tsum,
+                               int Ny, int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,
+                               float* maxcc, int* angidx, cudaStream_t st);
+cudaError_t launch_c2r_map_rt(int NX, const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny,
+                              int Nz, float inv_nm, double c, double inv_m, double mu_t, float* cc, cudaStream_t st);
+
 // register-resident hot kernels (match_fast.cu) for the sizes they cover
 bool fast_corr_y(int NY, int Ty);
 bool fast_inv_z(int NZ);
@@ -42,6 +58,11 @@ cudaError_t launch_c2r_b128(const float2* H, const float* mu0, const float* gam,
 cudaError_t launch_c2r_b64(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
                            int* angidx, cudaStream_t st);
+// x edge 512 with TMA tile loads (match_tma.cu); err: the context's device error word
+bool tma_c2r_available();
+cudaError_t launch_c2r_t256(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
+                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
+                            int* angidx, int* err, cudaStream_t st);
 cudaError_t c2c3d_batch(float2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
 cudaError_t c2c3d_batch64(double2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
 
@@ -52,6 +73,7 @@ struct MatchPlan {
     int N[3] = {0, 0, 0}, T[3] = {0, 0, 0};
     int B = 8;
     bool generic_only = false;  // force the generic kernels (tests compare both paths)
+    bool no_tma = false;        // the cp.async x-line kernel for the 512 x edge (comparisons)
     long long nvox = 0, nh1 = 0, tn = 0;
     int64_t bytes_held = 0;
     int64_t batch_bytes = 0;

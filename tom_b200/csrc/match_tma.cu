@@ -1,0 +1,268 @@
+// x-line kernel of the FLCF search for the x edge 512 with its tiles loaded by
+// the Tensor Memory Accelerator (cp.async.bulk.tensor), 1-GPU code.
+//
+// Same arithmetic as k_c2r_h256 (match_fast128.cu): a half-warp per x line,
+// 16 lines (16 consecutive y at one z) per block, the half-spectrum unpack,
+// 256 = 16 x 16 with one exchange, the running maximum over u = out/(N M) +
+// kappa and the FLCF at the read-modify-write (search/tom_os3_corr.m:151-176,
+// search/tom_os3_bestPeak.m:42-47).  What changes is how a rotation's tile
+// (all 257 kx rows of 16 y, 128 bytes per row) reaches shared memory: instead
+// of ~17 eight-byte cp.async per thread, one thread issues two tiled TMA
+// loads per rotation (boxes 16 y x 1 z x 256 kx and 16 y x 1 z x 1 kx over
+// H[b][kx][z][y], viewed as floats) that complete on a per-stage mbarrier.
+// Three stages are in flight.  The tensor maps cover only this GPU's own H
+// buffer, and no load multicasts.
+//
+// Shared layout of a stage: row kx at kx * 128 bytes, the 128-byte swizzle
+// of the TMA placing the 16-byte chunk c of row k at chunk c ^ (k mod 8), so
+// the half-warp's reads down a column (rows j + 16 k2, j = lane) fall on
+// distinct banks.  After every line has read its tile, the stage holds the
+// exchange (line yl at yl * 2 KB, [j][q ^ j]), then is refilled by the TMA.
+//
+// Waits are bounded: a stage that does not fill within the limit sets the
+// context's device error word (TOMGPU_ERR_TIMEOUT at the next synchronise),
+// the block waits (bounded) for its other loads and returns without touching
+// the results.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "ctx.h"
+#include "match.h"
+#include "twiddles.h"
+#include "warp_fft.cuh"
+
+namespace tg {
+
+namespace {
+
+constexpr int CT_YT = 16;                 // lines (y) per block
+constexpr int CT_STG = 3;                 // stages in flight
+constexpr int CT_ROWB = 128;              // bytes per kx row: 16 y x 8 bytes
+constexpr int CT_STAGE = 33792;           // 257 rows rounded up to 1 KB (swizzle atom)
+constexpr unsigned CT_TX = 257u * CT_ROWB;  // bytes one stage receives
+constexpr long long CT_WAIT_LIMIT = 1ll << 24;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_test_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait on one phase; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+    for (long long i = 0; i < CT_WAIT_LIMIT; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(dst),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+// NH = 256 = 16 (P) x 16 (Q), as k_c2r_h256.
+__global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUtensorMap tm_rows,
+                                                     const __grid_constant__ CUtensorMap tm_last,
+                                                     const float* __restrict__ mu0, const float* __restrict__ gam,
+                                                     const double* __restrict__ tsum, int Ny, int Nz, int nb,
+                                                     float inv_nm, double c_mean, double inv_m, double mu_t, int index0,
+                                                     float* __restrict__ maxcc, int* __restrict__ angidx,
+                                                     const float2* __restrict__ tw_h, const float2* __restrict__ tw_x,
+                                                     int* __restrict__ err) {
+    constexpr int NH = 256, NX = 2 * NH, P = 16, QN = 16;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    // the swizzled stages need a 1 KB aligned base (the launch adds the slack)
+    unsigned char* base =
+        smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    float2* T = reinterpret_cast<float2*>(base + CT_STG * CT_STAGE);  // [QN][P]: W256^(+q k1) at [q][k1]
+    float2* twx = T + P * QN;                                         // [NH]: W512^(+k)
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(twx + NH);
+    int* flag = reinterpret_cast<int*>(bars + CT_STG);
+    float* kaps = reinterpret_cast<float*>(flag + 4);  // [nb]
+    const int tid = threadIdx.x, line = tid >> 4, j = tid & 15;
+    const int y0 = blockIdx.x * CT_YT, z = blockIdx.y, y = y0 + line;
+    for (int i = tid; i < P * QN; i += blockDim.x) {
+        const int k1 = i >> 4, q = i & 15;
+        T[q * P + k1] = cconj(__ldg(tw_h + (q * k1) % NH));
+    }
+    for (int i = tid; i < NH; i += blockDim.x) twx[i] = cconj(__ldg(tw_x + i));
+    for (int b = tid; b < nb; b += blockDim.x) kaps[b] = (float)(c_mean * (tsum[b] * inv_m - mu_t));
+    if (tid == 0) {
+        for (int s = 0; s < CT_STG; ++s) mbar_init(smem_u32(bars + s), 1);
+        *flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&tm_rows)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&tm_last)) : "memory");
+    }
+    __syncthreads();
+    const unsigned sbase = smem_u32(base);
+    // rotation b into stage s: rows kx 0..255, then row 256 (box edges stop at 256)
+    auto issue = [&](int b, int s) {
+        if (tid == 0) {
+            const unsigned bar = smem_u32(bars + s), dst = sbase + (unsigned)(s * CT_STAGE);
+            mbar_expect_tx(bar, CT_TX);
+            tma_load_4d(dst, &tm_rows, 2 * y0, z, 0, b, bar);
+            tma_load_4d(dst + 256u * CT_ROWB, &tm_last, 2 * y0, z, 256, b, bar);
+        }
+    };
+    float bu[P][2];
+    unsigned bb[P];
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        bu[m][0] = bu[m][1] = -INFINITY;
+        bb[m] = 0u;
+    }
+    issue(0, 0);
+    if (1 < nb) issue(1, 1);
+    int cur = 0;  // stage of rotation b
+    for (int b = 0; b < nb; ++b) {
+        const int nxt = cur == 0 ? 2 : cur - 1;  // stage of rotation b + 2
+        if (b + 2 < nb) issue(b + 2, nxt);
+        const unsigned bar = smem_u32(bars + cur), parity = (unsigned)((b / CT_STG) & 1);
+        if (tid == 0 && !mbar_wait_bounded(bar, parity)) *flag = 1;
+        __syncthreads();
+        if (*flag) {
+            // the stage never filled: wait (bounded) for the loads still in
+            // flight, report, return without touching the results
+            if (tid == 0) {
+                tg_flag_error(err, TG_DEV_TIMEOUT);
+                for (int r = b + 1; r < nb && r <= b + 2; ++r) {
+                    const int s = r % CT_STG;
+                    mbar_wait_bounded(smem_u32(bars + s), (unsigned)((r / CT_STG) & 1));
+                }
+            }
+            return;
+        }
+        (void)mbar_test_wait(bar, parity);  // every thread observes the completed phase
+        const unsigned char* st = base + cur * CT_STAGE;
+        const int cy = line >> 1, hy = (line & 1) << 3;  // chunk and half of this line's y in a row
+        float2 u[QN];
+#pragma unroll
+        for (int k2 = 0; k2 < QN; ++k2) {
+            const int k = j + P * k2, kr = NH - k;
+            const float2 xa = *reinterpret_cast<const float2*>(st + k * CT_ROWB + ((cy ^ (k & 7)) << 4) + hy);
+            const float2 xc =
+                cconj(*reinterpret_cast<const float2*>(st + kr * CT_ROWB + ((cy ^ (kr & 7)) << 4) + hy));
+            const float2 d = cmul(twx[k], csub(xa, xc));
+            u[k2] = cadd(cadd(xa, xc), make_float2(-d.y, d.x));
+        }
+        __syncthreads();  // every line has read the tile: the stage takes the exchange
+        tgfft::dft16<+1>(u);
+        float2* xl = reinterpret_cast<float2*>(base + cur * CT_STAGE) + line * 256;
+#pragma unroll
+        for (int q = 0; q < QN; ++q) xl[j * 16 + (q ^ j)] = cmul(u[q], T[q * P + j]);
+        __syncwarp();
+        float2 v[P];
+#pragma unroll
+        for (int k1 = 0; k1 < P; ++k1) v[k1] = xl[k1 * 16 + (j ^ k1)];
+        tgfft::dft16<+1>(v);
+        const float kap = kaps[b];
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const float u0 = fmaf(v[m].x, inv_nm, kap);
+            const float u1 = fmaf(v[m].y, inv_nm, kap);
+            if (u0 > bu[m][0]) { bu[m][0] = u0; bb[m] = (bb[m] & 0xFFFF0000u) | (unsigned)b; }
+            if (u1 > bu[m][1]) { bu[m][1] = u1; bb[m] = (bb[m] & 0x0000FFFFu) | ((unsigned)b << 16); }
+        }
+        cur = cur == 2 ? 0 : cur + 1;
+        // the exchange writes precede the next TMA fill of this stage
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+    }
+    if (y >= Ny) return;
+    const float mt = (float)mu_t;
+    const long long row = ((long long)z * Ny + y) * NX;
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const long long v = row + 2 * (j + QN * m);
+        const float2 a = __ldg(reinterpret_cast<const float2*>(mu0 + v));
+        const float2 g = __ldg(reinterpret_cast<const float2*>(gam + v));
+        float2 cv = *reinterpret_cast<const float2*>(maxcc + v);
+        int2 ci = *reinterpret_cast<const int2*>(angidx + v);
+        bool ch = false;
+        const float c0 = g.x != 0.f ? (bu[m][0] - a.x * mt) * g.x : 0.f;
+        const float c1 = g.y != 0.f ? (bu[m][1] - a.y * mt) * g.y : 0.f;
+        const int b0 = g.x != 0.f ? (int)(bb[m] & 0xFFFFu) : 0, b1 = g.y != 0.f ? (int)(bb[m] >> 16) : 0;
+        if (c0 > cv.x) { cv.x = c0; ci.x = index0 + b0; ch = true; }
+        if (c1 > cv.y) { cv.y = c1; ci.y = index0 + b1; ch = true; }
+        if (ch) {
+            *reinterpret_cast<float2*>(maxcc + v) = cv;
+            *reinterpret_cast<int2*>(angidx + v) = ci;
+        }
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+}  // namespace
+
+bool tma_c2r_available() { return encode_fn() != nullptr; }
+
+cudaError_t launch_c2r_t256(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
+                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
+                            int* angidx, int* err, cudaStream_t st) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    // the TMA coordinate along y (floats) is 2 y0 = 32 blockIdx.x: a multiple of
+    // 16 bytes; strides are multiples of 16 bytes when Ny is even
+    if (Ny % 2 || nb < 1 || nb > 65535) return cudaErrorInvalidValue;
+    const cuuint64_t dims[4] = {(cuuint64_t)2 * Ny, (cuuint64_t)Nz, 257, (cuuint64_t)nb};
+    const cuuint64_t strides[3] = {(cuuint64_t)8 * Ny, (cuuint64_t)8 * Ny * Nz, (cuuint64_t)8 * Ny * Nz * 257};
+    const cuuint32_t box_rows[4] = {32, 1, 256, 1}, box_last[4] = {32, 1, 1, 1}, estr[4] = {1, 1, 1, 1};
+    CUtensorMap tm_rows, tm_last;
+    void* g = const_cast<float2*>(H);
+    if (enc(&tm_rows, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, g, dims, strides, box_rows, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
+        enc(&tm_last, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, g, dims, strides, box_last, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    const size_t smem = 1024 + (size_t)CT_STG * CT_STAGE + sizeof(float2) * (16 * 16 + 256) +
+                        sizeof(unsigned long long) * CT_STG + 4 * sizeof(int) + sizeof(float) * nb;
+    cudaError_t e = cudaFuncSetAttribute(k_c2r_t256, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e) return e;
+    dim3 grid((Ny + CT_YT - 1) / CT_YT, Nz);
+    k_c2r_t256<<<grid, 256, smem, st>>>(tm_rows, tm_last, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0,
+                                        maxcc, angidx, twiddle_table<float2>(256), twiddle_table<float2>(512), err);
+    return cudaGetLastError();
+}
+
+}  // namespace tg

@@ -466,13 +466,13 @@ class MatchPlan:
     """
 
     def __init__(self, vol_shape_xyz, tmpl_shape_xyz, batch: int = 0, ctx: Context | None = None,
-                 generic: bool = False):
+                 generic: bool = False, path: int | None = None):
         self.ctx = ctx or default_context()
         self.vol_shape = tuple(int(s) for s in vol_shape_xyz)
         self.tmpl_shape = tuple(int(s) for s in tmpl_shape_xyz)
         p = MatchParams()
         p.batch = int(batch)
-        p.path = 1 if generic else 0
+        p.path = int(path) if path is not None else (1 if generic else 0)
         h = ctypes.c_void_p()
         self.ctx.check(lib().tomgpu_match_plan_create(self.ctx.handle, _cdims(self.vol_shape),
                                                       _cdims(self.tmpl_shape), ctypes.byref(p), ctypes.byref(h)))
