@@ -57,9 +57,9 @@ def parse():
     p.add_argument("--rot-per-step", type=int, default=64)
     p.add_argument("--batch", type=int, default=0,
                    help="rotation batch; 0 = autotune over 8, 16, 32, 64 before the timed region")
-    p.add_argument("--path", type=int, default=0, choices=[0, 1, 2],
+    p.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
                    help="kernel path of the plan: 0 fastest (TMA x-line tiles at the 512 x edge), 1 generic, "
-                        "2 as 0 with cp.async x-line tiles")
+                        "2 as 0 with cp.async x-line tiles, 3 as 0 with the tcgen05 inverse z-DFT")
     p.add_argument("--e2e-rot", type=int, default=1024)
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-seconds", type=float, default=20.0)

@@ -193,7 +193,9 @@ typedef struct {
     int wedge_fp64;     /* reserved, 0 */
     int path;           /* 0: fastest kernels for the sizes; 1: generic kernels only;
                            2: as 0, but the x-line kernel of the 512 x edge loads its tiles
-                           with per-thread cp.async instead of TMA (for comparison) */
+                           with per-thread cp.async instead of TMA (for comparison);
+                           3: as 0, with the inverse z-DFT of the 256 z edge as tcgen05
+                           tensor-core contractions (split TF32, FP32 accumulation) */
     int reserved[5];
 } tomgpu_match_params;
 

@@ -126,7 +126,7 @@ def test_autotune_keeps_results(gpu, oracle):
     plan.close()
 
 
-@pytest.mark.parametrize("shape,batch", [((512, 40, 24), 5), ((512, 64, 32), 16), ((512, 512, 8), 3)])
+@pytest.mark.parametrize("shape,batch", [((512, 40, 24), 5), ((512, 64, 32), 16), ((512, 512, 16), 3)])
 def test_tma_x_lines_equal_cp_async_x_lines(gpu, oracle, shape, batch):
     """The 512 x edge's x-line kernel with TMA tile loads (the default) gives
     the cp.async kernel's results bit for bit (the same arithmetic; a y edge
@@ -157,3 +157,35 @@ def test_tma_x_lines_equal_cp_async_x_lines(gpu, oracle, shape, batch):
         assert np.abs(out[0][0] - ref_cc).max() <= REL * scale
         sep = (ref_cc - ref_2) > 2 * REL * scale
         assert np.array_equal(out[0][1][sep], ref_idx[sep])
+
+
+@pytest.mark.parametrize("shape", [(48, 40, 256), (64, 64, 256), (512, 24, 256)])
+def test_tcgen05_inverse_z_dft(gpu, oracle, shape):
+    """The inverse z-DFT of the 256 z edge with its radix-16 stages as tcgen05
+    tensor-core contractions (path 3, split TF32 with FP32 accumulation) against
+    the FP32 CUDA-core kernel (path 0) and the FP64 oracle's parity bar; the
+    device error word stays clear (no MMA wait ran out)."""
+    import torch
+    rng = np.random.default_rng(shape[0] + shape[1])
+    vol = rng.standard_normal(shape).astype(np.float32)
+    T = 16
+    tmpl = rng.standard_normal((T, T, T)).astype(np.float32)
+    mask = oracle.sphere_mask((T, T, T), 7).astype(np.float32)
+    angles = oracle.av3_angle_grid((0, 0, 0), (30, 30, 30), (330, 330, 180))[:9]
+    out = {}
+    for path in (0, 3):
+        plan = gpu.MatchPlan(vol.shape, tmpl.shape, batch=4, path=path)
+        plan.set_template(gpu.to_device(tmpl), gpu.to_device(mask))
+        plan.set_volume(gpu.to_device(vol))
+        cc, idx = plan.new_results()
+        plan.run(angles, cc, idx)
+        plan.ctx.synchronize()
+        torch.cuda.synchronize()
+        out[path] = gpu.from_device(cc).copy(), gpu.from_device(idx).copy()
+        plan.close()
+    ref_cc, ref_idx, ref_2 = oracle.find_template(vol, tmpl, mask, angles, keep_second=True)
+    scale = np.abs(ref_cc).max()
+    assert np.abs(out[3][0] - out[0][0]).max() <= 1e-5 * scale
+    assert np.abs(out[3][0] - ref_cc).max() <= REL * scale
+    sep = (ref_cc - ref_2) > 2 * REL * scale
+    assert np.array_equal(out[3][1][sep], ref_idx[sep])

@@ -740,11 +740,12 @@ int tomgpu_match_plan_create(tomgpu_ctx* ctx, const int vol[3], const int tm[3],
     if (!out || !dims_ok(vol) || !dims_ok(tm)) return fail(ctx, TOMGPU_ERR_ARG, "null pointer or bad dims");
     *out = nullptr;
     if (params && params->batch < 0) return fail(ctx, TOMGPU_ERR_ARG, "negative batch");
-    if (params && (params->path < 0 || params->path > 2)) return fail(ctx, TOMGPU_ERR_ARG, "path is 0, 1 or 2");
+    if (params && (params->path < 0 || params->path > 3)) return fail(ctx, TOMGPU_ERR_ARG, "path is 0, 1, 2 or 3");
     TG_TRY(use_device(ctx));
     tomgpu_match_plan* p = new tomgpu_match_plan();
     int rc = p->p.create(ctx, vol, tm, params ? params->batch : 0, params ? params->path == 1 : false);
     p->p.no_tma = params && params->path == 2;
+    p->p.tc_inv_z = params && params->path == 3;
     if (rc) {
         delete p;
         return rc;

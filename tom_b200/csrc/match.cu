@@ -989,7 +989,9 @@ int MatchPlan::run(const float* eulers, int R, int index_offset, float* maxcc, i
         }
         {
             ProfScope ps(ctx, TOMGPU_K_INV_Z);
-            if (!generic_only && fast_inv_z(N[2]))
+            if (!generic_only && tc_inv_z && N[2] == 256)
+                TG_TRY_CUDA(ctx, launch_inv_z_tc256(d_Q, d_H, N[1], (int)nh1, nb, ctx->d_err, st));
+            else if (!generic_only && fast_inv_z(N[2]))
                 TG_TRY_CUDA(ctx, launch_inv_z_fast(N[2], d_Q, d_H, N[1], (int)nh1, nb, st));
             else
                 TG_TRY_CUDA(ctx, launch_inv_z(N[2], d_Q, d_H, N[1], (int)nh1, nb, st));

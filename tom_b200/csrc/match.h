@@ -63,6 +63,8 @@ bool tma_c2r_available();
 cudaError_t launch_c2r_t256(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
                             int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
                             int* angidx, int* err, cudaStream_t st);
+// z edge 256 with the radix-16 stages on tcgen05 tensor cores (inv_z_tc.cu)
+cudaError_t launch_inv_z_tc256(const float2* Q, float2* H, int Ny, int nh1, int nb, int* err, cudaStream_t st);
 cudaError_t c2c3d_batch(float2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
 cudaError_t c2c3d_batch64(double2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);
 
@@ -74,6 +76,7 @@ struct MatchPlan {
     int B = 8;
     bool generic_only = false;  // force the generic kernels (tests compare both paths)
     bool no_tma = false;        // the cp.async x-line kernel for the 512 x edge (comparisons)
+    bool tc_inv_z = false;      // the z edge 256's inverse z-DFT on tcgen05 tensor cores
     long long nvox = 0, nh1 = 0, tn = 0;
     int64_t bytes_held = 0;
     int64_t batch_bytes = 0;

@@ -162,6 +162,9 @@ CONFIGS = {
     # the y-column (512) and x-line (512) kernels of the benchmark on a thin z slab
     "profile_512x512x48": dict(N=(512, 512, 48), T=40, n_copies=4, n_blobs=8, rho=16, snr=0.1,
                                max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
+    # the z edge 256 (the inverse z pass) and x edge 512 on a thin y slab, for profiler captures
+    "profile_512x64x256": dict(N=(512, 64, 256), T=40, n_copies=4, n_blobs=8, rho=16, snr=0.1,
+                               max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
     "exhaustive_512x512x256": dict(N=(512, 512, 256), T=40, n_copies=40, n_blobs=8, rho=16, snr=0.1,
                                    max_tilt=55, mask_radius=16, angles=((0, 0, 0), (10, 10, 10), (350, 350, 180))),
     # the 928 / 464 kernels on small volumes, for profiler captures
