@@ -43,9 +43,11 @@ UNIT = "rot*voxel/s"
 
 # DRAM bytes (read + write) per launch of a kernel class at a rotation batch,
 # from one ncu capture of a 512x128x64 volume (the same x edge), scaled by the
-# voxel count of the 512x512x256 tomogram.
+# voxel count of the 512x512x256 tomogram (batch 16 and 32: the cp.async
+# x-line kernel; 64: the TMA one, the default).
 TRAFFIC = {"exhaustive_512x512x256": {"c2r_flcf": {16: 16 * (336639232 + 22247680),
-                                                  32: 16 * (606162432 + 24264960)}}}
+                                                  32: 16 * (606162432 + 24264960),
+                                                  64: 16 * (1168364800 + 26934016)}}}
 
 
 def parse():

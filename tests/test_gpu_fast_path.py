@@ -126,12 +126,13 @@ def test_autotune_keeps_results(gpu, oracle):
     plan.close()
 
 
-@pytest.mark.parametrize("shape,batch", [((512, 40, 24), 5), ((512, 64, 32), 16), ((512, 512, 16), 3)])
+@pytest.mark.parametrize("shape,batch", [((512, 40, 24), 5), ((512, 64, 32), 16), ((512, 512, 16), 3),
+                                         ((928, 40, 24), 5), ((928, 30, 16), 3)])
 def test_tma_x_lines_equal_cp_async_x_lines(gpu, oracle, shape, batch):
-    """The 512 x edge's x-line kernel with TMA tile loads (the default) gives
-    the cp.async kernel's results bit for bit (the same arithmetic; a y edge
-    that is not a multiple of 16 exercises the TMA's zero fill), and meets the
-    oracle's parity bar."""
+    """The x-line kernels of the 512 and 928 x edges with TMA tile loads (the
+    default) give the cp.async kernels' results bit for bit (the same
+    arithmetic; a y edge that is not a multiple of the tile's 16 or 8 lines
+    exercises the TMA's zero fill), and meet the oracle's parity bar."""
     import torch
     rng = np.random.default_rng(shape[1])
     vol = rng.standard_normal(shape).astype(np.float32)

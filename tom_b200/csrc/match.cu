@@ -1001,6 +1001,9 @@ int MatchPlan::run(const float* eulers, int R, int index_offset, float* maxcc, i
             if (!generic_only && !no_tma && N[0] == 512 && N[1] % 2 == 0 && tma_c2r_available())
                 TG_TRY_CUDA(ctx, launch_c2r_t256(d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean, 1.0 / msize,
                                                  tmean, index_offset + off, maxcc, angidx, ctx->d_err, st));
+            else if (!generic_only && !no_tma && N[0] == 928 && N[1] % 2 == 0 && tma_c2r_available())
+                TG_TRY_CUDA(ctx, launch_c2r_t464(d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean, 1.0 / msize,
+                                                 tmean, index_offset + off, maxcc, angidx, ctx->d_err, st));
             else if (!generic_only && N[0] % 2 == 0 && fast_c2r(N[0] / 2))
                 TG_TRY_CUDA(ctx, launch_c2r_fast(N[0] / 2, d_H, d_mu0, d_gam, d_tsum, N[1], N[2], nb, inv_nm, vmean,
                                                  1.0 / msize, tmean, index_offset + off, maxcc, angidx, st));

@@ -63,6 +63,10 @@ bool tma_c2r_available();
 cudaError_t launch_c2r_t256(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
                             int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
                             int* angidx, int* err, cudaStream_t st);
+// x edge 928 with TMA tile loads (match_fast29.cu)
+cudaError_t launch_c2r_t464(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
+                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
+                            int* angidx, int* err, cudaStream_t st);
 // z edge 256 with the radix-16 stages on tcgen05 tensor cores (inv_z_tc.cu)
 cudaError_t launch_inv_z_tc256(const float2* Q, float2* H, int Ny, int nh1, int nb, int* err, cudaStream_t st);
 cudaError_t c2c3d_batch(float2* data, const int t[3], int nb, int dir, double scale, cudaStream_t st);

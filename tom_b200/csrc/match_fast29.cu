@@ -24,6 +24,7 @@
 #include "match.h"
 #include "pq29.cuh"
 #include "tile_copy.cuh"
+#include "tma_util.cuh"
 #include "twiddles.h"
 #include "warp_fft.cuh"
 
@@ -268,6 +269,144 @@ __global__ void __launch_bounds__(16 * C2_YT, 3) k_c2r_p464(const float2* __rest
     }
 }
 
+// k_c2r_p464 with its tiles loaded by the Tensor Memory Accelerator: one
+// thread issues two tiled loads per rotation (boxes 8 y x 1 z x 256 kx and
+// 8 y x 1 z x 209 kx over H viewed as floats, 64-byte rows with the 64-byte
+// swizzle: chunk c of row k at chunk c ^ ((k >> 1) mod 4)) completing on a
+// per-stage mbarrier, instead of ~29 eight-byte cp.async per thread.  Two
+// stages; waits bounded (a stage that never fills sets the device error word
+// and the block returns without touching the results).  1-GPU code: the maps
+// cover this GPU's own H, no load multicasts.
+constexpr int T4_STAGE = 30720;              // 465 rows x 64 bytes, rounded up to 1 KB
+constexpr unsigned T4_TX = 465u * 64u;
+constexpr long long T4_WAIT_LIMIT = 1ll << 20;
+
+__global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_t464(const __grid_constant__ CUtensorMap tm_a,
+                                                            const __grid_constant__ CUtensorMap tm_b,
+                                                            const float* __restrict__ mu0,
+                                                            const float* __restrict__ gam,
+                                                            const double* __restrict__ tsum, int Ny, int Nz, int nb,
+                                                            float inv_nm, double c_mean, double inv_m, double mu_t,
+                                                            int index0, float* __restrict__ maxcc,
+                                                            int* __restrict__ angidx, const float2* __restrict__ tw_h,
+                                                            const float2* __restrict__ tw_x, tgpq::Cos29 cs,
+                                                            int* __restrict__ err) {
+    constexpr int NH = 464, NX = 2 * NH, P = 29, YT = C2_YT;
+    if (err && *reinterpret_cast<volatile int*>(err)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char* base = smem_raw + ((1024u - (tgtma::smem_u32(smem_raw) & 1023u)) & 1023u);
+    float2* xb = reinterpret_cast<float2*>(base + 2 * T4_STAGE);  // [YT][29][17] exchange
+    float2* T = xb + YT * C2_XL;                                     // [16][32]: W464^(+q k1) at [q][k1]
+    float2* twx = T + 16 * 32;                                       // [NH]: W928^(+k)
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(twx + NH);
+    int* flag = reinterpret_cast<int*>(bars + 2);
+    float* kaps = reinterpret_cast<float*>(flag + 2);  // [nb]
+    const int tid = threadIdx.x, line = tid >> 4, q = tid & 15;
+    const int y0 = blockIdx.x * YT, z = blockIdx.y, y = y0 + line;
+    for (int i = tid; i < P * 16; i += blockDim.x) {
+        const int k1 = i >> 4, qq = i & 15;
+        T[qq * 32 + k1] = cconj(__ldg(tw_h + (qq * k1) % NH));
+    }
+    for (int i = tid; i < NH; i += blockDim.x) twx[i] = cconj(__ldg(tw_x + i));
+    for (int b = tid; b < nb; b += blockDim.x) kaps[b] = (float)(c_mean * (tsum[b] * inv_m - mu_t));
+    if (tid == 0) {
+        tgtma::mbar_init(tgtma::smem_u32(bars), 1);
+        tgtma::mbar_init(tgtma::smem_u32(bars + 1), 1);
+        *flag = 0;
+        tgtma::fence_barrier_init();
+        tgtma::prefetch_map(&tm_a);
+        tgtma::prefetch_map(&tm_b);
+    }
+    __syncthreads();
+    const unsigned sbase = tgtma::smem_u32(base);
+    auto issue = [&](int b, int s) {
+        if (tid == 0) {
+            const unsigned bar = tgtma::smem_u32(bars + s), dst = sbase + (unsigned)(s * T4_STAGE);
+            tgtma::mbar_expect_tx(bar, T4_TX);
+            tgtma::load_4d(dst, &tm_a, 2 * y0, z, 0, b, bar);
+            tgtma::load_4d(dst + 256u * 64u, &tm_b, 2 * y0, z, 256, b, bar);
+        }
+    };
+    float bu[P][2];
+    unsigned bb[P];
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        bu[m][0] = bu[m][1] = -INFINITY;
+        bb[m] = 0u;
+    }
+    issue(0, 0);
+    float2* xl = xb + line * C2_XL;
+    const int cy = line >> 1, hy = (line & 1) << 3;  // chunk and half of this line's y in a 64-byte row
+    for (int b = 0; b < nb; ++b) {
+        if (b + 1 < nb) issue(b + 1, (b + 1) & 1);
+        const int cur = b & 1;
+        const unsigned bar = tgtma::smem_u32(bars + cur), parity = (unsigned)((b >> 1) & 1);
+        if (tid == 0 && !tgtma::mbar_wait_bounded(bar, parity, T4_WAIT_LIMIT)) *flag = 1;
+        __syncthreads();
+        if (*flag) {
+            if (tid == 0) {
+                tg_flag_error(err, TG_DEV_TIMEOUT);
+                if (b + 1 < nb) tgtma::mbar_wait_bounded(tgtma::smem_u32(bars + ((b + 1) & 1)),
+                                                         (unsigned)(((b + 1) >> 1) & 1), T4_WAIT_LIMIT);
+            }
+            return;
+        }
+        (void)tgtma::mbar_test_wait(bar, parity);
+        const unsigned char* st = base + cur * T4_STAGE;
+        // unpack and the inner 16-point DFTs: k = k1 + 29 k2
+#pragma unroll 1
+        for (int k1 = q; k1 < P; k1 += 16) {
+            float2 u[16];
+#pragma unroll
+            for (int k2 = 0; k2 < 16; ++k2) {
+                const int k = k1 + P * k2, kr = NH - k;
+                const float2 xa = *reinterpret_cast<const float2*>(st + k * 64 + ((cy ^ ((k >> 1) & 3)) << 4) + hy);
+                const float2 xc =
+                    cconj(*reinterpret_cast<const float2*>(st + kr * 64 + ((cy ^ ((kr >> 1) & 3)) << 4) + hy));
+                const float2 d = cmul(twx[k], csub(xa, xc));
+                u[k2] = cadd(cadd(xa, xc), make_float2(-d.y, d.x));
+            }
+            tgfft::dft16<+1>(u);
+#pragma unroll
+            for (int qq = 0; qq < 16; ++qq) xl[k1 * C2_XR + qq] = cmul(u[qq], T[qq * 32 + k1]);
+        }
+        __syncwarp();
+        float2 v[P];
+#pragma unroll
+        for (int k1 = 0; k1 < P; ++k1) v[k1] = xl[k1 * C2_XR + q];
+        const float kap = kaps[b];
+        tgpq::dft29_emit<+1>(v, cs, [&](int m, float2 x) {
+            const float u0 = fmaf(x.x, inv_nm, kap);
+            const float u1 = fmaf(x.y, inv_nm, kap);
+            if (u0 > bu[m][0]) { bu[m][0] = u0; bb[m] = (bb[m] & 0xFFFF0000u) | (unsigned)b; }
+            if (u1 > bu[m][1]) { bu[m][1] = u1; bb[m] = (bb[m] & 0x0000FFFFu) | ((unsigned)b << 16); }
+        });
+        tgtma::fence_proxy_async();
+        __syncthreads();  // the stage is refilled and the exchange rewritten next
+    }
+    if (y >= Ny) return;
+    const float mt = (float)mu_t;
+    const long long row = ((long long)z * Ny + y) * NX;
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const long long v = row + 2 * (q + 16 * m);
+        const float2 a = __ldg(reinterpret_cast<const float2*>(mu0 + v));
+        const float2 g = __ldg(reinterpret_cast<const float2*>(gam + v));
+        float2 cur = *reinterpret_cast<const float2*>(maxcc + v);
+        int2 ci = *reinterpret_cast<const int2*>(angidx + v);
+        bool ch = false;
+        const float c0 = g.x != 0.f ? (bu[m][0] - a.x * mt) * g.x : 0.f;
+        const float c1 = g.y != 0.f ? (bu[m][1] - a.y * mt) * g.y : 0.f;
+        const int b0 = g.x != 0.f ? (int)(bb[m] & 0xFFFFu) : 0, b1 = g.y != 0.f ? (int)(bb[m] >> 16) : 0;
+        if (c0 > cur.x) { cur.x = c0; ci.x = index0 + b0; ch = true; }
+        if (c1 > cur.y) { cur.y = c1; ci.y = index0 + b1; ch = true; }
+        if (ch) {
+            *reinterpret_cast<float2*>(maxcc + v) = cur;
+            *reinterpret_cast<int2*>(angidx + v) = ci;
+        }
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_corr_y_p928(const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y, long long ncols,
@@ -297,6 +436,30 @@ cudaError_t launch_c2r_p464(const float2* H, const float* mu0, const float* gam,
     k_c2r_p464<<<g, 16 * C2_YT, smem, st>>>(H, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0, maxcc,
                                             angidx, twiddle_table<float2>(464), twiddle_table<float2>(928),
                                             cos29_table());
+    return cudaGetLastError();
+}
+
+}  // namespace tg
+
+namespace tg {
+
+cudaError_t launch_c2r_t464(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
+                            int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
+                            int* angidx, int* err, cudaStream_t st) {
+    // the TMA coordinate along y (floats) is 16 blockIdx.x: 64 bytes
+    if (Ny % 2 || nb < 1 || nb > 65535) return cudaErrorInvalidValue;
+    CUtensorMap tm_a, tm_b;
+    if (!encode_h_map(&tm_a, H, Ny, Nz, 465, nb, C2_YT, 256, CU_TENSOR_MAP_SWIZZLE_64B) ||
+        !encode_h_map(&tm_b, H, Ny, Nz, 465, nb, C2_YT, 209, CU_TENSOR_MAP_SWIZZLE_64B))
+        return cudaErrorInvalidValue;
+    const size_t smem = 1024 + 2 * (size_t)T4_STAGE + sizeof(float2) * (C2_YT * C2_XL + 16 * 32 + 464) +
+                        sizeof(unsigned long long) * 2 + 2 * sizeof(int) + sizeof(float) * nb;
+    cudaError_t e = cudaFuncSetAttribute(k_c2r_t464, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e) return e;
+    dim3 g((Ny + C2_YT - 1) / C2_YT, Nz);
+    k_c2r_t464<<<g, 16 * C2_YT, smem, st>>>(tm_a, tm_b, mu0, gam, tsum, Ny, Nz, nb, inv_nm, c, inv_m, mu_t, index0,
+                                            maxcc, angidx, twiddle_table<float2>(464), twiddle_table<float2>(928),
+                                            cos29_table(), err);
     return cudaGetLastError();
 }
 

@@ -23,11 +23,9 @@
 // context's device error word (TOMGPU_ERR_TIMEOUT at the next synchronise),
 // the block waits (bounded) for its other loads and returns without touching
 // the results.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
 #include "ctx.h"
 #include "match.h"
+#include "tma_util.cuh"
 #include "twiddles.h"
 #include "warp_fft.cuh"
 
@@ -42,46 +40,7 @@ constexpr int CT_STAGE = 33792;           // 257 rows rounded up to 1 KB (swizzl
 constexpr unsigned CT_TX = 257u * CT_ROWB;  // bytes one stage receives
 constexpr long long CT_WAIT_LIMIT = 1ll << 20;
 
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool mbar_test_wait(unsigned bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// bounded wait on one phase; false when the limit ran out
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
-    for (long long i = 0; i < CT_WAIT_LIMIT; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
-                                            unsigned bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-        "[%6];" ::"r"(dst),
-        "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
-        : "memory");
-}
+using tgtma::smem_u32;
 
 // NH = 256 = 16 (P) x 16 (Q), as k_c2r_h256.
 __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUtensorMap tm_rows,
@@ -113,11 +72,11 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
     for (int i = tid; i < NH; i += blockDim.x) twx[i] = cconj(__ldg(tw_x + i));
     for (int b = tid; b < nb; b += blockDim.x) kaps[b] = (float)(c_mean * (tsum[b] * inv_m - mu_t));
     if (tid == 0) {
-        for (int s = 0; s < CT_STG; ++s) mbar_init(smem_u32(bars + s), 1);
+        for (int s = 0; s < CT_STG; ++s) tgtma::mbar_init(smem_u32(bars + s), 1);
         *flag = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&tm_rows)) : "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&tm_last)) : "memory");
+        tgtma::fence_barrier_init();
+        tgtma::prefetch_map(&tm_rows);
+        tgtma::prefetch_map(&tm_last);
     }
     __syncthreads();
     const unsigned sbase = smem_u32(base);
@@ -125,9 +84,9 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
     auto issue = [&](int b, int s) {
         if (tid == 0) {
             const unsigned bar = smem_u32(bars + s), dst = sbase + (unsigned)(s * CT_STAGE);
-            mbar_expect_tx(bar, CT_TX);
-            tma_load_4d(dst, &tm_rows, 2 * y0, z, 0, b, bar);
-            tma_load_4d(dst + 256u * CT_ROWB, &tm_last, 2 * y0, z, 256, b, bar);
+            tgtma::mbar_expect_tx(bar, CT_TX);
+            tgtma::load_4d(dst, &tm_rows, 2 * y0, z, 0, b, bar);
+            tgtma::load_4d(dst + 256u * CT_ROWB, &tm_last, 2 * y0, z, 256, b, bar);
         }
     };
     float bu[P][2];
@@ -144,7 +103,7 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
         const int nxt = cur == 0 ? 2 : cur - 1;  // stage of rotation b + 2
         if (b + 2 < nb) issue(b + 2, nxt);
         const unsigned bar = smem_u32(bars + cur), parity = (unsigned)((b / CT_STG) & 1);
-        if (tid == 0 && !mbar_wait_bounded(bar, parity)) *flag = 1;
+        if (tid == 0 && !tgtma::mbar_wait_bounded(bar, parity, CT_WAIT_LIMIT)) *flag = 1;
         __syncthreads();
         if (*flag) {
             // the stage never filled: wait (bounded) for the loads still in
@@ -153,12 +112,12 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
                 tg_flag_error(err, TG_DEV_TIMEOUT);
                 for (int r = b + 1; r < nb && r <= b + 2; ++r) {
                     const int s = r % CT_STG;
-                    mbar_wait_bounded(smem_u32(bars + s), (unsigned)((r / CT_STG) & 1));
+                    tgtma::mbar_wait_bounded(smem_u32(bars + s), (unsigned)((r / CT_STG) & 1), CT_WAIT_LIMIT);
                 }
             }
             return;
         }
-        (void)mbar_test_wait(bar, parity);  // every thread observes the completed phase
+        (void)tgtma::mbar_test_wait(bar, parity);  // every thread observes the completed phase
         const unsigned char* st = base + cur * CT_STAGE;
         const int cy = line >> 1, hy = (line & 1) << 3;  // chunk and half of this line's y in a row
         float2 u[QN];
@@ -191,7 +150,7 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
         }
         cur = cur == 2 ? 0 : cur + 1;
         // the exchange writes precede the next TMA fill of this stage
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tgtma::fence_proxy_async();
         __syncthreads();
     }
     if (y >= Ny) return;
@@ -217,7 +176,9 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
     }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+}  // namespace
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static bool tried = false;
     if (!tried) {
@@ -233,29 +194,29 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-}  // namespace
+bool encode_h_map(CUtensorMap* map, const void* H, int Ny, int Nz, int nh1, int nb, int yt, int rows,
+                  CUtensorMapSwizzle swizzle) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)2 * Ny, (cuuint64_t)Nz, (cuuint64_t)nh1, (cuuint64_t)nb};
+    const cuuint64_t strides[3] = {(cuuint64_t)8 * Ny, (cuuint64_t)8 * Ny * Nz, (cuuint64_t)8 * Ny * Nz * nh1};
+    const cuuint32_t box[4] = {(cuuint32_t)(2 * yt), 1, (cuuint32_t)rows, 1}, estr[4] = {1, 1, 1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void*>(H), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
-bool tma_c2r_available() { return encode_fn() != nullptr; }
+bool tma_c2r_available() { return tensor_map_encoder() != nullptr; }
 
 cudaError_t launch_c2r_t256(const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny, int Nz,
                             int nb, float inv_nm, double c, double inv_m, double mu_t, int index0, float* maxcc,
                             int* angidx, int* err, cudaStream_t st) {
-    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
-    if (!enc) return cudaErrorNotSupported;
     // the TMA coordinate along y (floats) is 2 y0 = 32 blockIdx.x: a multiple of
     // 16 bytes; strides are multiples of 16 bytes when Ny is even
     if (Ny % 2 || nb < 1 || nb > 65535) return cudaErrorInvalidValue;
-    const cuuint64_t dims[4] = {(cuuint64_t)2 * Ny, (cuuint64_t)Nz, 257, (cuuint64_t)nb};
-    const cuuint64_t strides[3] = {(cuuint64_t)8 * Ny, (cuuint64_t)8 * Ny * Nz, (cuuint64_t)8 * Ny * Nz * 257};
-    const cuuint32_t box_rows[4] = {32, 1, 256, 1}, box_last[4] = {32, 1, 1, 1}, estr[4] = {1, 1, 1, 1};
     CUtensorMap tm_rows, tm_last;
-    void* g = const_cast<float2*>(H);
-    if (enc(&tm_rows, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, g, dims, strides, box_rows, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
-        enc(&tm_last, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, g, dims, strides, box_last, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    if (!encode_h_map(&tm_rows, H, Ny, Nz, 257, nb, CT_YT, 256, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !encode_h_map(&tm_last, H, Ny, Nz, 257, nb, CT_YT, 1, CU_TENSOR_MAP_SWIZZLE_128B))
         return cudaErrorInvalidValue;
     const size_t smem = 1024 + (size_t)CT_STG * CT_STAGE + sizeof(float2) * (16 * 16 + 256) +
                         sizeof(unsigned long long) * CT_STG + 4 * sizeof(int) + sizeof(float) * nb;
