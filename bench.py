@@ -42,12 +42,17 @@ METRIC = "TM rot*voxel/s (exhaustive FLCF, 512x512x256 tomogram, 40^3 template)"
 UNIT = "rot*voxel/s"
 
 # DRAM bytes (read + write) per launch of a kernel class at a rotation batch,
-# from one ncu capture of a 512x128x64 volume (the same x edge), scaled by the
-# voxel count of the 512x512x256 tomogram (batch 16 and 32: the cp.async
-# x-line kernel; 64: the TMA one, the default).
+# from ncu captures of thinner volumes with the same x and y edges, scaled by
+# the voxel count (every term of these kernels' traffic scales with it):
+# 512x128x64 (batch 16, 32: the cp.async x-line kernel) and 512x512x48
+# (batch 64: the TMA x-line kernel and the y-column kernel) for the
+# 512x512x256 tomogram; 928x928x48 (batch 32) for the 928x928x464 one.
 TRAFFIC = {"exhaustive_512x512x256": {"c2r_flcf": {16: 16 * (336639232 + 22247680),
                                                   32: 16 * (606162432 + 24264960),
-                                                  64: 16 * (1168364800 + 26934016)}}}
+                                                  64: 256 / 48 * (3435212032 + 94609920)},
+                                     "corr_y": {64: 256 / 48 * (303350272 + 3173413120)}},
+           "exhaustive_928x928x464": {"c2r_flcf": {32: 464 / 48 * (5964541184 + 316938496)},
+                                      "corr_y": {32: 464 / 48 * (440176384 + 5247565312)}}}
 
 
 def parse():
