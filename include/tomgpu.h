@@ -192,8 +192,10 @@ typedef struct {
                            per-batch buffers fit in half the free device memory, else 8 */
     int wedge_fp64;     /* reserved, 0 */
     int path;           /* 0: fastest kernels for the sizes; 1: generic kernels only;
-                           2: as 0, but the x-line kernel of the 512 x edge loads its tiles
-                           with per-thread cp.async instead of TMA (for comparison);
+                           2: as 0, but the x-line kernels of the 512 / 928 x edges load their
+                           tiles with per-thread cp.async instead of TMA and the y-column
+                           kernel of the 512 y edge reads its constants from shared memory
+                           instead of tensor memory (for comparison);
                            3: as 0, with the inverse z-DFT of the 256 z edge as tcgen05
                            tensor-core contractions (split TF32, FP32 accumulation) */
     int reserved[5];

@@ -129,8 +129,10 @@ def test_autotune_keeps_results(gpu, oracle):
 @pytest.mark.parametrize("shape,batch", [((512, 40, 24), 5), ((512, 64, 32), 16), ((512, 512, 16), 3),
                                          ((928, 40, 24), 5), ((928, 30, 16), 3)])
 def test_tma_x_lines_equal_cp_async_x_lines(gpu, oracle, shape, batch):
-    """The x-line kernels of the 512 and 928 x edges with TMA tile loads (the
-    default) give the cp.async kernels' results bit for bit (the same
+    """The x-line kernels of the 512 and 928 x edges with TMA tile loads and
+    the 512 y-column kernel with its F_I values and twiddles in tensor memory
+    (the default, path 0) give the results of the kernels without them
+    (path 2: cp.async tiles, shared-memory constants) bit for bit (the same
     arithmetic; a y edge that is not a multiple of the tile's 16 or 8 lines
     exercises the TMA's zero fill), and meet the oracle's parity bar."""
     import torch

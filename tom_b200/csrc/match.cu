@@ -983,7 +983,7 @@ int MatchPlan::run(const float* eulers, int R, int index_offset, float* maxcc, i
         {
             ProfScope ps(ctx, TOMGPU_K_CORR_Y);
             if (!generic_only && fast_corr_y(N[1], T[1]))
-                TG_TRY_CUDA(ctx, launch_corr_y_fast(N[1], d_fimg, d_Z, d_Q, T[1], d0y, ncols, nb, st));
+                TG_TRY_CUDA(ctx, launch_corr_y_fast(N[1], d_fimg, d_Z, d_Q, T[1], d0y, ncols, nb, st, !no_tma));
             else
                 TG_TRY_CUDA(ctx, launch_corr_y(N[1], d_fimg, d_Z, d_Q, T[1], d0y, ncols, nb, st));
         }

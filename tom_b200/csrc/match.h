@@ -34,8 +34,9 @@ bool fast_c2r(int NH);
 bool fast_spec_z(int NZ, int Tz);
 cudaError_t launch_spec_z_fast(int NZ, const float2* A, float2* Z, int Ty, int Tz, int d0z, int nh1, int nb,
                                cudaStream_t st);
+// tmem: the y edge 512's columns keep F_I and their twiddles in tensor memory
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
-                               long long ncols, int nb, cudaStream_t st);
+                               long long ncols, int nb, cudaStream_t st, bool tmem = false);
 cudaError_t launch_inv_z_fast(int NZ, const float2* Q, float2* H, int Ny, int nh1, int nb, cudaStream_t st);
 cudaError_t launch_c2r_fast(int NH, const float2* H, const float* mu0, const float* gam, const double* tsum, int Ny,
                             int Nz, int nb, float inv_nm, double c, double inv_m, double mu_t, int index0,

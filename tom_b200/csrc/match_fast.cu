@@ -23,6 +23,59 @@
 
 namespace tg {
 
+namespace {
+
+// Tensor-memory helpers of the y-column kernel: each thread keeps per-lane
+// constants (its F_I values, its inverse-FFT twiddles) in its own TMEM lane
+// and reads them back with tcgen05.ld instead of from shared memory.
+__device__ __forceinline__ void tm_st16(unsigned taddr, const float (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16};\n" ::"r"(taddr),
+        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]),
+        "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]));
+}
+__device__ __forceinline__ void tm_ld16(unsigned taddr, float (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]),
+          "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// The 512-point inverse warp transform (plan 8, 8, 8) with the twiddles of
+// stages 2 and 3 read from this thread's TMEM lane: columns c2 + 16 q and
+// c3 + 16 q hold w_r (r = 1..7, conjugated) of the lane's butterfly q.
+__device__ __forceinline__ void warp_ifft512_tm(float2* v, float2* buf, unsigned c2, unsigned c3, int lane) {
+    tgwfft::wstage<512, 8, 1, +1>(v, nullptr, lane);
+    tgwfft::wstore<512, 8, 1>(v, buf, lane);
+    __syncwarp();
+    tgwfft::wload<512, 8>(v, buf, lane);
+    __syncwarp();
+#pragma unroll
+    for (int stage = 0; stage < 2; ++stage) {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            float t[16];
+            tm_ld16((stage == 0 ? c2 : c3) + 16u * q, t);
+#pragma unroll
+            for (int r = 1; r < 8; ++r) v[q * 8 + r] = cmul(v[q * 8 + r], make_float2(t[2 * r - 2], t[2 * r - 1]));
+            tgfft::dft8<+1>(v + q * 8);
+        }
+        if (stage == 0) {
+            tgwfft::wstore<512, 8, 8>(v, buf, lane);
+            __syncwarp();
+            tgwfft::wload<512, 8>(v, buf, lane);
+            __syncwarp();
+        }
+    }
+}
+
+}  // namespace
+
 template <int NY>
 __global__ void __launch_bounds__(256, 2) k_corr_y_w(const float2* __restrict__ fimg, const float2* __restrict__ Z,
                                                      float2* __restrict__ Q, int Ty, int d0y, long long ncols, int nb,
@@ -93,11 +146,20 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_w(const float2* __restrict__ 
 // staged F_I column (the product is F_I conj(X)).  For NY = 512 the two m of
 // a lane differ by 32, W_64^(32 i) = (-1)^i: even and odd terms are summed
 // once for both.  NI = ceil(Ty / 8) terms per residue.
-template <int NY, int NI>
+//
+// TM (y edge 512): the lane's F_I values and the twiddles of the inverse
+// transform's two twiddled stages live in tensor memory (TMEM, 256 columns
+// per block: warp w uses lanes 32 (w mod 4) + lane, columns 128 (w / 4) +
+// [0, 96)) and are read with tcgen05.ld, which takes those reads (74 of the
+// 317 shared-memory wavefronts per column and rotation) off the
+// shared-memory path that bounds this kernel.
+template <int NY, int NI, bool TM>
 __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ fimg, const float2* __restrict__ Z,
                                                      float2* __restrict__ Q, int Ty, int d0y, long long ncols, int nb,
                                                      const float2* __restrict__ tw_g) {
     constexpr int EPT = NY / 32, NB = EPT / 8;
+    static_assert(!TM || NY == 512, "the TMEM variant is built for the 512-point columns");
+    __shared__ unsigned tmem_slot;
     static_assert(tgwfft::WPlan<NY>::RL == 8 && (NB == 1 || NB == 2) && NI >= 1 && NI <= 8, "plan");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* tw = reinterpret_cast<float2*>(smem_raw);  // [NY + 64] stage tables
@@ -124,19 +186,67 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ 
     float2* fw = fs + warp * NY;
     float2* zw = zs + warp * 128;
     const int zslot0 = (lane & 7) * 8 + (lane >> 3), zslot1 = zslot0 + 4;  // t = lane, lane + 32
-    if (col < ncols) {
+    const bool active = col < ncols;
+    if constexpr (TM) {
+        if (warp == 0) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(
+                (unsigned)__cvta_generic_to_shared(&tmem_slot)));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
+    }
+    if (active) {
 #pragma unroll
         for (int i = 0; i < EPT; ++i) {
             const int p = tgwfft::out_pos<NY>(i, lane);
-            fw[p] = cmulc(fimg[col * NY + p], __ldg(tw_g + (d0y * p) % NY));  // each lane reads only its own
+            const float2 f = cmulc(fimg[col * NY + p], __ldg(tw_g + (d0y * p) % NY));  // each lane its own
+            if constexpr (!TM) fw[p] = f;
+            else fw[i * 32 + lane] = f;  // staged until the TMEM copy below
         }
         const float2* zc = Z + col * Ty;  // rotation 0
         zw[zslot0] = lane < Ty ? zc[lane] : make_float2(0.f, 0.f);
         zw[zslot1] = lane + 32 < Ty ? zc[lane + 32] : make_float2(0.f, 0.f);
     }
-    __syncthreads();  // the tables; the only block-wide barrier
-    if (col >= ncols) return;
-    for (int b = 0; b < nb; ++b) {
+    if constexpr (TM) asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();  // the tables (and the TMEM allocation)
+    unsigned tw_base = 0;
+    if constexpr (TM) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        tw_base = tmem_slot + ((unsigned)(32 * (warp & 3)) << 16) + 128u * (unsigned)(warp >> 2);
+        if (active) {
+            // columns [0, 32): the lane's 16 F_I values; [32, 64) and [64, 96): the
+            // conjugated twiddles of stage 2 (stride 8) and stage 3 (stride 64)
+            float t[16];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float2 f = fw[(8 * h + i) * 32 + lane];
+                    t[2 * i] = f.x;
+                    t[2 * i + 1] = f.y;
+                }
+                tm_st16(tw_base + 16u * h, t);
+            }
+#pragma unroll
+            for (int stage = 0; stage < 2; ++stage) {
+                const int NS = stage == 0 ? 8 : 64;
+                const float2* tab = tw + (stage == 0 ? 0 : 64);
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int k = (lane + 32 * q) % NS;
+#pragma unroll
+                    for (int r = 1; r < 8; ++r) {
+                        const float2 w = cconj(tab[r * NS + k]);
+                        t[2 * r - 2] = w.x;
+                        t[2 * r - 1] = w.y;
+                    }
+                    t[14] = t[15] = 0.f;
+                    tm_st16(tw_base + 32u + 32u * stage + 16u * q, t);
+                }
+            }
+            tm_wait_st();
+        }
+    }
+    for (int b = 0; b < (active ? nb : 0); ++b) {
         // next rotation's column: two loads per lane, parked in registers
         float2 n0 = make_float2(0.f, 0.f), n1 = make_float2(0.f, 0.f);
         if (b + 1 < nb) {
@@ -181,9 +291,20 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ 
         }
         tgfft::dft8<-1>(v);
         if constexpr (NB == 2) tgfft::dft8<-1>(v + 8);
+        if constexpr (TM) {
 #pragma unroll
-        for (int i = 0; i < EPT; ++i) v[i] = cmulc(fw[tgwfft::out_pos<NY>(i, lane)], v[i]);
-        tgwfft::warp_fft<NY, +1>(v, buf, tw, lane);
+            for (int h = 0; h < 2; ++h) {
+                float t[16];
+                tm_ld16(tw_base + 16u * h, t);
+#pragma unroll
+                for (int i = 0; i < 8; ++i) v[8 * h + i] = cmulc(make_float2(t[2 * i], t[2 * i + 1]), v[8 * h + i]);
+            }
+            warp_ifft512_tm(v, buf, tw_base + 32u, tw_base + 64u, lane);
+        } else {
+#pragma unroll
+            for (int i = 0; i < EPT; ++i) v[i] = cmulc(fw[tgwfft::out_pos<NY>(i, lane)], v[i]);
+            tgwfft::warp_fft<NY, +1>(v, buf, tw, lane);
+        }
         float2* qc = Q + ((long long)b * ncols + col) * NY;
 #pragma unroll
         for (int i = 0; i < EPT; ++i) qc[tgwfft::out_pos<NY>(i, lane)] = v[i];
@@ -191,6 +312,14 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ 
         nx[zslot0] = n0;
         nx[zslot1] = n1;
         __syncwarp();
+    }
+    if constexpr (TM) {
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (warp == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem_slot));
+        }
     }
 }
 
@@ -403,41 +532,42 @@ cudaError_t launch_spec_z_fast(int NZ, const float2* A, float2* Z, int Ty, int T
     return cudaGetLastError();
 }
 
-template <int NY, int NI>
+template <int NY, int NI, bool TM>
 static cudaError_t launch_corr_y_s_ni(const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
                                       long long ncols, int nb, cudaStream_t st) {
     const unsigned g = (unsigned)((ncols + 7) / 8);
     const size_t smem = sizeof(float2) * (NY * 17 + 64 + 8 * 128 + 3 * 7 * 32);
-    cudaFuncSetAttribute(k_corr_y_s<NY, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_corr_y_s<NY, NI><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(NY));
+    cudaFuncSetAttribute(k_corr_y_s<NY, NI, TM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_corr_y_s<NY, NI, TM><<<g, 256, smem, st>>>(fimg, Z, Q, Ty, d0y, ncols, nb, twiddle_table<float2>(NY));
     return cudaGetLastError();
 }
 
-template <int NY>
+template <int NY, bool TM>
 static cudaError_t launch_corr_y_s(const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y, long long ncols,
                                    int nb, cudaStream_t st) {
     switch ((Ty + 7) / 8) {
-        case 1: return launch_corr_y_s_ni<NY, 1>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
-        case 2: return launch_corr_y_s_ni<NY, 2>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
-        case 3: return launch_corr_y_s_ni<NY, 3>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
-        case 4: return launch_corr_y_s_ni<NY, 4>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
-        case 5: return launch_corr_y_s_ni<NY, 5>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
-        case 6: return launch_corr_y_s_ni<NY, 6>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
-        case 7: return launch_corr_y_s_ni<NY, 7>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
-        case 8: return launch_corr_y_s_ni<NY, 8>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 1: return launch_corr_y_s_ni<NY, 1, TM>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 2: return launch_corr_y_s_ni<NY, 2, TM>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 3: return launch_corr_y_s_ni<NY, 3, TM>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 4: return launch_corr_y_s_ni<NY, 4, TM>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 5: return launch_corr_y_s_ni<NY, 5, TM>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 6: return launch_corr_y_s_ni<NY, 6, TM>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 7: return launch_corr_y_s_ni<NY, 7, TM>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        case 8: return launch_corr_y_s_ni<NY, 8, TM>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_corr_y_fast(int NY, const float2* fimg, const float2* Z, float2* Q, int Ty, int d0y,
-                               long long ncols, int nb, cudaStream_t st) {
+                               long long ncols, int nb, cudaStream_t st, bool tmem) {
     if (NY == 928) return launch_corr_y_p928(fimg, Z, Q, Ty, d0y, ncols, nb, st);
     const unsigned g = (unsigned)((ncols + 7) / 8);
     const size_t smem = sizeof(float2) * (NY * 17 + 64 + 8 * 128);
     if (NY == 512 || NY == 256) {
         if (Ty < 1 || Ty > 64) return cudaErrorInvalidValue;
-        return NY == 512 ? launch_corr_y_s<512>(fimg, Z, Q, Ty, d0y, ncols, nb, st)
-                         : launch_corr_y_s<256>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        if (NY == 256) return launch_corr_y_s<256, false>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
+        return tmem ? launch_corr_y_s<512, true>(fimg, Z, Q, Ty, d0y, ncols, nb, st)
+                    : launch_corr_y_s<512, false>(fimg, Z, Q, Ty, d0y, ncols, nb, st);
     }
     if (NY == 128) {
         cudaFuncSetAttribute(k_corr_y_w<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
