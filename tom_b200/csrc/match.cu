@@ -886,19 +886,48 @@ int MatchPlan::set_volume(const float* vol) {
     double* v64 = nullptr;
     double2 *f1 = nullptr, *f2 = nullptr, *fm = nullptr;
     double* m2 = nullptr;
+    bool owns_ws = true;  // false while the workspace is borrowed from Q and H
     auto cleanup = [&]() {
+        if (!owns_ws) return;
         if (v64) cudaFree(v64);
         if (f1) cudaFree(f1);
         if (f2) cudaFree(f2);
         if (fm) cudaFree(fm);
         if (m2) cudaFree(m2);
     };
-    if (cudaMalloc(&v64, sizeof(double) * nvox) || cudaMalloc(&f1, sizeof(double2) * hs) ||
-        cudaMalloc(&f2, sizeof(double2) * hs) || cudaMalloc(&fm, sizeof(double2) * hs) ||
-        cudaMalloc(&m2, sizeof(double) * nvox)) {
-        cudaGetLastError();
-        cleanup();
-        return fail(ctx, TOMGPU_ERR_OOM, "set_volume FP64 workspace allocation failed");
+    // The FP64 workspace (about 40 bytes per voxel) lives in the rotation-batch
+    // buffers Q and H when they are large enough: they are idle between batch
+    // calls, and a search over many tomograms then allocates nothing per volume.
+    // Otherwise it is allocated for this call.
+    {
+        struct Piece { void** p; size_t bytes; };
+        const Piece pieces[] = {{(void**)&v64, sizeof(double) * nvox}, {(void**)&m2, sizeof(double) * nvox},
+                                {(void**)&f1, sizeof(double2) * hs}, {(void**)&f2, sizeof(double2) * hs},
+                                {(void**)&fm, sizeof(double2) * hs}};
+        const size_t cap = d_Q && d_H ? sizeof(float2) * hs * (size_t)B : 0;
+        char* bufs[2] = {reinterpret_cast<char*>(d_Q), reinterpret_cast<char*>(d_H)};
+        size_t used[2] = {0, 0};
+        bool borrowed = cap > 0;
+        for (const Piece& pc : pieces) {
+            const size_t b = (pc.bytes + 255) & ~size_t(255);
+            int k = used[0] + b <= cap ? 0 : (used[1] + b <= cap ? 1 : -1);
+            if (k < 0) { borrowed = false; break; }
+            *pc.p = bufs[k] + used[k];
+            used[k] += b;
+        }
+        if (!borrowed) {
+            v64 = m2 = nullptr;
+            f1 = f2 = fm = nullptr;
+            if (cudaMalloc(&v64, sizeof(double) * nvox) || cudaMalloc(&f1, sizeof(double2) * hs) ||
+                cudaMalloc(&f2, sizeof(double2) * hs) || cudaMalloc(&fm, sizeof(double2) * hs) ||
+                cudaMalloc(&m2, sizeof(double) * nvox)) {
+                cudaGetLastError();
+                cleanup();
+                return fail(ctx, TOMGPU_ERR_OOM, "set_volume FP64 workspace allocation failed");
+            }
+        } else {
+            owns_ws = false;
+        }
     }
     int rc = TOMGPU_OK;
     do {
