@@ -145,8 +145,12 @@ __global__ void __launch_bounds__(256) k_inv_z_tc256(const float2* __restrict__ 
     unsigned* tmem_slot = reinterpret_cast<unsigned*>(bar + 1);
     int* flag = reinterpret_cast<int*>(tmem_slot + 1);
     const int tid = threadIdx.x, warp = tid >> 5;
-    // a block of this launch that already timed out: the rest return at once
-    if (err && *reinterpret_cast<volatile int*>(err)) return;
+    // once a block of this launch has timed out, the rest return at once (one
+    // read, shared, so the whole block decides alike)
+    __shared__ int skip_block;
+    if (threadIdx.x == 0) skip_block = err && *reinterpret_cast<volatile int*>(err);
+    __syncthreads();
+    if (skip_block) return;
     const int k1 = tid >> 4, yl = tid & 15;  // stage A row (k1, y); stage B row (q = k1, y)
     const int y = blockIdx.x * 16 + yl, kx = blockIdx.y, b = blockIdx.z;
     const bool ok = y < Ny;

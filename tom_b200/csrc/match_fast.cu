@@ -19,32 +19,12 @@
 #include "ctx.h"
 #include "match.h"
 #include "twiddles.h"
+#include "tmem_util.cuh"
 #include "warp_fft.cuh"
 
 namespace tg {
 
 namespace {
-
-// Tensor-memory helpers of the y-column kernel: each thread keeps per-lane
-// constants (its F_I values, its inverse-FFT twiddles) in its own TMEM lane
-// and reads them back with tcgen05.ld instead of from shared memory.
-__device__ __forceinline__ void tm_st16(unsigned taddr, const float (&v)[16]) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16};\n" ::"r"(taddr),
-        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]),
-        "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]));
-}
-__device__ __forceinline__ void tm_ld16(unsigned taddr, float (&v)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];\n"
-        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]),
-          "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 // The 512-point inverse warp transform (plan 8, 8, 8) with the twiddles of
 // stages 2 and 3 read from this thread's TMEM lane: columns c2 + 16 q and
@@ -60,7 +40,7 @@ __device__ __forceinline__ void warp_ifft512_tm(float2* v, float2* buf, unsigned
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             float t[16];
-            tm_ld16((stage == 0 ? c2 : c3) + 16u * q, t);
+            tgtm::ld16((stage == 0 ? c2 : c3) + 16u * q, t);
 #pragma unroll
             for (int r = 1; r < 8; ++r) v[q * 8 + r] = cmul(v[q * 8 + r], make_float2(t[2 * r - 2], t[2 * r - 1]));
             tgfft::dft8<+1>(v + q * 8);
@@ -188,11 +168,7 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ 
     const int zslot0 = (lane & 7) * 8 + (lane >> 3), zslot1 = zslot0 + 4;  // t = lane, lane + 32
     const bool active = col < ncols;
     if constexpr (TM) {
-        if (warp == 0) {
-            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(
-                (unsigned)__cvta_generic_to_shared(&tmem_slot)));
-            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-        }
+        if (warp == 0) tgtm::alloc<256>(&tmem_slot);
     }
     if (active) {
 #pragma unroll
@@ -206,12 +182,12 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ 
         zw[zslot0] = lane < Ty ? zc[lane] : make_float2(0.f, 0.f);
         zw[zslot1] = lane + 32 < Ty ? zc[lane + 32] : make_float2(0.f, 0.f);
     }
-    if constexpr (TM) asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    if constexpr (TM) tgtm::fence_before();
     __syncthreads();  // the tables (and the TMEM allocation)
     unsigned tw_base = 0;
     if constexpr (TM) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        tw_base = tmem_slot + ((unsigned)(32 * (warp & 3)) << 16) + 128u * (unsigned)(warp >> 2);
+        tgtm::fence_after();
+        tw_base = tgtm::lane_addr(tmem_slot, warp, 128u * (unsigned)(warp >> 2));
         if (active) {
             // columns [0, 32): the lane's 16 F_I values; [32, 64) and [64, 96): the
             // conjugated twiddles of stage 2 (stride 8) and stage 3 (stride 64)
@@ -224,7 +200,7 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ 
                     t[2 * i] = f.x;
                     t[2 * i + 1] = f.y;
                 }
-                tm_st16(tw_base + 16u * h, t);
+                tgtm::st16(tw_base + 16u * h, t);
             }
 #pragma unroll
             for (int stage = 0; stage < 2; ++stage) {
@@ -240,10 +216,10 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ 
                         t[2 * r - 1] = w.y;
                     }
                     t[14] = t[15] = 0.f;
-                    tm_st16(tw_base + 32u + 32u * stage + 16u * q, t);
+                    tgtm::st16(tw_base + 32u + 32u * stage + 16u * q, t);
                 }
             }
-            tm_wait_st();
+            tgtm::wait_st();
         }
     }
     for (int b = 0; b < (active ? nb : 0); ++b) {
@@ -295,7 +271,7 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ 
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 float t[16];
-                tm_ld16(tw_base + 16u * h, t);
+                tgtm::ld16(tw_base + 16u * h, t);
 #pragma unroll
                 for (int i = 0; i < 8; ++i) v[8 * h + i] = cmulc(make_float2(t[2 * i], t[2 * i + 1]), v[8 * h + i]);
             }
@@ -314,11 +290,11 @@ __global__ void __launch_bounds__(256, 2) k_corr_y_s(const float2* __restrict__ 
         __syncwarp();
     }
     if constexpr (TM) {
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        tgtm::fence_before();
         __syncthreads();
         if (warp == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(tmem_slot));
+            tgtm::fence_after();
+            tgtm::dealloc<256>(tmem_slot);
         }
     }
 }

@@ -292,7 +292,12 @@ __global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_t464(const __grid_constan
                                                             const float2* __restrict__ tw_x, tgpq::Cos29 cs,
                                                             int* __restrict__ err) {
     constexpr int NH = 464, NX = 2 * NH, P = 29, YT = C2_YT;
-    if (err && *reinterpret_cast<volatile int*>(err)) return;
+    // once a block of this launch has timed out, the rest return at once (one
+    // read, shared, so the whole block decides alike)
+    __shared__ int skip_block;
+    if (threadIdx.x == 0) skip_block = err && *reinterpret_cast<volatile int*>(err);
+    __syncthreads();
+    if (skip_block) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char* base = smem_raw + ((1024u - (tgtma::smem_u32(smem_raw) & 1023u)) & 1023u);
     float2* xb = reinterpret_cast<float2*>(base + 2 * T4_STAGE);  // [YT][29][17] exchange

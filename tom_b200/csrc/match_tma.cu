@@ -19,13 +19,21 @@
 // distinct banks.  After every line has read its tile, the stage holds the
 // exchange (line yl at yl * 2 KB, [j][q ^ j]), then is refilled by the TMA.
 //
+// Per-thread constants in tensor memory: a thread's 16 unpack twiddles
+// W512^k (k = j + 16 k2) and its 16 exchange twiddles W256^(q j) depend only
+// on its lane in the line, so they sit in its TMEM lane (128 columns per
+// block, warp w at lanes 32 (w mod 4), columns 64 (w / 4) + [0, 64)) and are
+// read with tcgen05.ld, which takes 32 of a thread's 96 shared-memory
+// accesses per rotation off the shared-memory pipe.
+//
 // Waits are bounded: a stage that does not fill within the limit sets the
 // context's device error word (TOMGPU_ERR_TIMEOUT at the next synchronise),
-// the block waits (bounded) for its other loads and returns without touching
-// the results.
+// the block waits (bounded) for its other loads, releases its TMEM and
+// returns without touching the results.
 #include "ctx.h"
 #include "match.h"
 #include "tma_util.cuh"
+#include "tmem_util.cuh"
 #include "twiddles.h"
 #include "warp_fft.cuh"
 
@@ -52,8 +60,12 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
                                                      const float2* __restrict__ tw_h, const float2* __restrict__ tw_x,
                                                      int* __restrict__ err) {
     constexpr int NH = 256, NX = 2 * NH, P = 16, QN = 16;
-    // a block of this launch that already timed out: the rest return at once
-    if (err && *reinterpret_cast<volatile int*>(err)) return;
+    // once a block of this launch has timed out, the rest return at once (one
+    // read, shared, so the whole block decides alike)
+    __shared__ int skip_block;
+    if (threadIdx.x == 0) skip_block = err && *reinterpret_cast<volatile int*>(err);
+    __syncthreads();
+    if (skip_block) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // the swizzled stages need a 1 KB aligned base (the launch adds the slack)
     unsigned char* base =
@@ -71,6 +83,9 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
     }
     for (int i = tid; i < NH; i += blockDim.x) twx[i] = cconj(__ldg(tw_x + i));
     for (int b = tid; b < nb; b += blockDim.x) kaps[b] = (float)(c_mean * (tsum[b] * inv_m - mu_t));
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(flag + 1);
+    const int warp = tid >> 5;
+    if (warp == 0) tgtm::alloc<128>(tmem_slot);
     if (tid == 0) {
         for (int s = 0; s < CT_STG; ++s) tgtma::mbar_init(smem_u32(bars + s), 1);
         *flag = 0;
@@ -78,7 +93,27 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
         tgtma::prefetch_map(&tm_rows);
         tgtma::prefetch_map(&tm_last);
     }
+    tgtm::fence_before();
     __syncthreads();
+    tgtm::fence_after();
+    // this thread's constants into its TMEM lane: columns [0, 32) the unpack
+    // twiddles of k = j + 16 k2, [32, 64) the exchange twiddles T[q][j]
+    const unsigned taddr = tgtm::lane_addr(*tmem_slot, warp, 64u * (unsigned)(warp >> 2));
+    {
+        float t[16];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int c = 8 * (h & 1) + i;
+                const float2 w = h < 2 ? twx[j + P * c] : T[c * P + j];
+                t[2 * i] = w.x;
+                t[2 * i + 1] = w.y;
+            }
+            tgtm::st16(taddr + 16u * h, t);
+        }
+        tgtm::wait_st();
+    }
     const unsigned sbase = smem_u32(base);
     // rotation b into stage s: rows kx 0..255, then row 256 (box edges stop at 256)
     auto issue = [&](int b, int s) {
@@ -107,7 +142,7 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
         __syncthreads();
         if (*flag) {
             // the stage never filled: wait (bounded) for the loads still in
-            // flight, report, return without touching the results
+            // flight, report; the block leaves the loop and the results alone
             if (tid == 0) {
                 tg_flag_error(err, TG_DEV_TIMEOUT);
                 for (int r = b + 1; r < nb && r <= b + 2; ++r) {
@@ -115,26 +150,31 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
                     tgtma::mbar_wait_bounded(smem_u32(bars + s), (unsigned)((r / CT_STG) & 1), CT_WAIT_LIMIT);
                 }
             }
-            return;
+            break;
         }
         (void)tgtma::mbar_test_wait(bar, parity);  // every thread observes the completed phase
         const unsigned char* st = base + cur * CT_STAGE;
         const int cy = line >> 1, hy = (line & 1) << 3;  // chunk and half of this line's y in a row
         float2 u[QN];
+        float tk[16];
 #pragma unroll
         for (int k2 = 0; k2 < QN; ++k2) {
             const int k = j + P * k2, kr = NH - k;
+            if ((k2 & 7) == 0) tgtm::ld16(taddr + 2u * (unsigned)k2, tk);
             const float2 xa = *reinterpret_cast<const float2*>(st + k * CT_ROWB + ((cy ^ (k & 7)) << 4) + hy);
             const float2 xc =
                 cconj(*reinterpret_cast<const float2*>(st + kr * CT_ROWB + ((cy ^ (kr & 7)) << 4) + hy));
-            const float2 d = cmul(twx[k], csub(xa, xc));
+            const float2 d = cmul(make_float2(tk[2 * (k2 & 7)], tk[2 * (k2 & 7) + 1]), csub(xa, xc));
             u[k2] = cadd(cadd(xa, xc), make_float2(-d.y, d.x));
         }
         __syncthreads();  // every line has read the tile: the stage takes the exchange
         tgfft::dft16<+1>(u);
         float2* xl = reinterpret_cast<float2*>(base + cur * CT_STAGE) + line * 256;
 #pragma unroll
-        for (int q = 0; q < QN; ++q) xl[j * 16 + (q ^ j)] = cmul(u[q], T[q * P + j]);
+        for (int q = 0; q < QN; ++q) {
+            if ((q & 7) == 0) tgtm::ld16(taddr + 32u + 2u * (unsigned)q, tk);
+            xl[j * 16 + (q ^ j)] = cmul(u[q], make_float2(tk[2 * (q & 7)], tk[2 * (q & 7) + 1]));
+        }
         __syncwarp();
         float2 v[P];
 #pragma unroll
@@ -153,7 +193,14 @@ __global__ void __launch_bounds__(256, 2) k_c2r_t256(const __grid_constant__ CUt
         tgtma::fence_proxy_async();
         __syncthreads();
     }
-    if (y >= Ny) return;
+    const bool failed = *flag != 0;
+    tgtm::fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tgtm::fence_after();
+        tgtm::dealloc<128>(*tmem_slot);
+    }
+    if (failed || y >= Ny) return;
     const float mt = (float)mu_t;
     const long long row = ((long long)z * Ny + y) * NX;
 #pragma unroll
