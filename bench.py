@@ -67,8 +67,8 @@ def parse():
     p.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
                    help="kernel path of the plan: 0 fastest (TMA x-line tiles at the 512 x edge), 1 generic, "
                         "2 as 0 with cp.async x-line tiles, 3 as 0 with the tcgen05 inverse z-DFT")
-    p.add_argument("--e2e-rot", type=int, default=1024)
-    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-rot", type=int, default=2048)
+    p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=20.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
