@@ -25,6 +25,7 @@
 #include "pq29.cuh"
 #include "tile_copy.cuh"
 #include "tma_util.cuh"
+#include "tmem_util.cuh"
 #include "twiddles.h"
 #include "warp_fft.cuh"
 
@@ -276,7 +277,9 @@ __global__ void __launch_bounds__(16 * C2_YT, 3) k_c2r_p464(const float2* __rest
 // per-stage mbarrier, instead of ~29 eight-byte cp.async per thread.  Two
 // stages; waits bounded (a stage that never fills sets the device error word
 // and the block returns without touching the results).  1-GPU code: the maps
-// cover this GPU's own H, no load multicasts.
+// cover this GPU's own H, no load multicasts.  A thread's unpack twiddles and
+// exchange twiddles (for its k1 = q and q + 16) sit in its TMEM lane and are
+// read with tcgen05.ld instead of from shared memory.
 constexpr int T4_STAGE = 30720;              // 465 rows x 64 bytes, rounded up to 1 KB
 constexpr unsigned T4_TX = 465u * 64u;
 constexpr long long T4_WAIT_LIMIT = 1ll << 20;
@@ -314,6 +317,9 @@ __global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_t464(const __grid_constan
     }
     for (int i = tid; i < NH; i += blockDim.x) twx[i] = cconj(__ldg(tw_x + i));
     for (int b = tid; b < nb; b += blockDim.x) kaps[b] = (float)(c_mean * (tsum[b] * inv_m - mu_t));
+    unsigned* tmem_slot = reinterpret_cast<unsigned*>(flag + 1);
+    const int warp = tid >> 5;
+    if (warp == 0) tgtm::alloc<128>(tmem_slot);
     if (tid == 0) {
         tgtma::mbar_init(tgtma::smem_u32(bars), 1);
         tgtma::mbar_init(tgtma::smem_u32(bars + 1), 1);
@@ -322,7 +328,34 @@ __global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_t464(const __grid_constan
         tgtma::prefetch_map(&tm_a);
         tgtma::prefetch_map(&tm_b);
     }
+    tgtm::fence_before();
     __syncthreads();
+    tgtm::fence_after();
+    // this thread's constants into its TMEM lane (warp w: lanes 32 w): for
+    // it = 0, 1 (k1 = q + 16 it) columns 64 it + [0, 32) the unpack twiddles
+    // of k = k1 + 29 k2 and 64 it + [32, 64) the exchange twiddles T[qq][k1]
+    // (zeros where k1 >= 29)
+    const unsigned taddr = tgtm::lane_addr(*tmem_slot, warp, 0u);
+    {
+        float t[16];
+#pragma unroll
+        for (int it = 0; it < 2; ++it) {
+            const int k1 = q + 16 * it;
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int c = 8 * (h & 1) + i;
+                    float2 w = make_float2(0.f, 0.f);
+                    if (k1 < P) w = h < 2 ? twx[k1 + P * c] : T[c * 32 + k1];
+                    t[2 * i] = w.x;
+                    t[2 * i + 1] = w.y;
+                }
+                tgtm::st16(taddr + 64u * (unsigned)it + 16u * (unsigned)h, t);
+            }
+        }
+        tgtm::wait_st();
+    }
     const unsigned sbase = tgtma::smem_u32(base);
     auto issue = [&](int b, int s) {
         if (tid == 0) {
@@ -354,26 +387,41 @@ __global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_t464(const __grid_constan
                 if (b + 1 < nb) tgtma::mbar_wait_bounded(tgtma::smem_u32(bars + ((b + 1) & 1)),
                                                          (unsigned)(((b + 1) >> 1) & 1), T4_WAIT_LIMIT);
             }
-            return;
+            break;
         }
         (void)tgtma::mbar_test_wait(bar, parity);
         const unsigned char* st = base + cur * T4_STAGE;
-        // unpack and the inner 16-point DFTs: k = k1 + 29 k2
+        // unpack and the inner 16-point DFTs: k = k1 + 29 k2, k1 = q + 16 it;
+        // every lane takes part in the TMEM loads (warp-collective), the
+        // lanes with k1 >= 29 skip the arithmetic
 #pragma unroll 1
-        for (int k1 = q; k1 < P; k1 += 16) {
+        for (int it = 0; it < 2; ++it) {
+            const int k1 = q + 16 * it;
+            const bool ok = k1 < P;
             float2 u[16];
+            float tk[16];
 #pragma unroll
             for (int k2 = 0; k2 < 16; ++k2) {
-                const int k = k1 + P * k2, kr = NH - k;
+                if ((k2 & 7) == 0) {
+                    __syncwarp();
+                    tgtm::ld16(taddr + 64u * (unsigned)it + 2u * (unsigned)k2, tk);
+                }
+                const int k = ok ? k1 + P * k2 : 0, kr = NH - k;
                 const float2 xa = *reinterpret_cast<const float2*>(st + k * 64 + ((cy ^ ((k >> 1) & 3)) << 4) + hy);
                 const float2 xc =
                     cconj(*reinterpret_cast<const float2*>(st + kr * 64 + ((cy ^ ((kr >> 1) & 3)) << 4) + hy));
-                const float2 d = cmul(twx[k], csub(xa, xc));
+                const float2 d = cmul(make_float2(tk[2 * (k2 & 7)], tk[2 * (k2 & 7) + 1]), csub(xa, xc));
                 u[k2] = cadd(cadd(xa, xc), make_float2(-d.y, d.x));
             }
             tgfft::dft16<+1>(u);
 #pragma unroll
-            for (int qq = 0; qq < 16; ++qq) xl[k1 * C2_XR + qq] = cmul(u[qq], T[qq * 32 + k1]);
+            for (int qq = 0; qq < 16; ++qq) {
+                if ((qq & 7) == 0) {
+                    __syncwarp();
+                    tgtm::ld16(taddr + 64u * (unsigned)it + 32u + 2u * (unsigned)qq, tk);
+                }
+                if (ok) xl[k1 * C2_XR + qq] = cmul(u[qq], make_float2(tk[2 * (qq & 7)], tk[2 * (qq & 7) + 1]));
+            }
         }
         __syncwarp();
         float2 v[P];
@@ -389,7 +437,14 @@ __global__ void __launch_bounds__(16 * C2_YT, 2) k_c2r_t464(const __grid_constan
         tgtma::fence_proxy_async();
         __syncthreads();  // the stage is refilled and the exchange rewritten next
     }
-    if (y >= Ny) return;
+    const bool failed = *flag != 0;
+    tgtm::fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tgtm::fence_after();
+        tgtm::dealloc<128>(*tmem_slot);
+    }
+    if (failed || y >= Ny) return;
     const float mt = (float)mu_t;
     const long long row = ((long long)z * Ny + y) * NX;
 #pragma unroll
