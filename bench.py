@@ -45,12 +45,14 @@ UNIT = "rot*voxel/s"
 # from ncu captures of thinner volumes with the same x and y edges, scaled by
 # the voxel count (every term of these kernels' traffic scales with it):
 # 512x128x64 (batch 16, 32: the cp.async x-line kernel) and 512x512x48
-# (batch 64: the TMA x-line kernel and the y-column kernel) for the
-# 512x512x256 tomogram; 928x928x48 (batch 32) for the 928x928x464 one.
+# (batch 64: the TMA x-line kernel and the y-column kernel), 512x64x256 at
+# batch 16 (the z-line kernel; its traffic also scales with the batch) for
+# the 512x512x256 tomogram; 928x928x48 (batch 32) for the 928x928x464 one.
 TRAFFIC = {"exhaustive_512x512x256": {"c2r_flcf": {16: 16 * (336639232 + 22247680),
                                                   32: 16 * (606162432 + 24264960),
                                                   64: 256 / 48 * (3435212032 + 94609920)},
-                                     "corr_y": {64: 256 / 48 * (303350272 + 3173413120)}},
+                                     "corr_y": {64: 256 / 48 * (303350272 + 3173413120)},
+                                     "inv_z": {64: 32 * (538986496 + 487509760)}},
            "exhaustive_928x928x464": {"c2r_flcf": {32: 464 / 48 * (5964541184 + 316938496)},
                                       "corr_y": {32: 464 / 48 * (440176384 + 5247565312)}}}
 
@@ -485,6 +487,14 @@ def main():
     achieved = ab / avg_s / 1e9 if avg_s > 0 else 0.0
     traffic = TRAFFIC.get(args.workload, {}).get(dom, {}).get(args.batch)
     shares = {k: round(v[0] / max(sum(x[0] for x in kt.values()), 1e-9), 4) for k, v in kt.items()}
+    # the same figure for every kernel class with algorithmic bytes
+    rooflines = {}
+    for kind, (kms, kn) in kt.items():
+        kb = algorithmic_bytes(kind, cfg, nb)
+        if kb and kn:
+            ks = kms / kn / 1e3
+            rooflines[kind] = {"avg_launch_ms": ks * 1e3, "achieved": kb / ks / 1e9, "frac": kb / ks / 1e9 / peak,
+                               "traffic": TRAFFIC.get(args.workload, {}).get(kind, {}).get(args.batch)}
 
     # accuracy: top-K peaks of the max-CC map rescored in FP64 by direct sums
     rescore = None
@@ -567,7 +577,7 @@ def main():
                 "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                              "algorithmic_bytes_per_launch": ab, "avg_launch_ms": avg_s * 1e3},
-                "kernel_share": shares, "fp64_rescore": rescore,
+                "kernel_share": shares, "rooflines": rooflines, "fp64_rescore": rescore,
                 "seconds_per_search": {"device": len(grid) * nvox * world / value,
                                        "e2e": len(grid) * nvox * world / e2e["value"] if e2e else None,
                                        "note": "the whole angle grid at this rate, one template"},
