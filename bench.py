@@ -81,6 +81,9 @@ def parse():
     p.add_argument("--learned-steps", type=int, default=400, help="timed training steps of the learned_256 workload")
     p.add_argument("--align-particles", type=int, default=40,
                    help="particles timed for --workload align_2048 (extrapolated to 2048)")
+    p.add_argument("--align-path", type=int, default=0, choices=[0, 1, 2],
+                   help="align_2048: 0 the batched engine (entries of all particles of a box edge), 1 one job at "
+                        "a time, 2 batched without the pruned last inverse DFT")
     p.add_argument("--workload", default=WORKLOAD,
                    help="exhaustive_512x512x256 (the benchmark), profile_256x256x128 (profiler captures) or "
                         "align_2048 (batched subtomogram alignment, not the headline metric)")
@@ -378,12 +381,28 @@ def run_align(args):
     first = {}
     for j in jobs:
         first.setdefault(j["ref"].shape, j)
-    tb.av3_align_batch(list(first.values()), ctx)
+    tb.av3_align_batch(list(first.values()), ctx, path=args.align_path)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    angles, shifts, peaks = tb.av3_align_batch(jobs, ctx)
-    torch.cuda.synchronize()
-    dt = time.perf_counter() - t0
+
+    def timed(sub):
+        """median and minimum wall time of three calls on sub (all on the device at the end)"""
+        ts = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            out = tb.av3_align_batch(sub, ctx, path=args.align_path)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t)
+        return float(np.median(ts)), float(min(ts)), out
+
+    l0 = ctx.launches
+    clocks = ClockSampler(local)
+    clocks.start()
+    h0 = time.time()
+    dt, dt_min, (angles, shifts, peaks) = timed(jobs)
+    clocks.mark(h0, time.time())
+    clk = clocks.stop()
+    launches = (ctx.launches - l0) // 3
     ok = [np.allclose(a, t[0]) for a, t in zip(angles, truth)]
     vox = [int(np.prod(j["ref"].shape)) for j in jobs]
     rv = 1331 * sum(vox)
@@ -391,17 +410,26 @@ def run_align(args):
     for j, v in zip(jobs, vox):
         per_size.setdefault(j["ref"].shape[0], 0)
         per_size[j["ref"].shape[0]] += 1
+    # each box edge on its own: seconds per particle, and the 2048-particle
+    # workload (edges drawn uniformly from the five) from them
+    per_size_s = {}
+    for n in sorted(per_size):
+        sub = [j for j in jobs if j["ref"].shape[0] == n]
+        per_size_s[n] = timed(sub)[0] / len(sub)
     sizes = (32, 48, 64, 80, 96)
-    mean_vox = np.mean([s ** 3 for s in sizes])
-    est_full = dt / sum(vox) * 2048 * mean_vox
+    if all(n in per_size_s for n in sizes):
+        est_full = 2048 / len(sizes) * sum(per_size_s[n] for n in sizes)
+    else:
+        est_full = dt / sum(vox) * 2048 * np.mean([s ** 3 for s in sizes])
     line = {"metric": "subtomogram alignment rot*voxel/s (tom_av3_align, 1331 triplets per particle)",
-            "value": rv / dt, "unit": "rot*voxel/s", "n_gpus": 1, "particles": len(jobs), "seconds": dt,
+            "value": rv / dt, "unit": "rot*voxel/s", "n_gpus": 1, "particles": len(jobs), "seconds": dt, "seconds_min": dt_min,
             "particles_per_s": len(jobs) / dt, "est_seconds_2048": est_full,
             "planted_angle_agreement": float(np.mean(ok)),
             "planted_angle_note": "fraction of particles whose scan maximum is the planted Euler triplet; "
                                   "not a pass mark: tom_av3_align's own objective (the FP64 oracle) also "
                                   "peaks at other grid triplets for noiseless 6-blob wedged phantoms",
-            "per_size": per_size, "gpu_launches": None,
+            "per_size": per_size, "seconds_per_particle": per_size_s, "gpu_launches": launches,
+            "align_path": args.align_path, "clocks": clk,
             "dtype": "f32", "data": "synthetic"}
     print(json.dumps(line), flush=True)
 
@@ -441,7 +469,8 @@ def main():
                 best, _ = plan.autotune(e, (int(t.item()),))
         args.batch = best
     cc, idx = plan.new_results()
-    rps = args.rot_per_step
+    # a step is a whole number of rotation batches, so every launch is full
+    rps = -(-args.rot_per_step // args.batch) * args.batch
 
     def step(s):
         e, start = chunk(grid, s, world, rank, rps)

@@ -53,8 +53,9 @@ int tomgpu_ctx_destroy(tomgpu_ctx* ctx);
  * (an event wait on the device; the call does not block the host). */
 int tomgpu_ctx_set_stream(tomgpu_ctx* ctx, void* cuda_stream);
 int tomgpu_ctx_synchronize(tomgpu_ctx* ctx);
-/* Release the device memory that tomgpu_match keeps in the context between
- * calls (no counterpart in the reference: TOM plans nothing across calls). */
+/* Release the device memory that tomgpu_match and tomgpu_av3_align keep in
+ * the context between calls (no counterpart in the reference: TOM plans
+ * nothing across calls). */
 int tomgpu_ctx_trim(tomgpu_ctx* ctx);
 /* Device kernel launches issued by this context since creation. */
 int64_t tomgpu_ctx_launch_count(const tomgpu_ctx* ctx);
@@ -333,6 +334,23 @@ typedef struct {
  * (1 float).  Host output arrays of n_jobs*3, n_jobs*3 and n_jobs floats. */
 int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs, float* angles,
                          float* shifts, float* ccf_peak);
+
+/* Engine choice for tomgpu_av3_align_ex_dev (NULL params: the defaults). */
+typedef struct {
+    int path;           /* 0 (default): the jobs with a cubic box of edge 24, 32, 40, 48, 64, 72, 80
+                           or 96 run batched, one stream of (particle, rotation) entries per edge
+                           and wedge form, the others one job at a time; 1: every job one at a
+                           time; 2: as 0 but the scan's last inverse DFT always over the whole
+                           box (0 evaluates it only where mask_ccf is non-zero, when every job
+                           of the edge has a mask_ccf with a small support) */
+    size_t batch_bytes; /* batched engine: device bytes of a batch's two half-spectrum sets
+                           (0: 256 MB) */
+} tomgpu_align_params;
+
+/* tomgpu_av3_align_dev with an engine choice; the same outputs. */
+int tomgpu_av3_align_ex_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs,
+                            const tomgpu_align_params* params, float* angles, float* shifts,
+                            float* ccf_peak);
 
 /* One aligned particle for the averaging step of av3_tomomatch. */
 typedef struct {

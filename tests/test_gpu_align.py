@@ -102,3 +102,68 @@ def test_tom_corr_forms(gpu, oracle, form):
                                        p2.astype(np.float32))
             got = gpu.tom_corr(a, b, "norm", mask, p1, p2)
     assert np.abs(got - ref).max() <= 1e-4 * np.abs(ref).max()
+
+
+def _job(oracle, n, k, wedge, rng_seed, phi=(0, 3, 6), psi=(0, 3, 6), theta=(6, 3, 12), mccf="sphere"):
+    e = (3.0 * (k % 3), 3.0, 9.0)
+    w = oracle.av3_wedge((n, n, n), -50, 55).astype(np.float32) if wedge else None
+    ref, part = _particle(oracle, n, e, (1, 0, -1), seed=rng_seed, wedge=w)
+    sph = oracle.sphere_mask((n, n, n), 4.0, strict=True).astype(np.float32)
+    m = {"sphere": sph, "negative": -sph, "none": None}[mccf]
+    return dict(ref=ref, part=part, phi=phi, psi=psi, theta=theta,
+                mask=oracle.sphere_mask((n, n, n), n / 2 - 2).astype(np.float32),
+                mask_ccf=m, wedge_ref=w, wedge_part=w)
+
+
+def test_batched_engine_equals_per_job(gpu, oracle):
+    """The batched engine (one entry stream per box edge and wedge form, a
+    batch smaller than a particle's scan so that batches span particles and
+    entry groups) gives the per-job results: same angles, shifts and peaks to
+    FP32 rounding.  A 28^3 job (no compiled edge) runs per job in both."""
+    jobs = []
+    spec = [(32, True), (32, True), (24, True), (32, False), (32, True), (48, True), (28, True), (32, False),
+            (24, False)]
+    for k, (n, wedge) in enumerate(spec):
+        jobs.append(_job(oracle, n, k, wedge, 300 + k))
+    # a negative mask_ccf (every in-mask product below zero: the maximum is the
+    # first zero voxel, outside the mask) at 40^3, and 64^3 without mask_ccf
+    # (no pruning of the final inverse)
+    jobs.append(_job(oracle, 40, 1, True, 320, mccf="negative"))
+    jobs.append(_job(oracle, 40, 2, True, 321))
+    jobs.append(_job(oracle, 64, 0, True, 322, mccf="none", phi=(0, 3, 3), psi=(0, 3, 3)))
+    half32 = 17 * 32 * 32 * 8
+    a0, s0, p0 = gpu.av3_align_batch(jobs, path=0, batch_bytes=2 * half32 * 10)
+    a1, s1, p1 = gpu.av3_align_batch(jobs, path=1)
+    assert np.array_equal(a0, a1), (a0, a1)
+    assert np.abs(s0 - s1).max() <= 2e-3, (s0, s1)
+    assert np.allclose(p0, p1, rtol=2e-4, atol=0), (p0, p1)
+    # the default batch (every scan in one batch) and the batched engine
+    # without the pruned last inverse agree too
+    for path in (0, 2):
+        a2, s2, p2 = gpu.av3_align_batch(jobs, path=path)
+        assert np.array_equal(a2, a1), path
+        assert np.abs(s2 - s1).max() <= 2e-3, path
+        assert np.allclose(p2, p1, rtol=2e-4, atol=0), path
+
+
+def test_batched_engine_matches_oracle_without_and_with_wedges(gpu, oracle):
+    """Batched engine against the FP64 oracle of tom_av3_align at 40^3 with
+    wedges (the oracle's own cross-wedged scan) and several particles."""
+    n = 40
+    w = oracle.av3_wedge((n, n, n), -55, 60).astype(np.float32)
+    jobs, want = [], []
+    for k in range(2):
+        euler = (9.0 - 3 * k, 6.0, 12.0)
+        ref, part = _particle(oracle, n, euler, (1, -1, 0), seed=500 + k, wedge=w)
+        mask = oracle.sphere_mask((n, n, n), n / 2 - 2).astype(np.float32)
+        mccf = oracle.sphere_mask((n, n, n), 4.0, strict=True).astype(np.float32)
+        phi, psi, theta = (3, 3, 9), (3, 3, 9), (9, 3, 15)
+        want.append(oracle.av3_align(ref, part, phi, psi, theta, mask, mccf, w, w)[:3])
+        jobs.append(dict(ref=ref, part=part, phi=phi, psi=psi, theta=theta, mask=mask, mask_ccf=mccf,
+                         wedge_ref=w, wedge_part=w))
+    ga, gs, gp = gpu.av3_align_batch(jobs, batch_bytes=2 * 21 * 40 * 40 * 8 * 7)
+    for k in range(2):
+        ra, rs, rp = want[k]
+        assert np.allclose(ga[k], ra), (k, ga[k], ra)
+        assert np.abs(gs[k] - rs).max() <= 0.0015, (gs[k], rs)
+        assert abs(gp[k] - rp) <= 1e-4 * abs(rp), (gp[k], rp)

@@ -49,6 +49,10 @@ class AlignJob(ctypes.Structure):
                 ("theta", ctypes.c_float * 3)]
 
 
+class AlignParams(ctypes.Structure):
+    _fields_ = [("path", ctypes.c_int), ("batch_bytes", ctypes.c_size_t)]
+
+
 class AvgItem(ctypes.Structure):
     _fields_ = [("particle", ctypes.c_void_p), ("wedge", ctypes.c_void_p), ("shift", ctypes.c_float * 3),
                 ("angles", ctypes.c_float * 3)]
@@ -151,6 +155,8 @@ _SIGS = {
                                        c_void_p]),
     "tomgpu_av3_align_dev": (ctypes.c_int, [c_void_p, ctypes.POINTER(AlignJob), ctypes.c_int, c_float_p, c_float_p,
                                             c_float_p]),
+    "tomgpu_av3_align_ex_dev": (ctypes.c_int, [c_void_p, ctypes.POINTER(AlignJob), ctypes.c_int,
+                                                ctypes.POINTER(AlignParams), c_float_p, c_float_p, c_float_p]),
     "tomgpu_match": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p, c_void_p, c_float_p,
                                     ctypes.c_int, ctypes.POINTER(MatchParams), c_void_p, c_void_p]),
 }

@@ -35,6 +35,7 @@
 #include "misc.h"
 #include "peak.h"
 #include "rotate_sample.cuh"
+#include "wedge_pair.cuh"
 
 namespace tg {
 
@@ -75,20 +76,6 @@ __global__ void k_al_rotate(const float* __restrict__ ref, const float* __restri
         for (int q = 0; q < 9; ++q) m[q] = mw[9 * e + q];
         W[(long long)e * nn + v] = rot_sample(wref, nx, ny, nz, m, cx, cy, cz, i, j, k);
     }
-}
-
-// The two source voxels of (W'(k) + W'(-k)) / 2 with W' = ifftshift(W):
-// ifftshift(v) and ifftshift(-v) (all boxes hold fewer than 2^31 voxels).
-TG_D void wedge_pair(int v, int nx, int ny, int nz, int& s1, int& s2) {
-    const int i = v % nx, t = v / nx, j = t % ny, k = t / ny;
-    const int hx = nx / 2, hy = ny / 2, hz = nz / 2;
-    const int a1 = i + hx < nx ? i + hx : i + hx - nx, b1 = j + hy < ny ? j + hy : j + hy - ny,
-              c1 = k + hz < nz ? k + hz : k + hz - nz;
-    const int mi = i ? nx - i : 0, mj = j ? ny - j : 0, mk = k ? nz - k : 0;
-    const int a2 = mi + hx < nx ? mi + hx : mi + hx - nx, b2 = mj + hy < ny ? mj + hy : mj + hy - ny,
-              c2 = mk + hz < nz ? mk + hz : mk + hz - nz;
-    s1 = a1 + nx * (b1 + ny * c1);
-    s2 = a2 + nx * (b2 + ny * c2);
 }
 
 // A[e][k] *= (W'(k) + W'(-k)) / 2 with W' = ifftshift(wedge_part) (the
@@ -267,6 +254,8 @@ __global__ void k_al_r2c_masked(const float* __restrict__ a, const float* __rest
 
 // matrix of tom_angles2rotmatrix (Sptrans/tom_sum_rotation.m): Rz(psi) Rx(theta) Rz(phi)
 // in double, passed to rot3d's matrix mode as single in column-major order
+}  // namespace
+
 void rotmatrix_as_float(double phi, double psi, double theta, float m9[9]) {
     const double d = 3.14159265358979323846 / 180.0;
     const double cf = std::cos(phi * d), sf = std::sin(phi * d), cp = std::cos(psi * d), sp = std::sin(psi * d);
@@ -302,6 +291,8 @@ std::vector<double> axis_values(const float r[3]) {
     return v;
 }
 
+namespace {
+
 struct Workspace {
     float2 *A = nullptr, *B = nullptr, *B0 = nullptr;  // the scan: half spectra; the refinement: complex
     float *Ar = nullptr, *Br = nullptr;                // the scan's real volumes
@@ -323,10 +314,26 @@ struct Workspace {
 struct AlignScratch {
     Workspace w;
     size_t cap[16] = {0};
+    std::vector<void*> pool;  // the batched engine's buffers, by index
+    std::vector<size_t> pool_cap;
     void release() {
         w.release();
         w = Workspace();
         for (size_t& c : cap) c = 0;
+        for (void* p : pool)
+            if (p) cudaFree(p);
+        pool.clear();
+        pool_cap.clear();
+    }
+    // grow-only buffer i to at least b bytes (the contents are not kept)
+    bool grow(int i, void** p, size_t b) {
+        if (b <= cap[i]) return true;
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        cap[i] = 0;
+        if (cudaMalloc(p, b) != cudaSuccess) return false;
+        cap[i] = b;
+        return true;
     }
 };
 
@@ -445,6 +452,89 @@ int corr_norm(tomgpu_ctx* ctx, const float* a, const float* b, const int n[3], c
     return rc;
 }
 
+// After the scan (av3_new/tom_av3_align.m:160-189): the first maximum of
+// ccf_max * mask_ccf gives the angle index (tom_av3_index2angle); the
+// reference rotated by those angles is correlated once more with the particle
+// (tom_corr 'norm' inside the mask, no wedges) and tom_peak(., 'spline') of
+// ccf * mask_ccf gives the shift and the peak.  cmax / amax are the scan's
+// running maximum and angle index volumes, nmask the mask's non-zero count.
+int align_finish(tomgpu_ctx* ctx, const tomgpu_align_job& job, int nph, int nps, const float* cmax,
+                 const float* amax, double nmask, AlignScratch* sc, float angles_out[3], float shifts_out[3],
+                 float* peak_out) {
+    const int* n = job.n;
+    const long long nn = (long long)n[0] * n[1] * n[2];
+    cudaStream_t st = ctx->stream;
+    const bool wedges = job.wedge_ref != nullptr;
+    Workspace& w = sc->w;
+    if (!sc->grow(0, (void**)&w.A, sizeof(float2) * nn) || !sc->grow(1, (void**)&w.B, sizeof(float2) * nn) ||
+        !sc->grow(6, (void**)&w.tmp, sizeof(float) * nn) || !sc->grow(7, (void**)&w.mats, sizeof(float) * 18) ||
+        !sc->grow(8, (void**)&w.aidx, sizeof(int)) || !sc->grow(9, (void**)&w.sums, sizeof(double)) ||
+        !sc->grow(10, (void**)&w.mea, sizeof(double)) || !sc->grow(11, (void**)&w.var, sizeof(double)) ||
+        !sc->grow(12, (void**)&w.spline, sizeof(double) * 8) ||
+        !sc->grow(13, (void**)&w.key, sizeof(unsigned long long))) {
+        cudaGetLastError();
+        sc->release();
+        return fail(ctx, TOMGPU_ERR_OOM, "alignment workspace allocation failed");
+    }
+    const float cx = (float)((n[0] + 1) / 2), cy = (float)((n[1] + 1) / 2), cz = (float)((n[2] + 1) / 2);
+    int rc = TOMGPU_OK;
+    cudaError_t e = cudaSuccess;
+    do {
+        // first maximum of ccf_max * mask_ccf
+        k_al_mul<<<grid_for(nn), 256, 0, st>>>(cmax, job.mask_ccf, w.tmp, nn);
+        if ((e = argmax_key(w.tmp, nn, w.key, st))) break;
+        unsigned long long key = 0;
+        if ((e = cudaMemcpyAsync(&key, w.key, sizeof key, cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaStreamSynchronize(st))) break;
+        if (!key) { rc = fail(ctx, TOMGPU_ERR_DEVICE, "no correlation peak above -99999"); break; }
+        const long long pv = (long long)(0xFFFFFFFFull - (key & 0xFFFFFFFFull));
+        float ai = 0;
+        if ((e = cudaMemcpy(&ai, amax + pv, sizeof(float), cudaMemcpyDeviceToHost))) break;
+        // tom_av3_index2angle
+        const double a3 = std::floor(ai / (double)(nph * nps));
+        const double rest = ai - a3 * nph * nps;
+        const double a2 = std::floor(rest / nph);
+        const double a1 = rest - a2 * nph;
+        const float eul[3] = {(float)(a1 * job.phi[1] + job.phi[0]), (float)(a2 * job.psi[1] + job.psi[0]),
+                              (float)(a3 * job.theta[1] + job.theta[0])};
+        // ccf_s = tom_corr(rot(ref, angles), part, 'norm', mask)
+        float em[9];
+        euler_matrix_host(eul, em);
+        if ((e = cudaMemcpyAsync(w.mats, em, sizeof em, cudaMemcpyHostToDevice, st))) break;
+        int zero = 0;
+        if ((e = cudaMemcpyAsync(w.aidx, &zero, sizeof zero, cudaMemcpyHostToDevice, st))) break;
+        k_al_rotate<<<dim3((unsigned)((nn + 255) / 256), 1), 256, 0, st>>>(job.ref, nullptr, job.mask, w.mats, nullptr,
+                                                                            n[0], n[1], n[2], cx, cy, cz, 0, nullptr,
+                                                                            w.A, nullptr);
+        k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(job.part, wedges ? job.mask : nullptr, w.B, nn);
+        if ((e = normalize_entries(w.A, job.mask, nn, 1, nmask, w, st, &ctx->launches))) break;
+        if ((e = normalize_entries(w.B, job.mask, nn, 1, nmask, w, st, &ctx->launches))) break;
+        if ((e = c2c3d<float2>(w.A, n, -1, 1.0, st))) break;
+        if ((e = c2c3d<float2>(w.B, n, -1, 1.0, st))) break;
+        k_al_cross<<<grid_for(nn), 256, 0, st>>>(w.B, w.A, nn);
+        if ((e = c2c3d<float2>(w.B, n, +1, 1.0 / (double)nn, st))) break;
+        k_al_map<<<grid_for(nn), 256, 0, st>>>(w.B, n[0], n[1], n[2], 1.0 / nmask, job.mask_ccf, w.tmp);
+        if ((e = argmax_key(w.tmp, nn, w.key, st))) break;
+        if ((e = cudaMemcpyAsync(&key, w.key, sizeof key, cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaStreamSynchronize(st))) break;
+        ctx->launches += 16;
+        if (!key) { rc = fail(ctx, TOMGPU_ERR_DEVICE, "no refinement peak above -99999"); break; }
+        const long long pv2 = (long long)(0xFFFFFFFFull - (key & 0xFFFFFFFFull));
+        const int p0[3] = {(int)(pv2 % n[0]), (int)((pv2 / n[0]) % n[1]), (int)(pv2 / ((long long)n[0] * n[1]))};
+        if ((e = spline_peak(w.tmp, n, p0, w.spline, st))) break;
+        double h[6];
+        if ((e = cudaMemcpyAsync(h, w.spline, sizeof h, cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaStreamSynchronize(st))) break;
+        for (int d = 0; d < 3; ++d) {
+            angles_out[d] = eul[d];
+            shifts_out[d] = (float)(h[d] - (std::floor(n[d] / 2.0) + 1.0));
+        }
+        *peak_out = (float)std::fmax(h[3], std::fmax(h[4], h[5]));
+    } while (0);
+    if (e && !rc) rc = cuda_fail(ctx, e, "av3_align");
+    return rc;
+}
+
 int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3], float* peak_out,
               size_t budget_voxels, AlignScratch* scratch) {
     const int* n = job.n;
@@ -471,16 +561,7 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
     AlignScratch& sc = scratch ? *scratch : local;
     Workspace& w = sc.w;
     // grow-only buffers, kept for the next job of the call
-    size_t* cap = sc.cap;
-    auto G = [&](int i, void** p, size_t b) {
-        if (b <= cap[i]) return true;
-        if (*p) cudaFree(*p);
-        *p = nullptr;
-        cap[i] = 0;
-        if (cudaMalloc(p, b) != cudaSuccess) return false;
-        cap[i] = b;
-        return true;
-    };
+    auto G = [&](int i, void** p, size_t b) { return sc.grow(i, p, b); };
     const long long nhn = (long long)(n[0] / 2 + 1) * n[1] * n[2];  // one half spectrum
     const long long ncx = std::max<long long>(nn, nhn * E);         // complex slots: E half spectra or one volume
     if (!G(0, (void**)&w.A, sizeof(float2) * ncx) || !G(1, (void**)&w.B, sizeof(float2) * ncx) ||
@@ -560,58 +641,7 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
             ctx->launches += 2 + 9;
         }
         if (e) break;
-        // first maximum of ccf_max * mask_ccf
-        k_al_mul<<<grid_for(nn), 256, 0, st>>>(w.cmax, job.mask_ccf, w.tmp, nn);
-        if ((e = argmax_key(w.tmp, nn, w.key, st))) break;
-        unsigned long long key = 0;
-        if ((e = cudaMemcpyAsync(&key, w.key, sizeof key, cudaMemcpyDeviceToHost, st))) break;
-        if ((e = cudaStreamSynchronize(st))) break;
-        if (!key) { rc = fail(ctx, TOMGPU_ERR_DEVICE, "no correlation peak above -99999"); break; }
-        const long long pv = (long long)(0xFFFFFFFFull - (key & 0xFFFFFFFFull));
-        float ai = 0;
-        if ((e = cudaMemcpy(&ai, w.amax + pv, sizeof(float), cudaMemcpyDeviceToHost))) break;
-        // tom_av3_index2angle
-        const int nth = (int)th.size();
-        (void)nth;
-        const double a3 = std::floor(ai / (double)(nph * nps));
-        const double rest = ai - a3 * nph * nps;
-        const double a2 = std::floor(rest / nph);
-        const double a1 = rest - a2 * nph;
-        const float eul[3] = {(float)(a1 * job.phi[1] + job.phi[0]), (float)(a2 * job.psi[1] + job.psi[0]),
-                              (float)(a3 * job.theta[1] + job.theta[0])};
-        // ccf_s = tom_corr(rot(ref, angles), part, 'norm', mask)
-        float em[9];
-        euler_matrix_host(eul, em);
-        if ((e = cudaMemcpyAsync(w.mats, em, sizeof em, cudaMemcpyHostToDevice, st))) break;
-        int zero = 0;
-        if ((e = cudaMemcpyAsync(w.aidx, &zero, sizeof zero, cudaMemcpyHostToDevice, st))) break;
-        k_al_rotate<<<dim3((unsigned)((nn + 255) / 256), 1), 256, 0, st>>>(job.ref, nullptr, job.mask, w.mats, nullptr,
-                                                                            n[0], n[1], n[2], cx, cy, cz, 0, nullptr,
-                                                                            w.A, nullptr);
-        k_al_r2c_masked<<<grid_for(nn), 256, 0, st>>>(job.part, wedges ? job.mask : nullptr, w.B, nn);
-        if ((e = normalize_entries(w.A, job.mask, nn, 1, nmask, w, st, &ctx->launches))) break;
-        if ((e = normalize_entries(w.B, job.mask, nn, 1, nmask, w, st, &ctx->launches))) break;
-        if ((e = c2c3d<float2>(w.A, n, -1, 1.0, st))) break;
-        if ((e = c2c3d<float2>(w.B, n, -1, 1.0, st))) break;
-        k_al_cross<<<grid_for(nn), 256, 0, st>>>(w.B, w.A, nn);
-        if ((e = c2c3d<float2>(w.B, n, +1, 1.0 / (double)nn, st))) break;
-        k_al_map<<<grid_for(nn), 256, 0, st>>>(w.B, n[0], n[1], n[2], 1.0 / nmask, job.mask_ccf, w.tmp);
-        if ((e = argmax_key(w.tmp, nn, w.key, st))) break;
-        if ((e = cudaMemcpyAsync(&key, w.key, sizeof key, cudaMemcpyDeviceToHost, st))) break;
-        if ((e = cudaStreamSynchronize(st))) break;
-        ctx->launches += 16;
-        if (!key) { rc = fail(ctx, TOMGPU_ERR_DEVICE, "no refinement peak above -99999"); break; }
-        const long long pv2 = (long long)(0xFFFFFFFFull - (key & 0xFFFFFFFFull));
-        const int p0[3] = {(int)(pv2 % n[0]), (int)((pv2 / n[0]) % n[1]), (int)(pv2 / ((long long)n[0] * n[1]))};
-        if ((e = spline_peak(w.tmp, n, p0, w.spline, st))) break;
-        double h[6];
-        if ((e = cudaMemcpyAsync(h, w.spline, sizeof h, cudaMemcpyDeviceToHost, st))) break;
-        if ((e = cudaStreamSynchronize(st))) break;
-        for (int d = 0; d < 3; ++d) {
-            angles_out[d] = eul[d];
-            shifts_out[d] = (float)(h[d] - (std::floor(n[d] / 2.0) + 1.0));
-        }
-        *peak_out = (float)std::fmax(h[3], std::fmax(h[4], h[5]));
+        rc = align_finish(ctx, job, nph, nps, w.cmax, w.amax, nmask, &sc, angles_out, shifts_out, peak_out);
     } while (0);
     if (e && !rc) rc = cuda_fail(ctx, e, "av3_align");
     if (!scratch) local.release();
@@ -619,6 +649,24 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
 }
 
 AlignScratch* align_scratch_new() { return new AlignScratch(); }
+
+void* align_scratch_buffer(AlignScratch* s, int i, size_t bytes) {
+    if ((size_t)i >= s->pool.size()) {
+        s->pool.resize(i + 1, nullptr);
+        s->pool_cap.resize(i + 1, 0);
+    }
+    if (bytes == 0) bytes = 1;
+    if (bytes <= s->pool_cap[i]) return s->pool[i];
+    if (s->pool[i]) cudaFree(s->pool[i]);
+    s->pool[i] = nullptr;
+    s->pool_cap[i] = 0;
+    if (cudaMalloc(&s->pool[i], bytes) != cudaSuccess) {
+        s->pool[i] = nullptr;
+        return nullptr;
+    }
+    s->pool_cap[i] = bytes;
+    return s->pool[i];
+}
 
 void align_scratch_free(AlignScratch* s) {
     if (!s) return;

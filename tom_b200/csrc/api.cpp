@@ -2,6 +2,7 @@
 // buffer management; the arithmetic runs in the CUDA translation units.
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -39,6 +40,11 @@ struct MatchCache {
 static void drop_match_cache(tomgpu_ctx* ctx) {
     delete static_cast<MatchCache*>(ctx->match_cache);
     ctx->match_cache = nullptr;
+}
+
+static void drop_align_scratch(tomgpu_ctx* ctx) {
+    tg::align_scratch_free(static_cast<tg::AlignScratch*>(ctx->align_scratch));
+    ctx->align_scratch = nullptr;
 }
 
 namespace tg {
@@ -198,6 +204,7 @@ int tomgpu_ctx_destroy(tomgpu_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     drop_match_cache(ctx);
+    drop_align_scratch(ctx);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_err) cudaFree(ctx->d_err);
     for (auto& p : ctx->pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
@@ -875,30 +882,54 @@ int tomgpu_corr_dev(tomgpu_ctx* ctx, const float* a, const float* b, const int d
     return corr_norm(ctx, a, b, dims, mask, psf1, psf2, out);
 }
 
-int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs, float* angles, float* shifts,
-                         float* ccf_peak) {
+int tomgpu_av3_align_ex_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs,
+                            const tomgpu_align_params* params, float* angles, float* shifts, float* ccf_peak) {
     if (!ctx) return TOMGPU_ERR_ARG;
     if (n_jobs < 0 || (n_jobs > 0 && (!jobs || !angles || !shifts || !ccf_peak)))
         return fail(ctx, TOMGPU_ERR_ARG, "null pointer or negative job count");
+    tomgpu_align_params prm{};
+    if (params) prm = *params;
+    if (prm.path < 0 || prm.path > 2) return fail(ctx, TOMGPU_ERR_ARG, "path must be 0, 1 or 2");
     TG_TRY(use_device(ctx));
-    AlignScratch* scratch = align_scratch_new();
-    int rc = TOMGPU_OK;
-    for (int j = 0; j < n_jobs && !rc; ++j) {
+    for (int j = 0; j < n_jobs; ++j) {
         const tomgpu_align_job& jb = jobs[j];
-        if (!dims_ok(jb.n)) {
-            rc = fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad box size");
-            break;
-        }
-        for (int a = 0; a < 3 && !rc; ++a) {
+        if (!dims_ok(jb.n)) return fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad box size");
+        for (int a = 0; a < 3; ++a) {
             const float* r = a == 0 ? jb.phi : (a == 1 ? jb.psi : jb.theta);
             if (r[1] < 0 || (r[1] == 0 && r[2] != r[0]) || r[2] < r[0])
-                rc = fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad angle range");
+                return fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad angle range");
         }
-        if (!rc) rc = align_job(ctx, jb, angles + 3 * j, shifts + 3 * j, ccf_peak + j, (size_t)1 << 24, scratch);
+        if (!jb.ref || !jb.part || !jb.mask)
+            return fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": job needs ref, part and mask");
+    }
+    // jobs of a compiled cubic edge run batched, per (edge, wedge form); the rest one by one
+    std::map<std::pair<int, int>, std::vector<int>> buckets;
+    std::vector<int> rest;
+    for (int j = 0; j < n_jobs; ++j) {
+        if (prm.path != 1 && align_fused_supported(jobs[j]))
+            buckets[{jobs[j].n[0], jobs[j].wedge_ref ? 1 : 0}].push_back(j);
+        else
+            rest.push_back(j);
+    }
+    if (!ctx->align_scratch) ctx->align_scratch = align_scratch_new();
+    AlignScratch* scratch = static_cast<AlignScratch*>(ctx->align_scratch);
+    int rc = TOMGPU_OK;
+    for (auto& kv : buckets) {
+        if (rc) break;
+        rc = align_fused(ctx, jobs, kv.second.data(), (int)kv.second.size(), angles, shifts, ccf_peak,
+                         prm.batch_bytes, prm.path != 2, scratch);
+    }
+    for (int j : rest) {
+        if (rc) break;
+        rc = align_job(ctx, jobs[j], angles + 3 * j, shifts + 3 * j, ccf_peak + j, (size_t)1 << 24, scratch);
     }
     cudaStreamSynchronize(ctx->stream);
-    align_scratch_free(scratch);
     return rc;
+}
+
+int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs, float* angles, float* shifts,
+                         float* ccf_peak) {
+    return tomgpu_av3_align_ex_dev(ctx, jobs, n_jobs, nullptr, angles, shifts, ccf_peak);
 }
 
 int tomgpu_ctx_trim(tomgpu_ctx* ctx) {
@@ -906,6 +937,7 @@ int tomgpu_ctx_trim(tomgpu_ctx* ctx) {
     TG_TRY(use_device(ctx));
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     drop_match_cache(ctx);
+    drop_align_scratch(ctx);
     return TOMGPU_OK;
 }
 

@@ -21,6 +21,9 @@ struct tomgpu_ctx {
     // tomgpu_match's plan and device buffers, kept for the next call with the
     // same sizes and parameters (released by tomgpu_ctx_trim and at destroy)
     void* match_cache = nullptr;
+    // tomgpu_av3_align's grow-only device workspace, kept for the next call
+    // (released by tomgpu_ctx_trim and at destroy)
+    void* align_scratch = nullptr;
     // kernel-class timers (tomgpu_ctx_profile)
     bool prof = false;
     struct Pending { int kind; cudaEvent_t a, b; };

@@ -181,6 +181,20 @@ template <int DIR, typename C> TG_D void dft5(C* v) {
     v[3] = csub(b2, q2);
 }
 
+// 6 = 2 x 3 by the prime-factor mapping (no twiddles): inputs n = 3 n1 + 2 n2
+// (mod 6) into two 3-point DFTs, then 2-point DFTs; output k = 3 k1 + 4 k2.
+template <int DIR, typename C> TG_D void dft6(C* v) {
+    C a[3] = {v[0], v[2], v[4]}, b[3] = {v[3], v[5], v[1]};
+    dft3<DIR>(a);
+    dft3<DIR>(b);
+    v[0] = cadd(a[0], b[0]);
+    v[3] = csub(a[0], b[0]);
+    v[4] = cadd(a[1], b[1]);
+    v[1] = csub(a[1], b[1]);
+    v[2] = cadd(a[2], b[2]);
+    v[5] = csub(a[2], b[2]);
+}
+
 // Prime radix P by direct summation, pairing k with P-k (real/imag symmetry):
 // X_k = a0 + sum_{n=1}^{(P-1)/2} [ (a_n + a_{P-n}) cos + i DIR (a_n - a_{P-n}) sin ].
 // Cos/sin of 2 pi m / P are read from the line's table (P divides L).
@@ -226,6 +240,7 @@ TG_D void dft(C* v, const C* __restrict__ tw, int q) {
     else if constexpr (R == 3) dft3<DIR>(v);
     else if constexpr (R == 4) dft4<DIR>(v[0], v[1], v[2], v[3]);
     else if constexpr (R == 5) dft5<DIR>(v);
+    else if constexpr (R == 6) dft6<DIR>(v);
     else if constexpr (R == 8) dft8<DIR>(v);
     else if constexpr (R == 16) dft16<DIR>(v);
     else if constexpr (R == 32) dft32<DIR>(v);

@@ -146,8 +146,28 @@ int corr_norm(tomgpu_ctx* ctx, const float* a, const float* b, const int n[3], c
 struct AlignScratch;
 AlignScratch* align_scratch_new();
 void align_scratch_free(AlignScratch* s);
+// Buffer i of the scratch's pool, grown to at least bytes (contents not kept);
+// nullptr when the allocation fails.
+void* align_scratch_buffer(AlignScratch* s, int i, size_t bytes);
 int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3], float shifts_out[3],
               float* peak_out, size_t budget_voxels, AlignScratch* scratch);
+// tom_angles2rotmatrix of (phi, psi, theta) in degrees, column-major, rounded to float
+void rotmatrix_as_float(double phi, double psi, double theta, float m9[9]);
+// the values of an angle range [start increment end] (one value when increment = 0)
+std::vector<double> axis_values(const float r[3]);
+// the step after a job's scan: angle of the first maximum of cmax * mask_ccf,
+// one more tom_corr at that angle, spline peak; nph / nps the phi and psi counts
+int align_finish(tomgpu_ctx* ctx, const tomgpu_align_job& job, int nph, int nps, const float* cmax,
+                 const float* amax, double nmask, AlignScratch* sc, float angles_out[3], float shifts_out[3],
+                 float* peak_out);
+// The fused alignment engine (align_fused.cu): jobs of one cubic box edge it
+// compiles, all with or all without wedges, scanned as one batch of
+// (particle, rotation) entries.  job_idx lists the jobs; outputs are indexed
+// by job.  budget_bytes bounds the per-batch spectra (0: the default);
+// allow_prune lets the last inverse DFT run only where mask_ccf is non-zero.
+bool align_fused_supported(const tomgpu_align_job& job);
+int align_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, const int* job_idx, int n, float* angles,
+                float* shifts, float* peaks, size_t budget_bytes, bool allow_prune, AlignScratch* sc);
 int av3_average_add(tomgpu_ctx* ctx, const int n[3], const tomgpu_avg_item* items, int K, double* avg, double* wei);
 int corr3d_peaks(tomgpu_ctx* ctx, const int n[3], const float* const* templates, int nt, const float* const* particles,
                  int np, const double* angles_deg, int nang, const float* mask, const tomgpu_wedge_spec* wedge_t,

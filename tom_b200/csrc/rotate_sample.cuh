@@ -46,4 +46,57 @@ __device__ __forceinline__ float rot_sample(const float* __restrict__ in, int sx
 }
 
 
+// The eight corner values of voxel (i, j, k) for rot_sample, as they are
+// read there (zero where a corner lies beyond the last voxel of an axis):
+// v000 v100 v010 v110 in .x .y .z .w of b[2 v], v001 v101 v011 v111 of b[2 v + 1].
+__device__ __forceinline__ void brick_corners(const float* __restrict__ in, int sx, int sy, int sz, int i, int j,
+                                              int k, float4* __restrict__ b) {
+    const long long sxy = (long long)sx * sy;
+    const long long v = i + (long long)j * sx + (long long)k * sxy;
+    const bool ex = i == sx - 1, ey = j == sy - 1, ez = k == sz - 1;
+    float4 lo, hi;
+    lo.x = in[v];
+    lo.y = ex ? 0.f : in[v + 1];
+    lo.z = ey ? 0.f : in[v + sx];
+    lo.w = (ex || ey) ? 0.f : in[v + sx + 1];
+    hi.x = ez ? 0.f : in[v + sxy];
+    hi.y = (ex || ez) ? 0.f : in[v + sxy + 1];
+    hi.z = (ey || ez) ? 0.f : in[v + sxy + sx];
+    hi.w = (ex || ey || ez) ? 0.f : in[v + sxy + sx + 1];
+    b[2 * v] = lo;
+    b[2 * v + 1] = hi;
+}
+
+// rot_sample reading the corners from a brick volume (brick_corners): the
+// same coordinates, bounds and float operations, so the same result, from two
+// 16-byte loads instead of eight scattered 4-byte ones.
+__device__ __forceinline__ float rot_sample_brick(const float4* __restrict__ bk, int sx, int sy, int sz,
+                                                  const float* m, float px, float py, float pz, int i, int j,
+                                                  int k) {
+    const float di = (float)(long long)__fsub_rn((float)i, px);
+    const float dj = (float)(long long)__fsub_rn((float)j, py);
+    const float dk = (float)(long long)__fsub_rn((float)k, pz);
+    const float rx = __fadd_rn(__fadd_rn(__fadd_rn(px, __fmul_rn(m[0], di)), __fmul_rn(m[1], dj)),
+                               __fmul_rn(m[2], dk));
+    if (rx < 0.f || rx > (float)(sx - 1)) return 0.f;
+    const float ry = __fadd_rn(__fadd_rn(__fadd_rn(py, __fmul_rn(m[3], di)), __fmul_rn(m[4], dj)),
+                               __fmul_rn(m[5], dk));
+    if (ry < 0.f || ry > (float)(sy - 1)) return 0.f;
+    const float rz = __fadd_rn(__fadd_rn(__fadd_rn(pz, __fmul_rn(m[6], di)), __fmul_rn(m[7], dj)),
+                               __fmul_rn(m[8], dk));
+    if (rz < 0.f || rz > (float)(sz - 1)) return 0.f;
+    const int fx = (int)rx, fy = (int)ry, fz = (int)rz;
+    const float wx = __fsub_rn(rx, (float)fx), wy = __fsub_rn(ry, (float)fy), wz = __fsub_rn(rz, (float)fz);
+    const float ux = __fsub_rn(1.f, wx), uy = __fsub_rn(1.f, wy), uz = __fsub_rn(1.f, wz);
+    const long long b = fx + (long long)fy * sx + (long long)fz * sx * sy;
+    const float4 lo = __ldg(bk + 2 * b), hi = __ldg(bk + 2 * b + 1);
+    const float a = __fadd_rn(lo.x, __fmul_rn(__fsub_rn(lo.y, lo.x), wx));
+    const float bb = __fadd_rn(__fmul_rn(lo.z, ux), __fmul_rn(lo.w, wx));
+    const float c = __fadd_rn(__fmul_rn(hi.x, ux), __fmul_rn(hi.y, wx));
+    const float d = __fadd_rn(__fmul_rn(hi.z, ux), __fmul_rn(hi.w, wx));
+    const float l2 = __fadd_rn(__fmul_rn(a, uy), __fmul_rn(bb, wy));
+    const float h2 = __fadd_rn(__fmul_rn(c, uy), __fmul_rn(d, wy));
+    return __fadd_rn(__fmul_rn(l2, uz), __fmul_rn(h2, wz));
+}
+
 }  // namespace tg

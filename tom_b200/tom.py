@@ -972,11 +972,13 @@ def tom_corr(a, b, *args, ctx: Context | None = None):
     return np.asfortranarray(from_device(out))
 
 
-def av3_align_batch(jobs, ctx: Context | None = None):
+def av3_align_batch(jobs, ctx: Context | None = None, path: int = 0, batch_bytes: int = 0):
     """Run tom_av3_align jobs on the GPU.  Each job is a dict with numpy
     volumes 'ref', 'part', 'mask' (None: tom_spheremask default), 'mask_ccf'
     (None: ones), 'wedge_ref', 'wedge_part' (None: no wedges / same as
     wedge_ref) and angle ranges 'phi', 'psi', 'theta' ([start incr end]).
+    path 0 batches the jobs of each compiled cubic edge, path 1 runs every job
+    alone; batch_bytes bounds a batch's spectra (0: the library default).
     Returns (angles[n,3], shifts[n,3], ccf_peak[n])."""
     import torch
     ctx = ctx or default_context()
@@ -1000,8 +1002,11 @@ def av3_align_batch(jobs, ctx: Context | None = None):
     angles = np.zeros((len(jobs), 3), np.float32)
     shifts = np.zeros((len(jobs), 3), np.float32)
     peaks = np.zeros(len(jobs), np.float32)
-    ctx.check(lib().tomgpu_av3_align_dev(ctx.handle, arr, len(jobs), angles.ctypes.data_as(_lib.c_float_p),
-                                         shifts.ctypes.data_as(_lib.c_float_p), peaks.ctypes.data_as(_lib.c_float_p)))
+    prm = _lib.AlignParams(int(path), int(batch_bytes))
+    ctx.check(lib().tomgpu_av3_align_ex_dev(ctx.handle, arr, len(jobs), ctypes.byref(prm),
+                                            angles.ctypes.data_as(_lib.c_float_p),
+                                            shifts.ctypes.data_as(_lib.c_float_p),
+                                            peaks.ctypes.data_as(_lib.c_float_p)))
     torch.cuda.synchronize(ctx.device)
     return angles, shifts, peaks
 
