@@ -58,14 +58,17 @@ namespace {
 // (every butterfly of a stage lives in registers, N * N / NT elements per
 // thread), and the radices of the line DFTs.
 template <int N> struct Cfg;
-template <> struct Cfg<24> { static constexpr int NT = 192, MINB = 4; typedef tgfft::seq<8, 3> R; };
-template <> struct Cfg<32> { static constexpr int NT = 256, MINB = 4; typedef tgfft::seq<8, 4> R; };
-template <> struct Cfg<40> { static constexpr int NT = 320, MINB = 3; typedef tgfft::seq<8, 5> R; };
-template <> struct Cfg<48> { static constexpr int NT = 288, MINB = 3; typedef tgfft::seq<16, 3> R; };
-template <> struct Cfg<64> { static constexpr int NT = 512, MINB = 2; typedef tgfft::seq<8, 8> R; };
-template <> struct Cfg<72> { static constexpr int NT = 384, MINB = 2; typedef tgfft::seq<8, 3, 3> R; };
-template <> struct Cfg<80> { static constexpr int NT = 448, MINB = 2; typedef tgfft::seq<16, 5> R; };
-template <> struct Cfg<96> { static constexpr int NT = 576, MINB = 2; typedef tgfft::seq<16, 6> R; };
+// NT / MINB: the (y, z)-plane kernels and the full x3 (N lines per tile);
+// NTX / MINBX: the x-line kernels, which pack two real lines into one complex
+// line (N / 2 lines per tile).
+template <> struct Cfg<24> { static constexpr int NT = 192, MINB = 4, NTX = 96, MINBX = 8; typedef tgfft::seq<8, 3> R; };
+template <> struct Cfg<32> { static constexpr int NT = 256, MINB = 4, NTX = 128, MINBX = 8; typedef tgfft::seq<8, 4> R; };
+template <> struct Cfg<40> { static constexpr int NT = 320, MINB = 3, NTX = 160, MINBX = 6; typedef tgfft::seq<8, 5> R; };
+template <> struct Cfg<48> { static constexpr int NT = 288, MINB = 3, NTX = 192, MINBX = 6; typedef tgfft::seq<16, 3> R; };
+template <> struct Cfg<64> { static constexpr int NT = 512, MINB = 2, NTX = 256, MINBX = 4; typedef tgfft::seq<8, 8> R; };
+template <> struct Cfg<72> { static constexpr int NT = 384, MINB = 2, NTX = 352, MINBX = 3; typedef tgfft::seq<8, 3, 3> R; };
+template <> struct Cfg<80> { static constexpr int NT = 448, MINB = 2, NTX = 224, MINBX = 4; typedef tgfft::seq<16, 5> R; };
+template <> struct Cfg<96> { static constexpr int NT = 576, MINB = 2, NTX = 288, MINBX = 3; typedef tgfft::seq<16, 6> R; };
 
 constexpr int kEdges[] = {24, 32, 40, 48, 64, 72, 80, 96};
 
@@ -105,17 +108,17 @@ struct Seg { int slot, g0, g1; };
 struct SegTab { Seg s[kMaxSlots + 1]; int n; };
 
 // One in-place Stockham stage of radix R (NS = product of the earlier radices)
-// over the N lines of length N of a tile, element e of line l at
-// s[l * LST + e * EST].  Butterfly b: line b % N, index j = b / N.
-template <int N, int R, int NS, int DIR, int NT, int EST, int LST>
+// over NL lines of length N of a tile, element e of line l at
+// s[l * LST + e * EST].  Butterfly b: line b % NL, index j = b / NL.
+template <int N, int NL, int R, int NS, int DIR, int NT, int EST, int LST>
 TG_D void pstage(float2* s, const float2* __restrict__ tw, int tid) {
-    constexpr int NBL = N / R, NB = N * NBL, BPT = (NB + NT - 1) / NT;
+    constexpr int NBL = N / R, NB = NL * NBL, BPT = (NB + NT - 1) / NT;
     float2 v[BPT][R];
 #pragma unroll
     for (int q = 0; q < BPT; ++q) {
         const int b = tid + q * NT;
         if (NB % NT == 0 || b < NB) {
-            const int l = b % N, j = b / N;
+            const int l = b % NL, j = b / NL;
             const float2* src = s + l * LST;
 #pragma unroll
             for (int r = 0; r < R; ++r) v[q][r] = src[(j + r * NBL) * EST];
@@ -136,7 +139,7 @@ TG_D void pstage(float2* s, const float2* __restrict__ tw, int tid) {
     for (int q = 0; q < BPT; ++q) {
         const int b = tid + q * NT;
         if (NB % NT == 0 || b < NB) {
-            const int l = b % N, j = b / N;
+            const int l = b % NL, j = b / NL;
             const int k = j % NS;
             float2* dst = s + l * LST;
             const int p0 = (j - k) * R + k;
@@ -147,20 +150,26 @@ TG_D void pstage(float2* s, const float2* __restrict__ tw, int tid) {
     __syncthreads();
 }
 
-template <int N, int DIR, int NT, int EST, int LST, int NS, int R, int... Rest>
+template <int N, int NL, int DIR, int NT, int EST, int LST, int NS, int R, int... Rest>
 TG_D void pstages(float2* s, const float2* __restrict__ tw, int tid) {
-    pstage<N, R, NS, DIR, NT, EST, LST>(s, tw, tid);
-    if constexpr (sizeof...(Rest) > 0) pstages<N, DIR, NT, EST, LST, NS * R, Rest...>(s, tw, tid);
+    pstage<N, NL, R, NS, DIR, NT, EST, LST>(s, tw, tid);
+    if constexpr (sizeof...(Rest) > 0) pstages<N, NL, DIR, NT, EST, LST, NS * R, Rest...>(s, tw, tid);
 }
-template <int N, int DIR, int NT, int EST, int LST, int... Rs>
+template <int N, int NL, int DIR, int NT, int EST, int LST, int... Rs>
 TG_D void pfft_seq(float2* s, const float2* __restrict__ tw, int tid, tgfft::seq<Rs...>) {
-    pstages<N, DIR, NT, EST, LST, 1, Rs...>(s, tw, tid);
+    pstages<N, NL, DIR, NT, EST, LST, 1, Rs...>(s, tw, tid);
 }
-// The N lines of a tile: DIR = -1 forward, +1 unnormalised inverse.  The
-// caller has synchronised after filling the tile; ends with a barrier.
+// NL lines of length N of a tile by NT threads: DIR = -1 forward, +1
+// unnormalised inverse.  The caller has synchronised after filling the tile;
+// ends with a barrier.
+template <int N, int NL, int NT, int DIR, int EST, int LST>
+TG_D void pfft_l(float2* s, const float2* __restrict__ tw, int tid) {
+    pfft_seq<N, NL, DIR, NT, EST, LST>(s, tw, tid, typename Cfg<N>::R{});
+}
+// the N lines of a plane-sized tile by the plane kernels' NT threads
 template <int N, int DIR, int EST, int LST>
 TG_D void pfft(float2* s, const float2* __restrict__ tw, int tid) {
-    pfft_seq<N, DIR, Cfg<N>::NT, EST, LST>(s, tw, tid, typename Cfg<N>::R{});
+    pfft_l<N, N, Cfg<N>::NT, DIR, EST, LST>(s, tw, tid);
 }
 
 // Block sum of two doubles added to out[0], out[1] (called by every thread).
@@ -211,14 +220,18 @@ enum XMode {
     X_STATS = 5,      // set-up: src with its sums inside srcmask, times the indicator
 };
 
-// grid (N z-slabs, entries); tile s[y * P + x].
+// grid (N z-slabs, entries).  The x-lines y = 2j and 2j + 1 of the slab
+// travel as one complex line Z = a + i b (tile s[j * P + x], N / 2 lines): the
+// inverse DFT of H_2j + i H_2j+1 (each Hermitian-extended) is a + i b, and
+// the forward DFT of a + i b gives H_2j = (Z_k + conj Z_-k) / 2 and H_2j+1 =
+// (Z_k - conj Z_-k) / 2i.
 template <int N, int MODE>
-__global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ax(float2* __restrict__ H, long long hstride,
+__global__ void __launch_bounds__(Cfg<N>::NTX, Cfg<N>::MINBX) k_ax(float2* __restrict__ H, long long hstride,
                                                    const Entry* __restrict__ ent, const __grid_constant__ SlotTab slots,
                                                    const float* __restrict__ src, const float* __restrict__ srcmask,
                                                    double* __restrict__ stats, int side,
                                                    const float2* __restrict__ tw, float inv_n3) {
-    constexpr int NT = Cfg<N>::NT, P = N + 1, NH = N / 2 + 1;
+    constexpr int NT = Cfg<N>::NTX, P = N + 1, NH = N / 2 + 1, NL = N / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* s = reinterpret_cast<float2*>(smem_raw);
     const int z = blockIdx.x, e = blockIdx.y, tid = threadIdx.x;
@@ -226,24 +239,34 @@ __global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ax(float2* __restr
     const long long zo = (long long)z * N * N;
     double acc0 = 0, acc1 = 0;
     if (MODE == X_C2R_R2C) {
-        for (int i = tid; i < NH * N; i += NT) {
-            const int kx = i / N, y = i - kx * N;
-            const float2 v = Hs[((long long)kx * N + z) * N + y];
-            s[y * P + kx] = v;
-            if (kx > 0 && 2 * kx != N) s[y * P + N - kx] = cconj(v);
+        for (int i = tid; i < NH * NL; i += NT) {
+            const int kx = i / NL, j = i - kx * NL;
+            const float4 h = *reinterpret_cast<const float4*>(Hs + ((long long)kx * N + z) * N + 2 * j);
+            float2 a = make_float2(h.x, h.y), b = make_float2(h.z, h.w);
+            if (kx == 0 || 2 * kx == N) {  // complex-to-real reads the real parts there
+                a.y = 0.f;
+                b.y = 0.f;
+            }
+            s[j * P + kx] = make_float2(a.x - b.y, a.y + b.x);
+            if (kx > 0 && 2 * kx != N) s[j * P + N - kx] = make_float2(a.x + b.y, b.x - a.y);
         }
         __syncthreads();
-        pfft<N, +1, 1, P>(s, tw, tid);
+        pfft_l<N, NL, NT, +1, 1, P>(s, tw, tid);
         const float* mask = slots.s[ent[e].slot].mask;
-        for (int i = tid; i < N * N; i += NT) {
-            const int y = i / N, x = i - y * N;
-            const float r = s[y * P + x].x * inv_n3;
-            const bool in = mask[zo + i] != 0.f;
-            if (in) {
-                acc0 += (double)r;
-                acc1 += (double)r * (double)r;
+        for (int i = tid; i < NL * N; i += NT) {
+            const int j = i / N, x = i - j * N;
+            const float2 v = s[j * P + x];
+            const float r0 = v.x * inv_n3, r1 = v.y * inv_n3;
+            const bool in0 = mask[zo + 2 * j * N + x] != 0.f, in1 = mask[zo + (2 * j + 1) * N + x] != 0.f;
+            if (in0) {
+                acc0 += (double)r0;
+                acc1 += (double)r0 * (double)r0;
             }
-            s[y * P + x] = make_float2(in ? r : 0.f, 0.f);
+            if (in1) {
+                acc0 += (double)r1;
+                acc1 += (double)r1 * (double)r1;
+            }
+            s[j * P + x] = make_float2(in0 ? r0 : 0.f, in1 ? r1 : 0.f);
         }
         __syncthreads();
     } else if (MODE == X_ROT_MASK || MODE == X_ROT_STATS) {
@@ -253,48 +276,63 @@ __global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ax(float2* __restr
 #pragma unroll
         for (int q = 0; q < 9; ++q) m[q] = en->mref[q];
         const float c = (float)((N + 1) / 2);
-        for (int i = tid; i < N * N; i += NT) {
-            const int y = i / N, x = i - y * N;
-            float a = rot_sample_brick(sl.refb, N, N, N, m, c, c, c, x, y, z);
-            const float mk = sl.mask[zo + i];
-            if (MODE == X_ROT_MASK) {
-                a = __fmul_rn(a, mk);
-            } else {
-                const bool in = mk != 0.f;
-                if (in) {
-                    acc0 += (double)a;
-                    acc1 += (double)a * (double)a;
+        for (int i = tid; i < NL * N; i += NT) {
+            const int j = i / N, x = i - j * N;
+            float a[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int y = 2 * j + h;
+                float v = rot_sample_brick(sl.refb, N, N, N, m, c, c, c, x, y, z);
+                const float mk = sl.mask[zo + y * N + x];
+                if (MODE == X_ROT_MASK) {
+                    v = __fmul_rn(v, mk);
+                } else {
+                    const bool in = mk != 0.f;
+                    if (in) {
+                        acc0 += (double)v;
+                        acc1 += (double)v * (double)v;
+                    }
+                    v = in ? v : 0.f;
                 }
-                a = in ? a : 0.f;
+                a[h] = v;
             }
-            s[y * P + x] = make_float2(a, 0.f);
+            s[j * P + x] = make_float2(a[0], a[1]);
         }
         __syncthreads();
     } else {
-        for (int i = tid; i < N * N; i += NT) {
-            const int y = i / N, x = i - y * N;
-            float a = src[zo + i];
-            if (MODE == X_IND) {
-                a = a != 0.f ? 1.f : 0.f;
-                acc0 += (double)a;
-            } else if (MODE == X_MUL) {
-                if (srcmask) a = a * srcmask[zo + i];
-            } else {
-                const bool in = srcmask[zo + i] != 0.f;
-                if (in) {
-                    acc0 += (double)a;
-                    acc1 += (double)a * (double)a;
+        for (int i = tid; i < NL * N; i += NT) {
+            const int j = i / N, x = i - j * N;
+            float a[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const long long vi = zo + (2 * j + h) * N + x;
+                float v = src[vi];
+                if (MODE == X_IND) {
+                    v = v != 0.f ? 1.f : 0.f;
+                    acc0 += (double)v;
+                } else if (MODE == X_MUL) {
+                    if (srcmask) v = v * srcmask[vi];
+                } else {
+                    const bool in = srcmask[vi] != 0.f;
+                    if (in) {
+                        acc0 += (double)v;
+                        acc1 += (double)v * (double)v;
+                    }
+                    v = in ? v : 0.f;
                 }
-                a = in ? a : 0.f;
+                a[h] = v;
             }
-            s[y * P + x] = make_float2(a, 0.f);
+            s[j * P + x] = make_float2(a[0], a[1]);
         }
         __syncthreads();
     }
-    pfft<N, -1, 1, P>(s, tw, tid);
-    for (int i = tid; i < NH * N; i += NT) {
-        const int kx = i / N, y = i - kx * N;
-        Hs[((long long)kx * N + z) * N + y] = s[y * P + kx];
+    pfft_l<N, NL, NT, -1, 1, P>(s, tw, tid);
+    for (int i = tid; i < NH * NL; i += NT) {
+        const int kx = i / NL, j = i - kx * NL;
+        const float2 zk = s[j * P + kx], zm = s[j * P + (kx == 0 ? 0 : N - kx)];
+        const float4 h = make_float4(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y), 0.5f * (zk.y + zm.y),
+                                     0.5f * (zm.x - zk.x));
+        *reinterpret_cast<float4*>(Hs + ((long long)kx * N + z) * N + 2 * j) = h;
     }
     if (MODE == X_ROT_STATS) block_add2<NT>(acc0, acc1, stats + 4 * e);
     if (MODE == X_C2R_R2C) block_add2<NT>(acc0, acc1, stats + 4 * e + 2 * side);
@@ -671,12 +709,13 @@ template <typename K> cudaError_t raise_smem(K kern, size_t bytes) {
 template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, const int* job_idx, int np,
                                float* angles, float* shifts, float* peaks, size_t budget, bool allow_prune,
                                AlignScratch* sc) {
-    constexpr int NT = Cfg<N>::NT, P = N + 1, NH = N / 2 + 1;
+    constexpr int NT = Cfg<N>::NT, NTX = Cfg<N>::NTX, P = N + 1, NH = N / 2 + 1;
     const long long nn = (long long)N * N * N;
     const long long hvol = (long long)NH * N * N;  // one half spectrum
     cudaStream_t st = ctx->stream;
     const bool wedges = jobs[job_idx[0]].wedge_ref != nullptr;
     const size_t tile = sizeof(float2) * N * P;
+    const size_t xtile = sizeof(float2) * (N / 2) * P;
     const float2* tw = twiddle_table<float2>(N);
     if (!tw) return fail(ctx, TOMGPU_ERR_OOM, "twiddle table");
     cudaError_t e = cudaSuccess;
@@ -889,7 +928,7 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
                 k_afill<<<blocks_for(nn), 256, 0, st>>>(cmax[k], amax[k], nn, -2.f);
                 if ((e = cudaMemsetAsync(pst, 0, 2 * sizeof(double), st))) break;
                 // F(mask != 0)
-                k_ax<N, X_IND><<<dim3(N, 1), NT, tile, st>>>(tmpH, hvol, nullptr, slots, jb.mask, nullptr, pst, 0, tw,
+                k_ax<N, X_IND><<<dim3(N, 1), NTX, xtile, st>>>(tmpH, hvol, nullptr, slots, jb.mask, nullptr, pst, 0, tw,
                                                                inv_n3);
                 k_ap<N, P_FWD><<<dim3(NH, 1), NT, tile, st>>>(nullptr, nullptr, hvol, nullptr, slots, nullptr, tw, tmpH,
                                                                mk[k], nullptr, nullptr, 0.0, nullptr, 0, 0);
@@ -899,7 +938,7 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
                     k_abricks<<<blocks_for(nn), 256, 0, st>>>(jb.wedge_ref, wrefb[k], N);
                     k_awph<<<blocks_for(hvol), 256, 0, st>>>(wp, wph[k], N);
                     // F(part * mask)
-                    k_ax<N, X_MUL><<<dim3(N, 1), NT, tile, st>>>(tmpH, hvol, nullptr, slots, jb.part, jb.mask, nullptr,
+                    k_ax<N, X_MUL><<<dim3(N, 1), NTX, xtile, st>>>(tmpH, hvol, nullptr, slots, jb.part, jb.mask, nullptr,
                                                                    0, tw, inv_n3);
                     k_ap<N, P_FWD><<<dim3(NH, 1), NT, tile, st>>>(nullptr, nullptr, hvol, nullptr, slots, nullptr, tw,
                                                                    tmpH, b0[k], nullptr, nullptr, 0.0, nullptr, 0, 0);
@@ -907,7 +946,7 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
                 } else {
                     // F(norm_inside_mask(part))
                     if ((e = cudaMemsetAsync(pst, 0, 2 * sizeof(double), st))) break;
-                    k_ax<N, X_STATS><<<dim3(N, 1), NT, tile, st>>>(tmpH, hvol, nullptr, slots, jb.part, jb.mask, pst,
+                    k_ax<N, X_STATS><<<dim3(N, 1), NTX, xtile, st>>>(tmpH, hvol, nullptr, slots, jb.part, jb.mask, pst,
                                                                      0, tw, inv_n3);
                     k_ap<N, P_FWD_NORM><<<dim3(NH, 1), NT, tile, st>>>(nullptr, nullptr, hvol, nullptr, slots, nullptr,
                                                                         tw, tmpH, b0[k], mk[k], pst, nmask[p], nullptr, 0, 0);
@@ -931,22 +970,22 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
             const Entry* eb = d_ent + e0;
             if ((e = cudaMemsetAsync(stats, 0, sizeof(double) * 4 * nb, st))) break;
             if (wedges) {
-                k_ax<N, X_ROT_MASK><<<dim3(N, nb), NT, tile, st>>>(HA, hvol, eb, slots, nullptr, nullptr, stats, 0,
+                k_ax<N, X_ROT_MASK><<<dim3(N, nb), NTX, xtile, st>>>(HA, hvol, eb, slots, nullptr, nullptr, stats, 0,
                                                                      tw, inv_n3);
                 k_ap<N, P_WEDGE_A><<<dim3(NH, nb), NT, tile, st>>>(HA, nullptr, hvol, eb, slots, stats, tw, nullptr,
                                                                     nullptr, nullptr, nullptr, 0.0, nullptr, 0, 0);
-                k_ax<N, X_C2R_R2C><<<dim3(N, nb), NT, tile, st>>>(HA, hvol, eb, slots, nullptr, nullptr, stats, 0, tw,
+                k_ax<N, X_C2R_R2C><<<dim3(N, nb), NTX, xtile, st>>>(HA, hvol, eb, slots, nullptr, nullptr, stats, 0, tw,
                                                                     inv_n3);
                 k_ap<N, P_WEDGE_B><<<dim3(NH, nb), NT, tile, st>>>(nullptr, HB, hvol, eb, slots, stats, tw, nullptr,
                                                                     nullptr, nullptr, nullptr, 0.0, nullptr, 0, 0);
-                k_ax<N, X_C2R_R2C><<<dim3(N, nb), NT, tile, st>>>(HB, hvol, eb, slots, nullptr, nullptr, stats, 1, tw,
+                k_ax<N, X_C2R_R2C><<<dim3(N, nb), NTX, xtile, st>>>(HB, hvol, eb, slots, nullptr, nullptr, stats, 1, tw,
                                                                     inv_n3);
                 k_ap<N, P_CROSS><<<dim3(NH, nb), NT, tile, st>>>(HA, HB, hvol, eb, slots, stats, tw, nullptr, nullptr,
                                                                   nullptr, nullptr, 0.0, prune ? CP : nullptr, nzmax,
                                                                   nymax);
                 ctx->launches += 6;
             } else {
-                k_ax<N, X_ROT_STATS><<<dim3(N, nb), NT, tile, st>>>(HA, hvol, eb, slots, nullptr, nullptr, stats, 0,
+                k_ax<N, X_ROT_STATS><<<dim3(N, nb), NTX, xtile, st>>>(HA, hvol, eb, slots, nullptr, nullptr, stats, 0,
                                                                       tw, inv_n3);
                 k_ap<N, P_CROSS_NW><<<dim3(NH, nb), NT, tile, st>>>(HA, HB, hvol, eb, slots, stats, tw, nullptr,
                                                                      nullptr, nullptr, nullptr, 0.0,
