@@ -131,6 +131,11 @@ def test_batched_engine_equals_per_job(gpu, oracle):
     jobs.append(_job(oracle, 40, 1, True, 320, mccf="negative"))
     jobs.append(_job(oracle, 40, 2, True, 321))
     jobs.append(_job(oracle, 64, 0, True, 322, mccf="none", phi=(0, 3, 3), psi=(0, 3, 3)))
+    # a graded reference wedge (not exact in half precision: full-precision
+    # corner bricks for the 40^3 edge; the binary wedges elsewhere use halves)
+    soft = _job(oracle, 40, 0, True, 323)
+    soft["wedge_ref"] = (0.7 * soft["wedge_ref"] + 0.1234567).astype(np.float32)
+    jobs.append(soft)
     half32 = 17 * 32 * 32 * 8
     a0, s0, p0 = gpu.av3_align_batch(jobs, path=0, batch_bytes=2 * half32 * 10)
     a1, s1, p1 = gpu.av3_align_batch(jobs, path=1)

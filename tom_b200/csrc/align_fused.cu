@@ -80,6 +80,7 @@ constexpr int kMaxGroups = 160;  // x3 entry groups per batch
 struct Slot {
     const float4* refb;   // bricks of the reference
     const float4* wrefb;  // bricks of the reference wedge (wedge form)
+    const uint4* wrefh;   // the same as half bricks when every wedge value is exact in half precision
     const float* mask;
     const float2* mk;     // F(mask != 0), [kx][z][y]
     const float2* b0;     // wedge form: F(part * mask); without: F(norm_inside_mask(part))
@@ -376,8 +377,14 @@ __global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ap(float2* __restr
             const int z = i / N, y = i - z * N;
             int s1, s2;
             wedge_pair(kx + N * (y + N * z), N, N, N, s1, s2);
-            const float w1 = rot_sample_brick(sl.wrefb, N, N, N, m, c, c, c, s1 % N, (s1 / N) % N, s1 / (N * N));
-            const float w2 = rot_sample_brick(sl.wrefb, N, N, N, m, c, c, c, s2 % N, (s2 / N) % N, s2 / (N * N));
+            float w1, w2;
+            if (sl.wrefh) {
+                w1 = rot_sample_brick(sl.wrefh, N, N, N, m, c, c, c, s1 % N, (s1 / N) % N, s1 / (N * N));
+                w2 = rot_sample_brick(sl.wrefh, N, N, N, m, c, c, c, s2 % N, (s2 / N) % N, s2 / (N * N));
+            } else {
+                w1 = rot_sample_brick(sl.wrefb, N, N, N, m, c, c, c, s1 % N, (s1 / N) % N, s1 / (N * N));
+                w2 = rot_sample_brick(sl.wrefb, N, N, N, m, c, c, c, s2 % N, (s2 / N) % N, s2 / (N * N));
+            }
             s[z * P + y] = cscale(sl.b0[po + i], 0.5f * (w1 + w2));
         }
         __syncthreads();
@@ -610,16 +617,23 @@ __global__ void k_prune_mark(const float* const* __restrict__ mccf, int N, int* 
     int* f = flags + (long long)blockIdx.y * 3 * N;
     const long long nn = (long long)N * N * N;
     const int H2 = N / 2;
+    unsigned long long first = ~0ull;
     for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += (long long)gridDim.x * blockDim.x) {
         if (m[v] != 0.f) {
             const int x = (int)(v % N), y = (int)((v / N) % N), z = (int)(v / ((long long)N * N));
             f[(z - H2 + N) % N] = 1;
             f[N + (y - H2 + N) % N] = 1;
             f[2 * N + (x - H2 + N) % N] = 1;
-        } else {
-            atomicMin(v0 + blockIdx.y, (unsigned long long)v);
+        } else if (first == ~0ull) {
+            first = (unsigned long long)v;  // the loop runs in increasing v: the thread's first zero
         }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, first, o);
+        first = t < first ? t : first;
+    }
+    if ((threadIdx.x & 31) == 0 && first != ~0ull) atomicMin(v0 + blockIdx.y, first);
 }
 
 // flags of the first zero voxel of each particle's mask_ccf
@@ -644,6 +658,35 @@ __global__ void k_abricks(const float* __restrict__ in, float4* __restrict__ out
         const int i = (int)(v % N), j = (int)((v / N) % N), k = (int)(v / ((long long)N * N));
         brick_corners(in, N, N, N, i, j, k, out);
     }
+}
+
+// half bricks: the eight corners of brick_corners as halves (the caller has
+// checked that every value is exact in half precision)
+__global__ void k_abricks_h(const float* __restrict__ in, uint4* __restrict__ out, int N) {
+    const long long nn = (long long)N * N * N;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn;
+         v += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(v % N), j = (int)((v / N) % N), k = (int)(v / ((long long)N * N));
+        float4 lo, hi;
+        brick_values(in, N, N, N, i, j, k, lo, hi);
+        const __half2 h0 = __floats2half2_rn(lo.x, lo.y), h1 = __floats2half2_rn(lo.z, lo.w);
+        const __half2 h2 = __floats2half2_rn(hi.x, hi.y), h3 = __floats2half2_rn(hi.z, hi.w);
+        uint4 u;
+        u.x = *reinterpret_cast<const unsigned*>(&h0);
+        u.y = *reinterpret_cast<const unsigned*>(&h1);
+        u.z = *reinterpret_cast<const unsigned*>(&h2);
+        u.w = *reinterpret_cast<const unsigned*>(&h3);
+        out[v] = u;
+    }
+}
+
+// ok[p] = 0 when a value of volume p is not exact in half precision (grid: blocks, volumes)
+__global__ void k_half_exact(const float* const* __restrict__ vols, long long nn, int* __restrict__ ok) {
+    const float* w = vols[blockIdx.y];
+    bool all = true;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += (long long)gridDim.x * blockDim.x)
+        if (__half2float(__float2half_rn(w[v])) != w[v]) all = false;
+    if (!__all_sync(0xffffffffu, all) && (threadIdx.x & 31) == 0) ok[blockIdx.y] = 0;
 }
 
 // (W'(k) + W'(-k)) / 2 of a wedge on the [kx][z][y] half grid
@@ -789,6 +832,8 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
     for (int p = 0; p < np; ++p)
         if (!jobs[job_idx[p]].mask_ccf) prune = false;
     const float** d_mccf = prune ? fb.get<const float*>(np) : nullptr;
+    const float** d_wvols = wedges ? fb.get<const float*>(np) : nullptr;
+    int* d_hok = wedges ? fb.get<int>(np) : nullptr;
     int* d_flags = prune ? fb.get<int>((size_t)np * 3 * N) : nullptr;
     unsigned long long* d_v0 = prune ? fb.get<unsigned long long>(np) : nullptr;
     if (!fb.ok) {
@@ -800,6 +845,17 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
     float* VP = nullptr;
     std::vector<int> pn3;  // per particle: nz, ny, nx of the pruned lists
     int nzmax = 0, nymax = 0, nxmax = 0;
+    // the b-side passes (rotated-wedge plane, its x-lines) run on a second
+    // stream beside the a-side ones (rotation, particle-wedge plane, x-lines)
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    if ((e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreateWithFlags(&ev_a, cudaEventDisableTiming)) ||
+        (e = cudaEventCreateWithFlags(&ev_b, cudaEventDisableTiming))) {
+        if (st2) cudaStreamDestroy(st2);
+        if (ev_a) cudaEventDestroy(ev_a);
+        return cuda_fail(ctx, e, "av3_align (fused): stream");
+    }
     int rc = TOMGPU_OK;
     do {
         if ((e = cudaMemcpyAsync(d_ent, ent.data(), sizeof(Entry) * total, cudaMemcpyHostToDevice, st))) break;
@@ -825,8 +881,22 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
             if ((e = cudaMemcpyAsync(flags.data(), d_flags, sizeof(int) * flags.size(), cudaMemcpyDeviceToHost, st)))
                 break;
         }
+        // half bricks for the reference wedges when all of them are exact in half precision
+        std::vector<int> hok(wedges ? np : 0, 1);
+        if (wedges) {
+            std::vector<const float*> wv(np);
+            for (int p = 0; p < np; ++p) wv[p] = jobs[job_idx[p]].wedge_ref;
+            if ((e = cudaMemcpyAsync(d_wvols, wv.data(), sizeof(float*) * np, cudaMemcpyHostToDevice, st))) break;
+            if ((e = cudaMemcpyAsync(d_hok, hok.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st))) break;
+            k_half_exact<<<dim3(blocks_for(nn), np), 256, 0, st>>>(d_wvols, nn, d_hok);
+            ctx->launches += 1;
+            if ((e = cudaMemcpyAsync(hok.data(), d_hok, sizeof(int) * np, cudaMemcpyDeviceToHost, st))) break;
+        }
         if ((e = cudaStreamSynchronize(st))) break;
         ctx->launches += 1;
+        bool halfw = wedges;
+        for (int p = 0; p < (int)hok.size(); ++p)
+            if (!hok[p]) halfw = false;
         for (int p = 0; p < np && !rc; ++p)
             if (nmask[p] < 2)
                 rc = fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(job_idx[p]) + ": mask needs at least two voxels");
@@ -935,7 +1005,14 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
                 ctx->launches += 4;
                 if (wedges) {
                     const float* wp = jb.wedge_part ? jb.wedge_part : jb.wedge_ref;
-                    k_abricks<<<blocks_for(nn), 256, 0, st>>>(jb.wedge_ref, wrefb[k], N);
+                    if (halfw) {
+                        sl.wrefh = reinterpret_cast<const uint4*>(wrefb[k]);
+                        k_abricks_h<<<blocks_for(nn), 256, 0, st>>>(jb.wedge_ref, reinterpret_cast<uint4*>(wrefb[k]),
+                                                                    N);
+                    } else {
+                        sl.wrefh = nullptr;
+                        k_abricks<<<blocks_for(nn), 256, 0, st>>>(jb.wedge_ref, wrefb[k], N);
+                    }
                     k_awph<<<blocks_for(hvol), 256, 0, st>>>(wp, wph[k], N);
                     // F(part * mask)
                     k_ax<N, X_MUL><<<dim3(N, 1), NTX, xtile, st>>>(tmpH, hvol, nullptr, slots, jb.part, jb.mask, nullptr,
@@ -970,16 +1047,18 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
             const Entry* eb = d_ent + e0;
             if ((e = cudaMemsetAsync(stats, 0, sizeof(double) * 4 * nb, st))) break;
             if (wedges) {
+                if ((e = cudaEventRecord(ev_a, st)) || (e = cudaStreamWaitEvent(st2, ev_a, 0))) break;
                 k_ax<N, X_ROT_MASK><<<dim3(N, nb), NTX, xtile, st>>>(HA, hvol, eb, slots, nullptr, nullptr, stats, 0,
                                                                      tw, inv_n3);
+                k_ap<N, P_WEDGE_B><<<dim3(NH, nb), NT, tile, st2>>>(nullptr, HB, hvol, eb, slots, stats, tw, nullptr,
+                                                                     nullptr, nullptr, nullptr, 0.0, nullptr, 0, 0);
                 k_ap<N, P_WEDGE_A><<<dim3(NH, nb), NT, tile, st>>>(HA, nullptr, hvol, eb, slots, stats, tw, nullptr,
                                                                     nullptr, nullptr, nullptr, 0.0, nullptr, 0, 0);
+                k_ax<N, X_C2R_R2C><<<dim3(N, nb), NTX, xtile, st2>>>(HB, hvol, eb, slots, nullptr, nullptr, stats, 1,
+                                                                     tw, inv_n3);
                 k_ax<N, X_C2R_R2C><<<dim3(N, nb), NTX, xtile, st>>>(HA, hvol, eb, slots, nullptr, nullptr, stats, 0, tw,
                                                                     inv_n3);
-                k_ap<N, P_WEDGE_B><<<dim3(NH, nb), NT, tile, st>>>(nullptr, HB, hvol, eb, slots, stats, tw, nullptr,
-                                                                    nullptr, nullptr, nullptr, 0.0, nullptr, 0, 0);
-                k_ax<N, X_C2R_R2C><<<dim3(N, nb), NTX, xtile, st>>>(HB, hvol, eb, slots, nullptr, nullptr, stats, 1, tw,
-                                                                    inv_n3);
+                if ((e = cudaEventRecord(ev_b, st2)) || (e = cudaStreamWaitEvent(st, ev_b, 0))) break;
                 k_ap<N, P_CROSS><<<dim3(NH, nb), NT, tile, st>>>(HA, HB, hvol, eb, slots, stats, tw, nullptr, nullptr,
                                                                   nullptr, nullptr, 0.0, prune ? CP : nullptr, nzmax,
                                                                   nymax);
@@ -1021,7 +1100,11 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
         }
     } while (0);
     if (e && !rc) rc = cuda_fail(ctx, e, "av3_align (fused)");
+    cudaStreamSynchronize(st2);
     cudaStreamSynchronize(st);
+    cudaStreamDestroy(st2);
+    cudaEventDestroy(ev_a);
+    cudaEventDestroy(ev_b);
     return rc;
 }
 

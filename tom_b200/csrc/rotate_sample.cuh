@@ -3,6 +3,7 @@
 // round-to-nearest intrinsics keep the float operation order of the
 // reference, so results are bit-identical to rot3d.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace tg {
@@ -49,12 +50,11 @@ __device__ __forceinline__ float rot_sample(const float* __restrict__ in, int sx
 // The eight corner values of voxel (i, j, k) for rot_sample, as they are
 // read there (zero where a corner lies beyond the last voxel of an axis):
 // v000 v100 v010 v110 in .x .y .z .w of b[2 v], v001 v101 v011 v111 of b[2 v + 1].
-__device__ __forceinline__ void brick_corners(const float* __restrict__ in, int sx, int sy, int sz, int i, int j,
-                                              int k, float4* __restrict__ b) {
+__device__ __forceinline__ void brick_values(const float* __restrict__ in, int sx, int sy, int sz, int i, int j,
+                                             int k, float4& lo, float4& hi) {
     const long long sxy = (long long)sx * sy;
     const long long v = i + (long long)j * sx + (long long)k * sxy;
     const bool ex = i == sx - 1, ey = j == sy - 1, ez = k == sz - 1;
-    float4 lo, hi;
     lo.x = in[v];
     lo.y = ex ? 0.f : in[v + 1];
     lo.z = ey ? 0.f : in[v + sx];
@@ -63,14 +63,38 @@ __device__ __forceinline__ void brick_corners(const float* __restrict__ in, int 
     hi.y = (ex || ez) ? 0.f : in[v + sxy + 1];
     hi.z = (ey || ez) ? 0.f : in[v + sxy + sx];
     hi.w = (ex || ey || ez) ? 0.f : in[v + sxy + sx + 1];
+}
+__device__ __forceinline__ void brick_corners(const float* __restrict__ in, int sx, int sy, int sz, int i, int j,
+                                              int k, float4* __restrict__ b) {
+    const long long v = i + (long long)j * sx + (long long)k * sx * sy;
+    float4 lo, hi;
+    brick_values(in, sx, sy, sz, i, j, k, lo, hi);
     b[2 * v] = lo;
     b[2 * v + 1] = hi;
 }
 
+// Corner loads of a brick volume: float bricks (two float4 per voxel) or
+// half bricks (one uint4 of eight halves per voxel, for volumes whose values
+// are all exact in half precision: the conversion back to float is exact).
+__device__ __forceinline__ void brick_load(const float4* __restrict__ bk, long long b, float4& lo, float4& hi) {
+    lo = __ldg(bk + 2 * b);
+    hi = __ldg(bk + 2 * b + 1);
+}
+__device__ __forceinline__ void brick_load(const uint4* __restrict__ bk, long long b, float4& lo, float4& hi) {
+    const uint4 u = __ldg(bk + b);
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+    const float2 c = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+    const float2 d = __half22float2(*reinterpret_cast<const __half2*>(&u.z));
+    const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&u.w));
+    lo = make_float4(a.x, a.y, c.x, c.y);
+    hi = make_float4(d.x, d.y, f.x, f.y);
+}
+
 // rot_sample reading the corners from a brick volume (brick_corners): the
 // same coordinates, bounds and float operations, so the same result, from two
-// 16-byte loads instead of eight scattered 4-byte ones.
-__device__ __forceinline__ float rot_sample_brick(const float4* __restrict__ bk, int sx, int sy, int sz,
+// 16-byte loads (one for half bricks) instead of eight scattered 4-byte ones.
+template <typename BK>
+__device__ __forceinline__ float rot_sample_brick(const BK* __restrict__ bk, int sx, int sy, int sz,
                                                   const float* m, float px, float py, float pz, int i, int j,
                                                   int k) {
     const float di = (float)(long long)__fsub_rn((float)i, px);
@@ -89,7 +113,8 @@ __device__ __forceinline__ float rot_sample_brick(const float4* __restrict__ bk,
     const float wx = __fsub_rn(rx, (float)fx), wy = __fsub_rn(ry, (float)fy), wz = __fsub_rn(rz, (float)fz);
     const float ux = __fsub_rn(1.f, wx), uy = __fsub_rn(1.f, wy), uz = __fsub_rn(1.f, wz);
     const long long b = fx + (long long)fy * sx + (long long)fz * sx * sy;
-    const float4 lo = __ldg(bk + 2 * b), hi = __ldg(bk + 2 * b + 1);
+    float4 lo, hi;
+    brick_load(bk, b, lo, hi);
     const float a = __fadd_rn(lo.x, __fmul_rn(__fsub_rn(lo.y, lo.x), wx));
     const float bb = __fadd_rn(__fmul_rn(lo.z, ux), __fmul_rn(lo.w, wx));
     const float c = __fadd_rn(__fmul_rn(hi.x, ux), __fmul_rn(hi.y, wx));
