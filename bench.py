@@ -81,6 +81,8 @@ def parse():
     p.add_argument("--learned-steps", type=int, default=400, help="timed training steps of the learned_256 workload")
     p.add_argument("--align-particles", type=int, default=40,
                    help="particles timed for --workload align_2048 (extrapolated to 2048)")
+    p.add_argument("--align-batch-mb", type=int, default=0,
+                   help="align_2048: device MB of a batch's spectra in the batched engine (0: the library default)")
     p.add_argument("--align-path", type=int, default=0, choices=[0, 1, 2],
                    help="align_2048: 0 the batched engine (entries of all particles of a box edge), 1 one job at "
                         "a time, 2 batched without the pruned last inverse DFT")
@@ -381,7 +383,7 @@ def run_align(args):
     first = {}
     for j in jobs:
         first.setdefault(j["ref"].shape, j)
-    tb.av3_align_batch(list(first.values()), ctx, path=args.align_path)
+    tb.av3_align_batch(list(first.values()), ctx, path=args.align_path, batch_bytes=args.align_batch_mb << 20)
     torch.cuda.synchronize()
 
     def timed(sub):
@@ -390,7 +392,7 @@ def run_align(args):
         for _ in range(3):
             torch.cuda.synchronize()
             t = time.perf_counter()
-            out = tb.av3_align_batch(sub, ctx, path=args.align_path)
+            out = tb.av3_align_batch(sub, ctx, path=args.align_path, batch_bytes=args.align_batch_mb << 20)
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t)
         return float(np.median(ts)), float(min(ts)), out
@@ -429,7 +431,7 @@ def run_align(args):
                                   "not a pass mark: tom_av3_align's own objective (the FP64 oracle) also "
                                   "peaks at other grid triplets for noiseless 6-blob wedged phantoms",
             "per_size": per_size, "seconds_per_particle": per_size_s, "gpu_launches": launches,
-            "align_path": args.align_path, "clocks": clk,
+            "align_path": args.align_path, "align_batch_mb": args.align_batch_mb, "clocks": clk,
             "dtype": "f32", "data": "synthetic"}
     print(json.dumps(line), flush=True)
 

@@ -344,7 +344,7 @@ typedef struct {
                            box (0 evaluates it only where mask_ccf is non-zero, when every job
                            of the edge has a mask_ccf with a small support) */
     size_t batch_bytes; /* batched engine: device bytes of a batch's two half-spectrum sets
-                           (0: 256 MB) */
+                           (0: 1 GB) */
 } tomgpu_align_params;
 
 /* tomgpu_av3_align_dev with an engine choice; the same outputs. */

@@ -67,8 +67,8 @@ template <> struct Cfg<40> { static constexpr int NT = 320, MINB = 3, NTX = 160,
 template <> struct Cfg<48> { static constexpr int NT = 288, MINB = 3, NTX = 192, MINBX = 6; typedef tgfft::seq<16, 3> R; };
 template <> struct Cfg<64> { static constexpr int NT = 512, MINB = 2, NTX = 256, MINBX = 4; typedef tgfft::seq<8, 8> R; };
 template <> struct Cfg<72> { static constexpr int NT = 384, MINB = 2, NTX = 352, MINBX = 3; typedef tgfft::seq<8, 3, 3> R; };
-template <> struct Cfg<80> { static constexpr int NT = 448, MINB = 2, NTX = 224, MINBX = 4; typedef tgfft::seq<16, 5> R; };
-template <> struct Cfg<96> { static constexpr int NT = 576, MINB = 2, NTX = 288, MINBX = 3; typedef tgfft::seq<16, 6> R; };
+template <> struct Cfg<80> { static constexpr int NT = 448, MINB = 2, NTX = 224, MINBX = 5; typedef tgfft::seq<16, 5> R; };
+template <> struct Cfg<96> { static constexpr int NT = 576, MINB = 2, NTX = 288, MINBX = 4; typedef tgfft::seq<16, 6> R; };
 
 constexpr int kEdges[] = {24, 32, 40, 48, 64, 72, 80, 96};
 
@@ -124,12 +124,16 @@ TG_D void pstage(float2* s, const float2* __restrict__ tw, int tid) {
 #pragma unroll
             for (int r = 0; r < R; ++r) v[q][r] = src[(j + r * NBL) * EST];
             if (NS > 1) {
+                // one table load per butterfly; the powers w^r by products
+                // (a few ulp, far inside the line DFT's own rounding)
                 const int k = j % NS;
+                float2 w1 = tgfft::ldtw(tw, k * (N / (NS * R)));
+                if (DIR > 0) w1 = cconj(w1);
+                float2 w = w1;
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    float2 w = tgfft::ldtw(tw, r * k * (N / (NS * R)));
-                    if (DIR > 0) w = cconj(w);
                     v[q][r] = cmul(v[q][r], w);
+                    if (r + 1 < R) w = cmul(w, w1);
                 }
             }
             tgfft::dft<R, DIR>(v[q], tw, N / R);
@@ -283,8 +287,9 @@ __global__ void __launch_bounds__(Cfg<N>::NTX, Cfg<N>::MINBX) k_ax(float2* __res
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int y = 2 * j + h;
-                float v = rot_sample_brick(sl.refb, N, N, N, m, c, c, c, x, y, z);
                 const float mk = sl.mask[zo + y * N + x];
+                // outside the mask the value is zero in both forms: no sample
+                float v = mk != 0.f ? rot_sample_brick(sl.refb, N, N, N, m, c, c, c, x, y, z) : 0.f;
                 if (MODE == X_ROT_MASK) {
                     v = __fmul_rn(v, mk);
                 } else {
@@ -796,7 +801,7 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
     const long long total = (long long)ent.size();
 
     // batch size: both half-spectrum sets of a batch within the budget
-    if (!budget) budget = (size_t)256 << 20;
+    if (!budget) budget = (size_t)1 << 30;
     const int emax = (int)std::max<long long>(1, std::min<long long>(512, (long long)(budget / (2 * sizeof(float2) * hvol))));
     const int gsz = std::max(4, (emax + kMaxGroups - kMaxSlots - 1) / (kMaxGroups - kMaxSlots));
     const int gmax = (emax + gsz - 1) / gsz + kMaxSlots;
