@@ -282,7 +282,9 @@ __global__ void __launch_bounds__(Cfg<N>::NTX, Cfg<N>::MINBX) k_ax(float2* __res
         for (int q = 0; q < 9; ++q) m[q] = en->mref[q];
         const float c = (float)((N + 1) / 2);
         for (int i = tid; i < NL * N; i += NT) {
-            const int j = i / N, x = i - j * N;
+            // a warp samples an 8 (x) x 8 (y) tile of the slab (two y per thread)
+            const int lane = i & 31, t = i >> 5;
+            const int x = (t % (N / 8)) * 8 + (lane & 7), j = (t / (N / 8)) * 4 + (lane >> 3);
             float a[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -379,7 +381,10 @@ __global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ap(float2* __restr
         for (int q = 0; q < 9; ++q) m[q] = en->mw[q];
         const float c = (float)((N + 1) / 2);
         for (int i = tid; i < N * N; i += NT) {
-            const int z = i / N, y = i - z * N;
+            // a warp samples an 8 (y) x 4 (z) tile of the plane: its source
+            // points span two rotated directions, fewer cache lines than a row
+            const int lane = i & 31, t = i >> 5;
+            const int y = (t % (N / 8)) * 8 + (lane & 7), z = (t / (N / 8)) * 4 + (lane >> 3);
             int s1, s2;
             wedge_pair(kx + N * (y + N * z), N, N, N, s1, s2);
             float w1, w2;
@@ -390,7 +395,7 @@ __global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ap(float2* __restr
                 w1 = rot_sample_brick(sl.wrefb, N, N, N, m, c, c, c, s1 % N, (s1 / N) % N, s1 / (N * N));
                 w2 = rot_sample_brick(sl.wrefb, N, N, N, m, c, c, c, s2 % N, (s2 / N) % N, s2 / (N * N));
             }
-            s[z * P + y] = cscale(sl.b0[po + i], 0.5f * (w1 + w2));
+            s[z * P + y] = cscale(sl.b0[po + z * N + y], 0.5f * (w1 + w2));
         }
         __syncthreads();
     } else {

@@ -76,11 +76,11 @@ __device__ __forceinline__ void brick_corners(const float* __restrict__ in, int 
 // Corner loads of a brick volume: float bricks (two float4 per voxel) or
 // half bricks (one uint4 of eight halves per voxel, for volumes whose values
 // are all exact in half precision: the conversion back to float is exact).
-__device__ __forceinline__ void brick_load(const float4* __restrict__ bk, long long b, float4& lo, float4& hi) {
+__device__ __forceinline__ void brick_load(const float4* __restrict__ bk, int b, float4& lo, float4& hi) {
     lo = __ldg(bk + 2 * b);
     hi = __ldg(bk + 2 * b + 1);
 }
-__device__ __forceinline__ void brick_load(const uint4* __restrict__ bk, long long b, float4& lo, float4& hi) {
+__device__ __forceinline__ void brick_load(const uint4* __restrict__ bk, int b, float4& lo, float4& hi) {
     const uint4 u = __ldg(bk + b);
     const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
     const float2 c = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
@@ -93,13 +93,16 @@ __device__ __forceinline__ void brick_load(const uint4* __restrict__ bk, long lo
 // rot_sample reading the corners from a brick volume (brick_corners): the
 // same coordinates, bounds and float operations, so the same result, from two
 // 16-byte loads (one for half bricks) instead of eight scattered 4-byte ones.
+// For integer-valued centres below 2^24 only (i - p is then an exact integer,
+// so rot_sample's truncation of it is the identity) and volumes of fewer
+// than 2^31 voxels (32-bit brick index).
 template <typename BK>
 __device__ __forceinline__ float rot_sample_brick(const BK* __restrict__ bk, int sx, int sy, int sz,
                                                   const float* m, float px, float py, float pz, int i, int j,
                                                   int k) {
-    const float di = (float)(long long)__fsub_rn((float)i, px);
-    const float dj = (float)(long long)__fsub_rn((float)j, py);
-    const float dk = (float)(long long)__fsub_rn((float)k, pz);
+    const float di = __fsub_rn((float)i, px);
+    const float dj = __fsub_rn((float)j, py);
+    const float dk = __fsub_rn((float)k, pz);
     const float rx = __fadd_rn(__fadd_rn(__fadd_rn(px, __fmul_rn(m[0], di)), __fmul_rn(m[1], dj)),
                                __fmul_rn(m[2], dk));
     if (rx < 0.f || rx > (float)(sx - 1)) return 0.f;
@@ -112,7 +115,7 @@ __device__ __forceinline__ float rot_sample_brick(const BK* __restrict__ bk, int
     const int fx = (int)rx, fy = (int)ry, fz = (int)rz;
     const float wx = __fsub_rn(rx, (float)fx), wy = __fsub_rn(ry, (float)fy), wz = __fsub_rn(rz, (float)fz);
     const float ux = __fsub_rn(1.f, wx), uy = __fsub_rn(1.f, wy), uz = __fsub_rn(1.f, wz);
-    const long long b = fx + (long long)fy * sx + (long long)fz * sx * sy;
+    const int b = fx + sx * (fy + sy * fz);
     float4 lo, hi;
     brick_load(bk, b, lo, hi);
     const float a = __fadd_rn(lo.x, __fmul_rn(__fsub_rn(lo.y, lo.x), wx));
