@@ -64,13 +64,19 @@ template <int N> struct Cfg;
 template <> struct Cfg<24> { static constexpr int NT = 192, MINB = 4, NTX = 96, MINBX = 8; typedef tgfft::seq<8, 3> R; };
 template <> struct Cfg<32> { static constexpr int NT = 256, MINB = 4, NTX = 128, MINBX = 8; typedef tgfft::seq<8, 4> R; };
 template <> struct Cfg<40> { static constexpr int NT = 320, MINB = 3, NTX = 160, MINBX = 6; typedef tgfft::seq<8, 5> R; };
-template <> struct Cfg<48> { static constexpr int NT = 288, MINB = 3, NTX = 192, MINBX = 6; typedef tgfft::seq<16, 3> R; };
+template <> struct Cfg<48> { static constexpr int NT = 160, MINB = 6, NTX = 192, MINBX = 6; typedef tgfft::seq<16, 3> R; };
 template <> struct Cfg<64> { static constexpr int NT = 256, MINB = 4, NTX = 256, MINBX = 4; typedef tgfft::seq<8, 8> R; };
 template <> struct Cfg<72> { static constexpr int NT = 384, MINB = 2, NTX = 352, MINBX = 3; typedef tgfft::seq<8, 3, 3> R; };
 template <> struct Cfg<80> { static constexpr int NT = 256, MINB = 3, NTX = 224, MINBX = 5; typedef tgfft::seq<16, 5> R; };
 template <> struct Cfg<96> { static constexpr int NT = 384, MINB = 2, NTX = 288, MINBX = 4; typedef tgfft::seq<16, 6> R; };
 
 constexpr int kEdges[] = {24, 32, 40, 48, 64, 72, 80, 96};
+
+// whole warps only: the kernels' warp shuffles name all 32 lanes
+template <int N> constexpr bool whole_warps() { return Cfg<N>::NT % 32 == 0 && Cfg<N>::NTX % 32 == 0; }
+static_assert(whole_warps<24>() && whole_warps<32>() && whole_warps<40>() && whole_warps<48>() &&
+                  whole_warps<64>() && whole_warps<72>() && whole_warps<80>() && whole_warps<96>(),
+              "block sizes must be multiples of 32");
 
 constexpr int kMaxSlots = 8;    // particles whose data is resident at once
 constexpr int kMaxPrune = 32;   // coordinates per axis of a pruned final inverse
