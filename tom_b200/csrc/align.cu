@@ -458,12 +458,11 @@ int corr_norm(tomgpu_ctx* ctx, const float* a, const float* b, const int n[3], c
 // (tom_corr 'norm' inside the mask, no wedges) and tom_peak(., 'spline') of
 // ccf * mask_ccf gives the shift and the peak.  cmax / amax are the scan's
 // running maximum and angle index volumes, nmask the mask's non-zero count.
-int align_finish(tomgpu_ctx* ctx, const tomgpu_align_job& job, int nph, int nps, const float* cmax,
-                 const float* amax, double nmask, AlignScratch* sc, float angles_out[3], float shifts_out[3],
-                 float* peak_out) {
+int align_finish(tomgpu_ctx* ctx, cudaStream_t st, const tomgpu_align_job& job, int nph, int nps,
+                 const float* cmax, const float* amax, double nmask, AlignScratch* sc, float angles_out[3],
+                 float shifts_out[3], float* peak_out) {
     const int* n = job.n;
     const long long nn = (long long)n[0] * n[1] * n[2];
-    cudaStream_t st = ctx->stream;
     const bool wedges = job.wedge_ref != nullptr;
     Workspace& w = sc->w;
     if (!sc->grow(0, (void**)&w.A, sizeof(float2) * nn) || !sc->grow(1, (void**)&w.B, sizeof(float2) * nn) ||
@@ -489,7 +488,8 @@ int align_finish(tomgpu_ctx* ctx, const tomgpu_align_job& job, int nph, int nps,
         if (!key) { rc = fail(ctx, TOMGPU_ERR_DEVICE, "no correlation peak above -99999"); break; }
         const long long pv = (long long)(0xFFFFFFFFull - (key & 0xFFFFFFFFull));
         float ai = 0;
-        if ((e = cudaMemcpy(&ai, amax + pv, sizeof(float), cudaMemcpyDeviceToHost))) break;
+        if ((e = cudaMemcpyAsync(&ai, amax + pv, sizeof(float), cudaMemcpyDeviceToHost, st))) break;
+        if ((e = cudaStreamSynchronize(st))) break;
         // tom_av3_index2angle
         const double a3 = std::floor(ai / (double)(nph * nps));
         const double rest = ai - a3 * nph * nps;
@@ -641,7 +641,7 @@ int align_job(tomgpu_ctx* ctx, const tomgpu_align_job& job, float angles_out[3],
             ctx->launches += 2 + 9;
         }
         if (e) break;
-        rc = align_finish(ctx, job, nph, nps, w.cmax, w.amax, nmask, &sc, angles_out, shifts_out, peak_out);
+        rc = align_finish(ctx, st, job, nph, nps, w.cmax, w.amax, nmask, &sc, angles_out, shifts_out, peak_out);
     } while (0);
     if (e && !rc) rc = cuda_fail(ctx, e, "av3_align");
     if (!scratch) local.release();

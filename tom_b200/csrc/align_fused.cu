@@ -78,7 +78,12 @@ static_assert(whole_warps<24>() && whole_warps<32>() && whole_warps<40>() && who
                   whole_warps<64>() && whole_warps<72>() && whole_warps<80>() && whole_warps<96>(),
               "block sizes must be multiples of 32");
 
-constexpr int kMaxSlots = 8;    // particles whose data is resident at once
+// Particles whose data is resident at once: a batch holds at most
+// kBatchParticles of them, and a particle's slot (its index mod kMaxSlots) is
+// reused only after the batch that follows its last one, which is when its
+// deferred final step has run.
+constexpr int kMaxSlots = 16;
+constexpr int kBatchParticles = 7;
 constexpr int kMaxPrune = 32;   // coordinates per axis of a pruned final inverse
 constexpr int kMaxGroups = 160;  // x3 entry groups per batch
 
@@ -863,15 +868,36 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
     int nzmax = 0, nymax = 0, nxmax = 0;
     // the b-side passes (rotated-wedge plane, its x-lines) run on a second
     // stream beside the a-side ones (rotation, particle-wedge plane, x-lines)
-    cudaStream_t st2 = nullptr;
-    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    // stream; each particle's final step (align_finish) runs on a third one,
+    // one batch later, beside the next batch's passes
+    cudaStream_t st2 = nullptr, stf = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_done = nullptr;
     if ((e = cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking)) ||
+        (e = cudaStreamCreateWithFlags(&stf, cudaStreamNonBlocking)) ||
         (e = cudaEventCreateWithFlags(&ev_a, cudaEventDisableTiming)) ||
-        (e = cudaEventCreateWithFlags(&ev_b, cudaEventDisableTiming))) {
+        (e = cudaEventCreateWithFlags(&ev_b, cudaEventDisableTiming)) ||
+        (e = cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming))) {
         if (st2) cudaStreamDestroy(st2);
+        if (stf) cudaStreamDestroy(stf);
         if (ev_a) cudaEventDestroy(ev_a);
+        if (ev_b) cudaEventDestroy(ev_b);
         return cuda_fail(ctx, e, "av3_align (fused): stream");
     }
+    std::vector<double> nmask(np);  // non-zero voxels of each particle's mask
+    std::vector<int> to_finish;     // particles whose scan ended in the previous batch
+    auto finish_pending = [&]() -> int {
+        if (to_finish.empty()) return TOMGPU_OK;
+        cudaError_t fe = cudaStreamWaitEvent(stf, ev_done, 0);
+        if (fe) return cuda_fail(ctx, fe, "av3_align (fused): final step");
+        for (int p : to_finish) {
+            const int j = job_idx[p], k = p % kMaxSlots;
+            const int frc = align_finish(ctx, stf, jobs[j], nph[p], nps[p], cmax[k], amax[k], nmask[p], sc,
+                                         angles + 3 * j, shifts + 3 * j, peaks + j);
+            if (frc) return frc;
+        }
+        to_finish.clear();
+        return TOMGPU_OK;
+    };
     int rc = TOMGPU_OK;
     do {
         if ((e = cudaMemcpyAsync(d_ent, ent.data(), sizeof(Entry) * total, cudaMemcpyHostToDevice, st))) break;
@@ -881,7 +907,6 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
         if ((e = cudaMemcpyAsync(d_masks, masks.data(), sizeof(float*) * np, cudaMemcpyHostToDevice, st))) break;
         if ((e = cudaMemsetAsync(d_nm, 0, sizeof(double) * np, st))) break;
         k_acount<<<dim3(blocks_for(nn), np), 256, 0, st>>>(d_masks, nn, d_nm);
-        std::vector<double> nmask(np);
         if ((e = cudaMemcpyAsync(nmask.data(), d_nm, sizeof(double) * np, cudaMemcpyDeviceToHost, st))) break;
         std::vector<int> flags;
         if (prune) {
@@ -981,10 +1006,10 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
         long long e0 = 0;
         int next_prep = 0;  // first particle whose slot is not yet prepared
         while (e0 < total && !rc && !e) {
-            // the batch: up to emax entries of at most kMaxSlots particles
+            // the batch: up to emax entries of at most kBatchParticles particles
             const int p_lo = (int)(std::upper_bound(first.begin(), first.end(), (int)e0) - first.begin()) - 1;
             long long e1 = std::min<long long>(total, e0 + emax);
-            const int p_cap = std::min(np, p_lo + kMaxSlots);
+            const int p_cap = std::min(np, p_lo + kBatchParticles);
             e1 = std::min<long long>(e1, first[p_cap]);
             const int nb = (int)(e1 - e0);
             const int p_hi = (int)(std::upper_bound(first.begin(), first.end(), (int)(e1 - 1)) - first.begin()) - 1;
@@ -1104,23 +1129,24 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
                 ctx->launches += 2;
             }
             if ((e = cudaGetLastError())) break;
-            // particles whose scan ended in this batch
-            for (int p = p_lo; p <= p_hi && !rc; ++p) {
-                if (first[p + 1] > e1) continue;
-                const int j = job_idx[p];
-                const int k = p % kMaxSlots;
-                rc = align_finish(ctx, jobs[j], nph[p], nps[p], cmax[k], amax[k], nmask[p], sc, angles + 3 * j,
-                                  shifts + 3 * j, peaks + j);
-            }
+            // the previous batch's finished particles, beside this batch's passes
+            if ((rc = finish_pending())) break;
+            if ((e = cudaEventRecord(ev_done, st))) break;
+            for (int p = p_lo; p <= p_hi; ++p)
+                if (first[p + 1] <= e1) to_finish.push_back(p);
             e0 = e1;
         }
+        if (!rc && !e) rc = finish_pending();
     } while (0);
     if (e && !rc) rc = cuda_fail(ctx, e, "av3_align (fused)");
     cudaStreamSynchronize(st2);
+    cudaStreamSynchronize(stf);
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st2);
+    cudaStreamDestroy(stf);
     cudaEventDestroy(ev_a);
     cudaEventDestroy(ev_b);
+    cudaEventDestroy(ev_done);
     return rc;
 }
 

@@ -156,10 +156,11 @@ void rotmatrix_as_float(double phi, double psi, double theta, float m9[9]);
 // the values of an angle range [start increment end] (one value when increment = 0)
 std::vector<double> axis_values(const float r[3]);
 // the step after a job's scan: angle of the first maximum of cmax * mask_ccf,
-// one more tom_corr at that angle, spline peak; nph / nps the phi and psi counts
-int align_finish(tomgpu_ctx* ctx, const tomgpu_align_job& job, int nph, int nps, const float* cmax,
-                 const float* amax, double nmask, AlignScratch* sc, float angles_out[3], float shifts_out[3],
-                 float* peak_out);
+// one more tom_corr at that angle, spline peak; nph / nps the phi and psi
+// counts; all work on stream st, which it synchronises
+int align_finish(tomgpu_ctx* ctx, cudaStream_t st, const tomgpu_align_job& job, int nph, int nps,
+                 const float* cmax, const float* amax, double nmask, AlignScratch* sc, float angles_out[3],
+                 float shifts_out[3], float* peak_out);
 // The fused alignment engine (align_fused.cu): jobs of one cubic box edge it
 // compiles, all with or all without wedges, scanned as one batch of
 // (particle, rotation) entries.  job_idx lists the jobs; outputs are indexed

@@ -188,13 +188,16 @@ def make_align_particles(n_particles, seed, sizes=(32, 48, 64, 80, 96), snr=0.05
     tom_b200.av3_align_batch plus the true Eulers and shifts."""
     rng = np.random.default_rng(seed)
     jobs, truth = [], []
-    phantoms = {}
+    phantoms, shared = {}, {}
     for p in range(n_particles):
         n = int(rng.choice(sizes))
         if n not in phantoms:
             phantoms[n] = BlobPhantom(np.random.default_rng(seed * 1000 + n), 6, n / 4)
+            # one reference, mask and ccf mask per box size, shared by its particles
+            # (an alignment run aligns every particle against the same reference)
+            shared[n] = (phantoms[n].template(n), sphere_mask(n, n / 2 - 2), sphere_mask(n, max_shift + 1))
         ph = phantoms[n]
-        ref = ph.template(n)
+        ref, mask, mccf = shared[n]
         # true orientation on the scan grid around a seeded start
         start = np.array([rng.uniform(30, 300), rng.uniform(30, 300), rng.uniform(30, 150)]).round()
         k = rng.integers(-int(search_half // search_step), int(search_half // search_step) + 1, 3)
@@ -209,11 +212,9 @@ def make_align_particles(n_particles, seed, sizes=(32, 48, 64, 80, 96), snr=0.05
         g = np.meshgrid(*[np.arange(-(n // 2), n - n // 2)] * 3, indexing="ij")
         with np.errstate(divide="ignore", invalid="ignore"):
             r = np.abs(g[0]) / np.abs(g[2])
-        w = np.ones((n, n, n), np.float32)
+        w = np.ones((n, n, n), np.float32, order="F")
         w[np.tan(np.deg2rad(90 - a)) > r] = 0
         part = np.real(np.fft.ifftn(np.fft.fftn(part) * np.fft.ifftshift(w))).astype(np.float32)
-        mask = sphere_mask(n, n / 2 - 2)
-        mccf = sphere_mask(n, max_shift + 1)
         rngs = [(float(s0 - search_half), float(search_step), float(s0 + search_half)) for s0 in start]
         jobs.append(dict(ref=ref, part=np.asfortranarray(part), mask=mask, mask_ccf=mccf, wedge_ref=w,
                          wedge_part=w, phi=rngs[0], psi=rngs[1], theta=rngs[2]))

@@ -984,12 +984,23 @@ def av3_align_batch(jobs, ctx: Context | None = None, path: int = 0, batch_bytes
     ctx = ctx or default_context()
     arr = (_lib.AlignJob * len(jobs))()
     keep = []
+    uploaded = {}  # id(array) -> (array, device tensor): a volume shared by jobs is uploaded once
+
+    def dev(a):
+        if a is None:
+            return None
+        hit = uploaded.get(id(a))
+        if hit is not None and hit[0] is a:
+            return hit[1]
+        t = to_device(np.asarray(a, np.float32), ctx.device)
+        uploaded[id(a)] = (a, t)
+        return t
+
     for j, jb in enumerate(jobs):
-        ref = np.asarray(jb["ref"], np.float32)
-        n = ref.shape
+        ref = jb["ref"]
+        n = np.shape(ref)
         mask = jb.get("mask")
         mask = tom_spheremask_default(n) if mask is None else mask
-        dev = lambda a: None if a is None else to_device(np.asarray(a, np.float32), ctx.device)
         t = dict(ref=dev(ref), part=dev(jb["part"]), mask=dev(mask), mask_ccf=dev(jb.get("mask_ccf")),
                  wedge_ref=dev(jb.get("wedge_ref")), wedge_part=dev(jb.get("wedge_part")))
         keep.append(t)
