@@ -80,7 +80,8 @@ def parse():
     p.add_argument("--learned-train", type=int, default=8, help="training tomograms of the learned_256 workload")
     p.add_argument("--learned-steps", type=int, default=400, help="timed training steps of the learned_256 workload")
     p.add_argument("--align-particles", type=int, default=40,
-                   help="particles timed for --workload align_2048 (extrapolated to 2048)")
+                   help="particles timed for --workload align_2048 (extrapolated to 2048 from the per-edge "
+                        "times; 2048 times the whole workload once)")
     p.add_argument("--align-batch-mb", type=int, default=0,
                    help="align_2048: device MB of a batch's spectra in the batched engine (0: the library default)")
     p.add_argument("--align-path", type=int, default=0, choices=[0, 1, 2],
@@ -386,16 +387,21 @@ def run_align(args):
     tb.av3_align_batch(list(first.values()), ctx, path=args.align_path, batch_bytes=args.align_batch_mb << 20)
     torch.cuda.synchronize()
 
+    reps = 1 if len(jobs) > 200 else 3
+
     def timed(sub):
-        """median and minimum wall time of three calls on sub (all on the device at the end)"""
+        """median and minimum wall time of `reps` calls on sub (all on the device at the end)"""
         ts = []
-        for _ in range(3):
+        for _ in range(reps):
             torch.cuda.synchronize()
             t = time.perf_counter()
-            out = tb.av3_align_batch(sub, ctx, path=args.align_path, batch_bytes=args.align_batch_mb << 20)
+            out = tb.av3_align_batch(sub, ctx, path=args.align_path, batch_bytes=args.align_batch_mb << 20,
+                                     timings=split)
             torch.cuda.synchronize()
             ts.append(time.perf_counter() - t)
         return float(np.median(ts)), float(min(ts)), out
+
+    split = {}
 
     l0 = ctx.launches
     clocks = ClockSampler(local)
@@ -404,7 +410,8 @@ def run_align(args):
     dt, dt_min, (angles, shifts, peaks) = timed(jobs)
     clocks.mark(h0, time.time())
     clk = clocks.stop()
-    launches = (ctx.launches - l0) // 3
+    launches = (ctx.launches - l0) // reps
+    split_all = dict(split)  # the last call on the whole batch: uploads and library call
     ok = [np.allclose(a, t[0]) for a, t in zip(angles, truth)]
     vox = [int(np.prod(j["ref"].shape)) for j in jobs]
     rv = 1331 * sum(vox)
@@ -415,16 +422,20 @@ def run_align(args):
     # each box edge on its own: seconds per particle, and the 2048-particle
     # workload (edges drawn uniformly from the five) from them
     per_size_s = {}
-    for n in sorted(per_size):
-        sub = [j for j in jobs if j["ref"].shape[0] == n]
-        per_size_s[n] = timed(sub)[0] / len(sub)
+    if len(jobs) <= 200:
+        for n in sorted(per_size):
+            sub = [j for j in jobs if j["ref"].shape[0] == n]
+            per_size_s[n] = timed(sub)[0] / len(sub)
     sizes = (32, 48, 64, 80, 96)
-    if all(n in per_size_s for n in sizes):
+    if len(jobs) == 2048:
+        est_full = dt  # the whole workload, measured
+    elif all(n in per_size_s for n in sizes):
         est_full = 2048 / len(sizes) * sum(per_size_s[n] for n in sizes)
     else:
         est_full = dt / sum(vox) * 2048 * np.mean([s ** 3 for s in sizes])
     line = {"metric": "subtomogram alignment rot*voxel/s (tom_av3_align, 1331 triplets per particle)",
             "value": rv / dt, "unit": "rot*voxel/s", "n_gpus": 1, "particles": len(jobs), "seconds": dt, "seconds_min": dt_min,
+            "upload_s": split_all.get("upload_s"), "call_s": split_all.get("call_s"),
             "particles_per_s": len(jobs) / dt, "est_seconds_2048": est_full,
             "planted_angle_agreement": float(np.mean(ok)),
             "planted_angle_note": "fraction of particles whose scan maximum is the planted Euler triplet; "

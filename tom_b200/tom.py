@@ -972,16 +972,20 @@ def tom_corr(a, b, *args, ctx: Context | None = None):
     return np.asfortranarray(from_device(out))
 
 
-def av3_align_batch(jobs, ctx: Context | None = None, path: int = 0, batch_bytes: int = 0):
+def av3_align_batch(jobs, ctx: Context | None = None, path: int = 0, batch_bytes: int = 0, timings=None):
     """Run tom_av3_align jobs on the GPU.  Each job is a dict with numpy
     volumes 'ref', 'part', 'mask' (None: tom_spheremask default), 'mask_ccf'
     (None: ones), 'wedge_ref', 'wedge_part' (None: no wedges / same as
     wedge_ref) and angle ranges 'phi', 'psi', 'theta' ([start incr end]).
     path 0 batches the jobs of each compiled cubic edge, path 1 runs every job
     alone; batch_bytes bounds a batch's spectra (0: the library default).
+    timings: an optional dict that receives the seconds of the uploads
+    ('upload_s') and of the library call ('call_s').
     Returns (angles[n,3], shifts[n,3], ccf_peak[n])."""
+    import time
     import torch
     ctx = ctx or default_context()
+    t0 = time.perf_counter()
     arr = (_lib.AlignJob * len(jobs))()
     keep = []
     uploaded = {}  # id(array) -> (array, device tensor): a volume shared by jobs is uploaded once
@@ -1014,11 +1018,16 @@ def av3_align_batch(jobs, ctx: Context | None = None, path: int = 0, batch_bytes
     shifts = np.zeros((len(jobs), 3), np.float32)
     peaks = np.zeros(len(jobs), np.float32)
     prm = _lib.AlignParams(int(path), int(batch_bytes))
+    torch.cuda.synchronize(ctx.device)
+    t1 = time.perf_counter()
     ctx.check(lib().tomgpu_av3_align_ex_dev(ctx.handle, arr, len(jobs), ctypes.byref(prm),
                                             angles.ctypes.data_as(_lib.c_float_p),
                                             shifts.ctypes.data_as(_lib.c_float_p),
                                             peaks.ctypes.data_as(_lib.c_float_p)))
     torch.cuda.synchronize(ctx.device)
+    if timings is not None:
+        timings["upload_s"] = t1 - t0
+        timings["call_s"] = time.perf_counter() - t1
     return angles, shifts, peaks
 
 
