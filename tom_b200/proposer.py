@@ -283,6 +283,38 @@ def refine(vol, template, mask, centres, angle_sets, window=2, batch=8, ctx=None
     return np.array(out_pos), np.asarray(vals, np.float64), np.array(out_idx)
 
 
+def rotation_matrices(eulers):
+    """The rot3d matrices of ZXZ Euler triplets [phi, psi, theta] in degrees,
+    (n, 3, 3) float64 (Sptrans/tom_rotatec.c:164-288, vectorised)."""
+    e = np.deg2rad(np.asarray(eulers, np.float64).reshape(-1, 3))
+    cf, sf = np.cos(e[:, 0]), np.sin(e[:, 0])
+    cp, sp = np.cos(e[:, 1]), np.sin(e[:, 1])
+    ct, st = np.cos(e[:, 2]), np.sin(e[:, 2])
+    R = np.empty((len(e), 3, 3))
+    R[:, 0, 0] = cp * cf - ct * sp * sf
+    R[:, 1, 0] = sp * cf + ct * cp * sf
+    R[:, 2, 0] = st * sf
+    R[:, 0, 1] = -cp * sf - ct * sp * cf
+    R[:, 1, 1] = -sp * sf + ct * cp * cf
+    R[:, 2, 1] = st * cf
+    R[:, 0, 2] = st * sp
+    R[:, 1, 2] = -st * cp
+    R[:, 2, 2] = ct
+    return R
+
+
+def neighbours(fine_grid, centres, max_deg):
+    """For each centre triplet, the indices of the fine-grid triplets whose
+    rotation lies within max_deg of it (geodesic angle of R_f R_c^T)."""
+    Rf = rotation_matrices(fine_grid).reshape(-1, 9)
+    Rc = rotation_matrices(centres).reshape(-1, 9)
+    lim = 1.0 + 2.0 * np.cos(np.deg2rad(max_deg))  # trace of a rotation by max_deg
+    out = []
+    for c in Rc:
+        out.append(np.nonzero(Rf @ c >= lim - 1e-9)[0])
+    return out
+
+
 def bin_members(fine_grid, coarse_grid):
     """Fine-grid indices of each coarse bin (nearest-rotation partition)."""
     b = coarse_bin(fine_grid, coarse_grid)
