@@ -144,3 +144,41 @@ def test_training_reduces_loss(gpu):
         last = net.train_step(x, tgt, fi, tb_, pos_weight=50.0, lr=1e-3)
     assert np.isfinite(last[0]) and last[0] < 0.5 * first[0]
     assert last[1] < 0.5 * first[1]
+
+
+def test_pruned_search_recalls_exhaustive_peaks(gpu):
+    """The pruned search (coarse sub-grid, its top peaks, the fine triplets
+    within a geodesic radius of each candidate's coarse rotation refined on
+    crops within +-3 voxels) finds the exhaustive fine search's peaks: every
+    exhaustive peak that sits on a particle by position, nearly all with the
+    same triplet, on a 128^3 tomogram with 12 particles whose orientations
+    lie on the fine grid."""
+    from tom_b200 import proposer as pr
+    from tom_b200 import synth
+    ctx = gpu.default_context()
+    N, T, K = (128, 128, 128), 32, 12
+    fine = gpu.tom_av3_angle_grid((0, 0, 0), (10, 10, 10), (350, 350, 170))
+    coarse = gpu.tom_av3_angle_grid((0, 0, 0), (30, 30, 30), (330, 330, 150))
+    d = synth.make_tomogram(N, T, K, 6, 10, 1.0, 60, seed=21, euler_pool=fine, mask_radius=T // 2 - 2)
+    mask = synth.sphere_mask(T, T // 2 - 2)
+    ccf, idf = pr.search(d["tomo"], d["template"], mask, fine, batch=16, ctx=ctx)
+    _, ref_pos, ref_idx = gpu.pick_peaks(ccf, idf, K, T / 2, ctx)
+    ref_pos = ref_pos - 1
+    # the exhaustive peaks on a particle (within 2 voxels of a placed centre)
+    truth = np.asarray(d["positions"], float)
+    on = np.linalg.norm(ref_pos[:, None, :] - truth[None], axis=2).min(axis=1) <= 2
+    assert on.sum() >= K - 1
+    ccc, idc = pr.search(d["tomo"], d["template"], mask, coarse, batch=16, ctx=ctx)
+    _, cpos, cidx = gpu.pick_peaks(ccc, idc, 2 * K, T / 2, ctx)
+    ok = cidx >= 0
+    cpos, cidx = cpos[ok] - 1, cidx[ok]
+    near = pr.neighbours(fine, coarse[cidx], 30.0)
+    assert all(0 < len(x) < len(fine) for x in near)
+    rpos, rcc, ridx = pr.refine(d["tomo"], d["template"], mask, cpos, [(fine[i], i) for i in near], window=3,
+                                ctx=ctx)
+    dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - rpos[None].astype(float), axis=2)
+    j = np.argmin(dd, axis=1)
+    found = dd[np.arange(K), j] <= 2
+    same = ridx[j] == ref_idx
+    assert found[on].all(), dd.min(axis=1)
+    assert (found & same)[on].mean() >= 0.9, (ridx[j], ref_idx)

@@ -41,3 +41,24 @@ def test_place_copies_spacing_and_borders():
         assert a[:, d].min() >= T / 2 - 0.5 and a[:, d].max() <= N[d] - T / 2 + 0.5
     dist = np.linalg.norm(a[:, None] - a[None], axis=-1)
     assert dist[np.triu_indices(len(a), 1)].min() >= T
+
+
+def test_rotation_matrices_and_geodesic_neighbours():
+    """proposer.rotation_matrices is the transpose of synth.rot3d_matrix (the
+    same rotation, column-major as tom_rotatec lists it) and neighbours()
+    returns exactly the fine triplets within the geodesic radius."""
+    from tom_b200 import proposer as pr
+    import tom_b200 as tb
+    rng = np.random.default_rng(5)
+    e = np.column_stack([rng.uniform(0, 360, 20), rng.uniform(0, 360, 20), rng.uniform(0, 180, 20)])
+    R = pr.rotation_matrices(e)
+    for k in range(len(e)):
+        assert np.allclose(R[k], synth.rot3d_matrix(e[k]).T, atol=1e-12)
+        assert np.allclose(R[k] @ R[k].T, np.eye(3), atol=1e-12)
+    fine = tb.tom_av3_angle_grid((0, 0, 0), (20, 20, 20), (340, 340, 180))
+    centres = e[:5]
+    Rf = pr.rotation_matrices(fine)
+    for c, ids in zip(centres, pr.neighbours(fine, centres, 25.0)):
+        Rc = pr.rotation_matrices([c])[0]
+        ang = np.degrees(np.arccos(np.clip((np.einsum("kij,ij->k", Rf, Rc) - 1) / 2, -1, 1)))
+        assert set(ids.tolist()) == set(np.nonzero(ang <= 25.0 + 1e-7)[0].tolist())
