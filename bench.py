@@ -520,7 +520,12 @@ def run_align(args):
         est_full = 2048 / len(sizes) * sum(per_size_s[n] for n in sizes)
     else:
         est_full = dt / sum(vox) * 2048 * np.mean([s ** 3 for s in sizes])
+    # flops by the survey's count for this config: (5 log2 n^3 + 20) per rot*voxel
+    flops = 1331 * sum(v * (5 * np.log2(v) + 20) for v in vox)
     line = {"metric": "subtomogram alignment rot*voxel/s (tom_av3_align, 1331 triplets per particle)",
+            "flop_per_s": flops / dt,
+            "flop_note": "(5 log2 n^3 + 20) flop per rot*voxel; FP32 CUDA-core nominal peak "
+                         "148 SMs x 128 lanes x 2 x 1.965 GHz = 74.4 TFLOP/s",
             "value": rv / dt, "unit": "rot*voxel/s", "n_gpus": 1, "particles": len(jobs), "seconds": dt, "seconds_min": dt_min,
             "upload_s": split_all.get("upload_s"), "call_s": split_all.get("call_s"),
             "particles_per_s": len(jobs) / dt, "est_seconds_2048": est_full,

@@ -337,8 +337,8 @@ int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jo
 
 /* Engine choice for tomgpu_av3_align_ex_dev (NULL params: the defaults). */
 typedef struct {
-    int path;           /* 0 (default): the jobs with a cubic box of edge 24, 32, 40, 48, 64, 72, 80
-                           or 96 run batched, one stream of (particle, rotation) entries per edge
+    int path;           /* 0 (default): the jobs with a cubic box of edge 24, 32, 40, 48, 56, 64, 72,
+                           80, 96, 100, 112, 120 or 128 run batched, one stream of (particle, rotation) entries per edge
                            and wedge form, the others one job at a time; 1: every job one at a
                            time; 2: as 0 but the scan's last inverse DFT always over the whole
                            box (0 evaluates it only where mask_ccf is non-zero, when every job

@@ -136,6 +136,12 @@ def test_batched_engine_equals_per_job(gpu, oracle):
     soft = _job(oracle, 40, 0, True, 323)
     soft["wedge_ref"] = (0.7 * soft["wedge_ref"] + 0.1234567).astype(np.float32)
     jobs.append(soft)
+    # the larger edges (radices 8 x 7, 4 x 5 x 5, 16 x 8), the last without
+    # mask_ccf (the full last inverse on two lines per complex line)
+    few = dict(phi=(0, 3, 3), psi=(0, 3, 3), theta=(6, 3, 9))
+    jobs.append(_job(oracle, 56, 1, True, 324, **few))
+    jobs.append(_job(oracle, 100, 2, True, 325, **few))
+    jobs.append(_job(oracle, 128, 0, False, 326, mccf="none", **few))
     half32 = 17 * 32 * 32 * 8
     a0, s0, p0 = gpu.av3_align_batch(jobs, path=0, batch_bytes=2 * half32 * 10)
     a1, s1, p1 = gpu.av3_align_batch(jobs, path=1)

@@ -69,13 +69,20 @@ template <> struct Cfg<64> { static constexpr int NT = 256, MINB = 4, NTX = 256,
 template <> struct Cfg<72> { static constexpr int NT = 384, MINB = 2, NTX = 352, MINBX = 3; typedef tgfft::seq<8, 3, 3> R; };
 template <> struct Cfg<80> { static constexpr int NT = 256, MINB = 3, NTX = 224, MINBX = 5; typedef tgfft::seq<16, 5> R; };
 template <> struct Cfg<96> { static constexpr int NT = 384, MINB = 2, NTX = 288, MINBX = 4; typedef tgfft::seq<16, 6> R; };
+template <> struct Cfg<56> { static constexpr int NT = 448, MINB = 2, NTX = 224, MINBX = 5; typedef tgfft::seq<8, 7> R; };
+template <> struct Cfg<100> { static constexpr int NT = 512, MINB = 1, NTX = 320, MINBX = 3; typedef tgfft::seq<4, 5, 5> R; };
+template <> struct Cfg<112> { static constexpr int NT = 800, MINB = 1, NTX = 416, MINBX = 2; typedef tgfft::seq<16, 7> R; };
+template <> struct Cfg<120> { static constexpr int NT = 960, MINB = 1, NTX = 480, MINBX = 2; typedef tgfft::seq<8, 3, 5> R; };
+template <> struct Cfg<128> { static constexpr int NT = 1024, MINB = 1, NTX = 512, MINBX = 2; typedef tgfft::seq<16, 8> R; };
 
-constexpr int kEdges[] = {24, 32, 40, 48, 64, 72, 80, 96};
+constexpr int kEdges[] = {24, 32, 40, 48, 56, 64, 72, 80, 96, 100, 112, 120, 128};
 
 // whole warps only: the kernels' warp shuffles name all 32 lanes
 template <int N> constexpr bool whole_warps() { return Cfg<N>::NT % 32 == 0 && Cfg<N>::NTX % 32 == 0; }
 static_assert(whole_warps<24>() && whole_warps<32>() && whole_warps<40>() && whole_warps<48>() &&
-                  whole_warps<64>() && whole_warps<72>() && whole_warps<80>() && whole_warps<96>(),
+                  whole_warps<56>() && whole_warps<64>() && whole_warps<72>() && whole_warps<80>() &&
+                  whole_warps<96>() && whole_warps<100>() && whole_warps<112>() && whole_warps<120>() &&
+                  whole_warps<128>(),
               "block sizes must be multiples of 32");
 
 // Particles whose data is resident at once: a batch holds at most
@@ -294,8 +301,16 @@ __global__ void __launch_bounds__(Cfg<N>::NTX, Cfg<N>::MINBX) k_ax(float2* __res
         const float c = (float)((N + 1) / 2);
         for (int i = tid; i < NL * N; i += NT) {
             // a warp samples an 8 (x) x 8 (y) tile of the slab (two y per thread)
-            const int lane = i & 31, t = i >> 5;
-            const int x = (t % (N / 8)) * 8 + (lane & 7), j = (t / (N / 8)) * 4 + (lane >> 3);
+            // where the edge allows, else a row
+            int x, j;
+            if constexpr (N % 8 == 0) {
+                const int lane = i & 31, t = i >> 5;
+                x = (t % (N / 8)) * 8 + (lane & 7);
+                j = (t / (N / 8)) * 4 + (lane >> 3);
+            } else {
+                j = i / N;
+                x = i - j * N;
+            }
             float a[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
@@ -392,10 +407,17 @@ __global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ap(float2* __restr
         for (int q = 0; q < 9; ++q) m[q] = en->mw[q];
         const float c = (float)((N + 1) / 2);
         for (int i = tid; i < N * N; i += NT) {
-            // a warp samples an 8 (y) x 4 (z) tile of the plane: its source
-            // points span two rotated directions, fewer cache lines than a row
-            const int lane = i & 31, t = i >> 5;
-            const int y = (t % (N / 8)) * 8 + (lane & 7), z = (t / (N / 8)) * 4 + (lane >> 3);
+            // a warp samples an 8 (y) x 4 (z) tile of the plane where the edge
+            // allows (source points spanning two rotated directions), else a row
+            int y, z;
+            if constexpr (N % 8 == 0) {
+                const int lane = i & 31, t = i >> 5;
+                y = (t % (N / 8)) * 8 + (lane & 7);
+                z = (t / (N / 8)) * 4 + (lane >> 3);
+            } else {
+                z = i / N;
+                y = i - z * N;
+            }
             int s1, s2;
             wedge_pair(kx + N * (y + N * z), N, N, N, s1, s2);
             float w1, w2;
@@ -515,42 +537,53 @@ __global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ap(float2* __restr
 }
 
 // ------------------------------------------------ cross-correlation maxima
-// grid (N z-slabs, groups): inverse x-DFT of each entry's C slab, ccf =
-// value / numel / nmask, running maximum (strict) and angle index (at >=) over
-// the group's entries in scan order; written fftshifted as (max, index).
+// grid (N z-slabs, groups): inverse x-DFT of each entry's C slab (two lines
+// per complex line, as in k_ax), ccf = value / numel / nmask, running maximum
+// (strict) and angle index (at >=) over the group's entries in scan order;
+// written fftshifted as (max, index).
 template <int N>
-__global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ax3(const float2* __restrict__ Bv, long long hstride,
-                                                    const Entry* __restrict__ ent,
-                                                    const __grid_constant__ SlotTab slots,
-                                                    const __grid_constant__ GroupTab groups,
-                                                    float2* __restrict__ partial, const float2* __restrict__ tw,
-                                                    float inv_n3) {
-    constexpr int NT = Cfg<N>::NT, P = N + 1, NH = N / 2 + 1, H2 = N / 2;
+__global__ void __launch_bounds__(Cfg<N>::NTX, 1) k_ax3(const float2* __restrict__ Bv, long long hstride,
+                                                       const Entry* __restrict__ ent,
+                                                       const __grid_constant__ SlotTab slots,
+                                                       const __grid_constant__ GroupTab groups,
+                                                       float2* __restrict__ partial, const float2* __restrict__ tw,
+                                                       float inv_n3) {
+    constexpr int NT = Cfg<N>::NTX, P = N + 1, NH = N / 2 + 1, NL = N / 2, H2 = N / 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* s = reinterpret_cast<float2*>(smem_raw);
-    float2* mx = s + N * P;
+    float2* mx = s + NL * P;  // [y][x] running (max, index)
     const int z = blockIdx.x, tid = threadIdx.x;
     const Group g = groups.g[blockIdx.y];
     const double inv_nm = 1.0 / slots.s[g.slot].nmask;
     for (int i = tid; i < N * N; i += NT) mx[i] = make_float2(-INFINITY, 0.f);
     for (int e = g.e0; e < g.e1; ++e) {
         const float2* Hs = Bv + (long long)e * hstride;
-        for (int i = tid; i < NH * N; i += NT) {
-            const int kx = i / N, y = i - kx * N;
-            const float2 v = Hs[((long long)kx * N + z) * N + y];
-            s[y * P + kx] = v;
-            if (kx > 0 && 2 * kx != N) s[y * P + N - kx] = cconj(v);
+        for (int i = tid; i < NH * NL; i += NT) {
+            const int kx = i / NL, j = i - kx * NL;
+            const float4 h = *reinterpret_cast<const float4*>(Hs + ((long long)kx * N + z) * N + 2 * j);
+            float2 a = make_float2(h.x, h.y), b = make_float2(h.z, h.w);
+            if (kx == 0 || 2 * kx == N) {
+                a.y = 0.f;
+                b.y = 0.f;
+            }
+            s[j * P + kx] = make_float2(a.x - b.y, a.y + b.x);
+            if (kx > 0 && 2 * kx != N) s[j * P + N - kx] = make_float2(a.x + b.y, b.x - a.y);
         }
         __syncthreads();
-        pfft<N, +1, 1, P>(s, tw, tid);
+        pfft_l<N, NL, NT, +1, 1, P>(s, tw, tid);
         const float ai = (float)ent[e].aidx;
-        for (int i = tid; i < N * N; i += NT) {
-            const int y = i / N, x = i - y * N;
-            const float c = (float)((double)(s[y * P + x].x * inv_n3) * inv_nm);
-            float2 r = mx[i];
-            if (c > r.x) r.x = c;
-            if (c >= r.x) r.y = ai;
-            mx[i] = r;
+        for (int i = tid; i < NL * N; i += NT) {
+            const int j = i / N, x = i - j * N;
+            const float2 v = s[j * P + x];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const float c = (float)((double)((h ? v.y : v.x) * inv_n3) * inv_nm);
+                float2& r = mx[(2 * j + h) * N + x];
+                float2 t = r;
+                if (c > t.x) t.x = c;
+                if (c >= t.x) t.y = ai;
+                r = t;
+            }
         }
         __syncthreads();
     }
@@ -789,7 +822,7 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
         (e = raise_smem(k_ap<N, P_WEDGE_A>, tile)) || (e = raise_smem(k_ap<N, P_WEDGE_B>, tile)) ||
         (e = raise_smem(k_ap<N, P_CROSS>, tile)) || (e = raise_smem(k_ap<N, P_CROSS_NW>, tile)) ||
         (e = raise_smem(k_ap<N, P_FWD>, tile)) || (e = raise_smem(k_ap<N, P_FWD_NORM>, tile)) ||
-        (e = raise_smem(k_ax3<N>, tile + sizeof(float2) * N * N)))
+        (e = raise_smem(k_ax3<N>, xtile + sizeof(float2) * N * N)))
         return cuda_fail(ctx, e, "av3_align (fused): shared memory attribute");
 
     // the scan of every particle, in the reference's loop order
@@ -1123,8 +1156,8 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
                 k_ax3s<<<dim3((prod + 127) / 128, es.n), 128, 0, st>>>(VP, prod, N, eb, slots, es);
                 ctx->launches += 2;
             } else {
-                k_ax3<N><<<dim3(N, groups.n), NT, tile + sizeof(float2) * N * N, st>>>(HB, hvol, eb, slots, groups,
-                                                                                       part, tw, inv_n3);
+                k_ax3<N><<<dim3(N, groups.n), NTX, xtile + sizeof(float2) * N * N, st>>>(HB, hvol, eb, slots,
+                                                                                         groups, part, tw, inv_n3);
                 k_amerge<<<dim3(blocks_for(nn), segs.n), 256, 0, st>>>(part, nn, segs, slots);
                 ctx->launches += 2;
             }
@@ -1171,6 +1204,11 @@ int align_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, const int* job_id
         case 72: return run_fused<72>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
         case 80: return run_fused<80>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
         case 96: return run_fused<96>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
+        case 56: return run_fused<56>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
+        case 100: return run_fused<100>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
+        case 112: return run_fused<112>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
+        case 120: return run_fused<120>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
+        case 128: return run_fused<128>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
         default: return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "fused alignment: box edge not compiled");
     }
 }
