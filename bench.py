@@ -69,8 +69,11 @@ def parse():
     p.add_argument("--path", type=int, default=0, choices=[0, 1, 2, 3],
                    help="kernel path of the plan: 0 fastest (TMA x-line tiles at the 512 x edge), 1 generic, "
                         "2 as 0 with cp.async x-line tiles, 3 as 0 with the tcgen05 inverse z-DFT")
-    p.add_argument("--e2e-rot", type=int, default=2048)
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-rot", type=int, default=0,
+                   help="rotations per end-to-end call; 0: the whole angle grid in one call (a whole search, "
+                        "as tom_os3_findTemplate makes it) when it holds at most 25,000 triplets, else 2048")
+    p.add_argument("--e2e-steps", type=int, default=0,
+                   help="end-to-end calls timed; 0: one for a whole-grid call, else 3")
     p.add_argument("--cpu-seconds", type=float, default=20.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -663,6 +666,11 @@ def main():
         idx_h = pin(cfg["N"], torch.int32)
         ectx = tb.Context(local)
         tb.match_host(tomo_h, d["template"], mask, grid[:8], batch=args.batch, ctx=ectx)  # warm-up
+        if args.e2e_rot <= 0:
+            # the whole grid, split across the ranks (angle partitioning)
+            args.e2e_rot = -(-len(grid) // world) if len(grid) <= 25000 else 2048
+        if args.e2e_steps <= 0:
+            args.e2e_steps = 1 if args.e2e_rot * world >= len(grid) else 3
         if dist:
             dist.barrier()
         t0 = time.perf_counter()
