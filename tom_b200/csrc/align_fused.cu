@@ -846,6 +846,7 @@ template <int N> int run_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, co
                     ent.push_back(en);
                 }
     }
+    if (ent.size() > (size_t)INT32_MAX) return fail(ctx, TOMGPU_ERR_UNSUPPORTED, "fused alignment: too many entries");
     first[np] = (int)ent.size();
     const long long total = (long long)ent.size();
 
@@ -1195,6 +1196,16 @@ bool align_fused_supported(const tomgpu_align_job& job) {
 int align_fused(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, const int* job_idx, int n, float* angles,
                 float* shifts, float* peaks, size_t budget_bytes, bool allow_prune, AlignScratch* sc) {
     if (n <= 0) return TOMGPU_OK;
+    // the per-particle set-up kernels take the particle as their grid's y index
+    constexpr int kMaxJobs = 32768;
+    if (n > kMaxJobs) {
+        for (int o = 0; o < n; o += kMaxJobs) {
+            const int rc = align_fused(ctx, jobs, job_idx + o, std::min(kMaxJobs, n - o), angles, shifts, peaks,
+                                       budget_bytes, allow_prune, sc);
+            if (rc) return rc;
+        }
+        return TOMGPU_OK;
+    }
     switch (jobs[job_idx[0]].n[0]) {
         case 24: return run_fused<24>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
         case 32: return run_fused<32>(ctx, jobs, job_idx, n, angles, shifts, peaks, budget_bytes, allow_prune, sc);
