@@ -192,7 +192,12 @@ typedef struct {
     int batch;          /* rotations per batch; 0 = the largest of 64, 32, 16 whose
                            per-batch buffers fit in half the free device memory, else 8 */
     int wedge_fp64;     /* reserved, 0 */
-    int path;           /* 0: fastest kernels for the sizes; 1: generic kernels only;
+    int path;           /* 0: fastest kernels for the sizes; 1: generic kernels only (they
+                           compare the CC of every rotation, so of two rotations whose CC
+                           rounds to the same float the first one is kept whatever the
+                           batch: tom_os3_bestPeak's rule; the fast x-line kernels of path 0
+                           compare out / (N M) + kappa within a batch, where such a tie can
+                           go to the later rotation);
                            2: as 0, but the x-line kernels of the 512 / 928 x edges load their
                            tiles with per-thread cp.async instead of TMA and the y-column
                            kernel of the 512 y edge reads its constants from shared memory
