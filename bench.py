@@ -363,6 +363,22 @@ def run_learned(args):
 
     rc, ra = recall(rpos, ridx)
     bc, ba = recall(bres_pos, bidx)
+    # equal candidate counts with the fine triplets within 30 degrees of each
+    # candidate's coarse rotation: the coarse map's own first peaks against the
+    # network's ranking of the first 4 x that many coarse peaks
+    cmp = {}
+    for C in (K // 2, K, 2 * K):
+        _, bp, bi = tb.pick_peaks(ccc2, idc2, C, T / 2, ctx)
+        okb = bi >= 0
+        bp, bi = bp[okb] - 1, bi[okb]
+        npos, nidx, _ = pr.rerank(net, ccc2, idc2, C, 4 * C, T / 2, ctx)
+        out = {}
+        for name, cp_, ci_ in (("coarse_peaks", bp, bi), ("network_ranked", npos, nidx)):
+            near = pr.neighbours(fine, coarse[ci_], 30.0)
+            rp, _, ri = pr.refine(d["tomo"], d["template"], mask, cp_, [(fine[i], i) for i in near], ctx=ctx)
+            pc, pa = recall(rp, ri)
+            out[name] = {"position": pc, "position_and_angle": pa}
+        cmp[str(C)] = out
     t_pruned = t_coarse + t_prop + t_ref
     line = {"metric": "learned-pruned search speed-up over the exhaustive fine search (256^3, 32^3 template)",
             "value": t_exh / t_pruned, "unit": "x", "higher_is_better": True, "n_gpus": 1,
@@ -374,6 +390,7 @@ def run_learned(args):
             "recall_network": {"position": rc, "position_and_angle": ra},
             "recall_coarse_peaks_without_network": {"position": bc, "position_and_angle": ba,
                                                     "pruned_s": t_coarse + t_bref},
+            "recall_by_candidates_radius_30deg": cmp,
             "training": {"flop_per_s": train_flops / t_train, "s_per_step": t_train / args.learned_steps,
                          "last_loss": losses[-1]},
             "scaling": "weak", "vs_baseline": None}

@@ -223,6 +223,25 @@ def propose(net, cc_coarse, n_cand, radius, top_bins, ctx=None):
     return pos, vals, bins
 
 
+def rerank(net, cc_coarse, idx_coarse, n_cand, n_pool, radius, ctx=None):
+    """Candidates of the coarse map re-ranked by the network: the n_pool first
+    coarse peaks (tom_peak rounds of radius `radius`), each scored by the
+    network's centre probability at its voxel, the n_cand best kept.
+    Returns (positions 0-based [x, y, z], coarse angle index, score)."""
+    import torch
+    ctx = ctx or net.ctx
+    x = torch.from_numpy(np.ascontiguousarray(normalise(from_device(cc_coarse).transpose(2, 1, 0)))).to(net.dev)
+    _, logit = net.forward(x)
+    heat = torch.sigmoid(logit)
+    _, pos, aidx = pick_peaks(cc_coarse, idx_coarse, n_pool, radius, ctx)
+    ok = aidx >= 0
+    pos, aidx = pos[ok] - 1, aidx[ok]
+    p = torch.as_tensor(pos, device=net.dev)
+    score = heat[p[:, 2], p[:, 1], p[:, 0]].cpu().numpy()
+    order = np.argsort(-score, kind="stable")[:n_cand]
+    return pos[order], aidx[order], score[order]
+
+
 def refine(vol, template, mask, centres, angle_sets, window=2, batch=8, ctx=None):
     """The fine search around each centre only: the FLCF on a periodic crop of
     edge L >= T + 2 window + 1 (an FFT length), with the centre's own angle
