@@ -419,10 +419,10 @@ def run_pruned(args):
     cfg, fine, d, mask = make_workload(name)
     T, K = cfg["T"], cfg["n_copies"]
     step = args.pruned_step
-    hi = [(360 // step) * step if (360 // step) * step < 360 else 360 - step, 0, 0]
-    coarse = tb.tom_av3_angle_grid((0, 0, 0), (step, step, step),
-                                   (hi[0], hi[0], (180 // step) * step if (180 // step) * step <= 175 else
-                                    ((180 // step) - 1) * step))
+    fstart, finc, fend = cfg["angles"]
+    if step % finc[0]:
+        raise SystemExit("--pruned-step must be a multiple of the fine step (%d)" % finc[0])
+    coarse = pr.coarse_grid(fstart, finc, fend, step // finc[0])
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -443,34 +443,24 @@ def run_pruned(args):
         if args.pruned_ref_out:
             np.savez(args.pruned_ref_out, pos=ref_pos, idx=ref_idx, vals=ref_vals, t_exh=t_exh)
     torch.cuda.empty_cache()
-    (ccc, idc), t_coarse = timed(lambda: pr.search(d["tomo"], d["template"], mask, coarse, batch=batch, ctx=ctx))
     C = int(round(args.pruned_cands * K))
-    (cvals, cpos, cidx), t_pick = timed(lambda: tb.pick_peaks(ccc, idc, C, T / 2, ctx))
-    cpos = cpos - 1
-    del ccc, idc
-    torch.cuda.empty_cache()
-    t0 = time.perf_counter()
-    ok = cidx >= 0
-    cpos, cidx = cpos[ok], cidx[ok]
-    near = pr.neighbours(fine, coarse[cidx], args.pruned_radius)
-    sets = [(fine[ids], ids) for ids in near]
-    t_sets = time.perf_counter() - t0
-    (rpos, rcc, ridx), t_ref = timed(lambda: pr.refine(d["tomo"], d["template"], mask, cpos, sets, ctx=ctx))
+    tm = {}
+    rpos, rcc, ridx = pr.pruned_search(d["tomo"], d["template"], mask, fine, coarse, C, args.pruned_radius,
+                                       batch=batch, ctx=ctx, timings=tm)
     dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - np.asarray(rpos)[None].astype(float), axis=2)
     j = np.argmin(dd, axis=1)
     found = dd[np.arange(len(ref_pos)), j] <= 2
     same = np.asarray(ridx)[j] == ref_idx
-    t_pruned = t_coarse + t_pick + t_sets + t_ref
+    t_pruned = tm["total"]
     line = {"metric": "pruned-search speed-up over the exhaustive fine search (928x928x464, 48^3 template)",
             "value": t_exh / t_pruned, "unit": "x", "higher_is_better": True, "n_gpus": 1,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": "pruned_928x928x464", "fine_angles": len(fine), "coarse_angles": len(coarse),
-                       "coarse_step_deg": step, "candidates": int(len(cpos)), "reference_peaks": K,
+                       "coarse_step_deg": step, "candidates": tm["candidates_n"], "reference_peaks": K,
                        "refine_radius_deg": args.pruned_radius,
-                       "refine_triplets_per_candidate": float(np.mean([len(x) for x in near]))},
+                       "refine_triplets_per_candidate": tm["triplets_per_candidate"]},
             "exhaustive_s": t_exh,
-            "pruned_s": {"total": t_pruned, "coarse": t_coarse, "candidates": t_pick, "triplet_sets": t_sets,
-                         "refine": t_ref},
+            "pruned_s": {k: tm[k] for k in ("total", "coarse", "candidates", "triplet_sets", "refine")},
             "recall": {"position": float(found.mean()), "position_and_triplet": float((found & same).mean())},
             "scaling": "weak", "vs_baseline": None}
     print(json.dumps(line), flush=True)

@@ -168,14 +168,11 @@ def test_pruned_search_recalls_exhaustive_peaks(gpu):
     truth = np.asarray(d["positions"], float)
     on = np.linalg.norm(ref_pos[:, None, :] - truth[None], axis=2).min(axis=1) <= 2
     assert on.sum() >= K - 1
-    ccc, idc = pr.search(d["tomo"], d["template"], mask, coarse, batch=16, ctx=ctx)
-    _, cpos, cidx = gpu.pick_peaks(ccc, idc, 2 * K, T / 2, ctx)
-    ok = cidx >= 0
-    cpos, cidx = cpos[ok] - 1, cidx[ok]
-    near = pr.neighbours(fine, coarse[cidx], 30.0)
-    assert all(0 < len(x) < len(fine) for x in near)
-    rpos, rcc, ridx = pr.refine(d["tomo"], d["template"], mask, cpos, [(fine[i], i) for i in near], window=3,
-                                ctx=ctx)
+    assert np.array_equal(coarse, pr.coarse_grid((0, 0, 0), (10, 10, 10), (350, 350, 170), 3))
+    tm = {}
+    rpos, rcc, ridx = pr.pruned_search(d["tomo"], d["template"], mask, fine, coarse, 2 * K, 30.0, window=3,
+                                       batch=16, ctx=ctx, timings=tm)
+    assert tm["candidates_n"] == 2 * K and 0 < tm["triplets_per_candidate"] < len(fine)
     dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - rpos[None].astype(float), axis=2)
     j = np.argmin(dd, axis=1)
     found = dd[np.arange(K), j] <= 2

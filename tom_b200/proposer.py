@@ -223,6 +223,55 @@ def propose(net, cc_coarse, n_cand, radius, top_bins, ctx=None):
     return pos, vals, bins
 
 
+def coarse_grid(fine_start, fine_incr, fine_end, factor):
+    """The sub-grid of every factor-th step of a tom_av3_angle_grid (start,
+    incr, end): the coarse grid of a pruned search."""
+    from .tom import tom_av3_angle_grid
+    inc = [i * factor for i in fine_incr]
+    end = [s + ((e - s) // c) * c for s, c, e in zip(fine_start, inc, fine_end)]
+    return tom_av3_angle_grid(fine_start, inc, end)
+
+
+def pruned_search(vol, template, mask, fine, coarse, n_cand, radius_deg, window=2, peak_radius=None, batch=32,
+                  ctx=None, timings=None):
+    """A pruned FLCF search: the exhaustive search over the coarse grid, its
+    n_cand first peaks (tom_peak rounds of radius peak_radius, default half
+    the template edge), and around each the fine triplets within radius_deg
+    (geodesic) of its coarse rotation searched on a crop (refine: the values
+    equal the full search's there), the best within +-window voxels.
+    timings: an optional dict that receives the seconds of the steps.
+    Returns (positions 0-based [x, y, z], cc, fine triplet index) per candidate."""
+    import time
+    import torch
+    ctx = ctx or default_context()
+    T = np.shape(template)[0]
+    clock = []
+
+    def mark():
+        torch.cuda.synchronize(ctx.device)
+        clock.append(time.perf_counter())
+
+    mark()
+    cc, idx = search(vol, template, mask, coarse, batch=batch, ctx=ctx)
+    mark()
+    _, pos, cidx = pick_peaks(cc, idx, n_cand, T / 2 if peak_radius is None else peak_radius, ctx)
+    del cc, idx
+    ok = cidx >= 0
+    pos, cidx = pos[ok] - 1, cidx[ok]
+    mark()
+    near = neighbours(fine, np.asarray(coarse)[cidx], radius_deg)
+    mark()
+    out = refine(vol, template, mask, pos, [(np.asarray(fine)[i], i) for i in near], window=window, ctx=ctx)
+    mark()
+    if timings is not None:
+        for k, name in enumerate(("coarse", "candidates", "triplet_sets", "refine")):
+            timings[name] = clock[k + 1] - clock[k]
+        timings["total"] = clock[-1] - clock[0]
+        timings["candidates_n"] = int(len(pos))
+        timings["triplets_per_candidate"] = float(np.mean([len(x) for x in near])) if near else 0.0
+    return out
+
+
 def rerank(net, cc_coarse, idx_coarse, n_cand, n_pool, radius, ctx=None):
     """Candidates of the coarse map re-ranked by the network: the n_pool first
     coarse peaks (tom_peak rounds of radius `radius`), each scored by the
