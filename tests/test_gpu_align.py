@@ -136,6 +136,16 @@ def test_batched_engine_equals_per_job(gpu, oracle):
     soft = _job(oracle, 40, 0, True, 323)
     soft["wedge_ref"] = (0.7 * soft["wedge_ref"] + 0.1234567).astype(np.float32)
     jobs.append(soft)
+    # a particle wedge other than the reference wedge (the 8-argument form
+    # with both), and a graded mask (the reference times the mask values,
+    # the statistics over its non-zero voxels)
+    two = _job(oracle, 32, 2, True, 327)
+    two["wedge_part"] = oracle.av3_wedge((32, 32, 32), -40, 65).astype(np.float32)
+    jobs.append(two)
+    graded = _job(oracle, 48, 1, True, 328)
+    r = np.sqrt(((np.indices((48, 48, 48)) - 24.0) ** 2).sum(0))
+    graded["mask"] = np.asfortranarray(np.clip((22.0 - r) / 4.0, 0.0, 1.0).astype(np.float32))
+    jobs.append(graded)
     # the larger edges (radices 8 x 7, 4 x 5 x 5, 16 x 8), the last without
     # mask_ccf (the full last inverse on two lines per complex line)
     few = dict(phi=(0, 3, 3), psi=(0, 3, 3), theta=(6, 3, 9))
