@@ -357,6 +357,14 @@ int tomgpu_av3_align_ex_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n
                             const tomgpu_align_params* params, float* angles, float* shifts,
                             float* ccf_peak);
 
+/* tomgpu_av3_align_ex_dev on host volumes (what a MEX gateway of
+ * tom_av3_align calls): the job's volume pointers are host arrays of its box
+ * size (x fastest).  Each distinct array is uploaded once, so jobs that share
+ * a reference, mask or wedge by pointer share one device copy; a pointer
+ * shared by jobs of different box sizes is an error.  params may be NULL. */
+int tomgpu_av3_align(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs,
+                     const tomgpu_align_params* params, float* angles, float* shifts, float* ccf_peak);
+
 /* One aligned particle for the averaging step of av3_tomomatch. */
 typedef struct {
     const float* particle;  /* box n, device (after av3_tomomatch's tom_limit(p, -3, 4, 'z')) */

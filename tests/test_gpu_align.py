@@ -188,3 +188,23 @@ def test_batched_engine_matches_oracle_without_and_with_wedges(gpu, oracle):
         assert np.allclose(ga[k], ra), (k, ga[k], ra)
         assert np.abs(gs[k] - rs).max() <= 0.0015, (gs[k], rs)
         assert abs(gp[k] - rp) <= 1e-4 * abs(rp), (gp[k], rp)
+
+
+def test_host_entry_point_equals_device_entry_point(gpu, oracle):
+    """tomgpu_av3_align (host volumes, each distinct array uploaded once: here
+    one reference and one mask shared by three particles, one mask_ccf
+    omitted) gives what tomgpu_av3_align_ex_dev gives on device copies."""
+    n = 32
+    base = _job(oracle, n, 0, True, 400)
+    jobs = []
+    for k in range(3):
+        jb = _job(oracle, n, k, True, 401 + k)
+        jb["ref"], jb["mask"] = base["ref"], base["mask"]
+        jobs.append(jb)
+    jobs[2]["mask_ccf"] = None
+    jobs.append(_job(oracle, 24, 1, False, 405))
+    a0, s0, p0 = gpu.av3_align_batch(jobs)
+    a1, s1, p1 = gpu.av3_align_host(jobs)
+    assert np.array_equal(a0, a1)
+    assert np.array_equal(s0, s1)
+    assert np.array_equal(p0, p1)

@@ -10,6 +10,7 @@ from .tom import (  # noqa: F401
     Context,
     MatchPlan,
     av3_align_batch,
+    av3_align_host,
     av3_average_add,
     av3_average_final,
     av3_tomomatch_average,

@@ -157,6 +157,8 @@ _SIGS = {
                                             c_float_p]),
     "tomgpu_av3_align_ex_dev": (ctypes.c_int, [c_void_p, ctypes.POINTER(AlignJob), ctypes.c_int,
                                                 ctypes.POINTER(AlignParams), c_float_p, c_float_p, c_float_p]),
+    "tomgpu_av3_align": (ctypes.c_int, [c_void_p, ctypes.POINTER(AlignJob), ctypes.c_int, ctypes.POINTER(AlignParams),
+                                        c_float_p, c_float_p, c_float_p]),
     "tomgpu_match": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p, c_void_p, c_float_p,
                                     ctypes.c_int, ctypes.POINTER(MatchParams), c_void_p, c_void_p]),
 }

@@ -932,6 +932,65 @@ int tomgpu_av3_align_dev(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jo
     return tomgpu_av3_align_ex_dev(ctx, jobs, n_jobs, nullptr, angles, shifts, ccf_peak);
 }
 
+int tomgpu_av3_align(tomgpu_ctx* ctx, const tomgpu_align_job* jobs, int n_jobs, const tomgpu_align_params* params,
+                     float* angles, float* shifts, float* ccf_peak) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (n_jobs < 0 || (n_jobs > 0 && (!jobs || !angles || !shifts || !ccf_peak)))
+        return fail(ctx, TOMGPU_ERR_ARG, "null pointer or negative job count");
+    TG_TRY(use_device(ctx));
+    // the distinct host arrays, each with its voxel count
+    std::map<const float*, long long> vols;
+    for (int j = 0; j < n_jobs; ++j) {
+        const tomgpu_align_job& jb = jobs[j];
+        if (!dims_ok(jb.n)) return fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": bad box size");
+        const long long nn = numel(jb.n);
+        const float* p[6] = {jb.ref, jb.part, jb.mask, jb.mask_ccf, jb.wedge_ref, jb.wedge_part};
+        for (const float* q : p) {
+            if (!q) continue;
+            auto it = vols.find(q);
+            if (it == vols.end()) vols.emplace(q, nn);
+            else if (it->second != nn)
+                return fail(ctx, TOMGPU_ERR_ARG, "job " + std::to_string(j) + ": an array shared by jobs of "
+                                                 "different box sizes");
+        }
+    }
+    long long total = 0;
+    for (auto& kv : vols) total += kv.second;
+    float* dev = nullptr;
+    if (total > 0 && cudaMalloc(&dev, sizeof(float) * total) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, TOMGPU_ERR_OOM, "av3_align: device copies of the volumes");
+    }
+    std::map<const float*, const float*> where;
+    long long off = 0;
+    int rc = TOMGPU_OK;
+    for (auto& kv : vols) {
+        if (cudaError_t e = cudaMemcpyAsync(dev + off, kv.first, sizeof(float) * kv.second, cudaMemcpyHostToDevice,
+                                            ctx->stream)) {
+            rc = cuda_fail(ctx, e, "av3_align: upload");
+            break;
+        }
+        where[kv.first] = dev + off;
+        off += kv.second;
+    }
+    if (!rc) {
+        std::vector<tomgpu_align_job> dj(jobs, jobs + n_jobs);
+        auto map = [&](const float* q) { return q ? where[q] : nullptr; };
+        for (auto& jb : dj) {
+            jb.ref = map(jb.ref);
+            jb.part = map(jb.part);
+            jb.mask = map(jb.mask);
+            jb.mask_ccf = map(jb.mask_ccf);
+            jb.wedge_ref = map(jb.wedge_ref);
+            jb.wedge_part = map(jb.wedge_part);
+        }
+        rc = tomgpu_av3_align_ex_dev(ctx, dj.data(), n_jobs, params, angles, shifts, ccf_peak);
+    }
+    cudaStreamSynchronize(ctx->stream);
+    if (dev) cudaFree(dev);
+    return rc;
+}
+
 int tomgpu_ctx_trim(tomgpu_ctx* ctx) {
     if (!ctx) return TOMGPU_ERR_ARG;
     TG_TRY(use_device(ctx));

@@ -1031,6 +1031,47 @@ def av3_align_batch(jobs, ctx: Context | None = None, path: int = 0, batch_bytes
     return angles, shifts, peaks
 
 
+def av3_align_host(jobs, ctx: Context | None = None, path: int = 0, batch_bytes: int = 0):
+    """av3_align_batch through the host-volume entry point tomgpu_av3_align
+    (the one a MEX gateway calls): the library uploads every distinct array
+    once.  Each array is passed as float32 in x-fastest order; an array used by
+    several jobs (the same numpy object) is converted and uploaded once."""
+    ctx = ctx or default_context()
+    arr = (_lib.AlignJob * len(jobs))()
+    conv = {}
+
+    def host(a):
+        if a is None:
+            return None
+        hit = conv.get(id(a))
+        if hit is None or hit[0] is not a:
+            hit = (a, np.asfortranarray(np.asarray(a, np.float32)))
+            conv[id(a)] = hit
+        return hit[1]
+
+    for j, jb in enumerate(jobs):
+        n = np.shape(jb["ref"])
+        mask = jb.get("mask")
+        if mask is None:
+            mask = jb.setdefault("_default_mask", tom_spheremask_default(n))
+        arr[j].n = (ctypes.c_int * 3)(*n)
+        for k, a in (("ref", jb["ref"]), ("part", jb["part"]), ("mask", mask), ("mask_ccf", jb.get("mask_ccf")),
+                     ("wedge_ref", jb.get("wedge_ref")), ("wedge_part", jb.get("wedge_part"))):
+            h = host(a)
+            setattr(arr[j], k, h.ctypes.data if h is not None else None)
+        arr[j].phi = (ctypes.c_float * 3)(*jb["phi"])
+        arr[j].psi = (ctypes.c_float * 3)(*jb["psi"])
+        arr[j].theta = (ctypes.c_float * 3)(*jb["theta"])
+    angles = np.zeros((len(jobs), 3), np.float32)
+    shifts = np.zeros((len(jobs), 3), np.float32)
+    peaks = np.zeros(len(jobs), np.float32)
+    prm = _lib.AlignParams(int(path), int(batch_bytes))
+    ctx.check(lib().tomgpu_av3_align(ctx.handle, arr, len(jobs), ctypes.byref(prm),
+                                     angles.ctypes.data_as(_lib.c_float_p), shifts.ctypes.data_as(_lib.c_float_p),
+                                     peaks.ctypes.data_as(_lib.c_float_p)))
+    return angles, shifts, peaks
+
+
 def tom_av3_align(ref, part, phi, psi, theta, mask=None, filter=None, mask_ccf=None, wedge_ref=None,
                   wedge_part=None, ctx: Context | None = None):
     """[angles shifts ccf_peak] = tom_av3_align(ref,part,phi,psi,theta,mask,filter,mask_ccf,wedge_ref,wedge_part)
