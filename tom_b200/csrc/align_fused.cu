@@ -54,6 +54,11 @@ namespace tg {
 
 namespace {
 
+template <int NT_, int MINB_, int NTX_, int MINBX_, typename R_> struct CfgOf {
+    static constexpr int NT = NT_, MINB = MINB_, NTX = NTX_, MINBX = MINBX_;
+    typedef R_ R;
+};
+
 // Per box edge: threads per block, blocks per SM the registers are sized for
 // (every butterfly of a stage lives in registers, N * N / NT elements per
 // thread), and the radices of the line DFTs.
@@ -61,19 +66,19 @@ template <int N> struct Cfg;
 // NT / MINB: the (y, z)-plane kernels and the full x3 (N lines per tile);
 // NTX / MINBX: the x-line kernels, which pack two real lines into one complex
 // line (N / 2 lines per tile).
-template <> struct Cfg<24> { static constexpr int NT = 192, MINB = 4, NTX = 96, MINBX = 8; typedef tgfft::seq<8, 3> R; };
-template <> struct Cfg<32> { static constexpr int NT = 256, MINB = 4, NTX = 128, MINBX = 8; typedef tgfft::seq<8, 4> R; };
-template <> struct Cfg<40> { static constexpr int NT = 320, MINB = 3, NTX = 160, MINBX = 6; typedef tgfft::seq<8, 5> R; };
-template <> struct Cfg<48> { static constexpr int NT = 160, MINB = 6, NTX = 192, MINBX = 6; typedef tgfft::seq<16, 3> R; };
-template <> struct Cfg<64> { static constexpr int NT = 256, MINB = 4, NTX = 256, MINBX = 4; typedef tgfft::seq<8, 8> R; };
-template <> struct Cfg<72> { static constexpr int NT = 384, MINB = 2, NTX = 352, MINBX = 3; typedef tgfft::seq<8, 3, 3> R; };
-template <> struct Cfg<80> { static constexpr int NT = 256, MINB = 3, NTX = 224, MINBX = 5; typedef tgfft::seq<16, 5> R; };
-template <> struct Cfg<96> { static constexpr int NT = 384, MINB = 2, NTX = 288, MINBX = 4; typedef tgfft::seq<16, 6> R; };
-template <> struct Cfg<56> { static constexpr int NT = 448, MINB = 2, NTX = 224, MINBX = 5; typedef tgfft::seq<8, 7> R; };
-template <> struct Cfg<100> { static constexpr int NT = 512, MINB = 1, NTX = 320, MINBX = 3; typedef tgfft::seq<4, 5, 5> R; };
-template <> struct Cfg<112> { static constexpr int NT = 800, MINB = 1, NTX = 416, MINBX = 2; typedef tgfft::seq<16, 7> R; };
-template <> struct Cfg<120> { static constexpr int NT = 960, MINB = 1, NTX = 480, MINBX = 2; typedef tgfft::seq<8, 3, 5> R; };
-template <> struct Cfg<128> { static constexpr int NT = 1024, MINB = 1, NTX = 512, MINBX = 2; typedef tgfft::seq<16, 8> R; };
+template <> struct Cfg<24> : CfgOf<192, 4, 96, 8, tgfft::seq<8, 3>> {};
+template <> struct Cfg<32> : CfgOf<256, 4, 128, 8, tgfft::seq<8, 4>> {};
+template <> struct Cfg<40> : CfgOf<320, 3, 160, 6, tgfft::seq<8, 5>> {};
+template <> struct Cfg<48> : CfgOf<160, 6, 192, 6, tgfft::seq<16, 3>> {};
+template <> struct Cfg<64> : CfgOf<256, 4, 256, 4, tgfft::seq<8, 8>> {};
+template <> struct Cfg<72> : CfgOf<384, 2, 352, 3, tgfft::seq<8, 3, 3>> {};
+template <> struct Cfg<80> : CfgOf<256, 3, 224, 5, tgfft::seq<16, 5>> {};
+template <> struct Cfg<96> : CfgOf<384, 2, 288, 4, tgfft::seq<16, 6>> {};
+template <> struct Cfg<56> : CfgOf<448, 2, 224, 5, tgfft::seq<8, 7>> {};
+template <> struct Cfg<100> : CfgOf<512, 1, 320, 3, tgfft::seq<4, 5, 5>> {};
+template <> struct Cfg<112> : CfgOf<800, 1, 416, 2, tgfft::seq<16, 7>> {};
+template <> struct Cfg<120> : CfgOf<960, 1, 480, 2, tgfft::seq<8, 3, 5>> {};
+template <> struct Cfg<128> : CfgOf<1024, 1, 512, 2, tgfft::seq<16, 8>> {};
 
 constexpr int kEdges[] = {24, 32, 40, 48, 56, 64, 72, 80, 96, 100, 112, 120, 128};
 
@@ -386,7 +391,8 @@ enum PMode {
 // grid (N/2 + 1 planes kx, entries); tile s[z * P + y]: y-lines at EST 1,
 // LST P; z-lines at EST P, LST 1.
 template <int N, int MODE>
-__global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ap(float2* __restrict__ A, float2* __restrict__ B, long long hstride,
+__global__ void __launch_bounds__(Cfg<N>::NT, Cfg<N>::MINB) k_ap(float2* __restrict__ A, float2* __restrict__ B,
+                                                                  long long hstride,
                                                    const Entry* __restrict__ ent, const __grid_constant__ SlotTab slots,
                                                    const double* __restrict__ stats, const float2* __restrict__ tw,
                                                    const float2* __restrict__ pin, float2* __restrict__ pout,
@@ -672,7 +678,8 @@ __global__ void k_prune_mark(const float* const* __restrict__ mccf, int N, int* 
     const long long nn = (long long)N * N * N;
     const int H2 = N / 2;
     unsigned long long first = ~0ull;
-    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn; v += (long long)gridDim.x * blockDim.x) {
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nn;
+         v += (long long)gridDim.x * blockDim.x) {
         if (m[v] != 0.f) {
             const int x = (int)(v % N), y = (int)((v / N) % N), z = (int)(v / ((long long)N * N));
             f[(z - H2 + N) % N] = 1;
@@ -757,7 +764,8 @@ __global__ void k_awph(const float* __restrict__ w, float* __restrict__ out, int
 }
 
 __global__ void k_afill(float* __restrict__ a, float* __restrict__ b, long long n, float v) {
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
         a[t] = v;
         b[t] = v;
     }
