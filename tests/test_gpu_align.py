@@ -208,3 +208,16 @@ def test_host_entry_point_equals_device_entry_point(gpu, oracle):
     assert np.array_equal(a0, a1)
     assert np.array_equal(s0, s1)
     assert np.array_equal(p0, p1)
+
+
+def test_batched_engine_remaining_edges(gpu, oracle):
+    """The compiled edges not covered above (radices 8 x 3 x 3, 16 x 5,
+    16 x 6, 16 x 7, 8 x 3 x 5) give the job-by-job results."""
+    few = dict(phi=(0, 3, 3), psi=(0, 3, 3), theta=(6, 3, 9))
+    jobs = [_job(oracle, n, k, True, 600 + k, **few) for k, n in enumerate((72, 80, 96, 112, 120))]
+    jobs.append(_job(oracle, 96, 1, False, 610, mccf="none", **few))
+    a0, s0, p0 = gpu.av3_align_batch(jobs, path=0)
+    a1, s1, p1 = gpu.av3_align_batch(jobs, path=1)
+    assert np.array_equal(a0, a1), (a0, a1)
+    assert np.abs(s0 - s1).max() <= 2e-3, (s0, s1)
+    assert np.allclose(p0, p1, rtol=2e-4, atol=0), (p0, p1)
