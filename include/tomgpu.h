@@ -456,6 +456,67 @@ int tomgpu_cnn_gather_dev(tomgpu_ctx* ctx, const float* f, int C, int64_t nv, co
 int tomgpu_cnn_scatter_add_dev(tomgpu_ctx* ctx, const float* g, int C, int64_t nv, const int64_t* idx, int P,
                                float* gf);
 
+/* U-Net candidate proposer (tom_b200/unet.py; no counterpart in the
+ * reference): BF16 3x3x3 convolutions on the tensor cores with FP32
+ * accumulation and the layers around them.  Activations are channels-last
+ * BF16 (uint16_t bit patterns), act[z][y][x][c] with channel stride cs; a
+ * call reads or writes the channel slice [off, off + C) (cs and off multiples
+ * of 8, buffers 16-byte aligned).  dims = {X, Y, Z}.  Master weights are FP32
+ * [Cout][Cin][27] (taps x fastest, t = 9 dz + 3 dy + dx, offset t - 13 in
+ * the order (dx, dy, dz) - 1).  Gradient outputs accumulate (zero them
+ * first).  Errors: TOMGPU_ERR_ARG for bad pointers / slices,
+ * TOMGPU_ERR_UNSUPPORTED for channel counts outside the built kernels,
+ * TOMGPU_ERR_TIMEOUT (from the next synchronising call) if a bounded device
+ * wait ran out. */
+/* The packed BF16 weights of one convolution (27 Cout Cin values): flip = 0
+ * the forward form, flip = 1 the input-gradient form (taps mirrored, channel
+ * roles swapped).  Cout, Cin multiples of 16, at most 96. */
+int tomgpu_unet_pack_weights_dev(tomgpu_ctx* ctx, const float* w, int cout, int cin, int flip, uint16_t* packed);
+/* out = act(conv3(in) + bias) on the tensor cores.  relu != 0 applies a
+ * ReLU; mask != null multiplies by (mask > 0) (the derivative of a ReLU whose
+ * output is mask; the input-gradient form).  Cin a multiple of 16 (<= 96),
+ * Cout one of 16, 32, 48, 64, 96. */
+int tomgpu_unet_conv3_dev(tomgpu_ctx* ctx, const uint16_t* in, int in_cs, int in_off, int cin, const int dims[3],
+                          const uint16_t* packed, int cout, const float* bias, int relu, const uint16_t* mask,
+                          int mask_cs, int mask_off, uint16_t* out, int out_cs, int out_off);
+/* gw[co][ci][t] += sum_v gout[v][co] in[v + off(t)][ci] on the tensor cores
+ * (Cin <= 96, Cout <= 64, multiples of 16). */
+int tomgpu_unet_conv3_wgrad_dev(tomgpu_ctx* ctx, const uint16_t* in, int in_cs, int in_off, int cin,
+                                const int dims[3], const uint16_t* gout, int g_cs, int g_off, int cout, float* gw);
+/* First layer: one FP32 input channel -> 16 BF16 channels (bias, ReLU), and
+ * its weight / bias gradients. */
+int tomgpu_unet_conv_first_dev(tomgpu_ctx* ctx, const float* vol, const int dims[3], const float* w, const float* b,
+                               uint16_t* out);
+int tomgpu_unet_conv_first_wgrad_dev(tomgpu_ctx* ctx, const float* vol, const int dims[3], const uint16_t* gout,
+                                     float* gw, float* gb);
+/* Candidate head over n voxels of 16 channels, w = 16 weights and the bias
+ * (17 floats): logit = w[16] + w[0..15] . f; backward: gf = g w (f > 0)
+ * (written), gw[0..15] += sum g f, gw[16] += sum g. */
+int tomgpu_unet_head_dev(tomgpu_ctx* ctx, const uint16_t* f, int64_t n, const float* w, float* logit);
+int tomgpu_unet_head_bwd_dev(tomgpu_ctx* ctx, const uint16_t* f, int64_t n, const float* w, const float* g,
+                             uint16_t* gf, float* gw);
+/* 2x2x2 average pool of a slice into a dense [C] volume (dims: the fine
+ * volume, even), and its backward: gin[v][off + c] (+)= gout[v / 2][c] / 8,
+ * times (mask > 0) when mask is given (mask shares gin's cs / off). */
+int tomgpu_unet_pool_dev(tomgpu_ctx* ctx, const uint16_t* in, int cs, int off, int C, const int dims[3],
+                         uint16_t* out);
+int tomgpu_unet_pool_bwd_dev(tomgpu_ctx* ctx, const uint16_t* gout, int C, const int dims[3], const uint16_t* mask,
+                             int cs, int off, uint16_t* gin, int accumulate);
+/* Nearest 2x upsample of a dense [C] volume into a slice of the fine volume
+ * (dims: fine), and its backward (sum of the 8 fine gradients). */
+int tomgpu_unet_upsample_dev(tomgpu_ctx* ctx, const uint16_t* in, int C, const int dims[3], uint16_t* out, int cs,
+                             int off);
+int tomgpu_unet_upsample_bwd_dev(tomgpu_ctx* ctx, const uint16_t* gout, int cs, int off, int C, const int dims[3],
+                                 uint16_t* gin);
+/* out[c] += sum over n voxels of g[v][off + c] (bias gradients; C <= 96). */
+int tomgpu_unet_channel_sum_dev(tomgpu_ctx* ctx, const uint16_t* g, int cs, int off, int C, int64_t n, float* out);
+/* Features at P voxels (flat indices) as FP32 F[c][p], and the scatter-add
+ * of a gradient G[c][p] back into distinct voxels of a BF16 gradient, where
+ * the ReLU features f are positive. */
+int tomgpu_unet_gather_dev(tomgpu_ctx* ctx, const uint16_t* f, int C, const int64_t* idx, int P, float* out);
+int tomgpu_unet_scatter_add_dev(tomgpu_ctx* ctx, const float* g, int C, const int64_t* idx, int P, const uint16_t* f,
+                                uint16_t* gf);
+
 /* ---------------------------------------------------------- peak analysis */
 
 /* tom_os3_analyzePeak(img, peakMap, template, 'PSR')

@@ -144,6 +144,32 @@ _SIGS = {
                                              c_void_p]),
     "tomgpu_cnn_scatter_add_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int64, c_void_p,
                                                   ctypes.c_int, c_void_p]),
+    "tomgpu_unet_pack_weights_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    c_void_p]),
+    "tomgpu_unet_conv3_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p,
+                                             c_void_p, ctypes.c_int, c_void_p, ctypes.c_int, c_void_p, ctypes.c_int,
+                                             ctypes.c_int, c_void_p, ctypes.c_int, ctypes.c_int]),
+    "tomgpu_unet_conv3_wgrad_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                   c_int_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                   c_void_p]),
+    "tomgpu_unet_conv_first_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_void_p, c_void_p]),
+    "tomgpu_unet_conv_first_wgrad_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_void_p, c_void_p]),
+    "tomgpu_unet_head_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p]),
+    "tomgpu_unet_head_bwd_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p, c_void_p,
+                                                c_void_p]),
+    "tomgpu_unet_pool_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p,
+                                            c_void_p]),
+    "tomgpu_unet_pool_bwd_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_void_p, ctypes.c_int,
+                                                ctypes.c_int, c_void_p, ctypes.c_int]),
+    "tomgpu_unet_upsample_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_int_p, c_void_p, ctypes.c_int,
+                                                ctypes.c_int]),
+    "tomgpu_unet_upsample_bwd_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                    c_int_p, c_void_p]),
+    "tomgpu_unet_channel_sum_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                   ctypes.c_int64, c_void_p]),
+    "tomgpu_unet_gather_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p, ctypes.c_int, c_void_p]),
+    "tomgpu_unet_scatter_add_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p, ctypes.c_int,
+                                                   c_void_p, c_void_p]),
     "tomgpu_analyze_psr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_int_p, c_void_p]),
     "tomgpu_template_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p]),
     "tomgpu_analyze_autocorr_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_int_p, c_void_p,

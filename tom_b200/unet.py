@@ -1,0 +1,253 @@
+"""U-Net candidate proposer (no counterpart in TOM).
+
+A 3-level 3-D U-Net (16 / 32 / 64 channels, 3x3x3 convolutions, 2x2x2
+average pooling, nearest 2x upsampling with channel concatenation) reads a
+normalised tomogram and predicts, per voxel, the probability of a particle
+centre (a 1x1 head) and, at candidate voxels, one of the coarse orientation
+bins (a dense head over the 16 features).  Labels come from the search itself
+(the peaks of an exhaustive search and the coarse bin of their angle); the
+pruned search then refines only around the proposals
+(search/tom_os3_findTemplate.m:255-307 is the loop it replaces there).
+
+Every layer runs on the library's own kernels through the C ABI
+(tomgpu_unet_*): the 3x3x3 convolutions, their input gradients and weight
+gradients as tcgen05 BF16 contractions with FP32 accumulation in tensor
+memory; the first layer (one input channel), the heads, pooling and
+upsampling as CUDA-core kernels; the losses, the dense orientation head and
+Adam from tomgpu_cnn_*.  Activations and activation gradients are BF16
+(channels-last), master weights, weight gradients and Adam state FP32; the
+BF16 packed weights are re-derived after every update.  torch holds the
+buffers only.
+
+Layers (name: Cin -> Cout at level): first 1 -> 16, e1b 16 -> 16 (L1);
+pool; e2a 16 -> 32, e2b 32 -> 32 (L2); pool; e3a 32 -> 64, e3b 64 -> 64 (L3);
+up, concat with e2: d2a 96 -> 32, d2b 32 -> 32 (L2); up, concat with e1:
+d1a 48 -> 16, d1b 16 -> 16 (L1); heads.  Every convolution is followed by a
+ReLU.  The volume edges must be multiples of 4.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from .tom import Context, _cdims, _tptr, default_context
+
+CONVS = (("e1b", 16, 16), ("e2a", 16, 32), ("e2b", 32, 32), ("e3a", 32, 64), ("e3b", 64, 64),
+         ("d2a", 96, 32), ("d2b", 32, 32), ("d1a", 48, 16), ("d1b", 16, 16))
+FEAT = 16
+
+
+def _call(ctx, name, *args):
+    ctx.check(getattr(_lib.lib(), name)(ctx.handle, *args))
+
+
+class UNetProposer:
+    """Parameters, Adam state, packed weights, activation buffers and the
+    forward / backward passes of the U-Net."""
+
+    def __init__(self, n_bins: int, ctx: Context | None = None, seed: int = 0, params: dict | None = None):
+        import torch
+        self.ctx = ctx or default_context()
+        self.dev = f"cuda:{self.ctx.device}"
+        self.n_bins = int(n_bins)
+        if params is None:
+            params = init_params(self.n_bins, seed)
+        self.p = {k: torch.from_numpy(np.ascontiguousarray(v, np.float32)).to(self.dev) for k, v in params.items()}
+        self.g = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        self.m = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        self.v = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        self.pf = {n: torch.empty(27 * ci * co, dtype=torch.int16, device=self.dev) for n, ci, co in CONVS}
+        self.pb = {n: torch.empty(27 * ci * co, dtype=torch.int16, device=self.dev) for n, ci, co in CONVS}
+        self.step_count = 0
+        self._shape = None
+        self._train_bufs = False
+        self.repack()
+
+    # ------------------------------------------------------------ weights
+    def repack(self):
+        """The BF16 packed forms of every 3x3x3 convolution's weights."""
+        for n, ci, co in CONVS:
+            _call(self.ctx, "tomgpu_unet_pack_weights_dev", _tptr(self.p["w_" + n]), co, ci, 0, _tptr(self.pf[n]))
+            _call(self.ctx, "tomgpu_unet_pack_weights_dev", _tptr(self.p["w_" + n]), co, ci, 1, _tptr(self.pb[n]))
+
+    def params_numpy(self):
+        return {k: v.cpu().numpy() for k, v in self.p.items()}
+
+    # ------------------------------------------------------------ buffers
+    def _alloc(self, shape_zyx, train):
+        import torch
+        if self._shape == tuple(shape_zyx) and (self._train_bufs or not train):
+            return
+        Z, Y, X = shape_zyx
+        if Z % 4 or Y % 4 or X % 4:
+            raise ValueError("volume edges must be multiples of 4")
+        L1, L2, L3 = (Z, Y, X), (Z // 2, Y // 2, X // 2), (Z // 4, Y // 4, X // 4)
+
+        def buf(L, c):
+            return torch.zeros(L + (c,), dtype=torch.int16, device=self.dev)
+
+        self.a = {"e1a": buf(L1, 16), "D1": buf(L1, 48), "p1": buf(L2, 16), "e2a": buf(L2, 32), "D2": buf(L2, 96),
+                  "p2": buf(L3, 32), "e3a": buf(L3, 64), "e3": buf(L3, 64), "d2a": buf(L2, 32), "d2": buf(L2, 32),
+                  "d1a": buf(L1, 16), "f": buf(L1, 16)}
+        self.logit = torch.empty(L1, dtype=torch.float32, device=self.dev)
+        if train:
+            self.ga = {"f": buf(L1, 16), "d1a": buf(L1, 16), "D1": buf(L1, 48), "d2": buf(L2, 32),
+                       "d2a": buf(L2, 32), "D2": buf(L2, 96), "e3": buf(L3, 64), "e3a": buf(L3, 64),
+                       "p2": buf(L3, 32), "e2a": buf(L2, 32), "p1": buf(L2, 16), "e1a": buf(L1, 16)}
+        self._shape = tuple(shape_zyx)
+        self._train_bufs = train
+        self.dims = [_cdims((X, Y, Z)), _cdims((X // 2, Y // 2, Z // 2)), _cdims((X // 4, Y // 4, Z // 4))]
+
+    def _conv(self, name, src, cs, off, cin, lvl, cout, dst, dcs, doff):
+        _call(self.ctx, "tomgpu_unet_conv3_dev", _tptr(src), cs, off, cin, self.dims[lvl], _tptr(self.pf[name]), cout,
+              _tptr(self.p["b_" + name]), 1, None, 0, 0, _tptr(dst), dcs, doff)
+
+    # ------------------------------------------------------------ forward
+    def forward(self, vol, train=False):
+        """vol: torch float32 [Z][Y][X] on the device (normalised).  Returns the
+        candidate logits [Z][Y][X] (a buffer reused by the next call)."""
+        ctx = self.ctx
+        self._alloc(tuple(vol.shape), train)
+        a = self.a
+        self.vol = vol
+        _call(ctx, "tomgpu_unet_conv_first_dev", _tptr(vol), self.dims[0], _tptr(self.p["w0"]), _tptr(self.p["b0"]),
+              _tptr(a["e1a"]))
+        self._conv("e1b", a["e1a"], 16, 0, 16, 0, 16, a["D1"], 48, 32)
+        _call(ctx, "tomgpu_unet_pool_dev", _tptr(a["D1"]), 48, 32, 16, self.dims[0], _tptr(a["p1"]))
+        self._conv("e2a", a["p1"], 16, 0, 16, 1, 32, a["e2a"], 32, 0)
+        self._conv("e2b", a["e2a"], 32, 0, 32, 1, 32, a["D2"], 96, 64)
+        _call(ctx, "tomgpu_unet_pool_dev", _tptr(a["D2"]), 96, 64, 32, self.dims[1], _tptr(a["p2"]))
+        self._conv("e3a", a["p2"], 32, 0, 32, 2, 64, a["e3a"], 64, 0)
+        self._conv("e3b", a["e3a"], 64, 0, 64, 2, 64, a["e3"], 64, 0)
+        _call(ctx, "tomgpu_unet_upsample_dev", _tptr(a["e3"]), 64, self.dims[1], _tptr(a["D2"]), 96, 0)
+        self._conv("d2a", a["D2"], 96, 0, 96, 1, 32, a["d2a"], 32, 0)
+        self._conv("d2b", a["d2a"], 32, 0, 32, 1, 32, a["d2"], 32, 0)
+        _call(ctx, "tomgpu_unet_upsample_dev", _tptr(a["d2"]), 32, self.dims[0], _tptr(a["D1"]), 48, 0)
+        self._conv("d1a", a["D1"], 48, 0, 48, 0, 16, a["d1a"], 16, 0)
+        self._conv("d1b", a["d1a"], 16, 0, 16, 0, 16, a["f"], 16, 0)
+        _call(ctx, "tomgpu_unet_head_dev", _tptr(a["f"]), self.logit.numel(), _tptr(self.p["head"]),
+              _tptr(self.logit))
+        return self.logit
+
+    def orient_logits(self, idx):
+        """Orientation logits [n_bins][P] at flat voxel indices idx (int64 tensor)
+        of the last forward pass; also returns the gathered features [16][P]."""
+        import torch
+        P = int(idx.numel())
+        fg = torch.empty((FEAT, P), device=self.dev)
+        _call(self.ctx, "tomgpu_unet_gather_dev", _tptr(self.a["f"]), FEAT, _tptr(idx), P, _tptr(fg))
+        out = torch.empty((self.n_bins, P), device=self.dev)
+        _call(self.ctx, "tomgpu_cnn_dense_fwd_dev", _tptr(self.p["Wo"]), _tptr(self.p["bo"]), _tptr(fg), self.n_bins,
+              FEAT, P, 0, _tptr(out))
+        return fg, out
+
+    # ------------------------------------------------------------ backward
+    def _bwd_conv(self, name, x, xcs, xoff, cin, lvl, g, gcs, goff, cout, gin, mask, mcs, moff, n_vox):
+        """Weight, bias and (when gin is given) input gradients of one convolution."""
+        ctx = self.ctx
+        _call(ctx, "tomgpu_unet_channel_sum_dev", _tptr(g), gcs, goff, cout, n_vox, _tptr(self.g["b_" + name]))
+        _call(ctx, "tomgpu_unet_conv3_wgrad_dev", _tptr(x), xcs, xoff, cin, self.dims[lvl], _tptr(g), gcs, goff, cout,
+              _tptr(self.g["w_" + name]))
+        if gin is not None:
+            _call(ctx, "tomgpu_unet_conv3_dev", _tptr(g), gcs, goff, cout, self.dims[lvl], _tptr(self.pb[name]), cin,
+                  None, 0, None if mask is None else _tptr(mask), mcs, moff, _tptr(gin), cin if mask is None else mcs,
+                  0 if mask is None else moff)
+
+    def backward(self, g_logit, orient=None):
+        """Accumulate the parameter gradients (zero them first) for the
+        gradient g_logit [Z][Y][X] of the candidate logits and, optionally,
+        orient = (idx, fg, g_orient_logits [n_bins][P]) of the orientation head."""
+        import torch
+        ctx, a, ga = self.ctx, self.a, self.ga
+        Z, Y, X = self._shape
+        n1 = X * Y * Z
+        n2, n3 = n1 // 8, n1 // 64
+        _call(ctx, "tomgpu_unet_head_bwd_dev", _tptr(a["f"]), n1, _tptr(self.p["head"]), _tptr(g_logit),
+              _tptr(ga["f"]), _tptr(self.g["head"]))
+        if orient is not None:
+            idx, fg, g_ol = orient
+            P = int(idx.numel())
+            g_fg = torch.empty_like(fg)
+            _call(ctx, "tomgpu_cnn_dense_bwd_dev", _tptr(self.p["Wo"]), _tptr(fg), _tptr(g_ol), self.n_bins, FEAT, P,
+                  _tptr(g_fg), _tptr(self.g["Wo"]), _tptr(self.g["bo"]))
+            _call(ctx, "tomgpu_unet_scatter_add_dev", _tptr(g_fg), FEAT, _tptr(idx), P, _tptr(a["f"]), _tptr(ga["f"]))
+        self._bwd_conv("d1b", a["d1a"], 16, 0, 16, 0, ga["f"], 16, 0, 16, ga["d1a"], a["d1a"], 16, 0, n1)
+        self._bwd_conv("d1a", a["D1"], 48, 0, 48, 0, ga["d1a"], 16, 0, 16, ga["D1"], a["D1"], 48, 0, n1)
+        _call(ctx, "tomgpu_unet_upsample_bwd_dev", _tptr(ga["D1"]), 48, 0, 32, self.dims[0], _tptr(ga["d2"]))
+        self._bwd_conv("d2b", a["d2a"], 32, 0, 32, 1, ga["d2"], 32, 0, 32, ga["d2a"], a["d2a"], 32, 0, n2)
+        self._bwd_conv("d2a", a["D2"], 96, 0, 96, 1, ga["d2a"], 32, 0, 32, ga["D2"], a["D2"], 96, 0, n2)
+        _call(ctx, "tomgpu_unet_upsample_bwd_dev", _tptr(ga["D2"]), 96, 0, 64, self.dims[1], _tptr(ga["e3"]))
+        self._bwd_conv("e3b", a["e3a"], 64, 0, 64, 2, ga["e3"], 64, 0, 64, ga["e3a"], a["e3a"], 64, 0, n3)
+        self._bwd_conv("e3a", a["p2"], 32, 0, 32, 2, ga["e3a"], 64, 0, 64, ga["p2"], None, 0, 0, n3)
+        _call(ctx, "tomgpu_unet_pool_bwd_dev", _tptr(ga["p2"]), 32, self.dims[1], _tptr(a["D2"]), 96, 64,
+              _tptr(ga["D2"]), 1)
+        self._bwd_conv("e2b", a["e2a"], 32, 0, 32, 1, ga["D2"], 96, 64, 32, ga["e2a"], a["e2a"], 32, 0, n2)
+        self._bwd_conv("e2a", a["p1"], 16, 0, 16, 1, ga["e2a"], 32, 0, 32, ga["p1"], None, 0, 0, n2)
+        _call(ctx, "tomgpu_unet_pool_bwd_dev", _tptr(ga["p1"]), 16, self.dims[0], _tptr(a["D1"]), 48, 32,
+              _tptr(ga["D1"]), 1)
+        self._bwd_conv("e1b", a["e1a"], 16, 0, 16, 0, ga["D1"], 48, 32, 16, ga["e1a"], a["e1a"], 16, 0, n1)
+        _call(ctx, "tomgpu_unet_conv_first_wgrad_dev", _tptr(self.vol), self.dims[0], _tptr(ga["e1a"]),
+              _tptr(self.g["w0"]), _tptr(self.g["b0"]))
+
+    # ------------------------------------------------------------ training
+    def zero_grad(self):
+        for t in self.g.values():
+            t.zero_()
+
+    def adam(self, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        self.step_count += 1
+        for k in self.p:
+            _call(self.ctx, "tomgpu_cnn_adam_dev", _tptr(self.p[k]), _tptr(self.g[k]), _tptr(self.m[k]),
+                  _tptr(self.v[k]), self.p[k].numel(), float(lr), float(beta1), float(beta2), float(eps),
+                  self.step_count)
+        self.repack()
+
+    def train_step(self, vol, target, pos_idx, pos_bins, pos_weight=50.0, lr=1e-3, w_orient=0.2):
+        """One Adam step on one sample.  vol, target: torch [Z][Y][X] on the
+        device; pos_idx: flat indices of the labelled centres (int64), pos_bins:
+        their coarse bins (int32).  Returns (centre loss, orientation loss)."""
+        import torch
+        ctx = self.ctx
+        self.zero_grad()
+        logit = self.forward(vol, train=True)
+        n = logit.numel()
+        loss = torch.zeros(2, dtype=torch.float64, device=self.dev)
+        g_logit = torch.empty_like(logit)
+        _call(ctx, "tomgpu_cnn_bce_dev", _tptr(logit), _tptr(target), n, float(pos_weight), _tptr(g_logit),
+              _tptr(loss[0:1]))
+        orient = None
+        P = int(pos_idx.numel())
+        if P > 0 and w_orient > 0:
+            fg, ol = self.orient_logits(pos_idx)
+            g_ol = torch.empty_like(ol)
+            _call(ctx, "tomgpu_cnn_softmax_ce_dev", _tptr(ol), _tptr(pos_bins), self.n_bins, P, _tptr(g_ol),
+                  _tptr(loss[1:2]))
+            g_ol.mul_(w_orient)
+            orient = (pos_idx, fg, g_ol)
+        self.backward(g_logit, orient)
+        self.adam(lr)
+        out = loss.cpu().numpy()
+        return float(out[0]), float(out[1])
+
+    def flops_per_voxel(self):
+        """Multiply-adds x 2 of one forward pass per full-resolution voxel."""
+        lv = {"e1b": 1, "e2a": 8, "e2b": 8, "e3a": 64, "e3b": 64, "d2a": 8, "d2b": 8, "d1a": 1, "d1b": 1}
+        macs = 27 * 16 + 16 + sum(27 * ci * co / lv[n] for n, ci, co in CONVS)
+        return 2 * macs
+
+
+def init_params(n_bins, seed=0):
+    """He-initialised FP32 parameters: w0 [16, 1, 27], b0 [16], per convolution
+    w_<name> [Cout, Cin, 27] and b_<name> [Cout], the candidate head
+    head [17] (16 weights, bias -4: rare positives start near p = 0.02) and
+    the orientation head Wo [n_bins, 16], bo [n_bins]."""
+    r = np.random.default_rng(seed)
+    p = {"w0": (r.standard_normal((16, 1, 27)) * np.sqrt(2.0 / 27)).astype(np.float32),
+         "b0": np.zeros(16, np.float32)}
+    for name, ci, co in CONVS:
+        p["w_" + name] = (r.standard_normal((co, ci, 27)) * np.sqrt(2.0 / (27 * ci))).astype(np.float32)
+        p["b_" + name] = np.zeros(co, np.float32)
+    p["head"] = np.concatenate([r.standard_normal(16) * 0.25, [-4.0]]).astype(np.float32)
+    p["Wo"] = (r.standard_normal((n_bins, 16)) * 0.25).astype(np.float32)
+    p["bo"] = np.zeros(n_bins, np.float32)
+    return p
