@@ -118,15 +118,18 @@ def test_first_layer_head_pool_upsample_and_sums(gpu):
     vol = rng.standard_normal((Z, Y, X)).astype(np.float32)
     w0 = (rng.standard_normal((16, 1, 27)) * 0.3).astype(np.float32)
     b0 = rng.standard_normal(16).astype(np.float32)
+    # (every buffer a kernel reads is held in a variable until the stream has
+    # synchronised: a temporary's memory could be reused by the next upload)
     e = torch.empty((Z, Y, X, 16), dtype=torch.int16, device=dev)
-    tv = _f32(vol, dev)
-    _call(ctx, "tomgpu_unet_conv_first_dev", _p(tv), dims, _p(_f32(w0, dev)), _p(_f32(b0, dev)), _p(e))
+    tv, tw0, tb0 = _f32(vol, dev), _f32(w0, dev), _f32(b0, dev)
+    _call(ctx, "tomgpu_unet_conv_first_dev", _p(tv), dims, _p(tw0), _p(tb0), _p(e))
     ctx.synchronize()
     _bf_close(_from_bf(e), np.maximum(uo.conv3(vol[..., None], w0, b0), 0))
     g = uo.bf16(rng.standard_normal((Z, Y, X, 16)))
     gw = torch.zeros(16 * 27, device=dev)
     gb = torch.zeros(16, device=dev)
-    _call(ctx, "tomgpu_unet_conv_first_wgrad_dev", _p(tv), dims, _p(_bf(g, dev)), _p(gw), _p(gb))
+    tg = _bf(g, dev)
+    _call(ctx, "tomgpu_unet_conv_first_wgrad_dev", _p(tv), dims, _p(tg), _p(gw), _p(gb))
     _, gw_ref, gb_ref = uo.conv3_grads(vol[..., None], w0, g)
     ctx.synchronize()
     _close(gw.cpu().numpy().reshape(16, 1, 27), gw_ref)
@@ -136,13 +139,15 @@ def test_first_layer_head_pool_upsample_and_sums(gpu):
     hw = rng.standard_normal(17).astype(np.float32)
     tf = _bf(f, dev)
     logit = torch.empty((Z, Y, X), device=dev)
-    _call(ctx, "tomgpu_unet_head_dev", _p(tf), n, _p(_f32(hw, dev)), _p(logit))
+    thw = _f32(hw, dev)
+    _call(ctx, "tomgpu_unet_head_dev", _p(tf), n, _p(thw), _p(logit))
     ctx.synchronize()
     _close(logit.cpu().numpy(), f @ hw[:16].astype(np.float64) + hw[16], 1e-5)
     gl = rng.standard_normal((Z, Y, X)).astype(np.float32)
     gf = torch.empty((Z, Y, X, 16), dtype=torch.int16, device=dev)
     ghw = torch.zeros(17, device=dev)
-    _call(ctx, "tomgpu_unet_head_bwd_dev", _p(tf), n, _p(_f32(hw, dev)), _p(_f32(gl, dev)), _p(gf), _p(ghw))
+    tgl = _f32(gl, dev)
+    _call(ctx, "tomgpu_unet_head_bwd_dev", _p(tf), n, _p(thw), _p(tgl), _p(gf), _p(ghw))
     ctx.synchronize()
     _bf_close(_from_bf(gf), gl[..., None] * hw[:16] * (f > 0))
     _close(ghw.cpu().numpy()[:16], np.einsum("zyx,zyxc->c", gl, f))
@@ -158,13 +163,14 @@ def test_first_layer_head_pool_upsample_and_sums(gpu):
     gp = uo.bf16(rng.standard_normal((Z // 2, Y // 2, X // 2, C)))
     base = uo.bf16(rng.standard_normal((Z, Y, X, cs)))
     tbase = _bf(base, dev)
-    _call(ctx, "tomgpu_unet_pool_bwd_dev", _p(_bf(gp, dev)), C, dims, _p(ta), cs, off, _p(tbase), 1)
+    tgp = _bf(gp, dev)
+    _call(ctx, "tomgpu_unet_pool_bwd_dev", _p(tgp), C, dims, _p(ta), cs, off, _p(tbase), 1)
     ctx.synchronize()
     _bf_close(_from_bf(tbase)[..., off:off + C],
               base[..., off:off + C] + uo.pool_bwd(gp) * (a[..., off:off + C] > 0))
     # upsampling into a slice and its backward
     u = torch.zeros((Z, Y, X, cs), dtype=torch.int16, device=dev)
-    _call(ctx, "tomgpu_unet_upsample_dev", _p(_bf(gp, dev)), C, dims, _p(u), cs, off)
+    _call(ctx, "tomgpu_unet_upsample_dev", _p(tgp), C, dims, _p(u), cs, off)
     ctx.synchronize()
     assert np.array_equal(_from_bf(u)[..., off:off + C], uo.up(gp))
     ub = torch.empty((Z // 2, Y // 2, X // 2, C), dtype=torch.int16, device=dev)
