@@ -96,6 +96,12 @@ def parse():
     p.add_argument("--pruned-radius", type=float, default=21.0,
                    help="pruned_928x928x464: fine triplets within this many degrees of a candidate's coarse "
                         "rotation are searched")
+    p.add_argument("--unet-train", type=int, default=16,
+                   help="learned_928x928x464: training tomograms (128^3, the workload's species, SNR 0.05-0.2)")
+    p.add_argument("--unet-steps", type=int, default=600, help="learned_928x928x464: U-Net training steps")
+    p.add_argument("--unet-bins", type=int, default=4,
+                   help="learned_928x928x464: orientation bins (30 degree grid) refined per candidate")
+    p.add_argument("--unet-lr", type=float, default=1e-3, help="learned_928x928x464: Adam learning rate")
     p.add_argument("--pruned-ref-out", default="", help="pruned_928x928x464: save the exhaustive peaks (.npz)")
     p.add_argument("--pruned-ref-in", default="", help="pruned_928x928x464: reuse saved exhaustive peaks")
     p.add_argument("--workload", default=WORKLOAD,
@@ -466,6 +472,123 @@ def run_pruned(args):
     print(json.dumps(line), flush=True)
 
 
+def run_learned_928(args):
+    """The learned-pruned search on the full-size tomogram (928x928x464, the
+    48^3 species, 7 degree grid of 70,304 triplets).  The U-Net (BF16 on the
+    tensor cores) is trained on --unet-train synthetic 128^3 tomograms of the
+    same species (SNR drawn from 0.05-0.2, +-60 degree wedge) labelled by the
+    search itself (the peaks of the exhaustive 30 degree search and their
+    angle bins); on the test tomogram it proposes candidates and orientation
+    bins, and the fine search runs only on crops around the candidates, over
+    the fine triplets within --pruned-radius degrees of the --unet-bins most
+    probable bins.  Against the exhaustive fine search: seconds and recall of
+    its top-K peaks (K = the particle count), by position (within 2 voxels)
+    and by position and triplet; the network's training FLOP/s and inference
+    time; and the candidate recall of the network alone and of the coarse
+    search's peaks at the same count."""
+    import torch
+    import tom_b200 as tb
+    from tom_b200 import proposer as pr
+    from tom_b200 import synth
+    from tom_b200 import unet
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    ctx = tb.default_context(local)
+    name = "exhaustive_928x928x464"
+    cfg, fine, d, mask = make_workload(name)
+    T, K = cfg["T"], cfg["n_copies"]
+    bins30 = tb.tom_av3_angle_grid((0, 0, 0), (30, 30, 30), (330, 330, 180))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - t
+
+    # the workload's species (the first draw of make_tomogram's generator)
+    ph = synth.BlobPhantom(np.random.default_rng(2024), cfg["n_blobs"], cfg["rho"])
+    rng = np.random.default_rng(31)
+    (samples), t_data = timed(lambda: [
+        unet.training_sample((128, 128, 128), T, 6, cfg["n_blobs"], cfg["rho"], float(rng.uniform(0.05, 0.2)), 60,
+                             7000 + s, ph, mask, bins30, ctx) for s in range(args.unet_train)])
+    net = unet.UNetProposer(len(bins30), ctx, seed=1)
+    unet.train(net, samples, max(1, args.warmup), lr=args.unet_lr)
+    losses, t_train = timed(lambda: unet.train(net, samples, args.unet_steps, lr=args.unet_lr, start=args.warmup))
+    train_flops = 3 * net.flops_per_voxel() * 128 ** 3 * args.unet_steps
+    del samples
+    torch.cuda.empty_cache()
+    batch = args.batch or 32
+    if args.pruned_ref_in:
+        z = np.load(args.pruned_ref_in)
+        ref_pos, ref_idx, t_exh = z["pos"], z["idx"], float(z["t_exh"])
+    else:
+        (ccf, idf), t_exh = timed(lambda: pr.search(d["tomo"], d["template"], mask, fine, batch=batch, ctx=ctx))
+        ref_vals, ref_pos, ref_idx = tb.pick_peaks(ccf, idf, K, T / 2, ctx)
+        ref_pos = ref_pos - 1
+        del ccf, idf
+        if args.pruned_ref_out:
+            np.savez(args.pruned_ref_out, pos=ref_pos, idx=ref_idx, vals=ref_vals, t_exh=t_exh)
+    torch.cuda.empty_cache()
+    C = int(round(args.pruned_cands * K))
+    tm = {}
+    rpos, rcc, ridx = unet.learned_pruned_search(d["tomo"], d["template"], mask, fine, bins30, net, C,
+                                                 args.unet_bins, args.pruned_radius, ctx=ctx, timings=tm)
+
+    def recall(pos, idx=None):
+        dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - np.asarray(pos)[None].astype(float), axis=2)
+        j = np.argmin(dd, axis=1)
+        found = dd[np.arange(len(ref_pos)), j] <= 2
+        if idx is None:
+            return float(found.mean())
+        return float(found.mean()), float((found & (np.asarray(idx)[j] == ref_idx)).mean())
+
+    rc, ra = recall(rpos, ridx)
+    # the network's candidates and bins alone, and the coarse 30 degree search's
+    # peaks at the same count (positions; the nearest bin of the reference triplet)
+    v = torch.from_numpy(np.ascontiguousarray(d["tomo"].transpose(2, 1, 0))).to(net.dev)
+    v = unet.normalise(v, ctx, out=v)
+    (cpos, _, cbins), t_prop = timed(lambda: unet.propose(net, v, C, T / 2, args.unet_bins))
+    del v
+    torch.cuda.empty_cache()
+    ref_bin = pr.coarse_bin(np.asarray(fine)[ref_idx], bins30)
+    dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - np.asarray(cpos)[None].astype(float), axis=2)
+    j = np.argmin(dd, axis=1)
+    near = dd[np.arange(len(ref_pos)), j] <= 2
+    bin_hit = np.array([ref_bin[i] in set(cbins[j[i]]) for i in range(len(ref_pos))])
+    (ccc, icc), t_c30 = timed(lambda: pr.search(d["tomo"], d["template"], mask, bins30, batch=batch, ctx=ctx))
+    _, bpos, bidx = tb.pick_peaks(ccc, icc, C, T / 2, ctx)
+    del ccc, icc
+    okb = bidx >= 0
+    bpos, bidx = bpos[okb] - 1, bidx[okb]
+    dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - bpos[None].astype(float), axis=2)
+    jb = np.argmin(dd, axis=1)
+    cnear = dd[np.arange(len(ref_pos)), jb] <= 2
+    cbin_hit = bidx[jb] == ref_bin
+    line = {"metric": "learned-pruned search speed-up over the exhaustive fine search (928x928x464, 48^3 template)",
+            "value": t_exh / tm["total"], "unit": "x", "higher_is_better": True, "n_gpus": 1,
+            "dtype": "bf16 network, f32 search", "data": "synthetic",
+            "config": {"workload": "learned_928x928x464", "fine_angles": len(fine), "bins": len(bins30),
+                       "candidates": tm["candidates_n"], "reference_peaks": K, "bins_per_candidate": args.unet_bins,
+                       "refine_radius_deg": args.pruned_radius,
+                       "refine_triplets_per_candidate": tm["triplets_per_candidate"],
+                       "train_tomograms": args.unet_train, "train_volume": [128, 128, 128],
+                       "train_steps": args.unet_steps},
+            "exhaustive_s": t_exh, "pruned_s": {k: tm[k] for k in ("total", "upload_normalise", "network",
+                                                                    "triplet_sets", "refine")},
+            "recall": {"position": rc, "position_and_triplet": ra},
+            "network_alone": {"candidate_recall": float(near.mean()),
+                              "bin_in_top_bins": float((near & bin_hit).mean()), "propose_s": t_prop},
+            "coarse_30deg_search_alone": {"candidate_recall": float(cnear.mean()),
+                                          "bin_hit": float((cnear & cbin_hit).mean()), "search_s": t_c30},
+            "training": {"flop_per_s": train_flops / t_train, "s_per_step": t_train / args.unet_steps,
+                         "first_loss": losses[0], "last_loss": losses[-1], "data_s": t_data},
+            "scaling": "weak", "vs_baseline": None}
+    print(json.dumps(line), flush=True)
+
+
 def run_align(args):
     """Batched uneven subtomogram alignment (2048 particles, edges 32-96, +-15 deg
     at 3 deg = 1331 triplets each, shifts <= 4): a stratified subset is timed and
@@ -557,6 +680,8 @@ def main():
         return run_align(args)
     if args.workload == "pruned_928x928x464":
         return run_pruned(args)
+    if args.workload == "learned_928x928x464":
+        return run_learned_928(args)
     if args.workload == "learned_256":
         return run_learned(args)
     import torch

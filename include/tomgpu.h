@@ -490,9 +490,10 @@ int tomgpu_unet_conv_first_dev(tomgpu_ctx* ctx, const float* vol, const int dims
 int tomgpu_unet_conv_first_wgrad_dev(tomgpu_ctx* ctx, const float* vol, const int dims[3], const uint16_t* gout,
                                      float* gw, float* gb);
 /* Candidate head over n voxels of 16 channels, w = 16 weights and the bias
- * (17 floats): logit = w[16] + w[0..15] . f; backward: gf = g w (f > 0)
- * (written), gw[0..15] += sum g f, gw[16] += sum g. */
-int tomgpu_unet_head_dev(tomgpu_ctx* ctx, const uint16_t* f, int64_t n, const float* w, float* logit);
+ * (17 floats): logit = w[16] + w[0..15] . f (prob != 0: its logistic
+ * sigmoid, the centre probability); backward: gf = g w (f > 0) (written),
+ * gw[0..15] += sum g f, gw[16] += sum g. */
+int tomgpu_unet_head_dev(tomgpu_ctx* ctx, const uint16_t* f, int64_t n, const float* w, int prob, float* logit);
 int tomgpu_unet_head_bwd_dev(tomgpu_ctx* ctx, const uint16_t* f, int64_t n, const float* w, const float* g,
                              uint16_t* gf, float* gw);
 /* 2x2x2 average pool of a slice into a dense [C] volume (dims: the fine
@@ -510,6 +511,9 @@ int tomgpu_unet_upsample_bwd_dev(tomgpu_ctx* ctx, const uint16_t* gout, int cs, 
                                  uint16_t* gin);
 /* out[c] += sum over n voxels of g[v][off + c] (bias gradients; C <= 96). */
 int tomgpu_unet_channel_sum_dev(tomgpu_ctx* ctx, const uint16_t* g, int cs, int off, int C, int64_t n, float* out);
+/* out = (vol - mean) / std over n values (moments in FP64 on the device;
+ * out may be vol). */
+int tomgpu_unet_normalise_dev(tomgpu_ctx* ctx, const float* vol, int64_t n, float* out);
 /* Features at P voxels (flat indices) as FP32 F[c][p], and the scatter-add
  * of a gradient G[c][p] back into distinct voxels of a BF16 gradient, where
  * the ReLU features f are positive. */

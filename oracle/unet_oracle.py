@@ -128,11 +128,13 @@ def forward(p, vol, bf=False):
     return a
 
 
-def backward(p, vol, a, g_logit, g_f_extra=None, bf=False):
+def backward(p, vol, a, g_logit, g_f_extra=None, bf=False, inter=None):
     """Gradients of every parameter for the upstream gradient g_logit [Z][Y][X]
     of the candidate logits (plus g_f_extra [Z][Y][X][16] on the features,
-    e.g. from the orientation head).  Returns a dict keyed like the params."""
+    e.g. from the orientation head).  Returns a dict keyed like the params;
+    inter, a dict, receives the activation gradients between the layers."""
     gr = {}
+    keep = inter if inter is not None else {}
     w = lambda k: _q(p[k], bf)  # noqa: E731
     mask = lambda g, act: g * (act > 0)  # noqa: E731
     g_logit = np.asarray(g_logit, np.float64)
@@ -142,25 +144,26 @@ def backward(p, vol, a, g_logit, g_f_extra=None, bf=False):
     if g_f_extra is not None:
         g = g + g_f_extra
     g = _q(mask(g, a["f"]), bf)
+    keep["f"] = g
 
     def layer(name, x, g_out, act_in=None):
         gx, gw_, gb_ = conv3_grads(x, w("w_" + name), g_out)
         gr["w_" + name], gr["b_" + name] = gw_, gb_
         return gx if act_in is None else mask(gx, act_in)
 
-    g = _q(layer("d1b", a["d1a"], g, a["d1a"]), bf)
-    gD1 = _q(layer("d1a", a["D1"], g, a["D1"]), bf)
-    g = _q(up_bwd(gD1[..., :32]), bf)
-    g = _q(layer("d2b", a["d2a"], g, a["d2a"]), bf)
-    gD2 = _q(layer("d2a", a["D2"], g, a["D2"]), bf)
-    g = _q(up_bwd(gD2[..., :64]), bf)
-    g = _q(layer("e3b", a["e3a"], g, a["e3a"]), bf)
-    g_p2 = _q(layer("e3a", a["p2"], g), bf)
-    g_e2 = _q(gD2[..., 64:] + mask(pool_bwd(g_p2), a["e2"]), bf)
-    g = _q(layer("e2b", a["e2a"], g_e2, a["e2a"]), bf)
-    g_p1 = _q(layer("e2a", a["p1"], g), bf)
-    g_e1 = _q(gD1[..., 32:] + mask(pool_bwd(g_p1), a["e1"]), bf)
-    g = _q(layer("e1b", a["e1a"], g_e1, a["e1a"]), bf)
+    g = keep["d1a"] = _q(layer("d1b", a["d1a"], g, a["d1a"]), bf)
+    gD1 = keep["D1"] = _q(layer("d1a", a["D1"], g, a["D1"]), bf)
+    g = keep["d2"] = _q(up_bwd(gD1[..., :32]), bf)
+    g = keep["d2a"] = _q(layer("d2b", a["d2a"], g, a["d2a"]), bf)
+    gD2 = keep["D2"] = _q(layer("d2a", a["D2"], g, a["D2"]), bf)
+    g = keep["e3"] = _q(up_bwd(gD2[..., :64]), bf)
+    g = keep["e3a"] = _q(layer("e3b", a["e3a"], g, a["e3a"]), bf)
+    g_p2 = keep["p2"] = _q(layer("e3a", a["p2"], g), bf)
+    g_e2 = keep["e2"] = _q(gD2[..., 64:] + mask(pool_bwd(g_p2), a["e2"]), bf)
+    g = keep["e2a"] = _q(layer("e2b", a["e2a"], g_e2, a["e2a"]), bf)
+    g_p1 = keep["p1"] = _q(layer("e2a", a["p1"], g), bf)
+    g_e1 = keep["e1"] = _q(gD1[..., 32:] + mask(pool_bwd(g_p1), a["e1"]), bf)
+    g = keep["e1a"] = _q(layer("e1b", a["e1a"], g_e1, a["e1a"]), bf)
     _, gr["w0"], gr["b0"] = conv3_grads(np.asarray(vol, np.float64)[..., None], np.asarray(p["w0"], np.float64), g)
     return gr
 

@@ -154,7 +154,7 @@ _SIGS = {
                                                    c_void_p]),
     "tomgpu_unet_conv_first_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_void_p, c_void_p]),
     "tomgpu_unet_conv_first_wgrad_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p, c_void_p, c_void_p]),
-    "tomgpu_unet_head_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p]),
+    "tomgpu_unet_head_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, c_void_p, ctypes.c_int, c_void_p]),
     "tomgpu_unet_head_bwd_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, c_void_p, c_void_p, c_void_p,
                                                 c_void_p]),
     "tomgpu_unet_pool_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_int_p,
@@ -167,6 +167,7 @@ _SIGS = {
                                                     c_int_p, c_void_p]),
     "tomgpu_unet_channel_sum_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_int64, c_void_p]),
+    "tomgpu_unet_normalise_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, c_void_p]),
     "tomgpu_unet_gather_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p, ctypes.c_int, c_void_p]),
     "tomgpu_unet_scatter_add_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p, ctypes.c_int,
                                                    c_void_p, c_void_p]),

@@ -461,8 +461,9 @@ __global__ void __launch_bounds__(448) k_uconv_first_wgrad(const float* __restri
         atomicAdd(gb + co, acc);
 }
 
-// candidate head: logit[v] = wb[16] + sum_c wb[c] f[v][c] (16 channels)
-__global__ void k_uhead(const unsigned short* __restrict__ f, long long n, const float* __restrict__ w,
+// candidate head: logit[v] = wb[16] + sum_c wb[c] f[v][c] (16 channels), or
+// its logistic sigmoid when prob != 0
+__global__ void k_uhead(const unsigned short* __restrict__ f, long long n, const float* __restrict__ w, int prob,
                         float* __restrict__ logit) {
     const float b = __ldg(w + 16);
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
@@ -472,7 +473,7 @@ __global__ void k_uhead(const unsigned short* __restrict__ f, long long n, const
         float s = b;
 #pragma unroll
         for (int c = 0; c < 16; ++c) s = fmaf(__ldg(w + c), bf2f((unsigned short)(u[c >> 1] >> (16 * (c & 1)))), s);
-        logit[v] = s;
+        logit[v] = prob ? 1.f / (1.f + expf(-s)) : s;
     }
 }
 
@@ -637,6 +638,42 @@ __global__ void k_uchan_sum(const unsigned short* __restrict__ g, int cs, int of
     }
 }
 
+// sums of x and x^2 over n values (FP64, one atomic add per block and sum)
+__global__ void __launch_bounds__(256) k_umoments(const float* __restrict__ x, long long n, double* __restrict__ s) {
+    __shared__ double red[2][8];
+    double a = 0.0, b = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double v = x[i];
+        a += v;
+        b += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        red[0][warp] = a;
+        red[1][warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double t = 0.0;
+        for (int k = 0; k < 8; ++k) t += red[threadIdx.x][k];
+        atomicAdd(s + threadIdx.x, t);
+    }
+}
+
+// out = (x - mean) / std from the sums (std 0 -> 1)
+__global__ void k_uaffine(const float* __restrict__ x, long long n, const double* __restrict__ s,
+                          float* __restrict__ out) {
+    const double mean = s[0] / (double)n;
+    const double var = s[1] / (double)n - mean * mean;
+    const float m = (float)mean, r = var > 0.0 ? (float)(1.0 / sqrt(var)) : 1.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (x[i] - m) * r;
+}
+
 // features at P voxels, as the dense layer's F[c][p] (FP32)
 __global__ void k_ugather(const unsigned short* __restrict__ f, int C, const long long* __restrict__ idx, int P,
                           float* __restrict__ out) {
@@ -799,11 +836,12 @@ int tomgpu_unet_conv_first_wgrad_dev(tomgpu_ctx* ctx, const float* vol, const in
     return TOMGPU_OK;
 }
 
-int tomgpu_unet_head_dev(tomgpu_ctx* ctx, const uint16_t* f, int64_t n, const float* w, float* logit) {
+int tomgpu_unet_head_dev(tomgpu_ctx* ctx, const uint16_t* f, int64_t n, const float* w, int prob, float* logit) {
     if (!ctx) return TOMGPU_ERR_ARG;
     if (!f || !w || !logit || n < 1) return fail(ctx, TOMGPU_ERR_ARG, "bad head arguments");
     TG_TRY(use_device(ctx));
-    k_uhead<<<grid_for(n, 256), 256, 0, ctx->stream>>>(reinterpret_cast<const unsigned short*>(f), n, w, logit);
+    k_uhead<<<grid_for(n, 256), 256, 0, ctx->stream>>>(reinterpret_cast<const unsigned short*>(f), n, w, prob,
+                                                       logit);
     TG_TRY_CUDA(ctx, cudaGetLastError());
     ctx->launches += 1;
     return TOMGPU_OK;
@@ -895,6 +933,20 @@ int tomgpu_unet_channel_sum_dev(tomgpu_ctx* ctx, const uint16_t* g, int cs, int 
         reinterpret_cast<const unsigned short*>(g), cs, off, C, n, out);
     TG_TRY_CUDA(ctx, cudaGetLastError());
     ctx->launches += 1;
+    return TOMGPU_OK;
+}
+
+int tomgpu_unet_normalise_dev(tomgpu_ctx* ctx, const float* vol, int64_t n, float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!vol || !out || n < 1) return fail(ctx, TOMGPU_ERR_ARG, "bad normalisation arguments");
+    TG_TRY(use_device(ctx));
+    TG_TRY(ensure_scratch(ctx, 2 * sizeof(double)));
+    double* s = static_cast<double*>(ctx->scratch);
+    TG_TRY_CUDA(ctx, cudaMemsetAsync(s, 0, 2 * sizeof(double), ctx->stream));
+    k_umoments<<<grid_for(n, 256), 256, 0, ctx->stream>>>(vol, n, s);
+    k_uaffine<<<grid_for(n, 256), 256, 0, ctx->stream>>>(vol, n, s, out);
+    TG_TRY_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 2;
     return TOMGPU_OK;
 }
 

@@ -103,9 +103,10 @@ class UNetProposer:
               _tptr(self.p["b_" + name]), 1, None, 0, 0, _tptr(dst), dcs, doff)
 
     # ------------------------------------------------------------ forward
-    def forward(self, vol, train=False):
+    def forward(self, vol, train=False, prob=False):
         """vol: torch float32 [Z][Y][X] on the device (normalised).  Returns the
-        candidate logits [Z][Y][X] (a buffer reused by the next call)."""
+        candidate logits [Z][Y][X] (prob: their sigmoid, the centre
+        probabilities; a buffer reused by the next call)."""
         ctx = self.ctx
         self._alloc(tuple(vol.shape), train)
         a = self.a
@@ -126,7 +127,7 @@ class UNetProposer:
         self._conv("d1a", a["D1"], 48, 0, 48, 0, 16, a["d1a"], 16, 0)
         self._conv("d1b", a["d1a"], 16, 0, 16, 0, 16, a["f"], 16, 0)
         _call(ctx, "tomgpu_unet_head_dev", _tptr(a["f"]), self.logit.numel(), _tptr(self.p["head"]),
-              _tptr(self.logit))
+              1 if prob else 0, _tptr(self.logit))
         return self.logit
 
     def orient_logits(self, idx):
@@ -251,3 +252,162 @@ def init_params(n_bins, seed=0):
     p["Wo"] = (r.standard_normal((n_bins, 16)) * 0.25).astype(np.float32)
     p["bo"] = np.zeros(n_bins, np.float32)
     return p
+
+
+# ------------------------------------------------------------------ inference
+
+
+def normalise(vol, ctx=None, out=None):
+    """(vol - mean) / std of a device volume (moments in FP64 on the device)."""
+    import torch
+    ctx = ctx or default_context()
+    out = torch.empty_like(vol) if out is None else out
+    _call(ctx, "tomgpu_unet_normalise_dev", _tptr(vol), vol.numel(), _tptr(out))
+    return out
+
+
+def infer(net, vol, slab=128, halo=32, prob=True):
+    """Centre probabilities (prob=False: logits) [Z][Y][X] and the features
+    [Z][Y][X][16] (BF16 bits) of a whole normalised volume, in z slabs of
+    `slab` planes each run with `halo` more planes on either side (zero beyond
+    the volume), which bounds the activation memory.  An output voxel reads
+    the input within 23 voxels of it (the ten convolutions at their levels
+    through the pooling and upsampling), and the slabs start on multiples of
+    4, so the pooling grids stay aligned: with halo >= 24 every voxel's
+    outputs are those of the whole-volume pass.  slab and halo are multiples
+    of 4."""
+    import torch
+    Z, Y, X = vol.shape
+    if slab % 4 or halo % 4 or Z % 4:
+        raise ValueError("slab, halo and the z edge must be multiples of 4")
+    out = torch.empty((Z, Y, X), dtype=torch.float32, device=net.dev)
+    feat = torch.empty((Z, Y, X, FEAT), dtype=torch.int16, device=net.dev)
+    for z0 in range(0, Z, slab):
+        z1 = min(Z, z0 + slab)
+        lo, hi = max(0, z0 - halo), min(Z, z1 + halo)
+        lg = net.forward(vol[lo:hi], prob=prob)
+        out[z0:z1].copy_(lg[z0 - lo:z1 - lo])
+        feat[z0:z1].copy_(net.a["f"][z0 - lo:z1 - lo])
+    return out, feat
+
+
+def orient_logits_at(net, feat, idx):
+    """Orientation logits [n_bins][P] at flat voxel indices idx (int64 tensor)
+    of a feature volume from infer()."""
+    import torch
+    P = int(idx.numel())
+    fg = torch.empty((FEAT, P), device=net.dev)
+    _call(net.ctx, "tomgpu_unet_gather_dev", _tptr(feat), FEAT, _tptr(idx), P, _tptr(fg))
+    out = torch.empty((net.n_bins, P), device=net.dev)
+    _call(net.ctx, "tomgpu_cnn_dense_fwd_dev", _tptr(net.p["Wo"]), _tptr(net.p["bo"]), _tptr(fg), net.n_bins, FEAT,
+          P, 0, _tptr(out))
+    return out
+
+
+def propose(net, vol, n_cand, radius, top_bins, slab=128, halo=32):
+    """Candidates of the network on a normalised device volume [Z][Y][X]: the
+    n_cand first maxima of the centre probability (tom_peak rounds with a ball
+    of `radius`), 0-based [x, y, z], their probabilities and the top_bins
+    orientation bins of each (most probable first)."""
+    import torch
+    from .tom import pick_peaks
+    prob, feat = infer(net, vol, slab, halo, prob=True)
+    Z, Y, X = prob.shape
+    dummy = torch.zeros((Z, Y, X), dtype=torch.int32, device=net.dev)
+    vals, pos, _ = pick_peaks(prob, dummy, n_cand, radius, net.ctx)
+    del dummy
+    ok = pos[:, 0] > 0
+    pos, vals = pos[ok] - 1, vals[ok]
+    fi = torch.from_numpy((pos[:, 0] + X * (pos[:, 1] + Y * pos[:, 2])).astype(np.int64)).to(net.dev)
+    ol = orient_logits_at(net, feat, fi)
+    bins = torch.topk(ol, k=min(top_bins, net.n_bins), dim=0).indices.t().cpu().numpy()
+    return pos, vals, bins
+
+
+def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bins, radius_deg, window=2,
+                          peak_radius=None, slab=128, halo=32, ctx=None, timings=None):
+    """The pruned search with the network in place of the coarse search: the
+    network's n_cand candidates on the tomogram, and around each the fine
+    triplets within radius_deg (geodesic) of its top_bins coarse orientation
+    bins searched on a crop (proposer.refine: the values equal the full
+    search's there), the best within +-window voxels.  vol: the tomogram as a
+    host array [x][y][z].  Returns (positions 0-based [x, y, z], cc, fine
+    triplet index) per candidate; timings receives the seconds per step."""
+    import time
+    import torch
+    from . import proposer as pr
+    ctx = ctx or net.ctx
+    T = np.shape(template)[0]
+    clock = []
+
+    def mark():
+        torch.cuda.synchronize(ctx.device)
+        clock.append(time.perf_counter())
+
+    mark()
+    v = torch.from_numpy(np.ascontiguousarray(np.asarray(vol, np.float32).transpose(2, 1, 0))).to(net.dev)
+    v = normalise(v, ctx, out=v)
+    mark()
+    pos, _, bins = propose(net, v, n_cand, T / 2 if peak_radius is None else peak_radius, top_bins, slab, halo)
+    del v
+    mark()
+    sets = []
+    coarse = np.asarray(coarse)
+    for b in bins:
+        near = pr.neighbours(fine, coarse[np.asarray(b)], radius_deg)
+        ids = np.unique(np.concatenate(near))
+        sets.append((np.asarray(fine)[ids], ids))
+    mark()
+    out = pr.refine(vol, template, mask, pos, sets, window=window, ctx=ctx)
+    mark()
+    if timings is not None:
+        for k, name in enumerate(("upload_normalise", "network", "triplet_sets", "refine")):
+            timings[name] = clock[k + 1] - clock[k]
+        timings["total"] = clock[-1] - clock[0]
+        timings["candidates_n"] = int(len(pos))
+        timings["triplets_per_candidate"] = float(np.mean([len(s[1]) for s in sets])) if sets else 0.0
+    return out
+
+
+# ------------------------------------------------------------------ training data
+
+
+def training_sample(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed, phantom, mask, coarse, ctx=None):
+    """A seeded synthetic tomogram and its labels from the search itself: the
+    n_copies first peaks of the exhaustive search over the coarse grid
+    (tom_peak rounds of radius T/2), their positions and angle indices (the
+    orientation bins).  Returns (normalised volume [Z][Y][X] float32,
+    positions 0-based [x, y, z], bins)."""
+    import torch
+    from . import proposer as pr
+    from . import synth
+    from .tom import pick_peaks
+    ctx = ctx or default_context()
+    d = synth.make_tomogram(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed=seed, mask_radius=T // 2 - 1,
+                            phantom=phantom)
+    cc, idx = pr.search(d["tomo"], d["template"], mask, coarse, batch=16, ctx=ctx)
+    _, pos, aidx = pick_peaks(cc, idx, n_copies, T / 2, ctx)
+    del cc, idx
+    ok = aidx >= 0
+    v = torch.from_numpy(np.ascontiguousarray(d["tomo"].transpose(2, 1, 0))).to(f"cuda:{ctx.device}")
+    v = normalise(v, ctx, out=v)
+    return v, pos[ok] - 1, aidx[ok].astype(np.int32)
+
+
+def train(net, samples, steps, pos_weight=50.0, lr=1e-3, w_orient=0.2, start=0):
+    """steps Adam steps cycling over samples [(volume, positions, bins)];
+    returns the (centre loss, orientation loss) of every step."""
+    import torch
+    from . import proposer as pr
+    prep = []
+    for v, pos, bins in samples:
+        Z, Y, X = v.shape
+        p = np.asarray(pos, np.int64).reshape(-1, 3)
+        fi = torch.from_numpy(p[:, 0] + X * (p[:, 1] + Y * p[:, 2])).to(net.dev)
+        prep.append((v, pr.heat_target((X, Y, Z), p, net.dev), fi,
+                     torch.from_numpy(np.asarray(bins, np.int32)).to(net.dev)))
+    out = []
+    for i in range(start, start + steps):
+        v, t, fi, b = prep[i % len(prep)]
+        out.append(net.train_step(v, t, fi, b, pos_weight=pos_weight, lr=lr, w_orient=w_orient))
+    return out
