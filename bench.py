@@ -102,6 +102,7 @@ def parse():
     p.add_argument("--unet-bins", type=int, default=4,
                    help="learned_928x928x464: orientation bins (30 degree grid) refined per candidate")
     p.add_argument("--unet-lr", type=float, default=1e-3, help="learned_928x928x464: Adam learning rate")
+    p.add_argument("--unet-edge", type=int, default=256, help="unet: the volume edge")
     p.add_argument("--pruned-ref-out", default="", help="pruned_928x928x464: save the exhaustive peaks (.npz)")
     p.add_argument("--pruned-ref-in", default="", help="pruned_928x928x464: reuse saved exhaustive peaks")
     p.add_argument("--workload", default=WORKLOAD,
@@ -589,6 +590,63 @@ def run_learned_928(args):
     print(json.dumps(line), flush=True)
 
 
+def run_unet(args):
+    """The U-Net proposer's own kernels on a --unet-edge^3 volume: the forward
+    pass (inference) and one training step (forward, backward, Adam, weight
+    repacking), each timed with CUDA events over --steps iterations after
+    --warmup; FLOP/s by the network's multiply-adds (forward 2 MAC per voxel,
+    a training step 3x the forward), against the measured dense BF16 peak."""
+    import torch
+    import tom_b200 as tb
+    from tom_b200 import unet
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    ctx = tb.default_context(local)
+    n = args.unet_edge
+    net = unet.UNetProposer(1008, ctx, seed=1)
+    g = torch.Generator(device=net.dev).manual_seed(3)
+    vol = torch.randn((n, n, n), device=net.dev, generator=g)
+    tgt = (torch.rand((n, n, n), device=net.dev, generator=g) < 1e-4).float()
+    idx = torch.randperm(n ** 3, device=net.dev, generator=g)[:64].contiguous()
+    bins = torch.randint(0, 1008, (64,), device=net.dev, dtype=torch.int32, generator=g)
+    st = torch.cuda.current_stream()
+
+    def ev_time(fn, k):
+        for _ in range(args.warmup):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(k):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    l0 = ctx.launches
+    fwd_ms = ev_time(lambda: net.forward(vol, prob=True), args.steps)
+    step_ms = ev_time(lambda: net.train_step(vol, tgt, idx, bins), args.steps)
+    fl = net.flops_per_voxel() * n ** 3
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 1590.0, "fallback"
+    if os.path.exists(path):
+        with open(path) as f:
+            peak, peak_src = float(json.load(f)["bf16_tflops"]), "measured"
+    line = {"metric": "U-Net proposer TFLOP/s (BF16 tcgen05 3x3x3 convolutions, FP32 accumulation)",
+            "value": fl / fwd_ms / 1e9, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": "unet_%d" % n, "volume": [n, n, n], "channels": [16, 32, 64]},
+            "forward_ms": fwd_ms, "train_step_ms": step_ms, "train_tflops": 3 * fl / step_ms / 1e9,
+            "flop_per_voxel_forward": net.flops_per_voxel(),
+            "roofline": {"bound": "tensor", "achieved": fl / fwd_ms / 1e9, "peak": peak, "unit": "TFLOP/s",
+                         "frac": fl / fwd_ms / 1e9 / peak, "peak_source": peak_src},
+            "gpu_launches": (ctx.launches - l0) // (2 * (args.warmup + args.steps)),
+            "scaling": "weak", "vs_baseline": None}
+    print(json.dumps(line), flush=True)
+
+
 def run_align(args):
     """Batched uneven subtomogram alignment (2048 particles, edges 32-96, +-15 deg
     at 3 deg = 1331 triplets each, shifts <= 4): a stratified subset is timed and
@@ -682,6 +740,8 @@ def main():
         return run_pruned(args)
     if args.workload == "learned_928x928x464":
         return run_learned_928(args)
+    if args.workload == "unet":
+        return run_unet(args)
     if args.workload == "learned_256":
         return run_learned(args)
     import torch

@@ -82,6 +82,7 @@ class UNetProposer:
         if Z % 4 or Y % 4 or X % 4:
             raise ValueError("volume edges must be multiples of 4")
         L1, L2, L3 = (Z, Y, X), (Z // 2, Y // 2, X // 2), (Z // 4, Y // 4, X // 4)
+        self.a = self.ga = self.logit = None  # release the previous shape's buffers first
 
         def buf(L, c):
             return torch.zeros(L + (c,), dtype=torch.int16, device=self.dev)
