@@ -103,6 +103,8 @@ def parse():
                    help="learned_928x928x464: orientation bins (30 degree grid) refined per candidate")
     p.add_argument("--unet-lr", type=float, default=1e-3, help="learned_928x928x464: Adam learning rate")
     p.add_argument("--unet-edge", type=int, default=256, help="unet: the volume edge")
+    p.add_argument("--unet-window", type=int, default=7,
+                   help="learned_928x928x464: refine window (+- voxels) around a candidate")
     p.add_argument("--pruned-ref-out", default="", help="pruned_928x928x464: save the exhaustive peaks (.npz)")
     p.add_argument("--pruned-ref-in", default="", help="pruned_928x928x464: reuse saved exhaustive peaks")
     p.add_argument("--workload", default=WORKLOAD,
@@ -478,8 +480,8 @@ def run_learned_928(args):
     48^3 species, 7 degree grid of 70,304 triplets).  The U-Net (BF16 on the
     tensor cores) is trained on --unet-train synthetic 128^3 tomograms of the
     same species (SNR drawn from 0.05-0.2, +-60 degree wedge) labelled by the
-    search itself (the peaks of the exhaustive 30 degree search and their
-    angle bins); on the test tomogram it proposes candidates and orientation
+    search itself (the peaks of the exhaustive fine search and the 30 degree
+    bins of their angles); on the test tomogram it proposes candidates and orientation
     bins, and the fine search runs only on crops around the candidates, over
     the fine triplets within --pruned-radius degrees of the --unet-bins most
     probable bins.  Against the exhaustive fine search: seconds and recall of
@@ -514,12 +516,18 @@ def run_learned_928(args):
     rng = np.random.default_rng(31)
     (samples), t_data = timed(lambda: [
         unet.training_sample((128, 128, 128), T, 6, cfg["n_blobs"], cfg["rho"], float(rng.uniform(0.05, 0.2)), 60,
-                             7000 + s, ph, mask, bins30, ctx) for s in range(args.unet_train)])
+                             7000 + s, ph, mask, bins30, fine, ctx) for s in range(args.unet_train)])
     net = unet.UNetProposer(len(bins30), ctx, seed=1)
     unet.train(net, samples, max(1, args.warmup), lr=args.unet_lr)
     losses, t_train = timed(lambda: unet.train(net, samples, args.unet_steps, lr=args.unet_lr, start=args.warmup))
     train_flops = 3 * net.flops_per_voxel() * 128 ** 3 * args.unet_steps
-    del samples
+    # the network on a training tomogram: its own labels recalled (a check of
+    # the pipeline's coordinate conventions and of what training reached)
+    v0, p0, _ = samples[0]
+    tpos, _, _ = unet.propose(net, v0, 2 * len(p0), T / 2, 1)
+    td = np.linalg.norm(np.asarray(p0)[:, None, :].astype(float) - np.asarray(tpos)[None].astype(float), axis=2)
+    train_recall = float((td.min(axis=1) <= 2).mean())
+    del samples, v0
     torch.cuda.empty_cache()
     batch = args.batch or 32
     if args.pruned_ref_in:
@@ -536,7 +544,8 @@ def run_learned_928(args):
     C = int(round(args.pruned_cands * K))
     tm = {}
     rpos, rcc, ridx = unet.learned_pruned_search(d["tomo"], d["template"], mask, fine, bins30, net, C,
-                                                 args.unet_bins, args.pruned_radius, ctx=ctx, timings=tm)
+                                                 args.unet_bins, args.pruned_radius, window=args.unet_window,
+                                                 ctx=ctx, timings=tm)
 
     def recall(pos, idx=None):
         dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - np.asarray(pos)[None].astype(float), axis=2)
@@ -557,8 +566,10 @@ def run_learned_928(args):
     ref_bin = pr.coarse_bin(np.asarray(fine)[ref_idx], bins30)
     dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - np.asarray(cpos)[None].astype(float), axis=2)
     j = np.argmin(dd, axis=1)
-    near = dd[np.arange(len(ref_pos)), j] <= 2
+    dmin = dd[np.arange(len(ref_pos)), j]
+    near = dmin <= args.unet_window
     bin_hit = np.array([ref_bin[i] in set(cbins[j[i]]) for i in range(len(ref_pos))])
+    net_by_radius = {str(r): float((dmin <= r).mean()) for r in (2, 4, 7, 12, 24)}
     (ccc, icc), t_c30 = timed(lambda: pr.search(d["tomo"], d["template"], mask, bins30, batch=batch, ctx=ctx))
     _, bpos, bidx = tb.pick_peaks(ccc, icc, C, T / 2, ctx)
     del ccc, icc
@@ -566,23 +577,28 @@ def run_learned_928(args):
     bpos, bidx = bpos[okb] - 1, bidx[okb]
     dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - bpos[None].astype(float), axis=2)
     jb = np.argmin(dd, axis=1)
-    cnear = dd[np.arange(len(ref_pos)), jb] <= 2
+    cmin = dd[np.arange(len(ref_pos)), jb]
+    cnear = cmin <= args.unet_window
+    coarse_by_radius = {str(r): float((cmin <= r).mean()) for r in (2, 4, 7, 12, 24)}
     cbin_hit = bidx[jb] == ref_bin
     line = {"metric": "learned-pruned search speed-up over the exhaustive fine search (928x928x464, 48^3 template)",
             "value": t_exh / tm["total"], "unit": "x", "higher_is_better": True, "n_gpus": 1,
             "dtype": "bf16 network, f32 search", "data": "synthetic",
             "config": {"workload": "learned_928x928x464", "fine_angles": len(fine), "bins": len(bins30),
                        "candidates": tm["candidates_n"], "reference_peaks": K, "bins_per_candidate": args.unet_bins,
-                       "refine_radius_deg": args.pruned_radius,
+                       "refine_radius_deg": args.pruned_radius, "refine_window": args.unet_window,
                        "refine_triplets_per_candidate": tm["triplets_per_candidate"],
                        "train_tomograms": args.unet_train, "train_volume": [128, 128, 128],
                        "train_steps": args.unet_steps},
             "exhaustive_s": t_exh, "pruned_s": {k: tm[k] for k in ("total", "upload_normalise", "network",
                                                                     "triplet_sets", "refine")},
             "recall": {"position": rc, "position_and_triplet": ra},
-            "network_alone": {"candidate_recall": float(near.mean()),
-                              "bin_in_top_bins": float((near & bin_hit).mean()), "propose_s": t_prop},
-            "coarse_30deg_search_alone": {"candidate_recall": float(cnear.mean()),
+            "network_alone": {"candidate_recall_within_window": float(near.mean()),
+                              "candidate_recall_by_radius": net_by_radius,
+                              "bin_in_top_bins": float((near & bin_hit).mean()), "propose_s": t_prop,
+                              "training_tomogram_label_recall": train_recall},
+            "coarse_30deg_search_alone": {"candidate_recall_within_window": float(cnear.mean()),
+                                          "candidate_recall_by_radius": coarse_by_radius,
                                           "bin_hit": float((cnear & cbin_hit).mean()), "search_s": t_c30},
             "training": {"flop_per_s": train_flops / t_train, "s_per_step": t_train / args.unet_steps,
                          "first_loss": losses[0], "last_loss": losses[-1], "data_s": t_data},

@@ -352,11 +352,12 @@ def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bi
     pos, _, bins = propose(net, v, n_cand, T / 2 if peak_radius is None else peak_radius, top_bins, slab, halo)
     del v
     mark()
-    sets = []
     coarse = np.asarray(coarse)
+    ub = np.unique(np.asarray(bins).reshape(-1))
+    per_bin = dict(zip(ub.tolist(), pr.neighbours(fine, coarse[ub], radius_deg)))
+    sets = []
     for b in bins:
-        near = pr.neighbours(fine, coarse[np.asarray(b)], radius_deg)
-        ids = np.unique(np.concatenate(near))
+        ids = np.unique(np.concatenate([per_bin[int(k)] for k in b]))
         sets.append((np.asarray(fine)[ids], ids))
     mark()
     out = pr.refine(vol, template, mask, pos, sets, window=window, ctx=ctx)
@@ -373,12 +374,12 @@ def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bi
 # ------------------------------------------------------------------ training data
 
 
-def training_sample(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed, phantom, mask, coarse, ctx=None):
+def training_sample(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed, phantom, mask, coarse, fine=None, ctx=None):
     """A seeded synthetic tomogram and its labels from the search itself: the
-    n_copies first peaks of the exhaustive search over the coarse grid
-    (tom_peak rounds of radius T/2), their positions and angle indices (the
-    orientation bins).  Returns (normalised volume [Z][Y][X] float32,
-    positions 0-based [x, y, z], bins)."""
+    n_copies first peaks of the exhaustive search (tom_peak rounds of radius
+    T/2) over the fine grid when given, else over the coarse grid, their
+    positions and the coarse bins of their angles.  Returns (normalised
+    volume [Z][Y][X] float32, positions 0-based [x, y, z], bins)."""
     import torch
     from . import proposer as pr
     from . import synth
@@ -386,13 +387,15 @@ def training_sample(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed, phantom, 
     ctx = ctx or default_context()
     d = synth.make_tomogram(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed=seed, mask_radius=T // 2 - 1,
                             phantom=phantom)
-    cc, idx = pr.search(d["tomo"], d["template"], mask, coarse, batch=16, ctx=ctx)
+    grid = coarse if fine is None else fine
+    cc, idx = pr.search(d["tomo"], d["template"], mask, grid, batch=16, ctx=ctx)
     _, pos, aidx = pick_peaks(cc, idx, n_copies, T / 2, ctx)
     del cc, idx
     ok = aidx >= 0
+    bins = aidx[ok] if fine is None else pr.coarse_bin(np.asarray(fine)[aidx[ok]], coarse)
     v = torch.from_numpy(np.ascontiguousarray(d["tomo"].transpose(2, 1, 0))).to(f"cuda:{ctx.device}")
     v = normalise(v, ctx, out=v)
-    return v, pos[ok] - 1, aidx[ok].astype(np.int32)
+    return v, pos[ok] - 1, np.asarray(bins, np.int32)
 
 
 def train(net, samples, steps, pos_weight=50.0, lr=1e-3, w_orient=0.2, start=0):
