@@ -102,6 +102,10 @@ def parse():
     p.add_argument("--unet-bins", type=int, default=4,
                    help="learned_928x928x464: orientation bins (30 degree grid) refined per candidate")
     p.add_argument("--unet-lr", type=float, default=1e-3, help="learned_928x928x464: Adam learning rate")
+    p.add_argument("--unet-pos-weight", type=float, default=300.0,
+                   help="learned_928x928x464: weight of the centre target's positive voxels")
+    p.add_argument("--unet-target-radius", type=float, default=3.0,
+                   help="learned_928x928x464: radius of the centre target's balls")
     p.add_argument("--unet-edge", type=int, default=256, help="unet: the volume edge")
     p.add_argument("--unet-window", type=int, default=7,
                    help="learned_928x928x464: refine window (+- voxels) around a candidate")
@@ -518,8 +522,9 @@ def run_learned_928(args):
         unet.training_sample((128, 128, 128), T, 6, cfg["n_blobs"], cfg["rho"], float(rng.uniform(0.05, 0.2)), 60,
                              7000 + s, ph, mask, bins30, fine, ctx) for s in range(args.unet_train)])
     net = unet.UNetProposer(len(bins30), ctx, seed=1)
-    unet.train(net, samples, max(1, args.warmup), lr=args.unet_lr)
-    losses, t_train = timed(lambda: unet.train(net, samples, args.unet_steps, lr=args.unet_lr, start=args.warmup))
+    kw = dict(lr=args.unet_lr, pos_weight=args.unet_pos_weight, target_radius=args.unet_target_radius)
+    unet.train(net, samples, max(1, args.warmup), **kw)
+    losses, t_train = timed(lambda: unet.train(net, samples, args.unet_steps, start=args.warmup, **kw))
     train_flops = 3 * net.flops_per_voxel() * 128 ** 3 * args.unet_steps
     # the network on a training tomogram: its own labels recalled (a check of
     # the pipeline's coordinate conventions and of what training reached)
@@ -589,6 +594,7 @@ def run_learned_928(args):
                        "refine_radius_deg": args.pruned_radius, "refine_window": args.unet_window,
                        "refine_triplets_per_candidate": tm["triplets_per_candidate"],
                        "train_tomograms": args.unet_train, "train_volume": [128, 128, 128],
+                       "pos_weight": args.unet_pos_weight, "target_radius": args.unet_target_radius,
                        "train_steps": args.unet_steps},
             "exhaustive_s": t_exh, "pruned_s": {k: tm[k] for k in ("total", "upload_normalise", "network",
                                                                     "triplet_sets", "refine")},

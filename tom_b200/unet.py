@@ -398,17 +398,34 @@ def training_sample(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed, phantom, 
     return v, pos[ok] - 1, np.asarray(bins, np.int32)
 
 
-def train(net, samples, steps, pos_weight=50.0, lr=1e-3, w_orient=0.2, start=0):
-    """steps Adam steps cycling over samples [(volume, positions, bins)];
-    returns the (centre loss, orientation loss) of every step."""
+def ball_target(shape_zyx, pos, radius, dev):
+    """1 within `radius` voxels of each label position, 0 elsewhere; [Z][Y][X]."""
     import torch
-    from . import proposer as pr
+    Z, Y, X = shape_zyx
+    t = np.zeros((Z, Y, X), np.float32)
+    r = int(np.floor(radius))
+    off = [(dx, dy, dz) for dz in range(-r, r + 1) for dy in range(-r, r + 1) for dx in range(-r, r + 1)
+           if dx * dx + dy * dy + dz * dz <= radius * radius]
+    for x, y, z in np.asarray(pos, np.int64).reshape(-1, 3):
+        for dx, dy, dz in off:
+            t[(z + dz) % Z, (y + dy) % Y, (x + dx) % X] = 1.0
+    return torch.from_numpy(t).to(dev)
+
+
+def train(net, samples, steps, pos_weight=300.0, lr=1e-3, w_orient=0.2, start=0, target_radius=3.0):
+    """steps Adam steps cycling over samples [(volume, positions, bins)]:
+    binary cross-entropy of the centre probability against balls of
+    target_radius around the labels (positives weighted by pos_weight: a
+    particle is a few hundred voxels of millions) and softmax cross-entropy
+    of the orientation bin at the labels.  Returns the (centre loss,
+    orientation loss) of every step."""
+    import torch
     prep = []
     for v, pos, bins in samples:
         Z, Y, X = v.shape
         p = np.asarray(pos, np.int64).reshape(-1, 3)
         fi = torch.from_numpy(p[:, 0] + X * (p[:, 1] + Y * p[:, 2])).to(net.dev)
-        prep.append((v, pr.heat_target((X, Y, Z), p, net.dev), fi,
+        prep.append((v, ball_target((Z, Y, X), p, target_radius, net.dev), fi,
                      torch.from_numpy(np.asarray(bins, np.int32)).to(net.dev)))
     out = []
     for i in range(start, start + steps):
