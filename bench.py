@@ -107,6 +107,8 @@ def parse():
     p.add_argument("--unet-target-radius", type=float, default=3.0,
                    help="learned_928x928x464: radius of the centre target's balls")
     p.add_argument("--unet-edge", type=int, default=256, help="unet: the volume edge")
+    p.add_argument("--unet-snr", default="0.05,0.2",
+                   help="learned_928x928x464: SNR range of the training tomograms (lo,hi)")
     p.add_argument("--unet-window", type=int, default=7,
                    help="learned_928x928x464: refine window (+- voxels) around a candidate")
     p.add_argument("--pruned-ref-out", default="", help="pruned_928x928x464: save the exhaustive peaks (.npz)")
@@ -518,8 +520,9 @@ def run_learned_928(args):
     # the workload's species (the first draw of make_tomogram's generator)
     ph = synth.BlobPhantom(np.random.default_rng(2024), cfg["n_blobs"], cfg["rho"])
     rng = np.random.default_rng(31)
+    snr_lo, snr_hi = (float(x) for x in args.unet_snr.split(","))
     (samples), t_data = timed(lambda: [
-        unet.training_sample((128, 128, 128), T, 6, cfg["n_blobs"], cfg["rho"], float(rng.uniform(0.05, 0.2)), 60,
+        unet.training_sample((128, 128, 128), T, 6, cfg["n_blobs"], cfg["rho"], float(rng.uniform(snr_lo, snr_hi)), 60,
                              7000 + s, ph, mask, bins30, fine, ctx) for s in range(args.unet_train)])
     net = unet.UNetProposer(len(bins30), ctx, seed=1)
     kw = dict(lr=args.unet_lr, pos_weight=args.unet_pos_weight, target_radius=args.unet_target_radius)
@@ -595,6 +598,7 @@ def run_learned_928(args):
                        "refine_triplets_per_candidate": tm["triplets_per_candidate"],
                        "train_tomograms": args.unet_train, "train_volume": [128, 128, 128],
                        "pos_weight": args.unet_pos_weight, "target_radius": args.unet_target_radius,
+                       "train_snr": [snr_lo, snr_hi],
                        "train_steps": args.unet_steps},
             "exhaustive_s": t_exh, "pruned_s": {k: tm[k] for k in ("total", "upload_normalise", "network",
                                                                     "triplet_sets", "refine")},

@@ -305,15 +305,24 @@ def orient_logits_at(net, feat, idx):
     return out
 
 
-def propose(net, vol, n_cand, radius, top_bins, slab=128, halo=32):
+def propose(net, vol, n_cand, radius, top_bins, slab=128, halo=32, border=16):
     """Candidates of the network on a normalised device volume [Z][Y][X]: the
     n_cand first maxima of the centre probability (tom_peak rounds with a ball
     of `radius`), 0-based [x, y, z], their probabilities and the top_bins
-    orientation bins of each (most probable first)."""
+    orientation bins of each (most probable first).  Voxels within `border`
+    of a face are not proposed: the network sees the zero padding there."""
     import torch
     from .tom import pick_peaks
     prob, feat = infer(net, vol, slab, halo, prob=True)
     Z, Y, X = prob.shape
+    if border > 0:
+        b = int(border)
+        prob[:b].zero_()
+        prob[Z - b:].zero_()
+        prob[:, :b].zero_()
+        prob[:, Y - b:].zero_()
+        prob[:, :, :b].zero_()
+        prob[:, :, X - b:].zero_()
     dummy = torch.zeros((Z, Y, X), dtype=torch.int32, device=net.dev)
     vals, pos, _ = pick_peaks(prob, dummy, n_cand, radius, net.ctx)
     del dummy
