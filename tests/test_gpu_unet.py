@@ -53,14 +53,17 @@ def _p(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-@pytest.mark.parametrize("cin,cout,masked", [(16, 16, False), (32, 64, False), (96, 32, False), (48, 16, True),
-                                             (64, 64, True), (16, 96, True), (32, 48, False)])
-def test_conv3_tensor_cores_vs_oracle(gpu, cin, cout, masked):
+@pytest.mark.parametrize("cin,cout,masked,Y", [(16, 16, False, 21), (32, 64, False, 21), (96, 32, False, 21),
+                                               (48, 16, True, 21), (64, 64, True, 21), (16, 96, True, 21),
+                                               (32, 48, False, 21), (16, 16, False, 45), (48, 32, True, 45),
+                                               (96, 96, False, 45), (64, 64, True, 70)])
+def test_conv3_tensor_cores_vs_oracle(gpu, cin, cout, masked, Y):
     import torch
     ctx = gpu.default_context()
     dev = f"cuda:{ctx.device}"
-    rng = np.random.default_rng(cin * 7 + cout)
-    Z, Y, X = 5, 21, 26  # partial tiles in x (8) and y (16)
+    rng = np.random.default_rng(cin * 7 + cout + Y)
+    # partial tiles in x (8) and y (16; blocks of two tiles where Y >= 34)
+    Z, X = 5, 26
     # the input as a channel slice of a wider buffer, the output likewise
     ics, ioff, ocs, ooff = cin + 16, 8, cout + 8, 8
     xin = uo.bf16(rng.standard_normal((Z, Y, X, ics)))
