@@ -111,6 +111,9 @@ def parse():
                    help="learned_928x928x464: SNR range of the training tomograms (lo,hi)")
     p.add_argument("--unet-window", type=int, default=7,
                    help="learned_928x928x464: refine window (+- voxels) around a candidate")
+    p.add_argument("--pruned-window", type=int, default=2,
+                   help="pruned_928x928x464: refine window (+- voxels) around a candidate (the crop is the FFT "
+                        "length >= T + 2 window + 1: 64 for the 48^3 template up to window 7)")
     p.add_argument("--pruned-ref-out", default="", help="pruned_928x928x464: save the exhaustive peaks (.npz)")
     p.add_argument("--pruned-ref-in", default="", help="pruned_928x928x464: reuse saved exhaustive peaks")
     p.add_argument("--workload", default=WORKLOAD,
@@ -461,7 +464,7 @@ def run_pruned(args):
     C = int(round(args.pruned_cands * K))
     tm = {}
     rpos, rcc, ridx = pr.pruned_search(d["tomo"], d["template"], mask, fine, coarse, C, args.pruned_radius,
-                                       batch=batch, ctx=ctx, timings=tm)
+                                       window=args.pruned_window, batch=batch, ctx=ctx, timings=tm)
     dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - np.asarray(rpos)[None].astype(float), axis=2)
     j = np.argmin(dd, axis=1)
     found = dd[np.arange(len(ref_pos)), j] <= 2
@@ -472,7 +475,7 @@ def run_pruned(args):
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": "pruned_928x928x464", "fine_angles": len(fine), "coarse_angles": len(coarse),
                        "coarse_step_deg": step, "candidates": tm["candidates_n"], "reference_peaks": K,
-                       "refine_radius_deg": args.pruned_radius,
+                       "refine_radius_deg": args.pruned_radius, "refine_window": args.pruned_window,
                        "refine_triplets_per_candidate": tm["triplets_per_candidate"]},
             "exhaustive_s": t_exh,
             "pruned_s": {k: tm[k] for k in ("total", "coarse", "candidates", "triplet_sets", "refine")},
