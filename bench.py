@@ -107,6 +107,8 @@ def parse():
     p.add_argument("--unet-target-radius", type=float, default=3.0,
                    help="learned_928x928x464: radius of the centre target's balls")
     p.add_argument("--unet-edge", type=int, default=256, help="unet: the volume edge")
+    p.add_argument("--unet-bin", type=int, default=2, choices=[1, 2],
+                   help="learned_928x928x464: run the network on the tomogram binned by this factor")
     p.add_argument("--unet-snr", default="0.05,0.2",
                    help="learned_928x928x464: SNR range of the training tomograms (lo,hi)")
     p.add_argument("--unet-window", type=int, default=7,
@@ -524,9 +526,15 @@ def run_learned_928(args):
     ph = synth.BlobPhantom(np.random.default_rng(2024), cfg["n_blobs"], cfg["rho"])
     rng = np.random.default_rng(31)
     snr_lo, snr_hi = (float(x) for x in args.unet_snr.split(","))
+    nb = args.unet_bin
+    E = 128 * nb  # training tomograms: 128^3 network inputs
+    # labels: the exhaustive fine search on unbinned training tomograms; the
+    # exhaustive 30 degree search (peaks within 4 voxels, 2 after binning) on
+    # the 8x larger binned ones
     (samples), t_data = timed(lambda: [
-        unet.training_sample((128, 128, 128), T, 6, cfg["n_blobs"], cfg["rho"], float(rng.uniform(snr_lo, snr_hi)), 60,
-                             7000 + s, ph, mask, bins30, fine, ctx) for s in range(args.unet_train)])
+        unet.training_sample((E, E, E), T, 6 * nb ** 3, cfg["n_blobs"], cfg["rho"],
+                             float(rng.uniform(snr_lo, snr_hi)), 60, 7000 + s, ph, mask, bins30,
+                             fine if nb == 1 else None, ctx, binning=nb) for s in range(args.unet_train)])
     net = unet.UNetProposer(len(bins30), ctx, seed=1)
     kw = dict(lr=args.unet_lr, pos_weight=args.unet_pos_weight, target_radius=args.unet_target_radius)
     unet.train(net, samples, max(1, args.warmup), **kw)
@@ -535,7 +543,7 @@ def run_learned_928(args):
     # the network on a training tomogram: its own labels recalled (a check of
     # the pipeline's coordinate conventions and of what training reached)
     v0, p0, _ = samples[0]
-    tpos, _, _ = unet.propose(net, v0, 2 * len(p0), T / 2, 1)
+    tpos, _, _ = unet.propose(net, v0, 2 * len(p0), T / 2 / nb, 1, border=16 // nb)
     td = np.linalg.norm(np.asarray(p0)[:, None, :].astype(float) - np.asarray(tpos)[None].astype(float), axis=2)
     train_recall = float((td.min(axis=1) <= 2).mean())
     del samples, v0
@@ -556,7 +564,7 @@ def run_learned_928(args):
     tm = {}
     rpos, rcc, ridx = unet.learned_pruned_search(d["tomo"], d["template"], mask, fine, bins30, net, C,
                                                  args.unet_bins, args.pruned_radius, window=args.unet_window,
-                                                 ctx=ctx, timings=tm)
+                                                 binning=nb, ctx=ctx, timings=tm)
 
     def recall(pos, idx=None):
         dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - np.asarray(pos)[None].astype(float), axis=2)
@@ -569,10 +577,7 @@ def run_learned_928(args):
     rc, ra = recall(rpos, ridx)
     # the network's candidates and bins alone, and the coarse 30 degree search's
     # peaks at the same count (positions; the nearest bin of the reference triplet)
-    v = torch.from_numpy(np.ascontiguousarray(d["tomo"].transpose(2, 1, 0))).to(net.dev)
-    v = unet.normalise(v, ctx, out=v)
-    (cpos, _, cbins), t_prop = timed(lambda: unet.propose(net, v, C, T / 2, args.unet_bins))
-    del v
+    (cpos, _, cbins), t_prop = timed(lambda: unet.propose_host(net, d["tomo"], C, T / 2, args.unet_bins, nb))
     torch.cuda.empty_cache()
     ref_bin = pr.coarse_bin(np.asarray(fine)[ref_idx], bins30)
     dd = np.linalg.norm(ref_pos[:, None, :].astype(float) - np.asarray(cpos)[None].astype(float), axis=2)
@@ -599,12 +604,11 @@ def run_learned_928(args):
                        "candidates": tm["candidates_n"], "reference_peaks": K, "bins_per_candidate": args.unet_bins,
                        "refine_radius_deg": args.pruned_radius, "refine_window": args.unet_window,
                        "refine_triplets_per_candidate": tm["triplets_per_candidate"],
-                       "train_tomograms": args.unet_train, "train_volume": [128, 128, 128],
+                       "train_tomograms": args.unet_train, "train_volume": [E, E, E], "binning": nb,
                        "pos_weight": args.unet_pos_weight, "target_radius": args.unet_target_radius,
                        "train_snr": [snr_lo, snr_hi],
                        "train_steps": args.unet_steps},
-            "exhaustive_s": t_exh, "pruned_s": {k: tm[k] for k in ("total", "upload_normalise", "network",
-                                                                    "triplet_sets", "refine")},
+            "exhaustive_s": t_exh, "pruned_s": {k: tm[k] for k in ("total", "network", "triplet_sets", "refine")},
             "recall": {"position": rc, "position_and_triplet": ra},
             "network_alone": {"candidate_recall_within_window": float(near.mean()),
                               "candidate_recall_by_radius": net_by_radius,

@@ -514,6 +514,8 @@ int tomgpu_unet_channel_sum_dev(tomgpu_ctx* ctx, const uint16_t* g, int cs, int 
 /* out = (vol - mean) / std over n values (moments in FP64 on the device;
  * out may be vol). */
 int tomgpu_unet_normalise_dev(tomgpu_ctx* ctx, const float* vol, int64_t n, float* out);
+/* 2x2x2 mean of an FP32 volume (dims even) into the half-size volume out. */
+int tomgpu_unet_bin2_dev(tomgpu_ctx* ctx, const float* vol, const int dims[3], float* out);
 /* Features at P voxels (flat indices) as FP32 F[c][p], and the scatter-add
  * of a gradient G[c][p] back into distinct voxels of a BF16 gradient, where
  * the ReLU features f are positive. */

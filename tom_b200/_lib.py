@@ -168,6 +168,7 @@ _SIGS = {
     "tomgpu_unet_channel_sum_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                    ctypes.c_int64, c_void_p]),
     "tomgpu_unet_normalise_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int64, c_void_p]),
+    "tomgpu_unet_bin2_dev": (ctypes.c_int, [c_void_p, c_void_p, c_int_p, c_void_p]),
     "tomgpu_unet_gather_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p, ctypes.c_int, c_void_p]),
     "tomgpu_unet_scatter_add_dev": (ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, c_void_p, ctypes.c_int,
                                                    c_void_p, c_void_p]),

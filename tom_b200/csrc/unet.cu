@@ -674,6 +674,20 @@ __global__ void k_uaffine(const float* __restrict__ x, long long n, const double
         out[i] = (x[i] - m) * r;
 }
 
+// 2 x 2 x 2 mean of an FP32 volume (even edges) into the half-size volume
+__global__ void k_ubin2(const float* __restrict__ in, int X, int Y, int Z, float* __restrict__ out) {
+    const int Xc = X / 2, Yc = Y / 2, Zc = Z / 2;
+    const long long n = (long long)Xc * Yc * Zc;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % Xc), y = (int)((i / Xc) % Yc), z = (int)(i / ((long long)Xc * Yc));
+        float s = 0.f;
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
+            s += __ldg(in + ((long long)(2 * z + (d >> 2)) * Y + 2 * y + ((d >> 1) & 1)) * X + 2 * x + (d & 1));
+        out[i] = 0.125f * s;
+    }
+}
+
 // features at P voxels, as the dense layer's F[c][p] (FP32)
 __global__ void k_ugather(const unsigned short* __restrict__ f, int C, const long long* __restrict__ idx, int P,
                           float* __restrict__ out) {
@@ -947,6 +961,18 @@ int tomgpu_unet_normalise_dev(tomgpu_ctx* ctx, const float* vol, int64_t n, floa
     k_uaffine<<<grid_for(n, 256), 256, 0, ctx->stream>>>(vol, n, s, out);
     TG_TRY_CUDA(ctx, cudaGetLastError());
     ctx->launches += 2;
+    return TOMGPU_OK;
+}
+
+int tomgpu_unet_bin2_dev(tomgpu_ctx* ctx, const float* vol, const int dims[3], float* out) {
+    if (!ctx) return TOMGPU_ERR_ARG;
+    if (!vol || !out || !dims3_ok(dims) || dims[0] % 2 || dims[1] % 2 || dims[2] % 2)
+        return fail(ctx, TOMGPU_ERR_ARG, "bad binning arguments (even edges)");
+    TG_TRY(use_device(ctx));
+    const long long n = (long long)dims[0] * dims[1] * dims[2] / 8;
+    k_ubin2<<<grid_for(n, 256), 256, 0, ctx->stream>>>(vol, dims[0], dims[1], dims[2], out);
+    TG_TRY_CUDA(ctx, cudaGetLastError());
+    ctx->launches += 1;
     return TOMGPU_OK;
 }
 

@@ -267,6 +267,28 @@ def normalise(vol, ctx=None, out=None):
     return out
 
 
+def bin2(vol, ctx=None):
+    """2x2x2 mean of a device volume [Z][Y][X] (even edges)."""
+    import torch
+    ctx = ctx or default_context()
+    Z, Y, X = vol.shape
+    out = torch.empty((Z // 2, Y // 2, X // 2), dtype=torch.float32, device=vol.device)
+    _call(ctx, "tomgpu_unet_bin2_dev", _tptr(vol), _cdims((X, Y, Z)), _tptr(out))
+    return out
+
+
+def prepare(vol_host, binning, ctx, dev):
+    """A host tomogram [x][y][z] on the device as the network's input:
+    [Z][Y][X], binned by 2 when binning == 2, normalised."""
+    import torch
+    v = torch.from_numpy(np.ascontiguousarray(np.asarray(vol_host, np.float32).transpose(2, 1, 0))).to(dev)
+    if binning == 2:
+        v = bin2(v, ctx)
+    elif binning != 1:
+        raise ValueError("binning is 1 or 2")
+    return normalise(v, ctx, out=v)
+
+
 def infer(net, vol, slab=128, halo=32, prob=True):
     """Centre probabilities (prob=False: logits) [Z][Y][X] and the features
     [Z][Y][X][16] (BF16 bits) of a whole normalised volume, in z slabs of
@@ -334,14 +356,28 @@ def propose(net, vol, n_cand, radius, top_bins, slab=128, halo=32, border=16):
     return pos, vals, bins
 
 
+def propose_host(net, vol, n_cand, radius, top_bins, binning=1, slab=128, halo=32):
+    """propose() on a host tomogram [x][y][z] (binned by 2 first when binning
+    == 2); radius in tomogram voxels; positions returned in tomogram voxels
+    (a binned candidate at the centre of its 2^3 block)."""
+    v = prepare(vol, binning, net.ctx, net.dev)
+    pos, vals, bins = propose(net, v, n_cand, radius / binning, top_bins, slab, halo, border=16 // binning)
+    del v
+    if binning == 2:
+        pos = np.minimum(2 * np.asarray(pos) + 1, np.asarray(np.shape(vol)) - 1)
+    return pos, vals, bins
+
+
 def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bins, radius_deg, window=2,
-                          peak_radius=None, slab=128, halo=32, ctx=None, timings=None):
+                          peak_radius=None, slab=128, halo=32, binning=1, ctx=None, timings=None):
     """The pruned search with the network in place of the coarse search: the
     network's n_cand candidates on the tomogram, and around each the fine
     triplets within radius_deg (geodesic) of its top_bins coarse orientation
     bins searched on a crop (proposer.refine: the values equal the full
     search's there), the best within +-window voxels.  vol: the tomogram as a
-    host array [x][y][z].  Returns (positions 0-based [x, y, z], cc, fine
+    host array [x][y][z]; binning 2 runs the network on the 2x2x2-binned
+    tomogram (twice the receptive field in tomogram voxels) and maps its
+    candidates back to the centres of their 2^3 blocks.  Returns (positions 0-based [x, y, z], cc, fine
     triplet index) per candidate; timings receives the seconds per step."""
     import time
     import torch
@@ -355,11 +391,9 @@ def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bi
         clock.append(time.perf_counter())
 
     mark()
-    v = torch.from_numpy(np.ascontiguousarray(np.asarray(vol, np.float32).transpose(2, 1, 0))).to(net.dev)
-    v = normalise(v, ctx, out=v)
     mark()
-    pos, _, bins = propose(net, v, n_cand, T / 2 if peak_radius is None else peak_radius, top_bins, slab, halo)
-    del v
+    pos, _, bins = propose_host(net, vol, n_cand, T / 2 if peak_radius is None else peak_radius, top_bins,
+                                binning, slab, halo)
     mark()
     coarse = np.asarray(coarse)
     ub = np.unique(np.asarray(bins).reshape(-1))
@@ -372,7 +406,7 @@ def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bi
     out = pr.refine(vol, template, mask, pos, sets, window=window, ctx=ctx)
     mark()
     if timings is not None:
-        for k, name in enumerate(("upload_normalise", "network", "triplet_sets", "refine")):
+        for k, name in enumerate(("start", "network", "triplet_sets", "refine")):
             timings[name] = clock[k + 1] - clock[k]
         timings["total"] = clock[-1] - clock[0]
         timings["candidates_n"] = int(len(pos))
@@ -383,13 +417,14 @@ def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bi
 # ------------------------------------------------------------------ training data
 
 
-def training_sample(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed, phantom, mask, coarse, fine=None, ctx=None):
+def training_sample(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed, phantom, mask, coarse, fine=None, ctx=None,
+                    binning=1):
     """A seeded synthetic tomogram and its labels from the search itself: the
     n_copies first peaks of the exhaustive search (tom_peak rounds of radius
     T/2) over the fine grid when given, else over the coarse grid, their
-    positions and the coarse bins of their angles.  Returns (normalised
-    volume [Z][Y][X] float32, positions 0-based [x, y, z], bins)."""
-    import torch
+    positions and the coarse bins of their angles.  binning 2: the volume
+    2x2x2-binned and the positions halved.  Returns (normalised volume
+    [Z][Y][X] float32, positions 0-based [x, y, z], bins)."""
     from . import proposer as pr
     from . import synth
     from .tom import pick_peaks
@@ -402,9 +437,8 @@ def training_sample(N, T, n_copies, n_blobs, rho, snr, max_tilt, seed, phantom, 
     del cc, idx
     ok = aidx >= 0
     bins = aidx[ok] if fine is None else pr.coarse_bin(np.asarray(fine)[aidx[ok]], coarse)
-    v = torch.from_numpy(np.ascontiguousarray(d["tomo"].transpose(2, 1, 0))).to(f"cuda:{ctx.device}")
-    v = normalise(v, ctx, out=v)
-    return v, pos[ok] - 1, np.asarray(bins, np.int32)
+    v = prepare(d["tomo"], binning, ctx, f"cuda:{ctx.device}")
+    return v, (pos[ok] - 1) // binning, np.asarray(bins, np.int32)
 
 
 def ball_target(shape_zyx, pos, radius, dev):
