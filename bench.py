@@ -107,6 +107,11 @@ def parse():
     p.add_argument("--unet-target-radius", type=float, default=3.0,
                    help="learned_928x928x464: radius of the centre target's balls")
     p.add_argument("--unet-edge", type=int, default=256, help="unet: the volume edge")
+    p.add_argument("--rerank-step", type=int, default=28,
+                   help="learned_928x928x464: coarse sub-grid step of the ranking comparison (degrees)")
+    p.add_argument("--rerank-radius", type=float, default=28.0,
+                   help="learned_928x928x464: fine triplets within this many degrees of a kept candidate's "
+                        "coarse rotation")
     p.add_argument("--unet-bin", type=int, default=2, choices=[1, 2],
                    help="learned_928x928x464: run the network on the tomogram binned by this factor")
     p.add_argument("--unet-snr", default="0.05,0.2",
@@ -597,6 +602,34 @@ def run_learned_928(args):
     cnear = cmin <= args.unet_window
     coarse_by_radius = {str(r): float((cmin <= r).mean()) for r in (2, 4, 7, 12, 24)}
     cbin_hit = bidx[jb] == ref_bin
+    # the network as a ranker of the coarse search's candidates: a coarse
+    # sub-grid search, its --pruned-cands x K first peaks, and the fine search
+    # (within --rerank-radius degrees of each candidate's coarse rotation, +-7
+    # voxels) on the n best of them, ranked by the network (its centre
+    # probability there) or, without the network, by their coarse CC
+    fstart, finc, fend = cfg["angles"]
+    cgrid = pr.coarse_grid(fstart, finc, fend, args.rerank_step // finc[0])
+    (ccg, icg), t_cg = timed(lambda: pr.search(d["tomo"], d["template"], mask, cgrid, batch=batch, ctx=ctx))
+    (pvals, ppos, pidx), t_pk = timed(lambda: tb.pick_peaks(ccg, icg, C, T / 2, ctx))
+    del ccg, icg
+    torch.cuda.empty_cache()
+    okp = pidx >= 0
+    ppos, pidx, pvals = ppos[okp] - 1, pidx[okp], pvals[okp]
+    score, t_score = timed(lambda: unet.rerank_scores(net, d["tomo"], ppos, nb))
+    near_sets = pr.neighbours(fine, np.asarray(cgrid)[pidx], args.rerank_radius)
+    rerank = {}
+    for n_keep in [int(round(f * K)) for f in (1.0, 1.1, 1.25, 1.5)]:
+        out = {}
+        for name, order in (("network_ranked", np.argsort(-score, kind="stable")),
+                            ("coarse_cc_ranked", np.argsort(-pvals, kind="stable"))):
+            keep = order[:n_keep]
+            (rp, _, ri), t_ref = timed(lambda: pr.refine(d["tomo"], d["template"], mask, ppos[keep],
+                                                         [(np.asarray(fine)[near_sets[i]], near_sets[i])
+                                                          for i in keep], window=7, ctx=ctx))
+            pc, pa = recall(rp, ri)
+            out[name] = {"position": pc, "position_and_triplet": pa, "refine_s": t_ref,
+                         "total_s": t_cg + t_pk + t_ref + (t_score if name == "network_ranked" else 0.0)}
+        rerank[str(n_keep)] = out
     line = {"metric": "learned-pruned search speed-up over the exhaustive fine search (928x928x464, 48^3 template)",
             "value": t_exh / tm["total"], "unit": "x", "higher_is_better": True, "n_gpus": 1,
             "dtype": "bf16 network, f32 search", "data": "synthetic",
@@ -614,6 +647,9 @@ def run_learned_928(args):
                               "candidate_recall_by_radius": net_by_radius,
                               "bin_in_top_bins": float((near & bin_hit).mean()), "propose_s": t_prop,
                               "training_tomogram_label_recall": train_recall},
+            "rerank": {"coarse_step_deg": args.rerank_step, "coarse_angles": len(cgrid),
+                       "pool": int(len(ppos)), "radius_deg": args.rerank_radius, "coarse_search_s": t_cg,
+                       "peaks_s": t_pk, "network_s": t_score, "by_kept_candidates": rerank},
             "coarse_30deg_search_alone": {"candidate_recall_within_window": float(cnear.mean()),
                                           "candidate_recall_by_radius": coarse_by_radius,
                                           "bin_hit": float((cnear & cbin_hit).mean()), "search_s": t_c30},

@@ -368,6 +368,25 @@ def propose_host(net, vol, n_cand, radius, top_bins, binning=1, slab=128, halo=3
     return pos, vals, bins
 
 
+def rerank_scores(net, vol, pos, binning=1, slab=128, halo=32):
+    """The network's centre probability at each candidate (0-based [x, y, z]
+    tomogram voxels) of a host tomogram [x][y][z]: the maximum over the
+    candidate's (binned) voxel and its 26 neighbours."""
+    import torch
+    v = prepare(vol, binning, net.ctx, net.dev)
+    prob, _ = infer(net, v, slab, halo, prob=True)
+    del v
+    Z, Y, X = prob.shape
+    p = torch.as_tensor(np.asarray(pos, np.int64) // binning, device=net.dev)
+    best = torch.full((p.shape[0],), -1.0, device=net.dev)
+    for dz in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                best = torch.maximum(best, prob[(p[:, 2] + dz).clamp(0, Z - 1), (p[:, 1] + dy).clamp(0, Y - 1),
+                                                (p[:, 0] + dx).clamp(0, X - 1)])
+    return best.cpu().numpy()
+
+
 def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bins, radius_deg, window=2,
                           peak_radius=None, slab=128, halo=32, binning=1, ctx=None, timings=None):
     """The pruned search with the network in place of the coarse search: the
