@@ -96,8 +96,9 @@ def parse():
     p.add_argument("--pruned-radius", type=float, default=21.0,
                    help="pruned_928x928x464: fine triplets within this many degrees of a candidate's coarse "
                         "rotation are searched")
-    p.add_argument("--unet-train", type=int, default=48,
-                   help="learned_928x928x464: training tomograms (128^3, the workload's species, SNR 0.05-0.2)")
+    p.add_argument("--unet-train", type=int, default=32,
+                   help="learned_928x928x464: training tomograms (128^3 network inputs: 256^3 binned by 2 with "
+                        "--unet-bin 2; the workload's species, SNR 0.05-0.2)")
     p.add_argument("--unet-steps", type=int, default=3000, help="learned_928x928x464: U-Net training steps")
     p.add_argument("--unet-bins", type=int, default=4,
                    help="learned_928x928x464: orientation bins (30 degree grid) refined per candidate")
