@@ -265,7 +265,7 @@ def test_unet_training_lowers_the_loss(gpu):
     assert last[0] < 0.5 * first[0] and last[1] < first[1]
 
 
-def test_slabbed_inference_equals_the_whole_volume(gpu):
+def test_normalise_bin_and_slabbed_inference(gpu):
     import torch
     from tom_b200 import unet
     ctx = gpu.default_context()
@@ -276,6 +276,9 @@ def test_slabbed_inference_equals_the_whole_volume(gpu):
     m = vol.double().mean().item()
     s = vol.double().std(unbiased=False).item()
     assert np.allclose(v.cpu().numpy(), (vol.cpu().numpy() - m) / s, atol=1e-5)
+    b = unet.bin2(vol, ctx)
+    ref = vol.cpu().numpy().astype(np.float64).reshape(28, 2, 36, 2, 20, 2).mean(axis=(1, 3, 5))
+    assert np.allclose(b.cpu().numpy(), ref, rtol=1e-6, atol=1e-6)
     whole, fw = unet.infer(net, v, slab=56, halo=24)
     slabbed, fs = unet.infer(net, v, slab=16, halo=24)
     ctx.synchronize()

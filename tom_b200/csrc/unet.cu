@@ -242,18 +242,26 @@ struct WgArgs {
     int* err;
 };
 
-constexpr int WG_NST = 2;
-constexpr int WG_A = 16 * DBOX;  // 128 rows of co (16 groups of 8) of one K = 128-voxel tile
-constexpr int WG_B = 12 * HSLOT; // up to 96 input channels with their halo
+constexpr int WG_NST = 4;
+constexpr int WG_A = 16 * DBOX;  // the bytes an M = 128 operand of co (16 groups of 8) spans
+// A stage holds the tile's real operands only: Cout / 8 output-gradient boxes
+// then Cin / 8 halo boxes.  An MMA's rows past Cout read whatever follows (the
+// stage's halo boxes, the next stage); those rows of the accumulator are
+// never read back.  The allocation ends WG_A bytes past the last stage's
+// start at least, so every such read stays inside it.
+__host__ __device__ constexpr int wg_stage(int cin, int cout) { return (cout / 8) * DBOX + (cin / 8) * HSLOT; }
+__host__ __device__ constexpr int wg_span(int stg) {
+    return WG_NST * stg > (WG_NST - 1) * stg + WG_A ? WG_NST * stg : (WG_NST - 1) * stg + WG_A;
+}
 
 // Weight gradient; grid (splits, groups).  Group g: taps (dz = g, all dy, dx)
 // when group_taps == 9, else (dz = g / 3, dy = g % 3, dx = 0..2).
 __global__ void __launch_bounds__(128) k_uconv_wgrad_tc(const __grid_constant__ CUtensorMap tin,
                                                         const __grid_constant__ CUtensorMap tdy, WgArgs a) {
-    constexpr int STG = WG_A + WG_B;
+    const int STG = wg_stage(a.cin, a.cout), ABYTES = (a.cout / 8) * DBOX;
     extern __shared__ __align__(1024) unsigned char smu[];
     unsigned char* sm = smu + ((1024u - (tgtma::smem_u32(smu) & 1023u)) & 1023u);
-    unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + WG_NST * STG);
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(sm + wg_span(STG));
     unsigned long long* freeb = full + WG_NST;
     unsigned long long* done = freeb + WG_NST;
     unsigned* tslot = reinterpret_cast<unsigned*>(done + 1);
@@ -293,7 +301,7 @@ __global__ void __launch_bounds__(128) k_uconv_wgrad_tc(const __grid_constant__ 
             tgtma::mbar_expect_tx(bar, (unsigned)(ng_out * DBOX + ng_in * HBOX));
             for (int j = 0; j < ng_out; ++j) tgtma::load_4d(dst + (unsigned)(j * DBOX), &tdy, 8 * j, x0, y0, tz, bar);
             for (int j = 0; j < ng_in; ++j)
-                tgtma::load_4d(dst + (unsigned)(WG_A + j * HSLOT), &tin, 8 * j, x0 - 1, y0 - 1, tz + dz - 1, bar);
+                tgtma::load_4d(dst + (unsigned)(ABYTES + j * HSLOT), &tin, 8 * j, x0 - 1, y0 - 1, tz + dz - 1, bar);
         };
         int issued = my < WG_NST ? my : WG_NST;
         for (int s = 0; s < issued; ++s) load(s);
@@ -307,7 +315,7 @@ __global__ void __launch_bounds__(128) k_uconv_wgrad_tc(const __grid_constant__ 
                 break;
             }
             tgtm::fence_after();
-            const unsigned abase = s0 + (unsigned)(st * STG), bbase = abase + WG_A;
+            const unsigned abase = s0 + (unsigned)(st * STG), bbase = abase + (unsigned)ABYTES;
             for (int i = 0; i < nt; ++i) {
                 const int dy = nt == 9 ? i / 3 : dy0, dx = nt == 9 ? i % 3 : i;
                 const unsigned d = tbase + (unsigned)(i * a.cin);
@@ -811,9 +819,11 @@ int tomgpu_unet_conv3_wgrad_dev(tomgpu_ctx* ctx, const uint16_t* in, int in_cs, 
     int splits = 148 / groups;
     if (splits < 1) splits = 1;
     if (splits > ntiles) splits = ntiles;
-    // 2 stages plus room for the unused operand rows past the last stage; more
-    // than half the SM's shared memory, so one block (512 TMEM columns) per SM
-    const size_t smem = 1024 + (size_t)WG_NST * (WG_A + WG_B) + WG_A + 256;
+    // the stages, the span of the last stage's operand rows, the barriers; at
+    // least 116 KB, more than half the SM's shared memory, so one block (512
+    // TMEM columns) per SM
+    size_t smem = 1024 + (size_t)wg_span(wg_stage(cin, cout)) + 256;
+    if (smem < 116 * 1024) smem = 116 * 1024;
     TG_TRY_CUDA(ctx, cudaFuncSetAttribute(k_uconv_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     WgArgs a{dims[0], dims[1], dims[2], cin, cout, group_taps, gw, ctx->d_err};
     k_uconv_wgrad_tc<<<dim3(splits, groups), 128, smem, ctx->stream>>>(tin, tdy, a);
