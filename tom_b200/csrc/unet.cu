@@ -442,6 +442,7 @@ __global__ void __launch_bounds__(448) k_uconv_first_wgrad(const float* __restri
     const int j = threadIdx.x;
     const int co = j < 432 ? j / 27 : j - 432, t = j < 432 ? j % 27 : -1;
     const int ox = t >= 0 ? t % 3 - 1 : 0, oy = t >= 0 ? t / 3 % 3 - 1 : 0, oz = t >= 0 ? t / 9 - 1 : 0;
+    const long long offl = ((long long)oz * Y + oy) * X + ox;
     const long long n = (long long)X * Y * Z;
     float acc = 0.f;
     for (long long base = (long long)blockIdx.x * CH; base < n; base += (long long)gridDim.x * CH) {
@@ -451,16 +452,25 @@ __global__ void __launch_bounds__(448) k_uconv_first_wgrad(const float* __restri
             gs[i / 16][i % 16] = v < n ? bf2f(g[v * 16 + (i % 16)]) : 0.f;
         }
         __syncthreads();
-        const long long lim = n - base < CH ? n - base : CH;
+        const int lim = n - base < CH ? (int)(n - base) : CH;
+        if (t < 0) {
+            for (int k = 0; k < lim; ++k) acc += gs[k][co];
+            continue;
+        }
+        // the chunk's voxels in order, coordinates stepped (no division per voxel);
+        // the tap's neighbour is v + offl wherever it lies inside the volume
+        int x = (int)(base % X), y = (int)((base / X) % Y), z = (int)(base / ((long long)X * Y));
+        const float* src = vol + base + offl;
         for (int k = 0; k < lim; ++k) {
-            const long long v = base + k;
-            if (t < 0) {
-                acc += gs[k][co];
-                continue;
+            if ((unsigned)(x + ox) < (unsigned)X && (unsigned)(y + oy) < (unsigned)Y && (unsigned)(z + oz) < (unsigned)Z)
+                acc = fmaf(gs[k][co], __ldg(src + k), acc);
+            if (++x == X) {
+                x = 0;
+                if (++y == Y) {
+                    y = 0;
+                    ++z;
+                }
             }
-            const int x = (int)(v % X) + ox, y = (int)((v / X) % Y) + oy, z = (int)(v / ((long long)X * Y)) + oz;
-            if (x < 0 || x >= X || y < 0 || y >= Y || z < 0 || z >= Z) continue;
-            acc = fmaf(gs[k][co], __ldg(vol + ((long long)z * Y + y) * X + x), acc);
         }
     }
     if (t >= 0)
