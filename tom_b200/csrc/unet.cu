@@ -433,45 +433,43 @@ __global__ void __launch_bounds__(256) k_uconv_first(const float* __restrict__ v
 
 // first layer's weight and bias gradients: thread j of a 448-thread block owns
 // output j (j < 432: (co = j / 27, t = j % 27); j >= 432: bias co = j - 432)
-// and sums over the block's voxels, then one atomic add per output
+// and sums over 8 x 8 x 8 voxel tiles staged in shared memory (the input with
+// its one-voxel halo, the output gradient as FP32), a strided set of tiles
+// per block, then one atomic add per output
 __global__ void __launch_bounds__(448) k_uconv_first_wgrad(const float* __restrict__ vol, int X, int Y, int Z,
                                                           const unsigned short* __restrict__ g,
                                                           float* __restrict__ gw, float* __restrict__ gb) {
-    constexpr int CH = 256;  // voxels staged per round
-    __shared__ float gs[CH][17];
+    constexpr int E = 8, H = E + 2;
+    __shared__ float xin[H * H * H];
+    __shared__ float gs[E * E * E][17];
     const int j = threadIdx.x;
     const int co = j < 432 ? j / 27 : j - 432, t = j < 432 ? j % 27 : -1;
-    const int ox = t >= 0 ? t % 3 - 1 : 0, oy = t >= 0 ? t / 3 % 3 - 1 : 0, oz = t >= 0 ? t / 9 - 1 : 0;
-    const long long offl = ((long long)oz * Y + oy) * X + ox;
-    const long long n = (long long)X * Y * Z;
+    const int ox = t >= 0 ? t % 3 : 1, oy = t >= 0 ? t / 3 % 3 : 1, oz = t >= 0 ? t / 9 : 1;  // 0..2 in the halo tile
+    const int tx = (X + E - 1) / E, ty = (Y + E - 1) / E, tz = (Z + E - 1) / E;
+    const int ntiles = tx * ty * tz;
     float acc = 0.f;
-    for (long long base = (long long)blockIdx.x * CH; base < n; base += (long long)gridDim.x * CH) {
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int bx = (tile % tx) * E, by = (tile / tx % ty) * E, bz = (tile / (tx * ty)) * E;
         __syncthreads();
-        for (int i = threadIdx.x; i < CH * 16; i += blockDim.x) {
-            const long long v = base + i / 16;
-            gs[i / 16][i % 16] = v < n ? bf2f(g[v * 16 + (i % 16)]) : 0.f;
+        for (int i = threadIdx.x; i < H * H * H; i += blockDim.x) {
+            const int x = bx - 1 + i % H, y = by - 1 + i / H % H, z = bz - 1 + i / (H * H);
+            xin[i] = ((unsigned)x < (unsigned)X && (unsigned)y < (unsigned)Y && (unsigned)z < (unsigned)Z)
+                         ? __ldg(vol + ((long long)z * Y + y) * X + x)
+                         : 0.f;
+        }
+        for (int i = threadIdx.x; i < E * E * E * 16; i += blockDim.x) {
+            const int c = i & 15, v = i >> 4;
+            const int x = bx + v % E, y = by + v / E % E, z = bz + v / (E * E);
+            gs[v][c] = (x < X && y < Y && z < Z) ? bf2f(g[(((long long)z * Y + y) * X + x) * 16 + c]) : 0.f;
         }
         __syncthreads();
-        const int lim = n - base < CH ? (int)(n - base) : CH;
-        if (t < 0) {
-            for (int k = 0; k < lim; ++k) acc += gs[k][co];
-            continue;
-        }
-        // the chunk's voxels in order, coordinates stepped (no division per voxel);
-        // the tap's neighbour is v + offl wherever it lies inside the volume
-        int x = (int)(base % X), y = (int)((base / X) % Y), z = (int)(base / ((long long)X * Y));
-        const float* src = vol + base + offl;
-        for (int k = 0; k < lim; ++k) {
-            if ((unsigned)(x + ox) < (unsigned)X && (unsigned)(y + oy) < (unsigned)Y && (unsigned)(z + oz) < (unsigned)Z)
-                acc = fmaf(gs[k][co], __ldg(src + k), acc);
-            if (++x == X) {
-                x = 0;
-                if (++y == Y) {
-                    y = 0;
-                    ++z;
-                }
+        for (int vz = 0; vz < E; ++vz)
+            for (int vy = 0; vy < E; ++vy) {
+                const float* row = xin + ((vz + oz) * H + vy + oy) * H + ox;
+                const int v0 = (vz * E + vy) * E;
+#pragma unroll
+                for (int vx = 0; vx < E; ++vx) acc = fmaf(gs[v0 + vx][co], t >= 0 ? row[vx] : 1.f, acc);
             }
-        }
     }
     if (t >= 0)
         atomicAdd(gw + co * 27 + t, acc);
@@ -861,7 +859,7 @@ int tomgpu_unet_conv_first_wgrad_dev(tomgpu_ctx* ctx, const float* vol, const in
     if (!vol || !gout || !gw || !dims3_ok(dims)) return fail(ctx, TOMGPU_ERR_ARG, "bad first-layer arguments");
     TG_TRY(use_device(ctx));
     const long long n = (long long)dims[0] * dims[1] * dims[2];
-    long long blocks = (n + 255) / 256;
+    long long blocks = (n + 511) / 512;
     if (blocks > 148 * 4) blocks = 148 * 4;
     k_uconv_first_wgrad<<<(int)blocks, 448, 0, ctx->stream>>>(vol, dims[0], dims[1], dims[2],
                                                                reinterpret_cast<const unsigned short*>(gout), gw, gb);
