@@ -53,3 +53,29 @@ def test_backward_matches_central_differences():
     gh = np.concatenate([gr["wh"], gr["bh"]])
     assert np.allclose(gh[:16], np.einsum("zyx,zyxc->c", wl, a["f"]))
     assert np.isclose(gh[16], wl.sum())
+
+
+def test_network_definition_matches_the_oracle():
+    from tom_b200 import unet
+    assert tuple(unet.CONVS) == tuple(uo.CONVS)
+    p = unet.init_params(11, seed=0)
+    for name, ci, co in unet.CONVS:
+        assert p["w_" + name].shape == (co, ci, 27) and p["b_" + name].shape == (co,)
+    assert p["w0"].shape == (16, 1, 27) and p["head"].shape == (17,) and p["head"][16] == -4.0
+    assert p["Wo"].shape == (11, 16) and p["bo"].shape == (11,)
+    # 2 x multiply-adds per full-resolution voxel: the first layer, the head,
+    # and each convolution at its level (1/8 per pooling)
+    macs = 27 * 16 + 16 + sum(27 * ci * co / {"e1b": 1, "d1a": 1, "d1b": 1, "e3a": 64, "e3b": 64}.get(n, 8)
+                             for n, ci, co in uo.CONVS)
+    assert unet.UNetProposer.flops_per_voxel(None) == 2 * macs == 113216
+
+
+def test_ball_targets():
+    from tom_b200 import unet
+    t = unet.ball_target((20, 24, 28), [[5, 6, 7], [0, 23, 19]], 3.0, "cpu").numpy()
+    assert t.shape == (20, 24, 28)
+    per_ball = sum(1 for dz in range(-3, 4) for dy in range(-3, 4) for dx in range(-3, 4)
+                   if dx * dx + dy * dy + dz * dz <= 9)
+    assert per_ball == 123 and t.sum() == 2 * per_ball
+    # positions are [x, y, z]; the second ball wraps around the x and y faces
+    assert t[7, 6, 5] == 1 and t[19, 23, 0] == 1 and t[19, 0, 27] == 1 and t[19, 20, 0] == 1
