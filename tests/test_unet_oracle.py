@@ -79,3 +79,10 @@ def test_ball_targets():
     assert per_ball == 123 and t.sum() == 2 * per_ball
     # positions are [x, y, z]; the second ball wraps around the x and y faces
     assert t[7, 6, 5] == 1 and t[19, 23, 0] == 1 and t[19, 0, 27] == 1 and t[19, 20, 0] == 1
+
+
+def test_binned_positions_map_to_their_block_centres():
+    from tom_b200 import unet
+    p = unet.unbin_positions([[0, 0, 0], [3, 5, 231], [463, 463, 231]], 2, (928, 928, 463))
+    assert p.tolist() == [[1, 1, 1], [7, 11, 462], [927, 927, 462]]
+    assert unet.unbin_positions([[4, 5, 6]], 1, (8, 8, 8)).tolist() == [[4, 5, 6]]

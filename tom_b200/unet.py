@@ -363,9 +363,17 @@ def propose_host(net, vol, n_cand, radius, top_bins, binning=1, slab=128, halo=3
     v = prepare(vol, binning, net.ctx, net.dev)
     pos, vals, bins = propose(net, v, n_cand, radius / binning, top_bins, slab, halo, border=16 // binning)
     del v
-    if binning == 2:
-        pos = np.minimum(2 * np.asarray(pos) + 1, np.asarray(np.shape(vol)) - 1)
-    return pos, vals, bins
+    return unbin_positions(pos, binning, np.shape(vol)), vals, bins
+
+
+def unbin_positions(pos, binning, shape_xyz):
+    """Tomogram voxels (0-based [x, y, z]) of positions on a volume binned by
+    `binning`: the voxel at the upper centre of each binned voxel's block,
+    inside the tomogram."""
+    pos = np.asarray(pos, np.int64).reshape(-1, 3)
+    if binning == 1:
+        return pos
+    return np.minimum(binning * pos + binning // 2, np.asarray(shape_xyz, np.int64) - 1)
 
 
 def rerank_scores(net, vol, pos, binning=1, slab=128, halo=32):
