@@ -20,6 +20,15 @@ tomogram, FP64 statistics, the search, download of max-CC and angle index
 inside the timed region).  Before the timed region the rotation batch is
 autotuned over 8, 16, 32 and 64 (those that fit); the device-resident plan is
 released before the end-to-end leg builds its own.
+
+Other workloads (`--workload`, each its own JSON line; not the headline):
+exhaustive_928x928x464 and exhaustive_128 (the same search at other sizes),
+pruned_928x928x464 (the pruned search against the exhaustive one),
+align_2048 (batched subtomogram alignment), learned_256 (the coarse-map CNN
+proposer), unet (the U-Net's tensor-core forward and training throughput)
+and learned_928x928x464 (the U-Net proposer on the full-size tomogram: its
+learned-pruned search, its candidates alone, and its ranking of the coarse
+search's candidates against their CC at equal counts).
 """
 from __future__ import annotations
 
