@@ -418,7 +418,6 @@ def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bi
         clock.append(time.perf_counter())
 
     mark()
-    mark()
     pos, _, bins = propose_host(net, vol, n_cand, T / 2 if peak_radius is None else peak_radius, top_bins,
                                 binning, slab, halo)
     mark()
@@ -433,7 +432,7 @@ def learned_pruned_search(vol, template, mask, fine, coarse, net, n_cand, top_bi
     out = pr.refine(vol, template, mask, pos, sets, window=window, ctx=ctx)
     mark()
     if timings is not None:
-        for k, name in enumerate(("start", "network", "triplet_sets", "refine")):
+        for k, name in enumerate(("network", "triplet_sets", "refine")):
             timings[name] = clock[k + 1] - clock[k]
         timings["total"] = clock[-1] - clock[0]
         timings["candidates_n"] = int(len(pos))
